@@ -1,0 +1,106 @@
+"""ctypes binding of libcurc_b200.so (include/curc_b200.h).
+
+The CUDA library is the only implementation: there is no Python or CPU
+fallback, and loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcurc_b200.so")
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C curc_b200` "
+                               "(or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        c_p, c_u64, c_int = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+        L.curc_ctx_create.argtypes = [c_int, ctypes.POINTER(c_p)]
+        L.curc_ctx_destroy.argtypes = [c_p]
+        L.curc_ctx_destroy.restype = None
+        L.curc_last_error.argtypes = [c_p]
+        L.curc_last_error.restype = ctypes.c_char_p
+        L.curc_pack_device.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_p, c_p, c_p]
+        L.curc_block_run.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_int, c_int]
+        L.curc_block_run_device.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_int, c_int]
+        L.curc_block_get.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(c_p), ctypes.POINTER(c_u64)]
+        L.curc_block_stage_ms.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
+        _lib = L
+    return _lib
+
+
+class CurcError(RuntimeError):
+    pass
+
+
+class Context:
+    """One CUDA stream and device arena on one GPU (curc_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        rc = lib().curc_ctx_create(device, ctypes.byref(self._h))
+        if rc != 0:
+            raise CurcError(f"curc_ctx_create: {lib().curc_last_error(None).decode()}")
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise CurcError(f"{what}: {lib().curc_last_error(self._h).decode()} (code {rc})")
+
+    def close(self):
+        if self._h:
+            lib().curc_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def block_run(self, seqs: np.ndarray, preserve_order: bool = False, paired_end: bool = False):
+        """seqs: (n, L) uint8 ASCII reads in block order, host memory."""
+        seqs = np.ascontiguousarray(seqs, dtype=np.uint8)
+        n, L = seqs.shape
+        self._check(lib().curc_block_run(self._h, seqs.ctypes.data, n, L, int(preserve_order), int(paired_end)),
+                    "curc_block_run")
+
+    def block_run_device(self, ptr: int, n: int, L: int, preserve_order=False, paired_end=False):
+        self._check(lib().curc_block_run_device(self._h, ctypes.c_void_p(ptr), n, L, int(preserve_order),
+                                                int(paired_end)), "curc_block_run_device")
+
+    def get(self, name: str, dtype=np.uint8) -> np.ndarray:
+        p, nb = ctypes.c_void_p(), ctypes.c_uint64()
+        self._check(lib().curc_block_get(self._h, name.encode(), ctypes.byref(p), ctypes.byref(nb)),
+                    f"curc_block_get({name})")
+        if nb.value == 0:
+            return np.zeros(0, dtype=dtype)
+        buf = (ctypes.c_uint8 * nb.value).from_address(p.value)
+        return np.frombuffer(bytes(buf), dtype=dtype)
+
+    def stage_ms(self, stage: str) -> float:
+        v = ctypes.c_float()
+        self._check(lib().curc_block_stage_ms(self._h, stage.encode(), ctypes.byref(v)), "curc_block_stage_ms")
+        return float(v.value)
+
+    def pack_device(self, seqs_ptr: int, n: int, L: int, packed_ptr: int, has_n_ptr: int, stream: int = 0):
+        self._check(lib().curc_pack_device(self._h, ctypes.c_void_p(seqs_ptr), n, L, ctypes.c_void_p(packed_ptr),
+                                           ctypes.c_void_p(has_n_ptr), ctypes.c_void_p(stream)), "curc_pack_device")

@@ -1,0 +1,290 @@
+// Block pipeline and C-ABI (include/curc_b200.h).
+//
+// One block of reads stays resident in HBM from the H2D copy of its ASCII
+// sequences to the final streams; only the streams (and, on request, stage
+// intermediates for parity checks) come back to the host.
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/curc_b200.h"
+#include "block.cuh"
+
+namespace curc {
+
+namespace {
+
+__global__ void gather_reads_kernel(const uint64_t* __restrict__ db, int W, const uint32_t* __restrict__ ids,
+                                    uint32_t m, uint64_t* __restrict__ out) {
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= uint64_t(m) * W) return;
+    const uint32_t i = uint32_t(t / W), w = uint32_t(t - uint64_t(i) * W);
+    out[t] = db[uint64_t(ids[i]) * W + w];
+}
+
+__global__ void ends_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ next,
+                            const uint32_t* __restrict__ prev, uint8_t* __restrict__ pf, uint8_t* __restrict__ sf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    pf[i] = prev[ids[i]] == INVALID;
+    sf[i] = next[ids[i]] == INVALID;
+}
+
+}  // namespace
+
+void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe) {
+    if (n_reads > 0xFFFFFFFFull) throw std::runtime_error("more than 2^32-1 reads in one block");
+    if (L < 1 || (L + 31) / 32 > 16) throw std::runtime_error("read length must be in [1, 512]");
+    p = BlockParams::derive(L, po, pe);
+    n = uint32_t(n_reads);
+    host.clear();
+    stage_ms.clear();
+    StageTimer T{stream};
+    cudaStream_t s = stream;
+    const int W = p.W;
+    uint32_t* counts = arena.alloc<uint32_t>(16);
+    uint32_t* err = arena.alloc<uint32_t>(1);
+    CURC_CHECK(cudaMemsetAsync(err, 0, 4, s));
+
+    // a1
+    T.begin("pack");
+    db = arena.alloc<uint64_t>(size_t(n) * W + 1);
+    uint8_t* has_n = arena.alloc<uint8_t>(n ? n : 1);
+    pack_reads(d_seq, n, L, db, has_n, err, s);
+    reads_id = arena.alloc<uint32_t>(n ? n : 1);
+    n_ids = arena.alloc<uint32_t>(n ? n : 1);
+    split_n_reads(has_n, n, reads_id, n_ids, counts, arena, s);
+    uint32_t hc[2];
+    CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
+    CURC_CHECK(cudaStreamSynchronize(s));
+    m = hc[0];
+    NN = hc[1];
+    nreads = arena.alloc<uint8_t>(size_t(NN) * L + 16);
+    gather_ascii_rows(d_seq, n_ids, NN, L, nreads, s);
+    T.end();
+    if (read_scalar(err, s)) throw std::runtime_error("pack: bulk copy wait timed out");
+    if (keep_intermediates) {
+        keep("packed", db, size_t(n) * W);
+        keep("has_n", has_n, n);
+    }
+
+    // a2
+    T.begin("sort_dedupe");
+    next = arena.alloc<uint32_t>(n ? n : 1);
+    prev = arena.alloc<uint32_t>(n ? n : 1);
+    offset = arena.alloc<uint16_t>(n ? n : 1);
+    fill<uint32_t>(next, INVALID, n, s);
+    fill<uint32_t>(prev, INVALID, n, s);
+    fill<uint16_t>(offset, INVALOFF, n, s);
+    sorted = arena.alloc<uint32_t>(m ? m : 1);
+    if (m) CURC_CHECK(cudaMemcpyAsync(sorted, reads_id, size_t(m) * 4, cudaMemcpyDeviceToDevice, s));
+    sort_ids_by_reads(db, W, L, sorted, m, arena, s);
+    dedupe_links(db, W, sorted, m, next, prev, offset, s);
+    T.end();
+    if (keep_intermediates) keep("sorted_ids", sorted, m);
+
+    // a3 + a4
+    T.begin("overlap");
+    overlap_link(p, db, sorted, m, next, prev, offset, arena, s, &ostats);
+    T.end();
+
+    // a5
+    T.begin("chain_filter");
+    ref_ids = arena.alloc<uint32_t>(m ? m : 1);
+    unmatch_ids = arena.alloc<uint32_t>(m ? m : 1);
+    chain_filter(n, sorted, m, next, prev, offset, ref_ids, unmatch_ids, counts, arena, s);
+    CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
+    CURC_CHECK(cudaStreamSynchronize(s));
+    n_ref = hc[0];
+    U = hc[1];
+    T.end();
+
+    // a6 (compress.cu:1576-1591)
+    T.begin("full_match");
+    {
+        auto mk = arena.mark();
+        uint8_t* pf = arena.alloc<uint8_t>(n_ref ? n_ref : 1);
+        uint8_t* sf = arena.alloc<uint8_t>(n_ref ? n_ref : 1);
+        uint32_t* pre = arena.alloc<uint32_t>(n_ref ? n_ref : 1);
+        uint32_t* suf = arena.alloc<uint32_t>(n_ref ? n_ref : 1);
+        if (n_ref) {
+            ends_kernel<<<grid_for(n_ref, 256), 256, 0, s>>>(ref_ids, n_ref, next, prev, pf, sf);
+            CURC_LAUNCH_CHECK();
+        }
+        select_flagged(ref_ids, pf, pre, n_ref, counts + 2, arena, s);
+        select_flagged(ref_ids, sf, suf, n_ref, counts + 3, arena, s);
+        const uint32_t cnt = read_scalar(counts + 3, s);
+        full_match_packed(p, db, pre, suf, cnt, next, prev, offset, arena, s);
+        arena.release(mk);
+    }
+    T.end();
+    if (keep_intermediates) {
+        keep("next", next, n);
+        keep("prev", prev, n);
+        keep("offset", offset, n);
+        keep("ref_ids", ref_ids, n_ref);
+        keep("unmatch_ids", unmatch_ids, U);
+    }
+
+    // a8
+    T.begin("assembly");
+    assemble(db, nullptr, L, W, ref_ids, n_ref, n, next, prev, offset, false, hq, arena, s);
+    T.end();
+    if (keep_intermediates) {
+        keep("hq_seq", hq.seq, hq.len);
+        keep("hq_records", hq.records, hq.n_records);
+    }
+
+    // a9 (compress.cu:1622-1640)
+    T.begin("mapping");
+    udb = arena.alloc<uint64_t>(size_t(U) * W + 1);
+    if (U) {
+        gather_reads_kernel<<<grid_for(uint64_t(U) * W, 256), 256, 0, s>>>(db, W, unmatch_ids, U, udb);
+        CURC_LAUNCH_CHECK();
+    }
+    mo.mm = arena.alloc<uint8_t>(U + NN + 1);
+    mo.strand = arena.alloc<uint8_t>(U + NN + 1);
+    mo.pos = arena.alloc<uint64_t>(U + NN + 1);
+    map_reads(p, hq.packed, hq.len, udb, U, nreads, NN, mo, arena, s);
+    T.end();
+    if (keep_intermediates) {
+        keep("map_mm", mo.mm, U + NN);
+        keep("map_strand", mo.strand, U + NN);
+        keep("map_pos", mo.pos, U + NN);
+    }
+
+    emit(T);
+    T.collect(stage_ms);
+    CURC_CHECK(cudaStreamSynchronize(s));
+}
+
+}  // namespace curc
+
+// ---------------------------------------------------------------- C-ABI
+
+struct curc_ctx {
+    int device = 0;
+    std::unique_ptr<curc::Block> block;
+    std::string err;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(curc_ctx* ctx, F&& f) {
+    try {
+        if (ctx) CURC_CHECK(cudaSetDevice(ctx->device));
+        f();
+        return CURC_OK;
+    } catch (const curc::CudaError& e) {
+        if (ctx) ctx->err = e.what();
+        return CURC_ERR_CUDA;
+    } catch (const std::invalid_argument& e) {
+        if (ctx) ctx->err = e.what();
+        return CURC_ERR_ARG;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->err = e.what();
+        return CURC_ERR_STATE;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int curc_ctx_create(int device, curc_ctx** out) {
+    if (!out) return CURC_ERR_ARG;
+    *out = nullptr;
+    try {
+        int count = 0;
+        CURC_CHECK(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count) throw std::invalid_argument("no such CUDA device");
+        CURC_CHECK(cudaSetDevice(device));
+        auto* c = new curc_ctx;
+        c->device = device;
+        c->block = std::make_unique<curc::Block>();
+        *out = c;
+        return CURC_OK;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return CURC_ERR_CUDA;
+    }
+}
+
+void curc_ctx_destroy(curc_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    delete ctx;
+}
+
+const char* curc_last_error(const curc_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int curc_pack_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, uint64_t* packed_dev,
+                     uint8_t* has_n_dev, void* stream) {
+    if (!ctx || (!seqs_dev && n) || (!packed_dev && n) || (!has_n_dev && n)) return CURC_ERR_ARG;
+    if (read_len < 1 || read_len > 512) {
+        ctx->err = "read length must be in [1, 512]";
+        return CURC_ERR_ARG;
+    }
+    return guarded(ctx, [&] {
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->block->stream;
+        curc::Arena& a = ctx->block->arena;
+        auto mk = a.mark();
+        uint32_t* err = a.alloc<uint32_t>(1);
+        CURC_CHECK(cudaMemsetAsync(err, 0, 4, s));
+        curc::pack_reads(reinterpret_cast<const uint8_t*>(seqs_dev), n, read_len, packed_dev, has_n_dev, err, s);
+        const uint32_t e = curc::read_scalar(err, s);
+        a.release(mk);
+        if (e) throw std::runtime_error("pack: bulk copy wait timed out");
+    });
+}
+
+int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
+                          int paired_end) {
+    if (!ctx || (!seqs_dev && n)) return CURC_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->block->arena.reset();
+        ctx->block->run(reinterpret_cast<const uint8_t*>(seqs_dev), n, read_len, preserve_order != 0,
+                        paired_end != 0);
+    });
+}
+
+int curc_block_run(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read_len, int preserve_order,
+                   int paired_end) {
+    if (!ctx || (!seqs && n)) return CURC_ERR_ARG;
+    return guarded(ctx, [&] {
+        curc::Block& b = *ctx->block;
+        b.arena.reset();
+        const size_t bytes = size_t(n) * read_len;
+        uint8_t* d = b.arena.alloc<uint8_t>(bytes + 16);
+        CURC_CHECK(cudaMemcpyAsync(d, seqs, bytes, cudaMemcpyHostToDevice, b.stream));
+        b.run(d, n, read_len, preserve_order != 0, paired_end != 0);
+    });
+}
+
+int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* bytes) {
+    if (!ctx || !name || !ptr || !bytes) return CURC_ERR_ARG;
+    auto it = ctx->block->host.find(name);
+    if (it == ctx->block->host.end()) {
+        ctx->err = std::string("unknown result: ") + name;
+        return CURC_ERR_ARG;
+    }
+    *ptr = it->second.data();
+    *bytes = it->second.size();
+    return CURC_OK;
+}
+
+int curc_block_stage_ms(curc_ctx* ctx, const char* stage, float* ms) {
+    if (!ctx || !stage || !ms) return CURC_ERR_ARG;
+    auto it = ctx->block->stage_ms.find(stage);
+    if (it == ctx->block->stage_ms.end()) {
+        ctx->err = std::string("unknown stage: ") + stage;
+        return CURC_ERR_ARG;
+    }
+    *ms = it->second;
+    return CURC_OK;
+}
+
+}  // extern "C"

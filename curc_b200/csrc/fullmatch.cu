@@ -1,0 +1,291 @@
+// a6/a7: exact suffix-prefix merge of chain ends over every offset.
+//
+// Reference: full_match_gpu compress.cu:1003-1174 (packed reads) and
+// full_match_cpu compress.cu:1176-1347 (ASCII N reads, alphabet ACGNT).
+//
+// Per offset the reference (1) re-sorts the suffix list by read[off, L) with
+// a split on base off-1 and stable merges, (2) buckets both lists by a
+// 10-base (3-symbol for ASCII) prefix with 4^10 binary searches, and (3)
+// runs one sequential two-pointer merge per bucket.  Inside a bucket the
+// merge pairs, in order, the suffixes and prefixes of each run of equal
+// strings (with a rotation when a read meets itself), so here the work is
+// organised per run of equal suffix strings instead: no fixed 4^10 cost,
+// and one thread per run executes the reference's merge steps for that run.
+//
+// (1) is done as a parallel stable merge of the per-symbol runs: each
+// element's output position is its rank in its run plus, for every other
+// run, the number of elements that precede it (binary search).
+#include "stages.cuh"
+
+namespace curc {
+
+namespace {
+
+struct PackedAcc {
+    const uint64_t* db;
+    int W, L;
+    static constexpr int ALPHA = 4;
+    __device__ __forceinline__ int cmp(uint32_t a, int aoff, uint32_t b, int boff, int len) const {
+        return cmp_span(db + uint64_t(a) * W, aoff, db + uint64_t(b) * W, boff, len);
+    }
+    __device__ __forceinline__ int sym(uint32_t a, int pos) const { return code_at(db + uint64_t(a) * W, pos); }
+};
+
+struct AsciiAcc {
+    const uint8_t* r;
+    int W, L;  // W unused
+    static constexpr int ALPHA = 5;
+    __device__ __forceinline__ int cmp(uint32_t a, int aoff, uint32_t b, int boff, int len) const {
+        const uint8_t* x = r + uint64_t(a) * L + aoff;
+        const uint8_t* y = r + uint64_t(b) * L + boff;
+        for (int i = 0; i < len; ++i)
+            if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
+        return 0;
+    }
+    // partition symbols of compress.cu:1238-1249: A, C, G, N, everything else
+    __device__ __forceinline__ int sym(uint32_t a, int pos) const {
+        switch (r[uint64_t(a) * L + pos]) {
+            case 'A': return 0;
+            case 'C': return 1;
+            case 'G': return 2;
+            case 'N': return 3;
+            default: return 4;
+        }
+    }
+};
+
+template <class Acc>
+__global__ void run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf, uint32_t m, int off,
+                                  uint32_t* __restrict__ bounds) {
+    // bounds[c] = first index whose symbol at off-1 is >= c
+    const int c = threadIdx.x;
+    if (c > Acc::ALPHA) return;
+    uint32_t lo = 0, count = m;
+    while (count > 0) {
+        uint32_t step = count / 2, it = lo + step;
+        if (acc.sym(suf[it], off - 1) < c) {
+            lo = it + 1;
+            count -= step + 1;
+        } else {
+            count = step;
+        }
+    }
+    bounds[c] = c == Acc::ALPHA ? m : lo;
+}
+
+// Stable merge of the symbol runs by read[off, L).
+template <class Acc>
+__global__ void merge_runs_kernel(Acc acc, const uint32_t* __restrict__ suf, uint32_t m, int off,
+                                  const uint32_t* __restrict__ bounds, uint32_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    uint32_t bd[Acc::ALPHA + 1];
+#pragma unroll
+    for (int c = 0; c <= Acc::ALPHA; ++c) bd[c] = bounds[c];
+    int x = 0;
+    while (x + 1 <= Acc::ALPHA && bd[x + 1] <= i) ++x;
+    const uint32_t me = suf[i];
+    const int len = acc.L - off;
+    uint32_t pos = i - bd[x];
+#pragma unroll
+    for (int y = 0; y < Acc::ALPHA; ++y) {
+        if (y == x) continue;
+        uint32_t lo = bd[y], count = bd[y + 1] - bd[y];
+        // y < x: elements <= me precede; y > x: elements < me precede
+        while (count > 0) {
+            uint32_t step = count / 2, it = lo + step;
+            const int c = acc.cmp(suf[it], off, me, off, len);
+            if (c < 0 || (c == 0 && y < x)) {
+                lo = it + 1;
+                count -= step + 1;
+            } else {
+                count = step;
+            }
+        }
+        pos += lo - bd[y];
+    }
+    out[pos] = me;
+}
+
+// One thread per run of equal suffix strings: the reference's bucket merge
+// restricted to that run (compress.cu:1089-1160 / 1297-1336).
+template <class Acc>
+__global__ void merge_groups_kernel(Acc acc, uint32_t* pre, uint32_t mp, const uint32_t* __restrict__ suf,
+                                    uint32_t ms, int off, uint32_t* next, uint32_t* prev, uint16_t* offset) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ms) return;
+    const int len = acc.L - off;
+    const uint32_t s0 = suf[j];
+    if (j > 0 && acc.cmp(suf[j - 1], off, s0, off, len) == 0) return;
+    // prefixes P with P[0, len) == s0[off, L)
+    uint32_t lo = 0, count = mp;
+    while (count > 0) {
+        uint32_t step = count / 2, it = lo + step;
+        if (acc.cmp(pre[it], 0, s0, off, len) < 0) {
+            lo = it + 1;
+            count -= step + 1;
+        } else {
+            count = step;
+        }
+    }
+    uint32_t hi = lo;
+    while (hi < mp && acc.cmp(pre[hi], 0, s0, off, len) == 0) ++hi;
+    if (hi == lo) return;
+    uint32_t se = j + 1;
+    while (se < ms && acc.cmp(suf[se], off, s0, off, len) == 0) ++se;
+    uint32_t pi = lo, si = j;
+    while (pi < hi && si < se) {
+        uint32_t P = pre[pi];
+        const uint32_t S = suf[si];
+        if (P == S) {
+            const uint32_t cur = pi;
+            bool found = false;
+            while (pi + 1 < hi) {
+                ++pi;
+                if (pre[pi] != S) {
+                    found = true;
+                    break;
+                }
+            }
+            if (!found) {
+                pi = cur;
+                ++si;
+                continue;
+            }
+            P = pre[pi];
+            while (pi > cur) {
+                pre[pi] = pre[pi - 1];
+                --pi;
+            }
+            pre[pi] = P;
+        }
+        next[S] = P;
+        prev[P] = S;
+        offset[S] = uint16_t(off);
+        ++pi;
+        ++si;
+    }
+}
+
+__global__ void keep_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ link,
+                                  uint8_t* __restrict__ keep) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) keep[i] = link[ids[i]] == INVALID;
+}
+
+template <class Acc>
+void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt, uint32_t* next, uint32_t* prev,
+                     uint16_t* offset, Arena& a, cudaStream_t s) {
+    if (cnt == 0) return;
+    auto mk = a.mark();
+    uint32_t* suf2 = a.alloc<uint32_t>(cnt);
+    uint32_t* tmp = a.alloc<uint32_t>(cnt);
+    uint8_t* keep = a.alloc<uint8_t>(cnt);
+    uint32_t* bounds = a.alloc<uint32_t>(8);
+    uint32_t* counts = a.alloc<uint32_t>(2);
+    uint32_t mp = cnt, ms = cnt;
+    for (int off = 1; off < acc.L && mp > 0 && ms > 0; ++off) {
+        run_bounds_kernel<Acc><<<1, 32, 0, s>>>(acc, suf, ms, off, bounds);
+        CURC_LAUNCH_CHECK();
+        merge_runs_kernel<Acc><<<grid_for(ms, 256), 256, 0, s>>>(acc, suf, ms, off, bounds, suf2);
+        CURC_LAUNCH_CHECK();
+        merge_groups_kernel<Acc><<<grid_for(ms, 128), 128, 0, s>>>(acc, pre, mp, suf2, ms, off, next, prev, offset);
+        CURC_LAUNCH_CHECK();
+        keep_flags_kernel<<<grid_for(mp, 256), 256, 0, s>>>(pre, mp, prev, keep);
+        CURC_LAUNCH_CHECK();
+        select_flagged(pre, keep, tmp, mp, counts + 0, a, s);
+        CURC_CHECK(cudaMemcpyAsync(pre, tmp, size_t(mp) * 4, cudaMemcpyDeviceToDevice, s));
+        keep_flags_kernel<<<grid_for(ms, 256), 256, 0, s>>>(suf2, ms, next, keep);
+        CURC_LAUNCH_CHECK();
+        select_flagged(suf2, keep, suf, ms, counts + 1, a, s);
+        uint32_t hc[2];
+        CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
+        CURC_CHECK(cudaStreamSynchronize(s));
+        mp = hc[0];
+        ms = hc[1];
+    }
+    a.release(mk);
+}
+
+__global__ void ascii_chunk_kernel(const uint8_t* __restrict__ r, int L, const uint32_t* __restrict__ ids, uint32_t m,
+                                   int chunk, uint64_t* __restrict__ key) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint8_t* p = r + uint64_t(ids[i]) * L + chunk * 8;
+    uint64_t v = 0;
+    for (int b = 0; b < 8; ++b) v = (v << 8) | (chunk * 8 + b < L ? p[b] : 0);
+    key[i] = v;
+}
+
+__global__ void ascii_dedupe_kernel(const uint8_t* __restrict__ r, int L, const uint32_t* __restrict__ ids, uint32_t m,
+                                    uint32_t* next, uint32_t* prev, uint16_t* offset) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= m) return;
+    const uint32_t a = ids[i], b = ids[i + 1];
+    const uint8_t* x = r + uint64_t(a) * L;
+    const uint8_t* y = r + uint64_t(b) * L;
+    for (int t = 0; t < L; ++t)
+        if (x[t] != y[t]) return;
+    prev[b] = a;
+    next[a] = b;
+    offset[a] = 0;
+}
+
+__global__ void ends_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ next,
+                                  const uint32_t* __restrict__ prev, uint8_t* __restrict__ pf, uint8_t* __restrict__ sf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    pf[i] = prev[ids[i]] == INVALID;
+    sf[i] = next[ids[i]] == INVALID;
+}
+
+}  // namespace
+
+void full_match_packed(const BlockParams& p, const uint64_t* db, uint32_t* pre, uint32_t* suf, uint32_t cnt,
+                       uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s) {
+    full_match_loop(PackedAcc{db, p.W, p.L}, pre, suf, cnt, next, prev, offset, a, s);
+}
+
+void sort_ids_by_ascii(const uint8_t* reads, int L, uint32_t* ids, uint32_t m, Arena& a, cudaStream_t s) {
+    // stable lexicographic (memcmp) order: LSD over 8-byte big-endian chunks
+    if (m <= 1) return;
+    auto mk = a.mark();
+    uint64_t* key = a.alloc<uint64_t>(m);
+    const int chunks = (L + 7) / 8;
+    for (int c = chunks - 1; c >= 0; --c) {
+        ascii_chunk_kernel<<<grid_for(m, 256), 256, 0, s>>>(reads, L, ids, m, c, key);
+        CURC_LAUNCH_CHECK();
+        const int lo = (c == chunks - 1) ? 8 * (8 * chunks - L) : 0;
+        radix_sort_pairs<uint64_t, uint32_t>(key, ids, m, lo, 64, a, s);
+    }
+    a.release(mk);
+}
+
+void full_match_ascii(const BlockParams& p, const uint8_t* reads, uint32_t* ids, uint32_t m, uint32_t n_total,
+                      uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s) {
+    // compress.cu:1179-1210: sort, duplicate links, prefix/suffix lists
+    fill<uint32_t>(next, INVALID, n_total, s);
+    fill<uint32_t>(prev, INVALID, n_total, s);
+    fill<uint16_t>(offset, INVALOFF, n_total, s);
+    if (m == 0) return;
+    sort_ids_by_ascii(reads, p.L, ids, m, a, s);
+    if (m > 1) {
+        ascii_dedupe_kernel<<<grid_for(m, 256), 256, 0, s>>>(reads, p.L, ids, m, next, prev, offset);
+        CURC_LAUNCH_CHECK();
+    }
+    auto mk = a.mark();
+    uint8_t* pf = a.alloc<uint8_t>(m);
+    uint8_t* sf = a.alloc<uint8_t>(m);
+    ends_flags_kernel<<<grid_for(m, 256), 256, 0, s>>>(ids, m, next, prev, pf, sf);
+    CURC_LAUNCH_CHECK();
+    uint32_t* pre = a.alloc<uint32_t>(m);
+    uint32_t* suf = a.alloc<uint32_t>(m);
+    uint32_t* counts = a.alloc<uint32_t>(2);
+    select_flagged(ids, pf, pre, m, counts + 0, a, s);
+    select_flagged(ids, sf, suf, m, counts + 1, a, s);
+    const uint32_t cnt = read_scalar(counts + 0, s);
+    full_match_loop(AsciiAcc{reads, 0, p.L}, pre, suf, cnt, next, prev, offset, a, s);
+    a.release(mk);
+}
+
+}  // namespace curc

@@ -1,0 +1,201 @@
+// a9: map leftover reads onto the pseudogenome.
+//
+// Reference: ReadMapper compress.cu:268-595 with util.cuh:233-270.
+// A sampled index of 28-mers every 5 positions (forward, then reverse
+// complemented for the second strand), buckets capped at 12 entries; each
+// read probes its 28-mers at every 2nd offset and keeps the first candidate
+// that strictly improves its mismatch count, stopping at <= 1 mismatch.
+//
+// Canonical index.  The reference fills buckets with non-atomic uint8
+// counters; here a bucket holds the first 12 sampled positions in ascending
+// order, stored in descending slots (the sequential outcome of
+// compress.cu:368-406).  It is built with a stable radix sort of (hash,
+// sample) pairs: each sample finds its rank in its bucket by looking back at
+// most 12 places, so no per-bucket atomics are needed.
+#include "stages.cuh"
+
+namespace curc {
+
+namespace {
+
+__global__ void sample_hash_kernel(const uint64_t* __restrict__ ref, uint64_t start, uint64_t count, int k, int step,
+                                   bool rc, uint32_t mask, uint32_t* __restrict__ hv, uint32_t* __restrict__ idx) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t km = word_unaligned(ref, start + i * step, k);
+        if (rc) km = revcomp_kmer(km, k);
+        hv[i] = uint32_t(murmur64(km) & mask);
+        idx[i] = uint32_t(i);
+    }
+}
+
+__global__ void bucket_caps_kernel(const uint32_t* __restrict__ hv, uint64_t count, uint32_t* __restrict__ cnt) {
+    for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < count; j += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t h = hv[j];
+        if (j > 0 && hv[j - 1] == h) continue;
+        uint32_t c = 1;
+        while (c < BlockParams::bucket_limit && j + c < count && hv[j + c] == h) ++c;
+        cnt[h] = c;
+    }
+}
+
+__global__ void bucket_fill_kernel(const uint32_t* __restrict__ hv, const uint32_t* __restrict__ idx, uint64_t count,
+                                   const uint32_t* __restrict__ kr, uint32_t* __restrict__ pos) {
+    for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < count; j += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t h = hv[j];
+        uint32_t rank = 0;
+        while (rank < BlockParams::bucket_limit && rank < j && hv[j - 1 - rank] == h) ++rank;
+        const uint32_t b = kr[h], c = kr[h + 1] - b;
+        if (rank < c) pos[b + c - 1 - rank] = idx[j];
+    }
+}
+
+struct MapIndex {
+    uint32_t mask;
+    const uint32_t* kr;
+    const uint32_t* pos;
+    uint64_t start;
+};
+
+template <bool RC>
+__device__ __forceinline__ int packed_mismatches(const uint64_t* __restrict__ ref, uint64_t mp,
+                                                 const uint64_t* __restrict__ rd, int L, int bound) {
+    // util.cuh:233-270: 32-base chunks, early exit once the bound is reached
+    int c = 0;
+    for (int i = 0; i < L && c < bound; i += 32) {
+        const int nb = L - i < 32 ? L - i : 32;
+        const uint64_t a = word_unaligned(ref, mp + i, nb);
+        uint64_t b;
+        if (!RC) {
+            b = word_at(rd, i, nb);
+        } else {
+            b = revcomp_kmer(word_at(rd, L - i - nb, nb), nb);
+        }
+        c += base_mismatches(a, b);
+    }
+    return c;
+}
+
+template <bool RC>
+__device__ __forceinline__ int ascii_mismatches(const uint64_t* __restrict__ ref, uint64_t mp,
+                                                const uint8_t* __restrict__ nd, int L, int bound) {
+    int c = 0;
+    for (int o = 0; o < L; ++o) {
+        const char rb = "ACGT"[code_at(ref, mp + o)];
+        const char qb = RC ? comp_char(char(nd[L - 1 - o])) : char(nd[o]);
+        if (rb != qb && ++c >= bound) break;
+    }
+    return c;
+}
+
+template <bool RC>
+__global__ void map_kernel(MapIndex ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
+                           const uint64_t* __restrict__ udb, uint32_t U, const uint8_t* __restrict__ ndb, uint32_t NN,
+                           int L, int W, int k, int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
+                           uint64_t* __restrict__ pos) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= U + NN) return;
+    int best = mm[i];
+    if (best <= BlockParams::target_mm) return;
+    const bool isn = i >= U;
+    const uint64_t* rd = isn ? nullptr : udb + uint64_t(i) * W;
+    const uint8_t* nd = isn ? ndb + uint64_t(i - U) * L : nullptr;
+    bool found = false;
+    uint64_t bpos = 0;
+    for (int j = 0; j + k <= L; j += BlockParams::read_step) {
+        uint64_t key;
+        if (!isn) {
+            key = word_at(rd, j, k);
+        } else {
+            key = 0;
+            for (int t = 0; t < k; ++t) key = (key << 2) | uint64_t(ascii_code(nd[j + t]));
+        }
+        const uint32_t h = uint32_t(murmur64(key) & ix.mask);
+        const uint32_t b = ix.kr[h];
+        uint32_t e = ix.kr[h + 1];
+        if (b == e) continue;
+        e = min(b + 12u, e);
+        const uint64_t shift = RC ? uint64_t(L - k - j) : uint64_t(j);
+        for (uint32_t q = b; q < e; ++q) {
+            const uint64_t refpos = ix.start + uint64_t(ix.pos[q]) * step;
+            if (refpos < shift) continue;
+            const uint64_t mp = refpos - shift;
+            if (mp + L > ref_len) continue;
+            const int c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best) : packed_mismatches<RC>(ref, mp, rd, L, best);
+            if (c < best) {
+                best = c;
+                bpos = mp;
+                found = true;
+                if (best <= BlockParams::target_mm) goto done;
+            }
+        }
+    }
+done:
+    if (found) {
+        mm[i] = uint8_t(best);
+        strand[i] = RC ? 1 : 0;
+        pos[i] = bpos;
+    }
+}
+
+inline int log2_exact(uint32_t x) {
+    int b = 0;
+    while ((1u << b) < x) ++b;
+    return b;
+}
+
+}  // namespace
+
+void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, const uint64_t* udb, uint32_t U,
+               const uint8_t* ndb, uint32_t NN, MapOut& out, Arena& a, cudaStream_t s) {
+    const uint32_t total = U + NN;
+    fill<uint8_t>(out.mm, uint8_t(p.max_mm + 1), total, s);
+    fill<uint8_t>(out.strand, 0, total, s);
+    fill<uint64_t>(out.pos, 0, total, s);
+    const int k = BlockParams::k1, step = BlockParams::ref_step;
+    if (total == 0 || ref_len < uint64_t(k)) return;
+    const uint64_t index_count = (ref_len - k + 1 + step - 1) / step;
+    struct Part { uint64_t start, count; };
+    Part parts[2];
+    int np = 1;
+    if (index_count > (1ull << 30)) {  // compress.cu:342-353
+        const uint64_t h = index_count / 2;
+        parts[0] = {0, h};
+        parts[1] = {h * step, index_count - h};
+        np = 2;
+    } else {
+        parts[0] = {0, index_count};
+    }
+    for (int rc = 0; rc < 2; ++rc) {
+        for (int q = 0; q < np; ++q) {
+            auto mk = a.mark();
+            const uint64_t count = parts[q].count;
+            const uint32_t hs = hash_size_for(count);
+            uint32_t* hv = a.alloc<uint32_t>(count);
+            uint32_t* idx = a.alloc<uint32_t>(count);
+            sample_hash_kernel<<<grid_for(count, 256, 4), 256, 0, s>>>(ref, parts[q].start, count, k, step, rc != 0,
+                                                                       hs - 1, hv, idx);
+            CURC_LAUNCH_CHECK();
+            radix_sort_pairs<uint32_t, uint32_t>(hv, idx, count, 0, log2_exact(hs), a, s);
+            uint32_t* kr = a.alloc<uint32_t>(size_t(hs) + 2);
+            CURC_CHECK(cudaMemsetAsync(kr, 0, (size_t(hs) + 2) * 4, s));
+            bucket_caps_kernel<<<grid_for(count, 256, 4), 256, 0, s>>>(hv, count, kr);
+            CURC_LAUNCH_CHECK();
+            exclusive_scan<uint32_t>(kr, kr, size_t(hs) + 2, nullptr, a, s);
+            uint32_t* pos = a.alloc<uint32_t>(std::min<uint64_t>(count, uint64_t(hs) * 12) + 2);
+            bucket_fill_kernel<<<grid_for(count, 256, 4), 256, 0, s>>>(hv, idx, count, kr, pos);
+            CURC_LAUNCH_CHECK();
+            MapIndex ix{hs - 1, kr, pos, parts[q].start};
+            const int g = grid_for(total, 128);
+            if (rc)
+                map_kernel<true><<<g, 128, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
+                                                   out.strand, out.pos);
+            else
+                map_kernel<false><<<g, 128, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
+                                                    out.strand, out.pos);
+            CURC_LAUNCH_CHECK();
+            a.release(mk);
+        }
+    }
+}
+
+}  // namespace curc

@@ -1,0 +1,313 @@
+// a2-a5: duplicate links, k-mer index over prefix reads, error-free overlap
+// linking over offsets 1..max_off-1, chain filter.
+//
+// Reference: compress.cu:1409-1420 (dedupe), 1427-1471 (index), 1473-1532
+// (overlap passes, atomicCAS linking), 1539-1585 (filter and partition).
+//
+// Determinism.  The reference links with atomicCAS, so which suffix wins a
+// contested prefix depends on scheduling.  Here the result is defined as the
+// sequential loop over suffixes in list order, and computed in parallel
+// exactly: every suffix whose equal-prefix run is claimed by it alone links
+// directly (runs of different suffix strings are disjoint); suffixes that
+// share a run are resolved by one thread per run, in list order.
+#include "stages.cuh"
+
+namespace curc {
+
+namespace {
+
+__global__ void dedupe_kernel(const uint64_t* __restrict__ db, int W, const uint32_t* __restrict__ sorted, uint32_t m,
+                              uint32_t* __restrict__ next, uint32_t* __restrict__ prev, uint16_t* __restrict__ offset) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= m) return;
+    const uint32_t a = sorted[i], b = sorted[i + 1];
+    const uint64_t* ra = db + uint64_t(a) * W;
+    const uint64_t* rb = db + uint64_t(b) * W;
+    for (int w = 0; w < W; ++w)
+        if (ra[w] != rb[w]) return;
+    next[a] = b;
+    prev[b] = a;
+    offset[a] = 0;
+}
+
+__global__ void link_flags_kernel(const uint32_t* __restrict__ sorted, uint32_t m, const uint32_t* __restrict__ next,
+                                  const uint32_t* __restrict__ prev, uint8_t* __restrict__ pre_f,
+                                  uint8_t* __restrict__ suf_f) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t id = sorted[i];
+    pre_f[i] = prev[id] == INVALID;
+    suf_f[i] = next[id] == INVALID;
+}
+
+__global__ void prefix_hash_kernel(const uint64_t* __restrict__ db, int W, int kip, int k, uint32_t mask,
+                                   const uint32_t* __restrict__ pre, uint32_t m, uint32_t* __restrict__ keys) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    keys[i] = uint32_t(murmur64(word_at(db + uint64_t(pre[i]) * W, kip, k)) & mask);
+}
+
+__global__ void bucket_count_kernel(const uint32_t* __restrict__ keys, uint32_t m, uint32_t* __restrict__ kr) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) atomicAdd(&kr[keys[i]], 1u);
+}
+
+struct OverlapCtx {
+    const uint64_t* db;
+    int W, L, k, kip;
+    uint32_t mask;
+    const uint32_t* va;  // prefix ids sorted by (bucket, read)
+    const uint32_t* kr;  // bucket ranges
+    uint32_t* next;
+    uint32_t* prev;
+    uint16_t* offset;
+};
+
+// First free non-self prefix of the equal run starting at lo, if equal.
+__device__ __forceinline__ void link_first_free(const OverlapCtx& c, uint32_t s, uint32_t lo, uint32_t e, int off) {
+    const uint64_t* sr = c.db + uint64_t(s) * c.W;
+    const int cl = c.L - off;
+    for (uint32_t q = lo; q < e; ++q) {
+        const uint32_t pr = c.va[q];
+        if (pr == s || c.prev[pr] != INVALID) continue;
+        if (cmp_span(c.db + uint64_t(pr) * c.W, 0, sr, off, cl) == 0) {
+            c.prev[pr] = s;
+            c.next[s] = pr;
+            c.offset[s] = uint16_t(off);
+        }
+        return;
+    }
+}
+
+// compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
+// bound of suffix[off, L) among the bucket's prefix[0, L-off).
+__global__ void probe_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uint32_t ms, int off,
+                             uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
+                             uint32_t* __restrict__ claim) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ms) return;
+    const uint32_t s = suf[j];
+    const uint64_t* sr = c.db + uint64_t(s) * c.W;
+    const uint32_t h = uint32_t(murmur64(word_at(sr, c.kip + off, c.k)) & c.mask);
+    uint32_t lo = c.kr[h];
+    const uint32_t e = c.kr[h + 1];
+    const int cl = c.L - off;
+    uint32_t count = e - lo;
+    while (count > 0) {
+        const uint32_t step = count / 2, it = lo + step;
+        if (cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl) < 0) {
+            lo = it + 1;
+            count -= step + 1;
+        } else {
+            count = step;
+        }
+    }
+    uint32_t r = INVALID;
+    if (lo < e && cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) == 0) {
+        r = lo;
+        atomicAdd(&claim[lo], 1u);
+    }
+    cand[j] = r;
+    cand_end[j] = e;
+}
+
+__global__ void resolve_solo_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uint32_t ms, int off,
+                                    const uint32_t* __restrict__ cand, const uint32_t* __restrict__ cand_end,
+                                    uint32_t* __restrict__ claim, uint8_t* __restrict__ contested) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ms) return;
+    const uint32_t lo = cand[j];
+    uint8_t f = 0;
+    if (lo != INVALID) {
+        if (claim[lo] == 1) {
+            link_first_free(c, suf[j], lo, cand_end[j], off);
+            claim[lo] = 0;
+        } else {
+            f = 1;
+        }
+    }
+    contested[j] = f;
+}
+
+__global__ void gather_cand_kernel(const uint32_t* __restrict__ cidx, uint32_t nc, const uint32_t* __restrict__ cand,
+                                   uint32_t* __restrict__ ckey) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nc) ckey[t] = cand[cidx[t]];
+}
+
+// One thread per contested run: its suffixes in list order, each taking the
+// first free non-self equal prefix (serial order of compress.cu:1474).
+__global__ void resolve_group_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, int off,
+                                     const uint32_t* __restrict__ ckey, const uint32_t* __restrict__ cidx, uint32_t nc,
+                                     const uint32_t* __restrict__ cand_end, uint32_t* __restrict__ claim) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nc) return;
+    const uint32_t lo = ckey[t];
+    if (t > 0 && ckey[t - 1] == lo) return;
+    for (uint32_t u = t; u < nc && ckey[u] == lo; ++u) {
+        const uint32_t j = cidx[u];
+        link_first_free(c, suf[j], lo, cand_end[j], off);
+    }
+    claim[lo] = 0;
+}
+
+__global__ void keep_unlinked_kernel(const uint32_t* __restrict__ suf, uint32_t ms, const uint32_t* __restrict__ next,
+                                     uint8_t* __restrict__ keep) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < ms) keep[j] = next[suf[j]] == INVALID;
+}
+
+__global__ void chain_res_kernel(uint32_t n, const uint32_t* __restrict__ next, const uint32_t* __restrict__ prev,
+                                 const uint16_t* __restrict__ offset, uint8_t* __restrict__ res) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t nx = next[r], pv = prev[r];
+    uint8_t keep = 0;
+    if (nx != INVALID && pv != INVALID) keep = 1;
+    else if (nx != INVALID && offset[r] == 0) keep = 1;
+    else if (pv != INVALID && offset[pv] == 0) keep = 1;
+    res[r] = keep;
+}
+
+// A link is dropped iff one of its ends is filtered out; concurrent writers
+// only ever store INVALID, so the result is schedule independent.
+__global__ void chain_unlink_kernel(uint32_t n, uint32_t* next, uint32_t* prev, const uint8_t* __restrict__ res) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n || res[r]) return;
+    const uint32_t nx = next[r];
+    if (nx != INVALID) {
+        prev[nx] = INVALID;
+        next[r] = INVALID;
+    }
+    const uint32_t pv = prev[r];
+    if (pv != INVALID) {
+        next[pv] = INVALID;
+        prev[r] = INVALID;
+    }
+}
+
+__global__ void gather_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint8_t* __restrict__ res,
+                                    uint8_t* __restrict__ f, uint8_t* __restrict__ nf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint8_t v = res[ids[i]];
+    f[i] = v;
+    nf[i] = !v;
+}
+
+inline int log2_exact(uint32_t x) {
+    int b = 0;
+    while ((1u << b) < x) ++b;
+    return b;
+}
+
+}  // namespace
+
+void dedupe_links(const uint64_t* db, int W, const uint32_t* sorted, uint32_t m, uint32_t* next, uint32_t* prev,
+                  uint16_t* offset, cudaStream_t s) {
+    if (m < 2) return;
+    dedupe_kernel<<<grid_for(m, 256), 256, 0, s>>>(db, W, sorted, m, next, prev, offset);
+    CURC_LAUNCH_CHECK();
+}
+
+void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sorted, uint32_t m, uint32_t* next,
+                  uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s, OverlapStats* st) {
+    if (m == 0) return;
+    auto mk = a.mark();
+    uint8_t* pre_f = a.alloc<uint8_t>(m);
+    uint8_t* suf_f = a.alloc<uint8_t>(m);
+    link_flags_kernel<<<grid_for(m, 256), 256, 0, s>>>(sorted, m, next, prev, pre_f, suf_f);
+    CURC_LAUNCH_CHECK();
+    uint32_t* pre = a.alloc<uint32_t>(m);
+    uint32_t* suf = a.alloc<uint32_t>(m);
+    uint32_t* suf2 = a.alloc<uint32_t>(m);
+    uint32_t* counts = a.alloc<uint32_t>(4);
+    select_flagged(sorted, pre_f, pre, m, counts + 0, a, s);
+    select_flagged(sorted, suf_f, suf, m, counts + 1, a, s);
+    uint32_t hc[2];
+    CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
+    CURC_CHECK(cudaStreamSynchronize(s));
+    const uint32_t mp = hc[0];
+    uint32_t ms = hc[1];
+
+    // index: stable sort of prefixes by bucket (compress.cu:1440-1471)
+    const uint32_t hs = hash_size_for(mp);
+    OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, pre, nullptr, next, prev, offset};
+    uint32_t* keys = a.alloc<uint32_t>(mp ? mp : 1);
+    if (mp) {
+        prefix_hash_kernel<<<grid_for(mp, 256), 256, 0, s>>>(db, p.W, p.kip, p.k, c.mask, pre, mp, keys);
+        CURC_LAUNCH_CHECK();
+        radix_sort_pairs<uint32_t, uint32_t>(keys, pre, mp, 0, log2_exact(hs), a, s);
+    }
+    uint32_t* kr = a.alloc<uint32_t>(size_t(hs) + 2);
+    CURC_CHECK(cudaMemsetAsync(kr, 0, (size_t(hs) + 2) * sizeof(uint32_t), s));
+    if (mp) {
+        bucket_count_kernel<<<grid_for(mp, 256), 256, 0, s>>>(keys, mp, kr);
+        CURC_LAUNCH_CHECK();
+    }
+    exclusive_scan<uint32_t>(kr, kr, size_t(hs) + 2, nullptr, a, s);
+    c.kr = kr;
+
+    uint32_t* claim = a.alloc<uint32_t>(mp ? mp : 1);
+    CURC_CHECK(cudaMemsetAsync(claim, 0, size_t(mp ? mp : 1) * sizeof(uint32_t), s));
+    uint32_t* cand = a.alloc<uint32_t>(ms ? ms : 1);
+    uint32_t* cand_end = a.alloc<uint32_t>(ms ? ms : 1);
+    uint8_t* flag = a.alloc<uint8_t>(ms ? ms : 1);
+    uint32_t* cidx = a.alloc<uint32_t>(ms ? ms : 1);
+    uint32_t* ckey = a.alloc<uint32_t>(ms ? ms : 1);
+
+    uint32_t passes = 0, contested_total = 0;
+    for (int off = 1; off < p.max_off && ms > 0 && mp > 0; ++off) {
+        ++passes;
+        const int g = grid_for(ms, 256);
+        probe_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim);
+        CURC_LAUNCH_CHECK();
+        resolve_solo_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim, flag);
+        CURC_LAUNCH_CHECK();
+        select_indices(flag, cidx, ms, counts + 2, a, s);
+        const uint32_t nc = read_scalar(counts + 2, s);
+        if (nc) {
+            contested_total += nc;
+            gather_cand_kernel<<<grid_for(nc, 256), 256, 0, s>>>(cidx, nc, cand, ckey);
+            CURC_LAUNCH_CHECK();
+            radix_sort_pairs<uint32_t, uint32_t>(ckey, cidx, nc, 0, 32, a, s);
+            resolve_group_kernel<<<grid_for(nc, 256), 256, 0, s>>>(c, suf, off, ckey, cidx, nc, cand_end, claim);
+            CURC_LAUNCH_CHECK();
+        }
+        keep_unlinked_kernel<<<g, 256, 0, s>>>(suf, ms, next, flag);
+        CURC_LAUNCH_CHECK();
+        select_flagged(suf, flag, suf2, ms, counts + 3, a, s);
+        std::swap(suf, suf2);
+        ms = read_scalar(counts + 3, s);
+    }
+    if (st) {
+        st->passes = passes;
+        st->contested = contested_total;
+    }
+    a.release(mk);
+}
+
+void chain_filter(uint32_t n, const uint32_t* sorted, uint32_t m, uint32_t* next, uint32_t* prev,
+                  const uint16_t* offset, uint32_t* ref_ids, uint32_t* unmatch_ids, uint32_t* counts, Arena& a,
+                  cudaStream_t s) {
+    // compress.cu:1539-1572
+    auto mk = a.mark();
+    uint8_t* res = a.alloc<uint8_t>(n ? n : 1);
+    if (n) {
+        chain_res_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, next, prev, offset, res);
+        CURC_LAUNCH_CHECK();
+        chain_unlink_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, next, prev, res);
+        CURC_LAUNCH_CHECK();
+    }
+    uint8_t* f = a.alloc<uint8_t>(m ? m : 1);
+    uint8_t* nf = a.alloc<uint8_t>(m ? m : 1);
+    if (m) {
+        gather_flags_kernel<<<grid_for(m, 256), 256, 0, s>>>(sorted, m, res, f, nf);
+        CURC_LAUNCH_CHECK();
+    }
+    select_flagged(sorted, f, ref_ids, m, counts + 0, a, s);
+    select_flagged(sorted, nf, unmatch_ids, m, counts + 1, a, s);
+    a.release(mk);
+}
+
+}  // namespace curc

@@ -1,0 +1,435 @@
+// Device-wide primitives: arena, scan, stable compaction, stable radix sort.
+#include <algorithm>
+
+#include "primitives.cuh"
+
+namespace curc {
+
+// ---------------------------------------------------------------- arena
+
+Arena::~Arena() {
+    for (auto& c : chunks_) cudaFree(c.base);
+}
+
+void* Arena::alloc_bytes(size_t bytes) {
+    bytes = (bytes + 255) & ~size_t(255);
+    if (bytes == 0) bytes = 256;
+    while (cur_ < chunks_.size()) {
+        Chunk& c = chunks_[cur_];
+        if (c.used + bytes <= c.size) {
+            void* p = c.base + c.used;
+            c.used += bytes;
+            high_water_ = std::max(high_water_, in_use());
+            return p;
+        }
+        if (cur_ + 1 < chunks_.size() && chunks_[cur_ + 1].size >= bytes) {
+            ++cur_;
+            chunks_[cur_].used = 0;
+            continue;
+        }
+        break;
+    }
+    size_t sz = std::max(bytes, chunk_);
+    char* p = nullptr;
+    CURC_CHECK(cudaMalloc(&p, sz));
+    // keep chunks ordered as used: insert after the current one
+    Chunk c{p, sz, bytes};
+    if (chunks_.empty()) {
+        chunks_.push_back(c);
+        cur_ = 0;
+    } else {
+        chunks_.insert(chunks_.begin() + cur_ + 1, c);
+        ++cur_;
+        for (size_t i = cur_ + 1; i < chunks_.size(); ++i) chunks_[i].used = 0;
+    }
+    high_water_ = std::max(high_water_, in_use());
+    return p;
+}
+
+size_t Arena::in_use() const {
+    size_t u = 0;
+    for (size_t i = 0; i <= cur_ && i < chunks_.size(); ++i) u += chunks_[i].used;
+    return u;
+}
+
+void Arena::reset() {
+    for (auto& c : chunks_) c.used = 0;
+    cur_ = 0;
+}
+
+void Arena::release(const Mark& m) {
+    if (chunks_.empty()) return;
+    for (size_t i = m.chunk + 1; i < chunks_.size(); ++i) chunks_[i].used = 0;
+    cur_ = m.chunk;
+    if (cur_ < chunks_.size()) chunks_[cur_].used = m.used;
+}
+
+// ---------------------------------------------------------------- scan
+
+namespace {
+constexpr int SCAN_THREADS = 256, SCAN_ITEMS = 8, SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <class T>
+__device__ T block_exclusive_sum(T v, T* block_total) {
+    __shared__ T warp_sums[SCAN_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < SCAN_THREADS / 32 ? warp_sums[lane] : T(0);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < SCAN_THREADS / 32) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    T warp_prefix = warp ? warp_sums[warp - 1] : T(0);
+    *block_total = warp_sums[SCAN_THREADS / 32 - 1];
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+template <class T>
+__global__ void __launch_bounds__(SCAN_THREADS) scan_reduce_kernel(const T* __restrict__ in, size_t n,
+                                                                   T* __restrict__ sums) {
+    const size_t base = size_t(blockIdx.x) * SCAN_TILE;
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        size_t idx = base + size_t(i) * SCAN_THREADS + threadIdx.x;
+        if (idx < n) s += in[idx];
+    }
+    T total;
+    block_exclusive_sum(s, &total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+template <class T>
+__global__ void __launch_bounds__(SCAN_THREADS) scan_apply_kernel(const T* in, T* out, size_t n,
+                                                                  const T* __restrict__ offsets, T* total) {
+    __shared__ T sm[SCAN_TILE];
+    const size_t base = size_t(blockIdx.x) * SCAN_TILE;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        size_t idx = base + size_t(i) * SCAN_THREADS + threadIdx.x;
+        sm[i * SCAN_THREADS + threadIdx.x] = idx < n ? in[idx] : T(0);
+    }
+    __syncthreads();
+    T local[SCAN_ITEMS];
+    T tsum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        local[i] = sm[threadIdx.x * SCAN_ITEMS + i];
+        tsum += local[i];
+    }
+    T btotal;
+    T run = block_exclusive_sum(tsum, &btotal);
+    if (offsets) run += offsets[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        T t = local[i];
+        sm[threadIdx.x * SCAN_ITEMS + i] = run;
+        run += t;
+    }
+    if (total && gridDim.x == 1 && threadIdx.x == 0) *total = btotal;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        size_t idx = base + size_t(i) * SCAN_THREADS + threadIdx.x;
+        if (idx < n) out[idx] = sm[i * SCAN_THREADS + threadIdx.x];
+    }
+}
+}  // namespace
+
+template <class T>
+void exclusive_scan(const T* in, T* out, size_t n, T* total, Arena& a, cudaStream_t s) {
+    if (n == 0) {
+        if (total) CURC_CHECK(cudaMemsetAsync(total, 0, sizeof(T), s));
+        return;
+    }
+    const size_t tiles = div_up(n, SCAN_TILE);
+    if (tiles == 1) {
+        scan_apply_kernel<T><<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total);
+        CURC_LAUNCH_CHECK();
+        return;
+    }
+    auto m = a.mark();
+    T* sums = a.alloc<T>(tiles);
+    scan_reduce_kernel<T><<<unsigned(tiles), SCAN_THREADS, 0, s>>>(in, n, sums);
+    CURC_LAUNCH_CHECK();
+    exclusive_scan<T>(sums, sums, tiles, total, a, s);
+    scan_apply_kernel<T><<<unsigned(tiles), SCAN_THREADS, 0, s>>>(in, out, n, sums, nullptr);
+    CURC_LAUNCH_CHECK();
+    a.release(m);
+}
+
+template void exclusive_scan<uint32_t>(const uint32_t*, uint32_t*, size_t, uint32_t*, Arena&, cudaStream_t);
+template void exclusive_scan<uint64_t>(const uint64_t*, uint64_t*, size_t, uint64_t*, Arena&, cudaStream_t);
+
+// ---------------------------------------------------------------- compaction
+
+namespace {
+constexpr int SEL_THREADS = 256, SEL_ITEMS = 8, SEL_TILE = SEL_THREADS * SEL_ITEMS;
+
+__global__ void __launch_bounds__(SEL_THREADS) count_flags_kernel(const uint8_t* __restrict__ flags, size_t n,
+                                                                  uint32_t* __restrict__ counts) {
+    const size_t base = size_t(blockIdx.x) * SEL_TILE;
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < SEL_ITEMS; ++i) {
+        size_t idx = base + size_t(i) * SEL_THREADS + threadIdx.x;
+        if (idx < n) c += flags[idx] != 0;
+    }
+    uint32_t total;
+    block_exclusive_sum<uint32_t>(c, &total);
+    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+template <class T, bool kIndices>
+__global__ void __launch_bounds__(SEL_THREADS) select_kernel(const T* __restrict__ in, const uint8_t* __restrict__ flags,
+                                                             size_t n, const uint32_t* __restrict__ offsets,
+                                                             T* __restrict__ out) {
+    // blocked arrangement: thread t owns tile items [t*ITEMS, (t+1)*ITEMS)
+    const size_t base = size_t(blockIdx.x) * SEL_TILE + size_t(threadIdx.x) * SEL_ITEMS;
+    uint8_t f[SEL_ITEMS];
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < SEL_ITEMS; ++i) {
+        size_t idx = base + i;
+        f[i] = idx < n ? flags[idx] != 0 : 0;
+        c += f[i];
+    }
+    uint32_t total;
+    uint32_t pos = block_exclusive_sum<uint32_t>(c, &total) + offsets[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < SEL_ITEMS; ++i) {
+        if (f[i]) {
+            if constexpr (kIndices) out[pos] = T(base + i);
+            else out[pos] = in[base + i];
+            ++pos;
+        }
+    }
+}
+
+template <class T, bool kIndices>
+void select_impl(const T* in, const uint8_t* flags, T* out, size_t n, uint32_t* count, Arena& a, cudaStream_t s) {
+    if (n == 0) {
+        CURC_CHECK(cudaMemsetAsync(count, 0, sizeof(uint32_t), s));
+        return;
+    }
+    auto m = a.mark();
+    const size_t tiles = div_up(n, SEL_TILE);
+    uint32_t* off = a.alloc<uint32_t>(tiles);
+    count_flags_kernel<<<unsigned(tiles), SEL_THREADS, 0, s>>>(flags, n, off);
+    CURC_LAUNCH_CHECK();
+    exclusive_scan<uint32_t>(off, off, tiles, count, a, s);
+    select_kernel<T, kIndices><<<unsigned(tiles), SEL_THREADS, 0, s>>>(in, flags, n, off, out);
+    CURC_LAUNCH_CHECK();
+    a.release(m);
+}
+}  // namespace
+
+template <class T>
+void select_flagged(const T* in, const uint8_t* flags, T* out, size_t n, uint32_t* count, Arena& a, cudaStream_t s) {
+    select_impl<T, false>(in, flags, out, n, count, a, s);
+}
+template void select_flagged<uint32_t>(const uint32_t*, const uint8_t*, uint32_t*, size_t, uint32_t*, Arena&,
+                                       cudaStream_t);
+template void select_flagged<uint64_t>(const uint64_t*, const uint8_t*, uint64_t*, size_t, uint32_t*, Arena&,
+                                       cudaStream_t);
+
+void select_indices(const uint8_t* flags, uint32_t* out, size_t n, uint32_t* count, Arena& a, cudaStream_t s) {
+    select_impl<uint32_t, true>(nullptr, flags, out, n, count, a, s);
+}
+
+// ---------------------------------------------------------------- radix sort
+
+namespace {
+constexpr int RS_THREADS = 256, RS_ROUNDS = 16, RS_TILE = RS_THREADS * RS_ROUNDS, RS_WARPS = RS_THREADS / 32;
+
+template <class K>
+__device__ __forceinline__ uint32_t digit_of(K k, int shift, uint32_t mask) {
+    return uint32_t(k >> shift) & mask;
+}
+
+template <class K>
+__global__ void __launch_bounds__(RS_THREADS) rs_hist_kernel(const K* __restrict__ keys, size_t n, int shift,
+                                                             uint32_t mask, uint32_t* __restrict__ hist,
+                                                             uint32_t tiles) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const size_t base = size_t(blockIdx.x) * RS_TILE;
+#pragma unroll 4
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+        size_t idx = base + size_t(r) * RS_THREADS + threadIdx.x;
+        if (idx < n) atomicAdd(&h[digit_of(keys[idx], shift, mask)], 1u);
+    }
+    __syncthreads();
+    hist[size_t(threadIdx.x) * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: items are ranked in index order.  Within a round of 256
+// items, a warp ranks equal digits with match_any; warps are ordered by a
+// per-round prefix over per-warp counts; rounds accumulate per digit.
+template <class K, class V>
+__global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const K* __restrict__ kin, const V* __restrict__ vin,
+                                                                K* __restrict__ kout, V* __restrict__ vout, size_t n,
+                                                                int shift, uint32_t mask,
+                                                                const uint32_t* __restrict__ offsets, uint32_t tiles) {
+    __shared__ uint32_t gbase[256];
+    __shared__ uint32_t run[256];
+    __shared__ uint32_t wcnt[RS_WARPS][256];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    gbase[tid] = offsets[size_t(tid) * tiles + blockIdx.x];
+    run[tid] = 0;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const size_t base = size_t(blockIdx.x) * RS_TILE;
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+        const size_t idx = base + size_t(r) * RS_THREADS + tid;
+        if (base + size_t(r) * RS_THREADS >= n) break;  // uniform across the block
+        const bool valid = idx < n;
+        K k{};
+        V v{};
+        uint32_t d = 256;
+        if (valid) {
+            k = kin[idx];
+            if (vin) v = vin[idx];
+            d = digit_of(k, shift, mask);
+        }
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; ++w) wcnt[w][tid] = 0;
+        __syncthreads();
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t rank = __popc(peers & lt_mask);
+        if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
+        __syncthreads();
+        uint32_t acc = 0;
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; ++w) {
+            uint32_t c = wcnt[w][tid];
+            wcnt[w][tid] = acc;
+            acc += c;
+        }
+        __syncthreads();
+        if (valid) {
+            const uint32_t pos = gbase[d] + run[d] + wcnt[warp][d] + rank;
+            kout[pos] = k;
+            if (vout) vout[pos] = v;
+        }
+        __syncthreads();
+        run[tid] += acc;
+    }
+}
+}  // namespace
+
+template <class K, class V>
+void radix_sort_pairs(K* keys, V* vals, size_t n, int begin_bit, int end_bit, Arena& a, cudaStream_t s) {
+    if (n <= 1 || end_bit <= begin_bit) return;
+    if (n > 0xFFFFFFFFull) throw std::runtime_error("radix_sort_pairs: more than 2^32 items");
+    auto m = a.mark();
+    K* kalt = a.alloc<K>(n);
+    V* valt = vals ? a.alloc<V>(n) : nullptr;
+    const uint32_t tiles = uint32_t(div_up(n, RS_TILE));
+    uint32_t* hist = a.alloc<uint32_t>(size_t(256) * tiles);
+    K* kc = keys;
+    V* vc = vals;
+    for (int shift = begin_bit; shift < end_bit; shift += 8) {
+        const int bits = std::min(8, end_bit - shift);
+        const uint32_t mask = (1u << bits) - 1u;
+        rs_hist_kernel<K><<<tiles, RS_THREADS, 0, s>>>(kc, n, shift, mask, hist, tiles);
+        CURC_LAUNCH_CHECK();
+        exclusive_scan<uint32_t>(hist, hist, size_t(256) * tiles, nullptr, a, s);
+        K* ko = (kc == keys) ? kalt : keys;
+        V* vo = vals ? ((vc == vals) ? valt : vals) : nullptr;
+        rs_scatter_kernel<K, V><<<tiles, RS_THREADS, 0, s>>>(kc, vc, ko, vo, n, shift, mask, hist, tiles);
+        CURC_LAUNCH_CHECK();
+        kc = ko;
+        vc = vo;
+    }
+    if (kc != keys) {
+        CURC_CHECK(cudaMemcpyAsync(keys, kc, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
+        if (vals) CURC_CHECK(cudaMemcpyAsync(vals, vc, n * sizeof(V), cudaMemcpyDeviceToDevice, s));
+    }
+    a.release(m);
+}
+
+template void radix_sort_pairs<uint64_t, uint32_t>(uint64_t*, uint32_t*, size_t, int, int, Arena&, cudaStream_t);
+template void radix_sort_pairs<uint32_t, uint32_t>(uint32_t*, uint32_t*, size_t, int, int, Arena&, cudaStream_t);
+template void radix_sort_pairs<uint64_t, uint64_t>(uint64_t*, uint64_t*, size_t, int, int, Arena&, cudaStream_t);
+
+// ---------------------------------------------------------------- misc
+
+namespace {
+__global__ void gather_words_kernel(const uint64_t* __restrict__ src, const uint32_t* __restrict__ idx, size_t n,
+                                    int stride, int word, uint64_t* __restrict__ out) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        out[i] = src[size_t(idx[i]) * stride + word];
+}
+
+template <class T>
+__global__ void fill_kernel(T* p, T v, size_t n) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        p[i] = v;
+}
+
+__global__ void iota_kernel(uint32_t* p, size_t n) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        p[i] = uint32_t(i);
+}
+
+int persistent_grid(size_t n) {
+    size_t g = div_up(n, 256);
+    return int(std::max<size_t>(1, std::min<size_t>(g, size_t(SM_COUNT_B200) * 16)));
+}
+}  // namespace
+
+void gather_words(const uint64_t* src, const uint32_t* idx, size_t n, int stride, int word, uint64_t* out,
+                  cudaStream_t s) {
+    if (!n) return;
+    gather_words_kernel<<<persistent_grid(n), 256, 0, s>>>(src, idx, n, stride, word, out);
+    CURC_LAUNCH_CHECK();
+}
+
+template <class T>
+void fill(T* p, T v, size_t n, cudaStream_t s) {
+    if (!n) return;
+    fill_kernel<T><<<persistent_grid(n), 256, 0, s>>>(p, v, n);
+    CURC_LAUNCH_CHECK();
+}
+template void fill<uint8_t>(uint8_t*, uint8_t, size_t, cudaStream_t);
+template void fill<uint16_t>(uint16_t*, uint16_t, size_t, cudaStream_t);
+template void fill<uint32_t>(uint32_t*, uint32_t, size_t, cudaStream_t);
+template void fill<uint64_t>(uint64_t*, uint64_t, size_t, cudaStream_t);
+
+void iota(uint32_t* p, size_t n, cudaStream_t s) {
+    if (!n) return;
+    iota_kernel<<<persistent_grid(n), 256, 0, s>>>(p, n);
+    CURC_LAUNCH_CHECK();
+}
+
+void sort_ids_by_reads(const uint64_t* db, int W, int L, uint32_t* ids, size_t n, Arena& a, cudaStream_t s) {
+    // LSD over whole words, last word first; each word sorted stably, so the
+    // final order is lexicographic with ties kept in input order
+    // (compress.cu:1400-1407 under a stable comparison sort).
+    if (n <= 1) return;
+    auto m = a.mark();
+    uint64_t* keys = a.alloc<uint64_t>(n);
+    for (int w = W - 1; w >= 0; --w) {
+        gather_words(db, ids, n, W, w, keys, s);
+        int lo = 0;
+        if (w == W - 1) lo = 64 - 2 * (L - 32 * (W - 1));  // unused low bits are zero
+        radix_sort_pairs<uint64_t, uint32_t>(keys, ids, n, lo, 64, a, s);
+    }
+    a.release(m);
+}
+
+}  // namespace curc

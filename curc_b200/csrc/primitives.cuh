@@ -1,0 +1,84 @@
+// Device-wide primitives used by every stage: a bump arena over device
+// memory, exclusive scan, stable compaction, and a stable LSD radix sort.
+// All are deterministic: results never depend on thread scheduling.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace curc {
+
+// Bump allocator over large device chunks.  reset() keeps the chunks, so a
+// pipeline that runs block after block allocates device memory only while
+// it grows.  Alignment 256 bytes (TMA and vector loads need 16).
+class Arena {
+public:
+    explicit Arena(size_t chunk = size_t(1) << 30) : chunk_(chunk) {}
+    ~Arena();
+    Arena(const Arena&) = delete;
+    Arena& operator=(const Arena&) = delete;
+
+    void* alloc_bytes(size_t bytes);
+    template <class T>
+    T* alloc(size_t n) { return static_cast<T*>(alloc_bytes(n * sizeof(T))); }
+    void reset();
+    size_t high_water() const { return high_water_; }
+    size_t in_use() const;
+
+    // Marks let a stage release its scratch once it is done.
+    struct Mark { size_t chunk, used; };
+    Mark mark() const { return {cur_, cur_ < chunks_.size() ? chunks_[cur_].used : 0}; }
+    void release(const Mark& m);
+
+private:
+    struct Chunk { char* base; size_t size, used; };
+    std::vector<Chunk> chunks_;
+    size_t cur_ = 0;
+    size_t chunk_;
+    size_t high_water_ = 0;
+};
+
+// out[i] = sum(in[0..i)); optionally *total = sum(in[0..n)) (device pointer).
+// In-place (out == in) is allowed.
+template <class T>
+void exclusive_scan(const T* in, T* out, size_t n, T* total, Arena& a, cudaStream_t s);
+
+// Stable compaction: out = [in[i] for i if flags[i]], *count = number kept.
+template <class T>
+void select_flagged(const T* in, const uint8_t* flags, T* out, size_t n, uint32_t* count, Arena& a,
+                    cudaStream_t s);
+
+// Same, writing the indices i with flags[i] set.
+void select_indices(const uint8_t* flags, uint32_t* out, size_t n, uint32_t* count, Arena& a, cudaStream_t s);
+
+// Stable LSD radix sort of (key, value) pairs on key bits [begin_bit,
+// end_bit).  keys/vals are overwritten with the sorted sequence.  vals may be
+// null (keys only).
+template <class K, class V>
+void radix_sort_pairs(K* keys, V* vals, size_t n, int begin_bit, int end_bit, Arena& a, cudaStream_t s);
+
+// Stable sort of ids by packed read content (W words per read, lexicographic
+// over all words): ids is permuted in place.
+void sort_ids_by_reads(const uint64_t* db, int W, int L, uint32_t* ids, size_t n, Arena& a, cudaStream_t s);
+
+// Gather 64-bit words: out[i] = src[idx[i] * stride + word].
+void gather_words(const uint64_t* src, const uint32_t* idx, size_t n, int stride, int word, uint64_t* out,
+                  cudaStream_t s);
+
+template <class T>
+void fill(T* p, T v, size_t n, cudaStream_t s);
+
+void iota(uint32_t* p, size_t n, cudaStream_t s);
+
+// Reads back one device value (synchronises the stream).
+template <class T>
+T read_scalar(const T* dev, cudaStream_t s) {
+    T v;
+    CURC_CHECK(cudaMemcpyAsync(&v, dev, sizeof(T), cudaMemcpyDeviceToHost, s));
+    CURC_CHECK(cudaStreamSynchronize(s));
+    return v;
+}
+
+}  // namespace curc

@@ -1,0 +1,506 @@
+// a12: reverse-complement repeat removal in the pseudogenomes.
+//
+// Reference: RefMatcher compress.cu:631-1001.  An index of 36-mers of the
+// main pseudogenome every 5 bases (maRushPrime1 hash, buckets capped at 12);
+// each destination string is reverse complemented and probed every 3 bases
+// (in segments of 4 probes for packed destinations, the first hit ending the
+// segment); a hit is extended both ways and kept when the extension spans
+// more than 50 bases and the whole 36-mer matches.  Hits become (src, len,
+// dst) triples that are sorted, deduplicated and applied: each kept span of
+// the destination is replaced by '%', its source offset goes to MapOff and
+// its length to MapLen.
+//
+// Canonical semantics: the reference appends hits with atomicAdd and drops
+// those beyond its capacity in arrival order; here the hits kept are the
+// first `capacity` in probe order.  The index buckets hold the first 12
+// positions (as in mapper.cu).
+//
+// B200 design: one thread per segment (packed) or per probe (ASCII); the
+// extensions compare 32 bases per step with XOR and count-leading-zeros
+// instead of one base per step; the triples are ordered with three stable
+// radix passes; the sequential acceptance walk (each kept span depends on
+// the end of the previous one) runs in one thread over the deduplicated
+// triples, and the string compaction is a parallel copy.
+#include <cstring>
+
+#include "block.cuh"
+
+namespace curc {
+
+namespace {
+
+constexpr int RM_K = 36, RM_SRC_STEP = 5, RM_DEST_STEP = 3, RM_MIN = 50;
+
+struct Hit {
+    uint64_t src, len, dst;
+};
+
+__device__ __forceinline__ uint32_t sym_word(const uint64_t* bits, uint64_t pos) {
+    // four symbols as ASCII bytes, little endian (memcpy of 4 chars)
+    uint32_t v = 0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) v |= uint32_t(uint8_t("ACGT"[code_at(bits, pos + t)])) << (8 * t);
+    return v;
+}
+
+// maRushPrime1HashBinary<36> (compress.cu:597-615)
+__device__ __forceinline__ uint32_t marush_packed(const uint64_t* bits, uint64_t pos) {
+    uint64_t h = RM_K;
+#pragma unroll
+    for (uint32_t j = 0; j < RM_K / 4; ++j) {
+        uint32_t v = sym_word(bits, pos + 4 * j) + j;
+        h ^= v;
+        h *= 171717;
+    }
+    return uint32_t(h);
+}
+
+// maRushPrime1HashChar<36> (compress.cu:617-629)
+__device__ __forceinline__ uint32_t marush_ascii(const uint8_t* s) {
+    uint64_t h = RM_K;
+#pragma unroll
+    for (uint32_t j = 0; j < RM_K / 4; ++j) {
+        uint32_t v = uint32_t(s[4 * j]) | uint32_t(s[4 * j + 1]) << 8 | uint32_t(s[4 * j + 2]) << 16 |
+                     uint32_t(s[4 * j + 3]) << 24;
+        v += j;
+        h ^= v;
+        h *= 171717;
+    }
+    return uint32_t(h);
+}
+
+__global__ void rm_hash_kernel(const uint64_t* __restrict__ ref, uint64_t count, uint32_t mask,
+                               uint32_t* __restrict__ hv, uint32_t* __restrict__ idx) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += uint64_t(gridDim.x) * blockDim.x) {
+        hv[i] = marush_packed(ref, i * RM_SRC_STEP) & mask;
+        idx[i] = uint32_t(i);
+    }
+}
+
+// reverse complement of an ASCII string
+__global__ void rc_ascii_kernel(const uint8_t* __restrict__ in, uint64_t n, uint8_t* __restrict__ out) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        out[i] = uint8_t(comp_char(char(in[n - 1 - i])));
+}
+
+struct RmIndex {
+    const uint64_t* ref;
+    uint64_t rl;
+    uint32_t mask;
+    const uint32_t* kr;
+    const uint32_t* pos;
+};
+
+// Number of equal bases of a[ao..) and b[bo..) going right, at most lim.
+__device__ __forceinline__ uint64_t match_right(const uint64_t* a, uint64_t ao, const uint64_t* b, uint64_t bo,
+                                                uint64_t lim) {
+    uint64_t k = 0;
+    while (k < lim) {
+        const int nb = lim - k < 32 ? int(lim - k) : 32;
+        const uint64_t x = word_unaligned(a, ao + k, nb) ^ word_unaligned(b, bo + k, nb);
+        if (x) return k + (__clzll(x) - (64 - 2 * nb)) / 2;
+        k += nb;
+    }
+    return lim;
+}
+
+// Number of equal bases of a[..ao) and b[..bo) going left, at most lim.
+__device__ __forceinline__ uint64_t match_left(const uint64_t* a, uint64_t ao, const uint64_t* b, uint64_t bo,
+                                               uint64_t lim) {
+    uint64_t k = 0;
+    while (k < lim) {
+        const int nb = lim - k < 32 ? int(lim - k) : 32;
+        const uint64_t x = word_unaligned(a, ao - k - nb, nb) ^ word_unaligned(b, bo - k - nb, nb);
+        if (x) return k + uint64_t(__ffsll(x) - 1) / 2;  // equal 2-bit groups from the right
+        k += nb;
+    }
+    return lim;
+}
+
+// Packed destination (reverse complemented, dl bases, zero padded): the
+// reference's probe of one destination position against one bucket.
+__device__ bool probe_packed(const RmIndex& ix, const uint64_t* dest, uint64_t dl, uint64_t dpad, uint64_t dpos,
+                             bool dest_is_ref, Hit* hit) {
+    const uint32_t h = marush_packed(dest, dpos) & ix.mask;
+    const uint32_t b = ix.kr[h], e = ix.kr[h + 1];
+    for (uint32_t j = b; j < e; ++j) {
+        const uint64_t spos = uint64_t(ix.pos[j]) * RM_SRC_STEP;
+        if (dest_is_ref && (dl - spos < dpos)) continue;
+        // right: p1 from dpos+36 (never equal to dl when it starts beyond it)
+        const uint64_t d0 = dpos + RM_K, s0 = spos + RM_K;
+        uint64_t dlim = d0 <= dl ? dl - d0 : dpad - d0;  // bases readable on the dest side
+        const uint64_t slim = s0 <= ix.rl ? ix.rl - s0 : 0;
+        const uint64_t run = match_right(dest, d0, ix.ref, s0, min(dlim, slim));
+        const uint64_t right = d0 + run;
+        // left
+        const uint64_t lmax = min(dpos, spos);
+        const uint64_t k = match_left(dest, dpos, ix.ref, spos, lmax);
+        const uint64_t p1 = k < lmax ? dpos - 1 - k : dpos - k;
+        const uint64_t p2 = k < lmax ? spos - 1 - k : spos - k;
+        if (right - p1 > uint64_t(RM_MIN)) {
+            if (word_unaligned(dest, dpos, 32) != word_unaligned(ix.ref, spos, 32)) continue;
+            if (word_unaligned(dest, dpos + 32, 4) == word_unaligned(ix.ref, spos + 32, 4)) {
+                hit->src = p2 + 1;
+                hit->len = right - p1 - 1;
+                hit->dst = p1 + 1;
+                return true;
+            }
+        }
+    }
+    return false;
+}
+
+__global__ void probe_segments_kernel(RmIndex ix, const uint64_t* __restrict__ dest, uint64_t dl, uint64_t dpad,
+                                      uint64_t dic, uint64_t segs, bool dest_is_ref, uint8_t* __restrict__ flag,
+                                      Hit* __restrict__ hits) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < segs; i += uint64_t(gridDim.x) * blockDim.x) {
+        uint8_t f = 0;
+        for (uint64_t s = 0; s < 4; ++s) {
+            Hit h;
+            if (probe_packed(ix, dest, dl, dpad, (i * 4 + s) * RM_DEST_STEP, dest_is_ref, &h)) {
+                hits[i] = h;
+                f = 1;
+                break;
+            }
+        }
+        flag[i] = f;
+        (void)dic;
+    }
+}
+
+__global__ void probe_ascii_kernel(RmIndex ix, const uint8_t* __restrict__ dest, uint64_t dl, uint64_t dic,
+                                   uint8_t* __restrict__ flag, Hit* __restrict__ hits) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < dic; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t dpos = i * RM_DEST_STEP;
+        const uint32_t h = marush_ascii(dest + dpos) & ix.mask;
+        const uint32_t b = ix.kr[h], e = ix.kr[h + 1];
+        uint8_t f = 0;
+        for (uint32_t j = b; j < e; ++j) {
+            const uint64_t spos = uint64_t(ix.pos[j]) * RM_SRC_STEP;
+            uint64_t p1 = dpos + RM_K - 1, p2 = spos + RM_K - 1;
+            while (++p1 != dl && ++p2 != ix.rl && dest[p1] == uint8_t("ACGT"[code_at(ix.ref, p2)])) {}
+            const uint64_t right = p1;
+            p1 = dpos;
+            p2 = spos;
+            while (p1 != 0 && p2 != 0 && dest[--p1] == uint8_t("ACGT"[code_at(ix.ref, --p2)])) {}
+            if (right - p1 > uint64_t(RM_MIN)) {
+                int cl = RM_K;
+                uint64_t dc = dpos, sc = spos;
+                while (cl && dest[dc++] == uint8_t("ACGT"[code_at(ix.ref, sc++)])) --cl;
+                if (cl == 0) {
+                    hits[i] = Hit{p2 + 1, right - p1 - 1, p1 + 1};
+                    f = 1;
+                    break;
+                }
+            }
+        }
+        flag[i] = f;
+    }
+}
+
+__global__ void gather_hits_kernel(const Hit* __restrict__ in, const uint32_t* __restrict__ sel, uint32_t c,
+                                   uint64_t dl, bool dest_is_ref, Hit* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c) return;
+    Hit h = in[sel[t]];
+    h.dst = dl - (h.dst + h.len);  // back to forward coordinates (compress.cu:903-908)
+    if (dest_is_ref) {             // compress.cu:910-927
+        if (h.src > h.dst) {
+            const uint64_t x = h.src;
+            h.src = h.dst;
+            h.dst = x;
+        }
+        const uint64_t end = h.src + h.len;
+        if (end > h.dst) {
+            const uint64_t margin = (end - h.dst + 1) / 2;
+            h.len -= margin;
+            h.dst += margin;
+        }
+    }
+    out[t] = h;
+}
+
+__global__ void hit_key_kernel(const Hit* __restrict__ h, const uint32_t* __restrict__ idx, uint32_t c, int field,
+                               uint64_t* __restrict__ key) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c) return;
+    const Hit x = h[idx[t]];
+    key[t] = field == 0 ? x.len : (field == 1 ? x.src : x.dst);
+}
+
+__global__ void hit_unique_kernel(const Hit* __restrict__ h, const uint32_t* __restrict__ idx, uint32_t c,
+                                  uint8_t* __restrict__ keep, Hit* __restrict__ sorted) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c) return;
+    const Hit x = h[idx[t]];
+    sorted[t] = x;
+    bool k = true;
+    if (t > 0) {
+        const Hit y = h[idx[t - 1]];
+        k = !(x.src == y.src && x.len == y.len && x.dst == y.dst);
+    }
+    keep[t] = k;
+}
+
+__global__ void compact_hits_kernel(const Hit* __restrict__ in, const uint32_t* __restrict__ sel, uint32_t c,
+                                    Hit* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < c) out[t] = in[sel[t]];
+}
+
+__device__ __forceinline__ void put_frugal(uint8_t* out, uint64_t& n, uint64_t v) {
+    while (v >= 128) {
+        out[n++] = uint8_t(128 + (v % 128));
+        v /= 128;
+    }
+    out[n++] = uint8_t(v);
+}
+
+// compress.cu:946-992: the acceptance walk over the sorted distinct hits
+// (each kept span starts at or after the end of the previous one).  Writes
+// the kept spans, removed[k] = sum over spans j < k of (len_j - 1), the
+// MapOff / MapLen bytes, and info = {kept, MapOff bytes, MapLen bytes,
+// compacted length}.
+__global__ void accept_kernel(const Hit* __restrict__ h, uint32_t c, uint64_t dl, bool std32,
+                              uint64_t* __restrict__ span_dst, uint64_t* __restrict__ span_end,
+                              uint64_t* __restrict__ removed, uint8_t* __restrict__ map_off,
+                              uint8_t* __restrict__ map_len, uint64_t* __restrict__ info) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint64_t pos = 0, kept = 0, no = 0, nl = 0, rem = 0;
+    put_frugal(map_len, nl, RM_MIN);
+    removed[0] = 0;
+    for (uint32_t i = 0; i < c; ++i) {
+        Hit x = h[i];
+        if (x.dst < pos) {
+            const uint64_t ov = pos - x.dst;
+            if (ov >= x.len) continue;
+            x.len -= ov;
+            x.dst += ov;
+        }
+        if (x.len < uint64_t(RM_MIN)) continue;
+        span_dst[kept] = x.dst;
+        span_end[kept] = x.dst + x.len;
+        if (std32) {
+            const uint32_t v = uint32_t(x.src);
+            for (int t = 0; t < 4; ++t) map_off[no++] = uint8_t(v >> (8 * t));
+        } else {
+            for (int t = 0; t < 8; ++t) map_off[no++] = uint8_t(x.src >> (8 * t));
+        }
+        put_frugal(map_len, nl, x.len - RM_MIN);
+        rem += x.len - 1;
+        ++kept;
+        removed[kept] = rem;
+        pos = x.dst + x.len;
+    }
+    info[0] = kept;
+    info[1] = no;
+    info[2] = nl;
+    info[3] = dl - rem;
+}
+
+// Each kept span [sd_k, se_k) becomes one '%'; every other symbol moves left
+// by the symbols removed before it.
+__global__ void compact_string_kernel(const uint8_t* __restrict__ in, uint64_t dl, const uint64_t* __restrict__ sd,
+                                      const uint64_t* __restrict__ se, const uint64_t* __restrict__ removed,
+                                      uint64_t kept, uint8_t* __restrict__ out) {
+    for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < dl; q += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t lo = 0, cnt = kept;  // lo = number of spans starting at or before q
+        while (cnt > 0) {
+            const uint64_t step = cnt / 2, it = lo + step;
+            if (sd[it] <= q) {
+                lo = it + 1;
+                cnt -= step + 1;
+            } else {
+                cnt = step;
+            }
+        }
+        if (lo > 0 && q < se[lo - 1]) {
+            if (q == sd[lo - 1]) out[q - removed[lo - 1]] = '%';
+            continue;
+        }
+        out[q - removed[lo]] = in[q];
+    }
+}
+
+__global__ void rm_bucket_caps_kernel(const uint32_t* __restrict__ hv, uint64_t count, uint32_t* __restrict__ cnt) {
+    for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < count; j += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t h = hv[j];
+        if (j > 0 && hv[j - 1] == h) continue;
+        uint32_t c = 1;
+        while (c < 12 && j + c < count && hv[j + c] == h) ++c;
+        cnt[h] = c;
+    }
+}
+
+__global__ void rm_bucket_fill_kernel(const uint32_t* __restrict__ hv, const uint32_t* __restrict__ idx,
+                                      uint64_t count, const uint32_t* __restrict__ kr, uint32_t* __restrict__ pos) {
+    for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < count; j += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t h = hv[j];
+        uint32_t rank = 0;
+        while (rank < 12 && rank < j && hv[j - 1 - rank] == h) ++rank;
+        const uint32_t b = kr[h], c = kr[h + 1] - b;
+        if (rank < c) pos[b + c - 1 - rank] = idx[j];
+    }
+}
+
+inline int log2_ceil(uint32_t x) {
+    int b = 0;
+    while ((1u << b) < x) ++b;
+    return b;
+}
+
+struct RmResult {
+    std::vector<uint8_t> seq, map_off, map_len;
+};
+
+// One destination (compress.cu:856-993).  `dest` is the ASCII string on the
+// device (forward strand).
+void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_n, bool dest_is_ref, RmResult& r,
+                  Arena& a, cudaStream_t s) {
+    r.map_off.clear();
+    r.map_len.clear();
+    r.seq.resize(dl);
+    if (dl) CURC_CHECK(cudaMemcpyAsync(r.seq.data(), dest, dl, cudaMemcpyDeviceToHost, s));
+    const uint64_t dic = dl >= uint64_t(RM_K) ? (dl - RM_K + 1 + RM_DEST_STEP - 1) / RM_DEST_STEP : 0;
+    const uint64_t cap = uint64_t(double(dic) * (dest_is_ref ? 0.2 : 0.21));
+    if (dic == 0 || ix.rl < uint64_t(RM_K)) {
+        CURC_CHECK(cudaStreamSynchronize(s));
+        return;
+    }
+    auto mk = a.mark();
+    uint8_t* rc = a.alloc<uint8_t>(dl + 64);
+    rc_ascii_kernel<<<grid_for(dl, 256, 8), 256, 0, s>>>(dest, dl, rc);
+    CURC_LAUNCH_CHECK();
+    const uint64_t nslots = has_n ? dic : div_up(dic, 4);
+    uint8_t* flag = a.alloc<uint8_t>(nslots);
+    Hit* hits = a.alloc<Hit>(nslots);
+    if (!has_n) {
+        const uint64_t words = (dl + 31) / 32 + 8;
+        uint64_t* packed = a.alloc<uint64_t>(words);
+        CURC_CHECK(cudaMemsetAsync(packed, 0, words * 8, s));
+        pack_ascii_ref(rc, dl, packed, s);
+        const uint64_t dpad = (words - 1) * 32;
+        probe_segments_kernel<<<grid_for(nslots, 128), 128, 0, s>>>(ix, packed, dl, dpad, dic, nslots, dest_is_ref,
+                                                                    flag, hits);
+    } else {
+        CURC_CHECK(cudaMemsetAsync(rc + dl, 0, 64, s));
+        probe_ascii_kernel<<<grid_for(nslots, 128), 128, 0, s>>>(ix, rc, dl, dic, flag, hits);
+    }
+    CURC_LAUNCH_CHECK();
+    uint32_t* cnt = a.alloc<uint32_t>(4);
+    uint32_t* sel = a.alloc<uint32_t>(nslots);
+    select_indices(flag, sel, nslots, cnt, a, s);
+    uint32_t c = read_scalar(cnt, s);
+    if (c > cap) c = uint32_t(cap);  // capacity: the first hits in probe order
+    if (c == 0) {
+        a.release(mk);
+        CURC_CHECK(cudaStreamSynchronize(s));
+        return;
+    }
+    Hit* hv = a.alloc<Hit>(c);
+    gather_hits_kernel<<<grid_for(c, 256), 256, 0, s>>>(hits, sel, c, dl, dest_is_ref, hv);
+    CURC_LAUNCH_CHECK();
+    // sort by (dst, src, len): three stable passes, least significant first
+    uint32_t* idx = a.alloc<uint32_t>(c);
+    uint64_t* key = a.alloc<uint64_t>(c);
+    iota(idx, c, s);
+    for (int field = 0; field < 3; ++field) {
+        hit_key_kernel<<<grid_for(c, 256), 256, 0, s>>>(hv, idx, c, field, key);
+        CURC_LAUNCH_CHECK();
+        radix_sort_pairs<uint64_t, uint32_t>(key, idx, c, 0, 64, a, s);
+    }
+    uint8_t* keepf = a.alloc<uint8_t>(c);
+    Hit* sorted = a.alloc<Hit>(c);
+    hit_unique_kernel<<<grid_for(c, 256), 256, 0, s>>>(hv, idx, c, keepf, sorted);
+    CURC_LAUNCH_CHECK();
+    uint32_t* sel2 = a.alloc<uint32_t>(c);
+    select_indices(keepf, sel2, c, cnt + 1, a, s);
+    const uint32_t cu = read_scalar(cnt + 1, s);
+    Hit* uniq = a.alloc<Hit>(cu);
+    compact_hits_kernel<<<grid_for(cu, 256), 256, 0, s>>>(sorted, sel2, cu, uniq);
+    CURC_LAUNCH_CHECK();
+    uint64_t* sd = a.alloc<uint64_t>(cu + 1);
+    uint64_t* se = a.alloc<uint64_t>(cu + 1);
+    uint64_t* removed = a.alloc<uint64_t>(cu + 2);
+    uint8_t* moff = a.alloc<uint8_t>(uint64_t(cu) * 8 + 8);
+    uint8_t* mlen = a.alloc<uint8_t>(uint64_t(cu) * 10 + 16);
+    uint64_t* info = a.alloc<uint64_t>(4);
+    const bool std32 = ix.rl <= 0xFFFFFFFFull;
+    accept_kernel<<<1, 32, 0, s>>>(uniq, cu, dl, std32, sd, se, removed, moff, mlen, info);
+    CURC_LAUNCH_CHECK();
+    uint64_t hi[4];
+    CURC_CHECK(cudaMemcpyAsync(hi, info, 32, cudaMemcpyDeviceToHost, s));
+    CURC_CHECK(cudaStreamSynchronize(s));
+    r.map_off.resize(hi[1]);
+    r.map_len.resize(hi[2]);
+    if (hi[1]) CURC_CHECK(cudaMemcpyAsync(r.map_off.data(), moff, hi[1], cudaMemcpyDeviceToHost, s));
+    if (hi[2]) CURC_CHECK(cudaMemcpyAsync(r.map_len.data(), mlen, hi[2], cudaMemcpyDeviceToHost, s));
+    uint8_t* out = a.alloc<uint8_t>(hi[3] + 1);
+    compact_string_kernel<<<grid_for(dl, 256, 8), 256, 0, s>>>(dest, dl, sd, se, removed, hi[0], out);
+    CURC_LAUNCH_CHECK();
+    r.seq.resize(hi[3]);
+    if (hi[3]) CURC_CHECK(cudaMemcpyAsync(r.seq.data(), out, hi[3], cudaMemcpyDeviceToHost, s));
+    CURC_CHECK(cudaStreamSynchronize(s));
+    a.release(mk);
+}
+
+}  // namespace
+
+void Block::refmatch_all() {
+    // compress.cu:2053-2069: index on the main pseudogenome, applied to the
+    // unmapped, the unmapped-N and then the main pseudogenome itself.
+    cudaStream_t s = stream;
+    RmResult main_r, un_r, unn_r;
+    auto mk = arena.mark();
+    RmIndex ix{hq.packed, hq.len, 0, nullptr, nullptr};
+    const bool usable = hq.len >= uint64_t(RM_K);
+    if (usable) {
+        const uint64_t count = (hq.len - RM_K + 1 + RM_SRC_STEP - 1) / RM_SRC_STEP;
+        if (count > (1ull << 30)) throw std::runtime_error("RefMatcher: pseudogenome above the 2^30-entry index");
+        const uint32_t hs = hash_size_for(count);
+        ix.mask = hs - 1;
+        uint32_t* hv = arena.alloc<uint32_t>(count);
+        uint32_t* idx = arena.alloc<uint32_t>(count);
+        rm_hash_kernel<<<grid_for(count, 256, 4), 256, 0, s>>>(hq.packed, count, ix.mask, hv, idx);
+        CURC_LAUNCH_CHECK();
+        radix_sort_pairs<uint32_t, uint32_t>(hv, idx, count, 0, log2_ceil(hs), arena, s);
+        uint32_t* kr = arena.alloc<uint32_t>(size_t(hs) + 2);
+        CURC_CHECK(cudaMemsetAsync(kr, 0, (size_t(hs) + 2) * 4, s));
+        rm_bucket_caps_kernel<<<grid_for(count, 256, 4), 256, 0, s>>>(hv, count, kr);
+        CURC_LAUNCH_CHECK();
+        exclusive_scan<uint32_t>(kr, kr, size_t(hs) + 2, nullptr, arena, s);
+        uint32_t* pos = arena.alloc<uint32_t>(std::min<uint64_t>(count, uint64_t(hs) * 12) + 2);
+        rm_bucket_fill_kernel<<<grid_for(count, 256, 4), 256, 0, s>>>(hv, idx, count, kr, pos);
+        CURC_LAUNCH_CHECK();
+        ix.kr = kr;
+        ix.pos = pos;
+    }
+    if (usable) {
+        if (lq.len) refmatch_one(ix, lq.seq, lq.len, false, false, un_r, arena, s);
+        if (lqn.len) refmatch_one(ix, lqn.seq, lqn.len, true, false, unn_r, arena, s);
+        refmatch_one(ix, hq.seq, hq.len, false, true, main_r, arena, s);
+    } else {
+        // no index: every pseudogenome is kept as assembled
+        RmIndex none{hq.packed, 0, 0, nullptr, nullptr};
+        refmatch_one(none, lq.seq, lq.len, false, false, un_r, arena, s);
+        refmatch_one(none, lqn.seq, lqn.len, true, false, unn_r, arena, s);
+        refmatch_one(none, hq.seq, hq.len, false, true, main_r, arena, s);
+    }
+    arena.release(mk);
+    host["ref"] = std::move(main_r.seq);
+    host["unmap_ref"] = std::move(un_r.seq);
+    host["unmap_n_ref"] = std::move(unn_r.seq);
+    host["ref_off"] = std::move(main_r.map_off);
+    host["ref_len_map"] = std::move(main_r.map_len);
+    host["unmap_ref_off"] = std::move(un_r.map_off);
+    host["unmap_ref_len"] = std::move(un_r.map_len);
+    host["unmap_n_ref_off"] = std::move(unn_r.map_off);
+    host["unmap_n_ref_len"] = std::move(unn_r.map_len);
+    const uint64_t sizes[6] = {hq.len, lq.len, lqn.len, host["ref"].size(), host["unmap_ref"].size(),
+                               host["unmap_n_ref"].size()};
+    auto& v = host["sizes"];
+    v.resize(sizeof(sizes));
+    std::memcpy(v.data(), sizes, sizeof(sizes));
+}
+
+}  // namespace curc

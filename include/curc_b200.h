@@ -1,0 +1,81 @@
+/* C-ABI of the B200 pseudogenome path of CURC.
+ *
+ * Plain pointers and sizes only.  Every function returns 0 on success and a
+ * negative code on failure; curc_last_error() gives the message.  A context
+ * owns one CUDA stream and a device arena on one GPU; it is not thread safe
+ * (use one context per thread).  Device pointers passed in must be on the
+ * context's device; `stream` arguments are cudaStream_t values (NULL = the
+ * context's own stream).
+ *
+ * The reference has no library boundary: its seam is two C++ functions,
+ *   encode(char* buffer, const Param&, size_t n, size_t start, uint64_t* reads_db_host, size_t W)
+ *       src/compress.cuh:56, src/compress.cu:2151-2180
+ *   block_compress(uint64_t* reads_db_host, vector<uint32_t> reads_id, vector<char> N_reads_db_host,
+ *                  vector<uint32_t> N_reads_id, const Param&, uint8_t block_id, int device_count)
+ *       src/compress.cuh:48, src/compress.cu:1349-2148
+ * and the `curc -c` command line (src/main.cpp:53-161).  The entry points
+ * below replace those, one for one where noted.
+ */
+#ifndef CURC_B200_H
+#define CURC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct curc_ctx curc_ctx;
+
+#define CURC_OK 0
+#define CURC_ERR_ARG (-1)
+#define CURC_ERR_CUDA (-2)
+#define CURC_ERR_STATE (-3)
+#define CURC_ERR_IO (-4)
+
+/* Creates a context on `device` (get_device_count_and_init,
+ * src/compress.cu:2183-2195, per device). */
+int curc_ctx_create(int device, curc_ctx** out);
+void curc_ctx_destroy(curc_ctx* ctx);
+/* Last error message of the context (or of creation when ctx is NULL). */
+const char* curc_last_error(const curc_ctx* ctx);
+
+/* 2-bit packing of n reads of length L held as n*L ASCII bytes on the
+ * device; writes n*ceil(L/32) packed words and one N flag per read (1 when
+ * the read contains 'N').  Replaces encode(), src/compress.cu:2151-2180,
+ * plus the N test of src/preprocess.cpp:149-152. */
+int curc_pack_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, uint64_t* packed_dev,
+                     uint8_t* has_n_dev, void* stream);
+
+/* Compresses one block.  `seqs` holds n reads of length read_len as ASCII
+ * (host memory), in block order (paired end: mates interleaved, as
+ * src/preprocess.cpp:147-193 numbers them).  Runs the whole device path
+ * (pack, sort/dedupe, k-mer index, overlap linking, chain filter, full
+ * match, assembly, mapping, stream emission, unmapped pseudogenomes,
+ * reverse-complement repeat removal) and keeps every stream in the context
+ * until the next call.  Replaces block_compress(), src/compress.cu:1349-2148
+ * up to (not including) the entropy coders. */
+int curc_block_run(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read_len, int preserve_order,
+                   int paired_end);
+
+/* Same with the reads already on the device (n*read_len bytes). */
+int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
+                          int paired_end);
+
+/* Host view of a named result of the last block run ("strand", "mis_cnt",
+ * "mis_base", "read_off", "ref", ... and the stage intermediates
+ * "sorted_ids", "next", "prev", "offset", "hq_seq", ...).  The pointer stays
+ * valid until the next run or destroy.  Returns CURC_ERR_ARG for an unknown
+ * name. */
+int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* bytes);
+
+/* Milliseconds of device time of the last block run, by stage
+ * (CUDA events on the context's stream); names as curc_block_get. */
+int curc_block_stage_ms(curc_ctx* ctx, const char* stage, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -140,6 +140,7 @@ struct BlockStreams {
     std::vector<uint32_t> ref_ids, unmatch_ids;
     Pseudogenome hq;
     MapResult map;
+    std::vector<Record> records;             // emission order
 };
 
 void compress_block(const Params& p, const BlockInput& in, BlockStreams& out, int threads = 1);

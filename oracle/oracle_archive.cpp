@@ -283,6 +283,9 @@ std::string encode_block(const Params& p, const BlockStreams& s, const std::stri
     return o.str();
 }
 
+std::string read_file_pub(const std::string& path) { return read_file(path); }
+void write_file_pub(const std::string& path, const void* data, size_t n) { write_file(path, data, n); }
+
 // ---------------------------------------------------------------- ingest
 
 struct RawBlock {
@@ -395,6 +398,7 @@ struct Handle {
     std::vector<uint8_t> has_n;
     oracle::BlockStreams s;
     std::vector<uint8_t> hq_rec;  // packed Record view: u32 id, u8 n, u8 strand, u16 0, u64 pos
+    std::vector<uint8_t> all_rec;
     std::map<std::string, std::string> extra;
 };
 
@@ -419,14 +423,18 @@ void* oracle_block_new(const char* seqs, uint64_t n, int L, int po, int pe, int 
     h->has_n.assign(n, 0);
     for (uint32_t id : in.n_ids) h->has_n[id] = 1;
     oracle::compress_block(h->p, in, h->s, threads);
-    for (const auto& r : h->s.hq.records) {
-        uint8_t b[16] = {0};
-        std::memcpy(b, &r.read_id, 4);
-        b[4] = r.is_n;
-        b[5] = r.strand;
-        std::memcpy(b + 8, &r.pos, 8);
-        h->hq_rec.insert(h->hq_rec.end(), b, b + 16);
-    }
+    auto flat = [](const std::vector<oracle::Record>& rs, std::vector<uint8_t>& outv) {
+        for (const auto& r : rs) {
+            uint8_t b[16] = {0};
+            std::memcpy(b, &r.read_id, 4);
+            b[4] = r.is_n;
+            b[5] = r.strand;
+            std::memcpy(b + 8, &r.pos, 8);
+            outv.insert(outv.end(), b, b + 16);
+        }
+    };
+    flat(h->s.hq.records, h->hq_rec);
+    flat(h->s.records, h->all_rec);
     return h;
 }
 
@@ -444,6 +452,7 @@ int oracle_block_get(void* hv, const char* name, const void** ptr, uint64_t* byt
     else if (n == "unmatch_ids") view(s.unmatch_ids, ptr, bytes);
     else if (n == "hq_seq") view(s.hq.seq, ptr, bytes);
     else if (n == "hq_records") view(h->hq_rec, ptr, bytes);
+    else if (n == "records") view(h->all_rec, ptr, bytes);
     else if (n == "map_mm") view(s.map.mm, ptr, bytes);
     else if (n == "map_strand") view(s.map.strand, ptr, bytes);
     else if (n == "map_pos") view(s.map.pos, ptr, bytes);
@@ -524,5 +533,68 @@ int oracle_compress_files(const char* f1, const char* f2, const char* working_di
         std::fprintf(stderr, "oracle: %s\n", e.what());
         return 1;
     }
+}
+}
+
+namespace lzma2 {
+void lzma2_decompress(const char* infile, const char* outfile);
+}
+
+extern "C" {
+
+// Decodes one writeCompressed payload (LzmaLib.cpp:539-552 container).
+uint64_t oracle_read_compressed(const char* buf, uint64_t n, char** out) {
+    std::istringstream in(std::string(buf, n));
+    std::string dest;
+    readCompressed(in, dest);
+    *out = static_cast<char*>(std::malloc(dest.size() ? dest.size() : 1));
+    std::memcpy(*out, dest.data(), dest.size());
+    return dest.size();
+}
+
+// Decodes the ref.lzma2 payload: fast-lzma2, then the VarLenDNA coder, into
+// the joined pseudogenome of `total` symbols.
+uint64_t oracle_decode_ref(const char* buf, uint64_t n, uint64_t total, const char* tmpdir, char** out) {
+    std::string in = std::string(tmpdir) + "/ref_in.lzma2", mid = std::string(tmpdir) + "/ref_mid.bin";
+    oracle::write_file_pub(in, buf, n);
+    lzma2::lzma2_decompress(in.c_str(), mid.c_str());
+    std::string enc = oracle::read_file_pub(mid);
+    unlink(in.c_str());
+    unlink(mid.c_str());
+    *out = static_cast<char*>(std::malloc(total ? total : 1));
+    Uncompress(*out, total, enc.data(), enc.size(), VARLEN_DNA_CODER);
+    return total;
+}
+
+// Decodes a mismatch-offset stream of mismatch count m (util.cuh:307-343)
+// holding `records` records; writes uint16 values.
+uint64_t oracle_decode_offsets(const char* buf, uint64_t n, int read_len, int m, uint64_t records, uint16_t* out) {
+    std::vector<char> copy(buf, buf + n);
+    copy.resize(n + 64, 0);
+    auto run = [&](auto tag) {
+        constexpr size_t MaxL = decltype(tag)::value;
+        RangeCoder rc{};
+        rc.input(copy.data());
+        rc.StartDecode();
+        SIMPLE_MODEL<2> flag;
+        SIMPLE_MODEL<MaxL / 2 + 1> first;
+        SIMPLE_MODEL<MaxL> value;
+        uint64_t k = 0;
+        for (uint64_t r = 0; r < records; ++r) {
+            out[k++] = flag.decodeSymbol(&rc);
+            out[k++] = first.decodeSymbol(&rc);
+            if (m > 1) {
+                out[k++] = value.decodeSymbol(&rc);
+                if (m > 2)
+                    for (int t = 1; t < m; ++t) out[k++] = value.decodeSymbol(&rc);
+            }
+        }
+        rc.FinishDecode();
+        return k;
+    };
+    if (read_len <= 128) return run(std::integral_constant<size_t, 128>{});
+    if (read_len <= 256) return run(std::integral_constant<size_t, 256>{});
+    if (read_len <= 384) return run(std::integral_constant<size_t, 384>{});
+    return run(std::integral_constant<size_t, 512>{});
 }
 }

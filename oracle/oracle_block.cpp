@@ -183,6 +183,7 @@ void compress_block(const Params& p, const BlockInput& in, BlockStreams& out, in
         encode_offsets(mo, L, out.mis_off[mis[i]]);
     }
     out.mis_cnt = mis;
+    out.records = rec;
     // context recode (compress.cu:1889-1929): per context, destination bases
     // ranked by descending frequency, ties in listed order (insertion sort)
     {

@@ -82,3 +82,16 @@ $(OUT)/bsc: $(BSC_OBJ)
 	$(CXX) -o $@ $^ -lgomp -lpthread
 
 .PHONY: all
+
+# Golden-archive variant: same objects linked against the shared CUDA
+# runtime, plus the zero-filling cudaMalloc shim (ref_zero_alloc.c).
+golden: $(OUT)/curc_shared $(OUT)/libzero_alloc.so
+
+$(OUT)/curc_shared: $(CURC_OBJ) $(LZMA_OBJ) $(OUT)/libfast-lzma2.a
+	$(NVCC) $(ARCH) -cudart shared -o $@ $(CURC_OBJ) $(LZMA_OBJ) $(OUT)/libfast-lzma2.a -lgomp -lstdc++fs -lpthread
+
+$(OUT)/libzero_alloc.so: oracle/ref_zero_alloc.c
+	$(CC) -O2 -shared -fPIC -o $@ $< -L$(CUDA_HOME)/lib64 -lcudart -ldl
+
+CUDA_HOME ?= /usr/local/cuda
+.PHONY: golden

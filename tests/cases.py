@@ -1,0 +1,35 @@
+"""Seeded synthetic parity cases (small enough for the CPU oracle)."""
+import numpy as np
+
+from curc_b200 import synth
+
+
+def se(seed, n, L, glen, err=0.001, n_rate=0.0001):
+    w = synth.small_single(seed=seed, n_reads=n, read_len=L, genome_len=glen, err=err, n_rate=n_rate)
+    return w.sequences(), False, False
+
+
+def pe(seed, pairs, L, glen, po):
+    w = synth.paired_repeats(seed=seed, pairs=pairs, read_len=L, genome_len=glen, preserve_order=po)
+    return w.sequences(), po, True
+
+
+def duplicates(seed=7, n=3000, L=100):
+    """Many exact duplicates and periodic reads (self overlaps, cycles)."""
+    rng = np.random.default_rng(seed)
+    base = synth.ACGT[rng.integers(0, 4, size=(n // 10, L))]
+    reads = base[rng.integers(0, len(base), size=n)]
+    period = np.tile(synth.ACGT[rng.integers(0, 4, size=7)], L // 7 + 1)[:L]
+    reads[: n // 20] = period
+    return reads.copy(), False, False
+
+
+CASES = {
+    "se100_20k": lambda: se(11, 20_000, 100, 200_000),
+    "se75_20k": lambda: se(12, 20_000, 75, 150_000, err=0.003),
+    "se150_hiN": lambda: se(13, 10_000, 150, 100_000, err=0.004, n_rate=0.002),
+    "se250_8k": lambda: se(14, 8_000, 250, 300_000, err=0.002),
+    "pe150_po": lambda: pe(15, 8_000, 150, 400_000, True),
+    "pe150": lambda: pe(16, 8_000, 150, 400_000, False),
+    "dups": lambda: duplicates(),
+}
