@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pseudogenome path on the paired-end 150 bp workload.
+
+Workload (seeded synthetic, no public dataset): 10M read pairs x 150 bp
+(3 Gbases) from a 50 Mbp genome at 40% GC, 5% of it covered by 1-5 kbp
+repeat copies at 1% divergence, insert size Normal(400, 50), 0.2%
+substitutions, 0.01% N, --preserve_order, block_ratio 1 (one block).
+
+One step = one block through the whole device path (pack ... repeat removal),
+streams returned to the host.  `value` is Mbases/s with the ASCII reads
+already in HBM; `e2e` is the same through the C-ABI from pinned host memory
+(H2D of the reads and D2H of every stream inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank compresses its own block (independent blocks, no
+collective: weak scaling); the time is the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "Mbases/s on 1 B200, batched vs plain; bits/base learned vs plain; lossless"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=10_000_000)
+    ap.add_argument("--genome", type=int, default=50_000_000)
+    ap.add_argument("--cpu-sample-pairs", type=int, default=100_000)
+    ap.add_argument("--ref-sample-pairs", type=int, default=500_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def hbm_peak():
+    try:
+        return float(json.load(open(PEAKS_PATH))["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def workload(pairs, genome, seed):
+    from curc_b200 import synth
+    return synth.paired_repeats(seed=seed, pairs=pairs, read_len=150, genome_len=genome, preserve_order=True)
+
+
+# Algorithmic HBM bytes of the pack kernel per read: L ASCII bytes in,
+# ceil(L/32) packed words and one N flag out.
+def pack_bytes(n, L):
+    return n * (L + 8 * ((L + 31) // 32) + 1)
+
+
+def run_ours(a, rank, world):
+    import torch
+    from curc_b200 import Context, kernel_launches
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    w = workload(a.pairs, a.genome, seed=1 + 1000 * rank)
+    seqs = w.sequences()
+    n, L = seqs.shape
+    bases = n * L
+    # pinned host copy of the reads (e2e input) and a device copy (value input)
+    host = torch.empty(seqs.size, dtype=torch.uint8, pin_memory=True)
+    host.numpy()[:] = seqs.reshape(-1)
+    dseq = host.to(f"cuda:{dev}")
+    ctx = Context(dev)
+    ctx.keep_intermediates(False)
+
+    def dev_step():
+        ctx.block_run_device(dseq.data_ptr(), n, L, True, True)
+        return ctx.stage_ms("total")
+
+    def e2e_step():
+        ctx.block_run(host.numpy().reshape(n, L), True, True)
+
+    for _ in range(a.warmup):
+        dev_step()
+    stage_names = ["pack", "sort_dedupe", "overlap", "chain_filter", "full_match", "assembly", "mapping", "emit",
+                   "unmapped_refs", "refmatch"]
+    stage_tot = {k: 0.0 for k in stage_names}
+    l0 = kernel_launches()
+    with ClockSampler(dev) as clocks:
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev_ms = 0.0
+        for _ in range(a.steps):
+            dev_ms += dev_step()
+            for k in stage_names:
+                stage_tot[k] += ctx.stage_ms(k)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    launches = (kernel_launches() - l0) // max(1, a.steps)
+    # e2e through the C-ABI from pinned host memory
+    for _ in range(1):
+        e2e_step()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(a.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t1) / a.steps
+    d2h = sum(ctx.get(k).nbytes for k in ["strand", "mis_cnt", "mis_base", "id_to_pos", "ref", "unmap_ref",
+                                           "unmap_n_ref", "ref_off", "ref_len_map", "unmap_ref_off", "unmap_ref_len",
+                                           "unmap_n_ref_off", "unmap_n_ref_len"])
+    d2h += sum(ctx.get(f"mis_off_{m}").nbytes for m in range(1, L // 5 + 1))
+    step_s = dev_ms / 1000.0 / a.steps
+    if world > 1:
+        t = torch.tensor([step_s, e2e_s], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        step_s, e2e_s = float(t[0]), float(t[1])
+    res = dict(bases=bases, n=n, L=L, step_s=step_s, e2e_s=e2e_s, wall=wall, launches=launches,
+               stage_ms={k: v / a.steps for k, v in stage_tot.items()}, clocks=clocks.summary(),
+               h2d=int(seqs.size), d2h=int(d2h))
+    ctx.close()
+    return res
+
+
+def cpu_baseline(a):
+    """The CPU oracle (sequential restatement, OpenMP in the mapping loop) on
+    a bounded sample of the same workload."""
+    from tests.oracle_lib import OracleBlock
+    w = workload(a.cpu_sample_pairs, a.genome, seed=1)
+    seqs = w.sequences()
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    OracleBlock(seqs, True, True, threads=threads)
+    dt = time.perf_counter() - t
+    return {"value": seqs.size / dt / 1e6, "unit": "Mbases/s", "cores": threads, "kind": "port",
+            "sample": f"{a.cpu_sample_pairs} pairs x 150 bp of the same generator ({seqs.size / 1e6:.0f} Mbases), "
+                      f"block streams without the entropy coders, {dt:.1f} s"}
+
+
+def run_reference(a):
+    """The reference `curc -c` (built from its sources, oracle/_ref) end to
+    end on a bounded sample of the workload, on this box."""
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    exe = os.path.join(ref_dir, "curc_shared")
+    if not os.path.exists(exe):
+        return None, "reference build missing (oracle/_ref/curc_shared)"
+    w = workload(a.ref_sample_pairs, a.genome, seed=1)
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        files = w.write(os.path.join(td, "in"))
+        env = dict(os.environ, LD_PRELOAD=os.path.join(ref_dir, "libzero_alloc.so"))
+        for i in range(a.warmup + a.steps):
+            t = time.perf_counter()
+            r = subprocess.run([exe, "-c", "-i", ",".join(files), "-o", f"out{i}", "--working_dir", td,
+                                "--preserve_order"], cwd=ref_dir, env=env, capture_output=True, text=True,
+                               timeout=900)
+            dt = time.perf_counter() - t
+            if r.returncode != 0:
+                return None, f"reference exited {r.returncode}: {r.stdout[-200:]} {r.stderr[-200:]}"
+            os.remove(os.path.join(td, f"out{i}.curc"))
+            if i >= a.warmup:
+                times.append(dt)
+    mean = sum(times) / len(times)
+    return {"bases": w.bases, "s": mean, "steps": len(times)}, None
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if world > 1:
+        import torch
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    cfg = {"workload": f"paired-end 150 bp, {a.pairs} pairs ({2 * a.pairs * 150 / 1e9:.1f} Gbases) from a "
+                       f"{a.genome / 1e6:.0f} Mbp genome (40% GC, 5% repeats at 1% divergence), insert N(400,50), "
+                       "0.2% substitutions, 0.01% N, --preserve_order, block_ratio 1",
+           "global_batch": a.pairs * 2 * world, "read_len": 150, "parallelism": f"independent blocks x{world}",
+           "l2_flush": "inputs (3 GB ASCII per block) are larger than L2"}
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        ref, why = run_reference(a)
+        if ref is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        v = ref["bases"] / ref["s"] / 1e6
+        out = {"metric": METRIC, "value": v, "unit": "Mbases/s", "n_gpus": 1, "steps": ref["steps"],
+               "warmup": a.warmup, "ms_per_step": ref["s"] * 1000, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
+               "config": dict(cfg, sample=f"{a.ref_sample_pairs} pairs per step"),
+               "cpu_baseline": {"value": v, "unit": "Mbases/s", "cores": os.cpu_count(), "kind": "reference",
+                                "sample": f"reference curc -c end to end (GPU stages + host coders) on "
+                                          f"{a.ref_sample_pairs} pairs of the same generator"},
+               "e2e": {"value": v, "unit": "Mbases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return
+    r = run_ours(a, rank, world)
+    if rank != 0:
+        return
+    peak, peak_kind = hbm_peak()
+    pack_ms = r["stage_ms"]["pack"]
+    dominant = max(r["stage_ms"], key=r["stage_ms"].get)
+    achieved = pack_bytes(r["n"], r["L"]) / (pack_ms / 1000.0) / 1e9 if pack_ms > 0 else None
+    out = {
+        "metric": METRIC,
+        "value": r["bases"] * world / r["step_s"] / 1e6,
+        "unit": "Mbases/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": r["step_s"] * 1000,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": cfg,
+        "e2e": {"value": r["bases"] * world / r["e2e_s"] / 1e6, "unit": "Mbases/s",
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+        "roofline": {"kernel": "pack (stage a1)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                     "traffic": None},
+        "stage_ms": r["stage_ms"],
+        "dominant_stage": dominant,
+        "clocks": r["clocks"],
+        "gpu_launches": r["launches"],
+    }
+    if not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(a)
+    print(json.dumps(out))
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -34,8 +34,15 @@ def lib() -> ctypes.CDLL:
         L.curc_block_run_device.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_int, c_int]
         L.curc_block_get.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(c_p), ctypes.POINTER(c_u64)]
         L.curc_block_stage_ms.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
+        L.curc_ctx_keep_intermediates.argtypes = [c_p, c_int]
+        L.curc_kernel_launches.argtypes = []
+        L.curc_kernel_launches.restype = ctypes.c_uint64
         _lib = L
     return _lib
+
+
+def kernel_launches() -> int:
+    return int(lib().curc_kernel_launches())
 
 
 class CurcError(RuntimeError):
@@ -95,6 +102,9 @@ class Context:
             return np.zeros(0, dtype=dtype)
         buf = (ctypes.c_uint8 * nb.value).from_address(p.value)
         return np.frombuffer(bytes(buf), dtype=dtype)
+
+    def keep_intermediates(self, keep: bool):
+        self._check(lib().curc_ctx_keep_intermediates(self._h, int(keep)), "curc_ctx_keep_intermediates")
 
     def stage_ms(self, stage: str) -> float:
         v = ctypes.c_float()

@@ -44,6 +44,10 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     StageTimer T{stream};
     cudaStream_t s = stream;
     const int W = p.W;
+    cudaEvent_t ev0, ev1;
+    CURC_CHECK(cudaEventCreate(&ev0));
+    CURC_CHECK(cudaEventCreate(&ev1));
+    CURC_CHECK(cudaEventRecord(ev0, s));
     uint32_t* counts = arena.alloc<uint32_t>(16);
     uint32_t* err = arena.alloc<uint32_t>(1);
     CURC_CHECK(cudaMemsetAsync(err, 0, 4, s));
@@ -156,8 +160,14 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     }
 
     emit(T);
+    CURC_CHECK(cudaEventRecord(ev1, s));
     T.collect(stage_ms);
     CURC_CHECK(cudaStreamSynchronize(s));
+    float total = 0;
+    CURC_CHECK(cudaEventElapsedTime(&total, ev0, ev1));
+    stage_ms["total"] = total;
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
 }
 
 }  // namespace curc
@@ -275,6 +285,14 @@ int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* 
     *bytes = it->second.size();
     return CURC_OK;
 }
+
+int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep) {
+    if (!ctx) return CURC_ERR_ARG;
+    ctx->block->keep_intermediates = keep != 0;
+    return CURC_OK;
+}
+
+uint64_t curc_kernel_launches(void) { return curc::launches(); }
 
 int curc_block_stage_ms(curc_ctx* ctx, const char* stage, float* ms) {
     if (!ctx || !stage || !ms) return CURC_ERR_ARG;

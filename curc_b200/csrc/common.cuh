@@ -34,7 +34,14 @@ struct CudaError : std::runtime_error {
         }                                                                                     \
     } while (0)
 
-#define CURC_LAUNCH_CHECK() CURC_CHECK(cudaGetLastError())
+// Every kernel launch of the library goes through this check, which also
+// counts it (curc_kernel_launches).
+void count_launch();
+#define CURC_LAUNCH_CHECK()             \
+    do {                                \
+        ::curc::count_launch();         \
+        CURC_CHECK(cudaGetLastError()); \
+    } while (0)
 
 __host__ __device__ inline uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 

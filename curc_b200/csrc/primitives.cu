@@ -1,9 +1,16 @@
 // Device-wide primitives: arena, scan, stable compaction, stable radix sort.
 #include <algorithm>
+#include <atomic>
 
 #include "primitives.cuh"
 
 namespace curc {
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launches() { return g_launches.load(); }
 
 // ---------------------------------------------------------------- arena
 

@@ -10,6 +10,8 @@
 
 namespace curc {
 
+uint64_t launches();
+
 // Bump allocator over large device chunks.  reset() keeps the chunks, so a
 // pipeline that runs block after block allocates device memory only while
 // it grows.  Alignment 256 bytes (TMA and vector loads need 16).

@@ -70,10 +70,27 @@ def _substitute(rng: np.random.Generator, bases: np.ndarray, ti_tv: float | None
     return ACGT[out]
 
 
+DENSE_LIMIT = 20_000_000  # bases; above it errors are drawn sparsely
+
+
 def _apply_errors(rng, reads: np.ndarray, err, n_rate: float, ti_tv=None) -> None:
     """In place: substitutions with per-position rate ``err`` (scalar or array
-    of read length) and N bases at ``n_rate``."""
+    of read length) and N bases at ``n_rate``.  Small inputs draw one uniform
+    per base; large ones draw the number of events per read position
+    (binomial) and their reads uniformly, which has the same distribution."""
     n, L = reads.shape
+    if reads.size > DENSE_LIMIT:
+        rate = np.broadcast_to(np.asarray(err, dtype=np.float64), (L,))
+        for j in range(L):
+            k = rng.binomial(n, rate[j])
+            if k:
+                rows = rng.choice(n, size=k, replace=False) if k < n // 4 else np.nonzero(rng.random(n) < rate[j])[0]
+                reads[rows, j] = _substitute(rng, reads[rows, j], ti_tv)
+        if n_rate > 0:
+            k = rng.binomial(reads.size, n_rate)
+            flat = rng.integers(0, reads.size, size=k)
+            reads.reshape(-1)[flat] = ord("N")
+        return
     rate = np.broadcast_to(np.asarray(err, dtype=np.float64), (L,))
     m = rng.random((n, L)) < rate[None, :]
     if m.any():
@@ -86,8 +103,7 @@ def _apply_errors(rng, reads: np.ndarray, err, n_rate: float, ti_tv=None) -> Non
 def sample_single(rng, genome: np.ndarray, n: int, L: int, err, n_rate: float,
                   rc_frac: float = 0.5, ti_tv=None) -> np.ndarray:
     starts = rng.integers(0, len(genome) - L + 1, size=n)
-    idx = starts[:, None] + np.arange(L)[None, :]
-    reads = genome[idx]
+    reads = np.lib.stride_tricks.sliding_window_view(genome, L)[starts]
     rc = rng.random(n) < rc_frac
     reads[rc] = revcomp(reads[rc])
     _apply_errors(rng, reads, err, n_rate, ti_tv)
@@ -98,10 +114,9 @@ def sample_paired(rng, genome: np.ndarray, pairs: int, L: int, err, n_rate: floa
                   insert_mean=400.0, insert_sd=50.0, ti_tv=None):
     ins = np.clip(np.rint(rng.normal(insert_mean, insert_sd, size=pairs)), L, None).astype(np.int64)
     starts = rng.integers(0, len(genome) - ins + 1)
-    idx1 = starts[:, None] + np.arange(L)[None, :]
-    idx2 = (starts + ins - L)[:, None] + np.arange(L)[None, :]
-    m1 = genome[idx1]
-    m2 = revcomp(genome[idx2])
+    win = np.lib.stride_tricks.sliding_window_view(genome, L)
+    m1 = win[starts]
+    m2 = revcomp(win[starts + ins - L])
     flip = rng.random(pairs) < 0.5  # fragment from the reverse strand
     t1 = m1[flip].copy()
     m1[flip] = m2[flip]

@@ -63,6 +63,12 @@ int curc_block_run(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read_le
 int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
                           int paired_end);
 
+/* Whether block runs also copy the stage intermediates ("packed",
+ * "sorted_ids", "next", "prev", "offset", "ref_ids", "unmatch_ids", "hq_seq",
+ * "hq_records", "map_*") to the host for parity checks (default 1).  The
+ * streams are always returned.  No reference counterpart. */
+int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep);
+
 /* Host view of a named result of the last block run ("strand", "mis_cnt",
  * "mis_base", "read_off", "ref", ... and the stage intermediates
  * "sorted_ids", "next", "prev", "offset", "hq_seq", ...).  The pointer stays
@@ -70,8 +76,14 @@ int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint1
  * name. */
 int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* bytes);
 
+/* Number of kernels the library has launched in this process (no
+ * reference counterpart; used to report launches per benchmark step). */
+uint64_t curc_kernel_launches(void);
+
 /* Milliseconds of device time of the last block run, by stage
- * (CUDA events on the context's stream); names as curc_block_get. */
+ * (CUDA events on the context's stream): "pack", "sort_dedupe", "overlap",
+ * "chain_filter", "full_match", "assembly", "mapping", "emit",
+ * "unmapped_refs", "refmatch", and "total" (the whole run). */
 int curc_block_stage_ms(curc_ctx* ctx, const char* stage, float* ms);
 
 #ifdef __cplusplus
