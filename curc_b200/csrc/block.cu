@@ -180,8 +180,14 @@ struct curc_ctx {
     std::string err;
 };
 
+namespace curc {
+// Error message of the calls that have no context (creation, no-alloc).
+std::string& ctxless_error() {
+    thread_local std::string e;
+    return e;
+}
+}  // namespace curc
 namespace {
-thread_local std::string g_create_error;
 
 template <class F>
 int guarded(curc_ctx* ctx, F&& f) {
@@ -218,7 +224,7 @@ int curc_ctx_create(int device, curc_ctx** out) {
         *out = c;
         return CURC_OK;
     } catch (const std::exception& e) {
-        g_create_error = e.what();
+        curc::ctxless_error() = e.what();
         return CURC_ERR_CUDA;
     }
 }
@@ -229,7 +235,7 @@ void curc_ctx_destroy(curc_ctx* ctx) {
     delete ctx;
 }
 
-const char* curc_last_error(const curc_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+const char* curc_last_error(const curc_ctx* ctx) { return ctx ? ctx->err.c_str() : curc::ctxless_error().c_str(); }
 
 int curc_pack_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, uint64_t* packed_dev,
                      uint8_t* has_n_dev, void* stream) {

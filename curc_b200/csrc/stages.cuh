@@ -10,6 +10,8 @@
 
 namespace curc {
 
+std::string& ctxless_error();
+
 struct BlockParams {
     int L = 0, W = 0, max_off = 0, k = 0, kip = 0, max_mm = 0;
     bool preserve_order = false, paired_end = false;

@@ -48,6 +48,22 @@ const char* curc_last_error(const curc_ctx* ctx);
 int curc_pack_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, uint64_t* packed_dev,
                      uint8_t* has_n_dev, void* stream);
 
+/* Same packing, plus the N split of src/preprocess.cpp:147-193 (ids of the
+ * reads without N and of those with N, each ascending; counts_dev[0] and
+ * counts_dev[1] receive their numbers), without allocating device memory:
+ * for callers that manage all device memory through their own pool or that
+ * cannot take the device synchronisation a cudaMalloc may cause.  No
+ * counterpart in the reference.  Its scratch is a fixed array of about 512
+ * KB inside the library (held on every GPU that loads it until exit), which
+ * limits a call to 2^27 reads; larger calls return CURC_ERR_ARG.  Calls share
+ * that array, so calls that overlap on the GPU race; stream-ordered calls do
+ * not.  The first call on a device sets up the array's address and should
+ * come before any stream capture.  No context: errors are read with
+ * curc_last_error(NULL). */
+int curc_pack_split_noalloc(int device, const char* seqs_dev, uint64_t n, uint16_t read_len, uint64_t* packed_dev,
+                            uint8_t* has_n_dev, uint32_t* reads_id_dev, uint32_t* n_reads_id_dev,
+                            uint32_t* counts_dev, void* stream);
+
 /* Compresses one block.  `seqs` holds n reads of length read_len as ASCII
  * (host memory), in block order (paired end: mates interleaved, as
  * src/preprocess.cpp:147-193 numbers them).  Runs the whole device path
