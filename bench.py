@@ -178,7 +178,11 @@ def run_ours(a, rank, world):
         t = torch.tensor([step_s, e2e_s], dtype=torch.float64, device=f"cuda:{dev}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         step_s, e2e_s = float(t[0]), float(t[1])
-    res = dict(bases=bases, n=n, L=L, step_s=step_s, e2e_s=e2e_s, wall=wall, launches=launches,
+    stats = dict(zip(["reads", "non_n", "n_reads", "pseudogenome_reads", "unmatched", "mapped", "unmapped",
+                      "unmapped_n", "overlap_passes", "contested", "records", "mismatches"],
+                     [int(x) for x in ctx.get("stats", np.uint64)]))
+    stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
+    res = dict(bases=bases, n=n, L=L, step_s=step_s, e2e_s=e2e_s, wall=wall, launches=launches, stats=stats,
                stage_ms={k: v / a.steps for k, v in stage_tot.items()}, clocks=clocks.summary(),
                h2d=int(seqs.size), d2h=int(d2h))
     ctx.close()
@@ -285,6 +289,7 @@ def main():
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                      "traffic": None},
         "stage_ms": r["stage_ms"],
+        "block_stats": r["stats"],
         "dominant_stage": dominant,
         "clocks": r["clocks"],
         "gpu_launches": r["launches"],

@@ -18,9 +18,10 @@
 // B200 design: one thread per segment (packed) or per probe (ASCII); the
 // extensions compare 32 bases per step with XOR and count-leading-zeros
 // instead of one base per step; the triples are ordered with three stable
-// radix passes; the sequential acceptance walk (each kept span depends on
-// the end of the previous one) runs in one thread over the deduplicated
-// triples, and the string compaction is a parallel copy.
+// radix passes; the acceptance decisions (each depends on the end of the
+// previous kept span) are taken by one thread reading shared-memory tiles,
+// and the map streams and the string compaction are built in parallel from
+// scans over the kept spans.
 #include <cstring>
 
 #include "block.cuh"
@@ -248,54 +249,104 @@ __global__ void compact_hits_kernel(const Hit* __restrict__ in, const uint32_t* 
     if (t < c) out[t] = in[sel[t]];
 }
 
-__device__ __forceinline__ void put_frugal(uint8_t* out, uint64_t& n, uint64_t v) {
-    while (v >= 128) {
-        out[n++] = uint8_t(128 + (v % 128));
-        v /= 128;
+// compress.cu:946-992, the acceptance walk over the sorted distinct hits:
+// a hit starting before the end of the last kept span is trimmed (or
+// dropped when covered); it is kept when 50 or more bases remain.  The walk
+// carries one value (the end of the last kept span) from hit to hit, so one
+// thread decides; the block stages 2048 hits at a time in shared memory so
+// that thread reads only shared memory.  Everything else is parallel.
+constexpr int ACCEPT_CHUNK = 2048;
+
+__global__ void __launch_bounds__(1024) accept_decide_kernel(const Hit* __restrict__ h, uint32_t c,
+                                                             uint8_t* __restrict__ kept, uint64_t* __restrict__ adst,
+                                                             uint64_t* __restrict__ alen) {
+    __shared__ uint64_t sdst[ACCEPT_CHUNK], slen[ACCEPT_CHUNK];
+    __shared__ uint8_t skept[ACCEPT_CHUNK];
+    uint64_t pos = 0;  // meaningful in thread 0 only
+    for (uint32_t base = 0; base < c; base += ACCEPT_CHUNK) {
+        const uint32_t cnt = min(uint32_t(ACCEPT_CHUNK), c - base);
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            sdst[i] = h[base + i].dst;
+            slen[i] = h[base + i].len;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (uint32_t i = 0; i < cnt; ++i) {
+                uint64_t d = sdst[i], l = slen[i];
+                uint8_t k = 0;
+                if (d < pos) {
+                    const uint64_t ov = pos - d;
+                    if (ov >= l) {
+                        l = 0;
+                    } else {
+                        l -= ov;
+                        d += ov;
+                    }
+                }
+                if (l >= uint64_t(RM_MIN)) {
+                    k = 1;
+                    pos = d + l;
+                }
+                sdst[i] = d;
+                slen[i] = l;
+                skept[i] = k;
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            kept[base + i] = skept[i];
+            adst[base + i] = sdst[i];
+            alen[base + i] = slen[i];
+        }
+        __syncthreads();
     }
-    out[n++] = uint8_t(v);
 }
 
-// compress.cu:946-992: the acceptance walk over the sorted distinct hits
-// (each kept span starts at or after the end of the previous one).  Writes
-// the kept spans, removed[k] = sum over spans j < k of (len_j - 1), the
-// MapOff / MapLen bytes, and info = {kept, MapOff bytes, MapLen bytes,
-// compacted length}.
-__global__ void accept_kernel(const Hit* __restrict__ h, uint32_t c, uint64_t dl, bool std32,
-                              uint64_t* __restrict__ span_dst, uint64_t* __restrict__ span_end,
-                              uint64_t* __restrict__ removed, uint8_t* __restrict__ map_off,
-                              uint8_t* __restrict__ map_len, uint64_t* __restrict__ info) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    uint64_t pos = 0, kept = 0, no = 0, nl = 0, rem = 0;
-    put_frugal(map_len, nl, RM_MIN);
-    removed[0] = 0;
-    for (uint32_t i = 0; i < c; ++i) {
-        Hit x = h[i];
-        if (x.dst < pos) {
-            const uint64_t ov = pos - x.dst;
-            if (ov >= x.len) continue;
-            x.len -= ov;
-            x.dst += ov;
-        }
-        if (x.len < uint64_t(RM_MIN)) continue;
-        span_dst[kept] = x.dst;
-        span_end[kept] = x.dst + x.len;
-        if (std32) {
-            const uint32_t v = uint32_t(x.src);
-            for (int t = 0; t < 4; ++t) map_off[no++] = uint8_t(v >> (8 * t));
-        } else {
-            for (int t = 0; t < 8; ++t) map_off[no++] = uint8_t(x.src >> (8 * t));
-        }
-        put_frugal(map_len, nl, x.len - RM_MIN);
-        rem += x.len - 1;
-        ++kept;
-        removed[kept] = rem;
-        pos = x.dst + x.len;
+__device__ __forceinline__ uint32_t frugal_size(uint64_t v) {
+    uint32_t n = 1;
+    while (v >= 128) {
+        v /= 128;
+        ++n;
     }
-    info[0] = kept;
-    info[1] = no;
-    info[2] = nl;
-    info[3] = dl - rem;
+    return n;
+}
+
+// Per kept span k (hit i = sel[k]): span bounds, removed length, MapOff
+// entry, and the size of its MapLen entry.
+__global__ void kept_spans_kernel(const uint32_t* __restrict__ sel, uint32_t K, const Hit* __restrict__ h,
+                                  const uint64_t* __restrict__ adst, const uint64_t* __restrict__ alen, bool std32,
+                                  uint64_t* __restrict__ sd, uint64_t* __restrict__ se, uint64_t* __restrict__ rm,
+                                  uint32_t* __restrict__ lsize, uint8_t* __restrict__ map_off) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    const uint32_t i = sel[k];
+    const uint64_t d = adst[i], l = alen[i];
+    sd[k] = d;
+    se[k] = d + l;
+    rm[k] = l - 1;
+    lsize[k] = frugal_size(l - RM_MIN);
+    const uint64_t src = h[i].src;
+    if (std32) {
+        const uint32_t v = uint32_t(src);
+        for (int t = 0; t < 4; ++t) map_off[uint64_t(k) * 4 + t] = uint8_t(v >> (8 * t));
+    } else {
+        for (int t = 0; t < 8; ++t) map_off[uint64_t(k) * 8 + t] = uint8_t(src >> (8 * t));
+    }
+}
+
+// MapLen: LEB128(50) then LEB128(len - 50) per kept span.
+__global__ void map_len_kernel(const uint32_t* __restrict__ sel, uint32_t K, const uint64_t* __restrict__ alen,
+                               const uint32_t* __restrict__ loff, uint8_t* __restrict__ map_len) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) map_len[0] = uint8_t(RM_MIN);
+    if (k >= K) return;
+    uint64_t v = alen[sel[k]] - RM_MIN;
+    uint64_t o = 1 + uint64_t(loff[k]);
+    while (v >= 128) {
+        map_len[o++] = uint8_t(128 + (v % 128));
+        v /= 128;
+    }
+    map_len[o] = uint8_t(v);
 }
 
 // Each kept span [sd_k, se_k) becomes one '%'; every other symbol moves left
@@ -419,18 +470,36 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
     Hit* uniq = a.alloc<Hit>(cu);
     compact_hits_kernel<<<grid_for(cu, 256), 256, 0, s>>>(sorted, sel2, cu, uniq);
     CURC_LAUNCH_CHECK();
-    uint64_t* sd = a.alloc<uint64_t>(cu + 1);
-    uint64_t* se = a.alloc<uint64_t>(cu + 1);
-    uint64_t* removed = a.alloc<uint64_t>(cu + 2);
-    uint8_t* moff = a.alloc<uint8_t>(uint64_t(cu) * 8 + 8);
-    uint8_t* mlen = a.alloc<uint8_t>(uint64_t(cu) * 10 + 16);
-    uint64_t* info = a.alloc<uint64_t>(4);
-    const bool std32 = ix.rl <= 0xFFFFFFFFull;
-    accept_kernel<<<1, 32, 0, s>>>(uniq, cu, dl, std32, sd, se, removed, moff, mlen, info);
+    uint8_t* keptf = a.alloc<uint8_t>(cu);
+    uint64_t* adst = a.alloc<uint64_t>(cu);
+    uint64_t* alen = a.alloc<uint64_t>(cu);
+    accept_decide_kernel<<<1, 1024, 0, s>>>(uniq, cu, keptf, adst, alen);
     CURC_LAUNCH_CHECK();
-    uint64_t hi[4];
-    CURC_CHECK(cudaMemcpyAsync(hi, info, 32, cudaMemcpyDeviceToHost, s));
+    uint32_t* ksel = a.alloc<uint32_t>(cu);
+    select_indices(keptf, ksel, cu, cnt + 2, a, s);
+    const uint32_t K = read_scalar(cnt + 2, s);
+    const bool std32 = ix.rl <= 0xFFFFFFFFull;
+    uint64_t* sd = a.alloc<uint64_t>(K + 1);
+    uint64_t* se = a.alloc<uint64_t>(K + 1);
+    uint64_t* removed = a.alloc<uint64_t>(K + 2);
+    uint32_t* lsize = a.alloc<uint32_t>(K + 1);
+    uint8_t* moff = a.alloc<uint8_t>(uint64_t(K) * 8 + 8);
+    uint8_t* mlen = a.alloc<uint8_t>(uint64_t(K) * 10 + 16);
+    if (K) {
+        kept_spans_kernel<<<grid_for(K, 256), 256, 0, s>>>(ksel, K, uniq, adst, alen, std32, sd, se, removed, lsize,
+                                                            moff);
+        CURC_LAUNCH_CHECK();
+    }
+    exclusive_scan<uint64_t>(removed, removed, K, removed + K, a, s);
+    exclusive_scan<uint32_t>(lsize, lsize, K, cnt + 3, a, s);
+    map_len_kernel<<<grid_for(K ? K : 1, 256), 256, 0, s>>>(ksel, K, alen, lsize, mlen);
+    CURC_LAUNCH_CHECK();
+    uint64_t total_removed = 0;
+    uint32_t len_bytes = 0;
+    CURC_CHECK(cudaMemcpyAsync(&total_removed, removed + K, 8, cudaMemcpyDeviceToHost, s));
+    CURC_CHECK(cudaMemcpyAsync(&len_bytes, cnt + 3, 4, cudaMemcpyDeviceToHost, s));
     CURC_CHECK(cudaStreamSynchronize(s));
+    uint64_t hi[4] = {K, uint64_t(K) * (std32 ? 4 : 8), 1 + uint64_t(len_bytes), dl - total_removed};
     r.map_off.resize(hi[1]);
     r.map_len.resize(hi[2]);
     if (hi[1]) CURC_CHECK(cudaMemcpyAsync(r.map_off.data(), moff, hi[1], cudaMemcpyDeviceToHost, s));
@@ -501,6 +570,14 @@ void Block::refmatch_all() {
     auto& v = host["sizes"];
     v.resize(sizeof(sizes));
     std::memcpy(v.data(), sizes, sizeof(sizes));
+    // block statistics: reads, non-N reads, N reads, pseudogenome reads,
+    // unmatched, mapped, unmapped (non-N, N), overlap passes, contested
+    // suffixes, records, mismatches
+    const uint64_t stats[12] = {n, m, NN, n_ref, U, n_map, n_ug, n_un, ostats.passes, ostats.contested, n_records,
+                                n_mis};
+    auto& st = host["stats"];
+    st.resize(sizeof(stats));
+    std::memcpy(st.data(), stats, sizeof(stats));
 }
 
 }  // namespace curc

@@ -32,4 +32,8 @@ CASES = {
     "pe150_po": lambda: pe(15, 8_000, 150, 400_000, True),
     "pe150": lambda: pe(16, 8_000, 150, 400_000, False),
     "dups": lambda: duplicates(),
+    # high coverage: long chains and chain cycles in the assembly, many
+    # contested overlap runs
+    "se100_deep": lambda: se(18, 100_000, 100, 250_000, err=0.001),
+    "pe150_po_100k": lambda: pe(17, 100_000, 150, 2_000_000, True),
 }
