@@ -145,7 +145,13 @@ def run_ours(a, rank, world):
         dev_step()
     stage_names = ["pack", "sort_dedupe", "overlap", "chain_filter", "full_match", "assembly", "mapping", "emit",
                    "unmapped_refs", "refmatch"]
+    sub_names = ["sort_dedupe.radix", "overlap.index", "overlap.probe_resolve", "overlap.contested", "overlap.compact",
+                 "full_match.resort", "full_match.groups", "full_match.compact", "assembly.ranking",
+                 "assembly.order_place", "mapping.index_fwd", "mapping.map_fwd", "mapping.index_rc", "mapping.map_rc",
+                 "refmatch.index", "refmatch.probe_unmapped", "refmatch.probe_self", "refmatch.sort_unique",
+                 "refmatch.accept"]
     stage_tot = {k: 0.0 for k in stage_names}
+    sub_tot = {}
     l0 = kernel_launches()
     with ClockSampler(dev) as clocks:
         if world > 1:
@@ -157,6 +163,11 @@ def run_ours(a, rank, world):
             dev_ms += dev_step()
             for k in stage_names:
                 stage_tot[k] += ctx.stage_ms(k)
+            for k in sub_names:
+                try:
+                    sub_tot[k] = sub_tot.get(k, 0.0) + ctx.stage_ms(k)
+                except Exception:
+                    pass
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     launches = (kernel_launches() - l0) // max(1, a.steps)
@@ -183,7 +194,8 @@ def run_ours(a, rank, world):
                      [int(x) for x in ctx.get("stats", np.uint64)]))
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     res = dict(bases=bases, n=n, L=L, step_s=step_s, e2e_s=e2e_s, wall=wall, launches=launches, stats=stats,
-               stage_ms={k: v / a.steps for k, v in stage_tot.items()}, clocks=clocks.summary(),
+               stage_ms={k: v / a.steps for k, v in stage_tot.items()},
+               substage_ms={k: round(v / a.steps, 3) for k, v in sub_tot.items()}, clocks=clocks.summary(),
                h2d=int(seqs.size), d2h=int(d2h))
     ctx.close()
     return res
@@ -289,6 +301,7 @@ def main():
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                      "traffic": None},
         "stage_ms": r["stage_ms"],
+        "substage_ms": r["substage_ms"],
         "block_stats": r["stats"],
         "dominant_stage": dominant,
         "clocks": r["clocks"],

@@ -278,6 +278,7 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
     RankState* B = a.alloc<RankState>(n);
     uint32_t* active = a.alloc<uint32_t>(4);
     uint32_t left = 0;
+    SubStage sp_rank("assembly.ranking");
     RankState* R = run_ranking(n_total, m, pv, offset, pos_in_ids, nullptr, nullptr, A, B, active, &left, s);
     if (left) {
         // cycles: cut each in parallel, then rank its reads again (the other
@@ -305,6 +306,8 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
         R = run_ranking(n_total, m, pv, offset, pos_in_ids, cyc, keep, X, Y, active, &left, s);
         if (left) throw std::runtime_error("assemble: unresolved chain links after cutting cycles");
     }
+    sp_rank.stop();
+    SubStage sp_place("assembly.order_place");
     // chain order: first member in list order
     uint32_t* key = a.alloc<uint32_t>(n);
     fill<uint32_t>(key, INVALID, n, s);

@@ -41,7 +41,12 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     n = uint32_t(n_reads);
     host.clear();
     stage_ms.clear();
-    StageTimer T{stream};
+    pinned.reset();
+    StageTimer T{stream, {}, {}};
+    struct TimerScope {
+        explicit TimerScope(StageTimer* t) { active_timer() = t; }
+        ~TimerScope() { active_timer() = nullptr; }
+    } timer_scope(&T);
     cudaStream_t s = stream;
     const int W = p.W;
     cudaEvent_t ev0, ev1;
@@ -84,7 +89,10 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     fill<uint16_t>(offset, INVALOFF, n, s);
     sorted = arena.alloc<uint32_t>(m ? m : 1);
     if (m) CURC_CHECK(cudaMemcpyAsync(sorted, reads_id, size_t(m) * 4, cudaMemcpyDeviceToDevice, s));
-    sort_ids_by_reads(db, W, L, sorted, m, arena, s);
+    {
+        SubStage sp("sort_dedupe.radix");
+        sort_ids_by_reads(db, W, L, sorted, m, arena, s);
+    }
     dedupe_links(db, W, sorted, m, next, prev, offset, s);
     T.end();
     if (keep_intermediates) keep("sorted_ids", sorted, m);
@@ -174,11 +182,6 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
 
 // ---------------------------------------------------------------- C-ABI
 
-struct curc_ctx {
-    int device = 0;
-    std::unique_ptr<curc::Block> block;
-    std::string err;
-};
 
 namespace curc {
 // Error message of the calls that have no context (creation, no-alloc).
@@ -287,8 +290,8 @@ int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* 
         ctx->err = std::string("unknown result: ") + name;
         return CURC_ERR_ARG;
     }
-    *ptr = it->second.data();
-    *bytes = it->second.size();
+    *ptr = it->second.ptr;
+    *bytes = it->second.size;
     return CURC_OK;
 }
 

@@ -1,6 +1,7 @@
 // Device-resident state of one block and the pipeline driver.
 #pragma once
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -8,29 +9,12 @@
 
 namespace curc {
 
-// CUDA events around each stage on the block's stream.
-struct StageTimer {
-    cudaStream_t s;
-    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
-    void begin(const std::string& name) {
-        cudaEvent_t a, b;
-        CURC_CHECK(cudaEventCreate(&a));
-        CURC_CHECK(cudaEventCreate(&b));
-        CURC_CHECK(cudaEventRecord(a, s));
-        ev.push_back({name, {a, b}});
-    }
-    void end() { CURC_CHECK(cudaEventRecord(ev.back().second.second, s)); }
-    void collect(std::map<std::string, float>& out) {
-        CURC_CHECK(cudaStreamSynchronize(s));
-        for (auto& e : ev) {
-            float ms = 0;
-            CURC_CHECK(cudaEventElapsedTime(&ms, e.second.first, e.second.second));
-            out[e.first] += ms;
-            cudaEventDestroy(e.second.first);
-            cudaEventDestroy(e.second.second);
-        }
-        ev.clear();
-    }
+// A result returned to the host: a view into pinned staging memory (filled
+// by an async copy on the block's stream) or an owned small vector.
+struct HostBuf {
+    const uint8_t* ptr = nullptr;
+    size_t size = 0;
+    std::vector<uint8_t> own;
 };
 
 struct Block {
@@ -60,7 +44,8 @@ struct Block {
     uint16_t* off_all = nullptr;
     Assembled lq, lqn;
 
-    std::map<std::string, std::vector<uint8_t>> host;
+    std::map<std::string, HostBuf> host;
+    PinnedArena pinned;
     std::map<std::string, float> stage_ms;
 
     Block() { CURC_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); }
@@ -76,12 +61,32 @@ struct Block {
     // a12 on the three pseudogenomes; fills the ref / map streams
     void refmatch_all();
 
+    // D2H copy of a device array into pinned staging (async on the stream)
     template <class T>
     void keep(const std::string& name, const T* dev, size_t count) {
-        auto& v = host[name];
-        v.resize(count * sizeof(T));
-        if (count) CURC_CHECK(cudaMemcpyAsync(v.data(), dev, count * sizeof(T), cudaMemcpyDeviceToHost, stream));
+        HostBuf b;
+        b.size = count * sizeof(T);
+        if (count) {
+            uint8_t* p = pinned.alloc(b.size);
+            CURC_CHECK(cudaMemcpyAsync(p, dev, b.size, cudaMemcpyDeviceToHost, stream));
+            b.ptr = p;
+        }
+        host[name] = std::move(b);
+    }
+    void put(const std::string& name, std::vector<uint8_t>&& v) {
+        HostBuf b;
+        b.own = std::move(v);
+        b.ptr = b.own.data();
+        b.size = b.own.size();
+        host[name] = std::move(b);
     }
 };
 
 }  // namespace curc
+
+// The C-ABI context (include/curc_b200.h): one device, one block pipeline.
+struct curc_ctx {
+    int device = 0;
+    std::unique_ptr<curc::Block> block;
+    std::string err;
+};

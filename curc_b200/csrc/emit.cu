@@ -549,17 +549,11 @@ void Block::emit(StageTimer& T) {
         keep("id_to_pos", id_to_pos, n);
     }
     {
-        // per-class offset streams
-        std::vector<uint16_t> all(class_elems);
-        if (class_elems)
-            CURC_CHECK(cudaMemcpyAsync(all.data(), off_all, class_elems * 2, cudaMemcpyDeviceToHost, s));
-        CURC_CHECK(cudaStreamSynchronize(s));
+        // per-class offset streams: consecutive slices of off_all
         uint64_t b = 0;
         for (int mm = 1; mm <= p.max_mm; ++mm) {
             const uint64_t ne = uint64_t(class_count[mm]) * class_width(mm);
-            auto& v = host["mis_off_" + std::to_string(mm)];
-            v.resize(ne * 2);
-            if (ne) std::memcpy(v.data(), all.data() + b, ne * 2);
+            keep("mis_off_" + std::to_string(mm), off_all + b, ne);
             b += ne;
         }
     }

@@ -185,11 +185,16 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     uint32_t* counts = a.alloc<uint32_t>(2);
     uint32_t mp = cnt, ms = cnt;
     for (int off = 1; off < acc.L && mp > 0 && ms > 0; ++off) {
+        SubStage sp_merge("full_match.resort");
         run_bounds_kernel<Acc><<<1, 32, 0, s>>>(acc, suf, ms, off, bounds);
         CURC_LAUNCH_CHECK();
         merge_runs_kernel<Acc><<<grid_for(ms, 256), 256, 0, s>>>(acc, suf, ms, off, bounds, suf2);
         CURC_LAUNCH_CHECK();
+        sp_merge.stop();
+        SubStage sp_groups("full_match.groups");
         merge_groups_kernel<Acc><<<grid_for(ms, 128), 128, 0, s>>>(acc, pre, mp, suf2, ms, off, next, prev, offset);
+        sp_groups.stop();
+        SubStage sp_comp("full_match.compact");
         CURC_LAUNCH_CHECK();
         keep_flags_kernel<<<grid_for(mp, 256), 256, 0, s>>>(pre, mp, prev, keep);
         CURC_LAUNCH_CHECK();

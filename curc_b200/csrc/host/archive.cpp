@@ -1,0 +1,391 @@
+// Block stream coding and the .curc archive layout.
+//
+// Layout (must match the reference byte for byte; read by decompress.cu:
+// 760-814): archive header `u8 preserve_order, u8 paired_end, u16 read_len,
+// u8 blocks` (preprocess.cpp:261-266), then each block body: `u32 reads`,
+// 16-byte mismatch decoder table, [PO: u8 joined-length-fits-u32], u8
+// ref-length-fits-u32, three u64 pseudogenome lengths, then u64-length-
+// prefixed payloads in the order of compress.cu:2112-2146.
+//
+// The coders are the reference's vendored third-party libraries, linked
+// unmodified: fast-lzma2 (pseudogenome, positions), the LZMA SDK with PPMd7
+// and PgRC's VarLenDNACoder, the CLR range coder (mismatch offsets), and the
+// `bsc` executable built from libbsc (strand stream, run as a subprocess
+// exactly as util.cuh:527-535 does).  Independent streams are coded
+// concurrently; calls into the LZMA/PPMd container are serialised because
+// that library writes to a shared log stream.
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <future>
+#include <mutex>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifndef ABS
+#define ABS std::abs
+#endif
+#include <fast-lzma2/fast-lzma2.h>
+#include <lzma/VarLenDNACoder/LzmaLib.h>
+#include <range_coder/clr.cdr>
+#include <range_coder/simple_model.h>
+
+#include "host.hpp"
+
+namespace curc {
+namespace host {
+
+namespace {
+
+std::mutex g_lzmalib_mu;
+
+std::string container(const void* src, size_t n, uint8_t coder, int param, double est) {
+    // LzmaLib.cpp:539-552 container at level 3
+    std::lock_guard<std::mutex> g(g_lzmalib_mu);
+    std::ostringstream o;
+    writeCompressed(o, static_cast<const char*>(src), n, coder, 3, param, est);
+    return o.str();
+}
+
+// fast-lzma2 stream with the feeding pattern of the reference's file helper
+// (8 KiB input reads, 4 KiB output buffer), so the bytes are identical.
+std::string fl2(const void* data, size_t n, int level, int threads) {
+    FL2_CStream* cs = FL2_createCStreamMt(unsigned(threads), 0);
+    if (!cs) throw std::runtime_error("fast-lzma2: cannot create a compression context");
+    size_t r = FL2_initCStream(cs, level);
+    if (FL2_isError(r)) throw std::runtime_error(std::string("fast-lzma2: ") + FL2_getErrorName(r));
+    const unsigned char* src = static_cast<const unsigned char*>(data);
+    size_t consumed = 0;
+    unsigned char in_buffer[8 * 1024];
+    unsigned char out_buffer[4 * 1024];
+    FL2_inBuffer in = {in_buffer, sizeof(in_buffer), sizeof(in_buffer)};
+    FL2_outBuffer out = {out_buffer, sizeof(out_buffer), 0};
+    std::string res;
+    do {
+        if (in.pos == in.size) {
+            const size_t take = std::min(sizeof(in_buffer), n - consumed);
+            std::memcpy(in_buffer, src + consumed, take);
+            consumed += take;
+            in.size = take;
+            in.pos = 0;
+        }
+        r = FL2_compressStream(cs, &out, &in);
+        if (FL2_isError(r)) throw std::runtime_error(std::string("fast-lzma2: ") + FL2_getErrorName(r));
+        res.append(reinterpret_cast<const char*>(out_buffer), out.pos);
+        out.pos = 0;
+    } while (in.size == sizeof(in_buffer));
+    do {
+        r = FL2_endStream(cs, &out);
+        if (FL2_isError(r)) throw std::runtime_error(std::string("fast-lzma2: ") + FL2_getErrorName(r));
+        res.append(reinterpret_cast<const char*>(out_buffer), out.pos);
+        out.pos = 0;
+    } while (r);
+    FL2_freeCStream(cs);
+    return res;
+}
+
+std::string blob(const std::string& s) {
+    std::string o(8, '\0');
+    const uint64_t n = s.size();
+    std::memcpy(&o[0], &n, 8);
+    return o + s;
+}
+
+template <size_t MaxL>
+std::string offsets_coded(const uint16_t* a, size_t count, size_t m) {
+    // util.cuh:307-343
+    std::vector<char> buf(count * sizeof(uint16_t) + 1024);
+    RangeCoder rc{};
+    rc.output(buf.data());
+    rc.StartEncode();
+    SIMPLE_MODEL<2> flag;
+    SIMPLE_MODEL<MaxL / 2 + 1> first;
+    SIMPLE_MODEL<MaxL> value;
+    size_t i = 0;
+    while (i < count) {
+        flag.encodeSymbol(&rc, a[i++]);
+        first.encodeSymbol(&rc, a[i++]);
+        if (m > 1) {
+            value.encodeSymbol(&rc, a[i++]);
+            if (m > 2)
+                for (size_t k = 1; k < m; ++k) value.encodeSymbol(&rc, a[i++]);
+        }
+    }
+    rc.FinishEncode();
+    return std::string(buf.data(), rc.size_out());
+}
+
+std::string offsets(int L, const uint16_t* a, size_t count, size_t m) {
+    if (L <= 128) return offsets_coded<128>(a, count, m);
+    if (L <= 256) return offsets_coded<256>(a, count, m);
+    if (L <= 384) return offsets_coded<384>(a, count, m);
+    return offsets_coded<512>(a, count, m);
+}
+
+std::string read_file(const std::string& p) {
+    FILE* f = std::fopen(p.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open " + p);
+    std::string s;
+    char buf[1 << 16];
+    size_t k;
+    while ((k = std::fread(buf, 1, sizeof(buf), f)) > 0) s.append(buf, k);
+    std::fclose(f);
+    return s;
+}
+
+void write_file(const std::string& p, const void* d, size_t n) {
+    FILE* f = std::fopen(p.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write " + p);
+    if (n && std::fwrite(d, 1, n, f) != n) throw std::runtime_error("short write " + p);
+    std::fclose(f);
+}
+
+std::string bsc_strand(const std::string& bsc, const std::string& dir, const void* d, size_t n) {
+    static std::atomic<uint64_t> seq{0};
+    const std::string tag = std::to_string(getpid()) + "_" + std::to_string(seq.fetch_add(1));
+    const std::string in = dir + "/strand_" + tag + ".txt", out = dir + "/strand_" + tag + ".bsc";
+    write_file(in, d, n);
+    const std::string cmd = "'" + bsc + "' e '" + in + "' '" + out + "' -pm0 -e2 > /dev/null";
+    if (std::system(cmd.c_str()) != 0) throw std::runtime_error("bsc failed: " + cmd);
+    std::string s = read_file(out);
+    unlink(in.c_str());
+    unlink(out.c_str());
+    return s;
+}
+
+template <class T>
+std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr) {
+    // util.cuh:345-442
+    std::vector<T> base, notbase;
+    std::vector<uint8_t> off_flag, off_first, d_flag, d_first;
+    std::vector<uint16_t> off_val;
+    std::vector<int16_t> d_val;
+    const uint32_t pairs = uint32_t(n / 2);
+    std::vector<uint32_t> rank;
+    for (uint32_t i = 0; i < n; i += 2) {
+        base.push_back(T(id_to_pos[i]));
+        rank.push_back(i >> 1);
+    }
+    std::stable_sort(rank.begin(), rank.end(), [&](uint32_t a, uint32_t b) { return base[a] < base[b]; });
+    int64_t ref_prev = 0, prev = 0;
+    bool match = false;
+    for (uint32_t q = 0; q < pairs; ++q) {
+        const uint32_t i = rank[q] * 2;
+        const bool before = id_to_pos[i] < id_to_pos[i + 1];
+        const T rel = before ? T(id_to_pos[i + 1] - id_to_pos[i]) : T(id_to_pos[i] - id_to_pos[i + 1]);
+        const bool in16 = rel <= 0xFFFF;
+        off_flag.push_back(in16);
+        if (in16) {
+            off_first.push_back(before);
+            off_val.push_back(uint16_t(rel));
+            continue;
+        }
+        const int64_t delta = int64_t(rel) - ref_prev;
+        const bool d16 = delta <= INT16_MAX && delta >= INT16_MIN;
+        d_flag.push_back(d16);
+        if (d16) {
+            match = true;
+            d_first.push_back(before);
+            d_val.push_back(int16_t(delta));
+            ref_prev = int64_t(rel);
+        } else {
+            if (!match || ref_prev != prev) ref_prev = int64_t(rel);
+            notbase.push_back(T(id_to_pos[i + 1]));
+            match = false;
+        }
+        prev = int64_t(rel);
+    }
+    auto fb = std::async(std::launch::async, [&] { return fl2(base.data(), base.size() * sizeof(T), level, thr); });
+    auto fn = std::async(std::launch::async, [&] { return fl2(notbase.data(), notbase.size() * sizeof(T), level, thr); });
+    std::string o = blob(fb.get());
+    o += container(off_flag.data(), off_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    o += container(off_first.data(), off_first.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    o += container(off_val.data(), off_val.size() * 2, PPMD7_CODER, 3, 1);
+    o += container(d_flag.data(), d_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    o += container(d_first.data(), d_first.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    o += container(d_val.data(), d_val.size() * 2, PPMD7_CODER, 3, 1);
+    o += blob(fn.get());
+    return o;
+}
+
+std::string pe_order(const uint32_t* order, size_t n, int level, int thr) {
+    // util.cuh:444-525
+    std::vector<uint8_t> off_pair, non_off_pair, off8_flag, off8_val, d8_flag;
+    std::vector<int8_t> d8_val;
+    std::vector<uint32_t> offs;
+    std::vector<uint8_t> visit(n, 0);
+    std::vector<uint32_t> index(n);
+    for (uint32_t i = 0; i < n; ++i) index[order[i]] = i;
+    int64_t ref_prev = 0, prev = 0;
+    bool match = false;
+    for (uint32_t oi = 0; oi < n; ++oi) {
+        if (visit[oi]) continue;
+        const uint32_t o = order[oi];
+        const uint32_t po = o % 2 ? o - 1 : o + 1;
+        const uint32_t pi = index[po];
+        visit[pi] = 1;
+        const int64_t d = int64_t(pi) - int64_t(oi);
+        off8_flag.push_back(d <= 255);
+        if (d <= 255) {
+            off8_val.push_back(uint8_t(d));
+            off_pair.push_back(o % 2);
+            continue;
+        }
+        non_off_pair.push_back(o % 2);
+        const int64_t delta = d - ref_prev;
+        const bool d8 = delta >= INT8_MIN && delta <= INT8_MAX;
+        d8_flag.push_back(d8);
+        if (d8) {
+            match = true;
+            d8_val.push_back(int8_t(delta));
+            ref_prev = d;
+        } else {
+            if (!match || ref_prev != prev) ref_prev = d;
+            offs.push_back(uint32_t(d));
+            match = false;
+        }
+        prev = d;
+    }
+    auto fd = std::async(std::launch::async, [&] { return fl2(d8_val.data(), d8_val.size(), level, thr); });
+    auto fo = std::async(std::launch::async, [&] { return fl2(offs.data(), offs.size() * 4, level, thr); });
+    std::string out;
+    out += container(off8_flag.data(), off8_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    out += container(off8_val.data(), off8_val.size(), PPMD7_CODER, 2, 1);
+    out += container(d8_flag.data(), d8_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    out += container(off_pair.data(), off_pair.size(), PPMD7_CODER, 2, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    out += container(non_off_pair.data(), non_off_pair.size(), PPMD7_CODER, 2, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    out += blob(fd.get());
+    out += blob(fo.get());
+    return out;
+}
+
+}  // namespace
+
+std::string encode_block(const BlockView& v, const CoderParams& cp) {
+    const int L = v.read_len;
+    const auto& S = [&](const char* name) -> const Buf& { return v.get(name); };
+    std::string hdr;
+    auto put = [&](const void* p, size_t n) { hdr.append(static_cast<const char*>(p), n); };
+    put(&v.reads_count, 4);
+    put(S("decoder_table").ptr, 16);
+    const uint64_t* sizes = reinterpret_cast<const uint64_t*>(S("sizes").ptr);  // pre- and post-compaction
+    const uint64_t joined = sizes[0] + sizes[1] + sizes[2];
+    const uint8_t join_std = joined <= 0xFFFFFFFFull, ref_std = sizes[0] <= 0xFFFFFFFFull;
+    if (v.preserve_order) put(&join_std, 1);
+    put(&ref_std, 1);
+    put(sizes + 3, 24);
+
+    const int lvl = cp.flzma2_level, thr = cp.flzma2_threads;
+    // concurrent coders
+    std::future<std::string> f_idpos, f_strand, f_ref, f_peorder;
+    if (v.preserve_order) {
+        f_idpos = std::async(std::launch::async, [&] {
+            const Buf& b = S("id_to_pos");
+            const uint64_t* p = reinterpret_cast<const uint64_t*>(b.ptr);
+            const size_t n = b.size / 8;
+            if (!v.paired_end) {
+                if (join_std) {
+                    std::vector<uint32_t> v32(p, p + n);
+                    return fl2(v32.data(), v32.size() * 4, lvl, thr);
+                }
+                return fl2(p, n * 8, lvl, thr);
+            }
+            return join_std ? pe_id_to_pos<uint32_t>(p, n, lvl, thr) : pe_id_to_pos<uint64_t>(p, n, lvl, thr);
+        });
+    }
+    f_strand = std::async(std::launch::async, [&] {
+        const Buf& b = S("strand");
+        return bsc_strand(cp.bsc_path, cp.tmpdir, b.ptr, b.size);
+    });
+    f_ref = std::async(std::launch::async, [&] {
+        std::string joined_ref;
+        joined_ref.reserve(S("ref").size + S("unmap_ref").size + S("unmap_n_ref").size);
+        for (const char* nm : {"ref", "unmap_ref", "unmap_n_ref"})
+            joined_ref.append(reinterpret_cast<const char*>(S(nm).ptr), S(nm).size);
+        size_t clen = 0;
+        char* enc;
+        {
+            std::lock_guard<std::mutex> g(g_lzmalib_mu);
+            enc = Compress(clen, joined_ref.data(), joined_ref.size(), VARLEN_DNA_CODER, 3,
+                           PgSAHelpers::VarLenDNACoder::getCoderParam(
+                               PgSAHelpers::VarLenDNACoder::STATIC_CODES_CODER_PARAM,
+                               PgSAHelpers::VarLenDNACoder::AG_EXTENDED_CODES_ID),
+                           1);
+        }
+        std::string r = fl2(enc, clen, lvl, thr);
+        delete[] enc;
+        return r;
+    });
+    if (!v.preserve_order && v.paired_end) {
+        f_peorder = std::async(std::launch::async, [&] {
+            const Buf& b = S("pe_order");
+            return pe_order(reinterpret_cast<const uint32_t*>(b.ptr), b.size / 4, lvl, thr);
+        });
+    }
+    // mismatch offsets (CLR range coder) in parallel per class
+    const int max_mm = L / 5;
+    std::vector<std::future<std::string>> f_off;
+    for (int m = 1; m <= max_mm; ++m) {
+        f_off.push_back(std::async(std::launch::async, [&, m] {
+            const Buf& b = S(("mis_off_" + std::to_string(m)).c_str());
+            return offsets(L, reinterpret_cast<const uint16_t*>(b.ptr), b.size / 2, size_t(m));
+        }));
+    }
+    // the PPMd / LZMA streams (serialised inside `container`)
+    auto plain = [&](const char* nm, uint8_t coder, int param, double est) {
+        const Buf& b = S(nm);
+        return container(b.ptr, b.size, coder, param, est);
+    };
+    std::string read_off, unmap_n_off, unmap_off;
+    if (!v.preserve_order) {
+        read_off = plain("read_off", PPMD7_CODER, 3, 1);
+        unmap_n_off = plain("unmap_n_read_off", PPMD7_CODER, 3, 1);
+        unmap_off = plain("unmap_read_off", PPMD7_CODER, 3, 1);
+    }
+    const double est = simpleUintCompressionEstimate(S("ref").size, ref_std ? 0xFFFFFFFFull : ~0ull);
+    const int period = ref_std ? 2 : 3;
+    std::string maps;
+    for (auto pr : {std::make_pair("ref_off", "ref_len_map"), std::make_pair("unmap_ref_off", "unmap_ref_len"),
+                    std::make_pair("unmap_n_ref_off", "unmap_n_ref_len")}) {
+        maps += blob(plain(pr.first, LZMA_CODER, period, est));
+        maps += blob(plain(pr.second, LZMA_CODER, 0, 1));
+    }
+    const std::string mis_cnt = plain("mis_cnt", PPMD7_CODER, 2, 1);
+    const std::string mis_base = plain("mis_base", PPMD7_CODER, 2, COMPRESSION_ESTIMATION_MIS_SYM);
+
+    std::string out = hdr;
+    if (v.preserve_order) out += blob(f_idpos.get());
+    out += blob(f_strand.get());
+    out += blob(f_ref.get());
+    if (!v.preserve_order) {
+        out += blob(read_off);
+        out += blob(unmap_n_off);
+        out += blob(unmap_off);
+        if (v.paired_end) out += blob(f_peorder.get());
+    }
+    out += maps;
+    out += blob(mis_cnt);
+    out += blob(mis_base);
+    const uint8_t mm = uint8_t(max_mm);
+    out.append(reinterpret_cast<const char*>(&mm), 1);
+    for (auto& f : f_off) out += blob(f.get());
+    return out;
+}
+
+std::string archive_header(bool po, bool pe, int read_len, int blocks) {
+    std::string h(5, '\0');
+    h[0] = char(po);
+    h[1] = char(pe);
+    h[2] = char(read_len & 0xFF);
+    h[3] = char(read_len >> 8);
+    h[4] = char(blocks);
+    return h;
+}
+
+}  // namespace host
+}  // namespace curc

@@ -1,0 +1,152 @@
+// `curc` command line on the B200 path (options of src/main.cpp:55-67).
+// Compression: `curc -c -i in.fastq[,in_2.fastq] -o name [--working_dir d]
+// [--block_ratio r] [--flzma2_level l] [--flzma2_thread_num t]
+// [--preserve_order]` writes <working_dir>/<name>.curc.
+#include <dlfcn.h>
+#include <limits.h>
+#include <stdlib.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/curc_b200.h"
+
+namespace {
+
+bool has_ext(const std::string& p, const char* a, const char* b = nullptr) {
+    auto ends = [&](const char* e) {
+        const size_t n = std::strlen(e);
+        return p.size() >= n && p.compare(p.size() - n, n, e) == 0;
+    };
+    return ends(a) || (b && ends(b));
+}
+
+std::string self_dir() {
+    char buf[PATH_MAX];
+    const ssize_t k = readlink("/proc/self/exe", buf, sizeof(buf) - 1);
+    if (k <= 0) return ".";
+    buf[k] = 0;
+    std::string s(buf);
+    return s.substr(0, s.find_last_of('/'));
+}
+
+int usage() {
+    std::puts(
+        "curc (B200 path)\n"
+        "  -c, --compress            compress file\n"
+        "  -d, --decompress          decompress archive (use the reference decoder)\n"
+        "  -i, --input arg           input path (paired-end fastq paths are separated by commas)\n"
+        "  -o, --output arg          output file name\n"
+        "      --working_dir arg     working directory (default .)\n"
+        "      --block_ratio arg     ratio of block size (default 1)\n"
+        "      --flzma2_level arg    fast-lzma2 compression level [1...10] (default 10)\n"
+        "      --flzma2_thread_num   fast-lzma2 thread number (default 16)\n"
+        "      --preserve_order      preserve order information\n"
+        "      --device arg          CUDA device (default 0)\n");
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    bool comp = false, decomp = false, po = false;
+    std::string input, output, wd = ".";
+    double ratio = 1.0;
+    int level = 10, threads = 16, device = 0;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        auto val = [&]() -> std::string {
+            if (i + 1 >= argc) throw std::runtime_error("missing value for " + a);
+            return argv[++i];
+        };
+        try {
+            if (a == "-c" || a == "--compress") comp = true;
+            else if (a == "-d" || a == "--decompress") decomp = true;
+            else if (a == "-i" || a == "--input") input = val();
+            else if (a == "-o" || a == "--output") output = val();
+            else if (a == "--working_dir") wd = val();
+            else if (a == "--block_ratio") ratio = std::stod(val());
+            else if (a == "--flzma2_level") level = std::stoi(val());
+            else if (a == "--flzma2_thread_num") threads = std::stoi(val());
+            else if (a == "--preserve_order") po = true;
+            else if (a == "--device") device = std::stoi(val());
+            else if (a == "-h" || a == "--help") return usage();
+            else if (a == "--decode_buffer_size") val();
+            else throw std::runtime_error("unknown option " + a);
+        } catch (const std::exception& e) {
+            std::printf("%s\n", e.what());
+            return 0;
+        }
+    }
+    if (input.empty() || output.empty() || (!comp && !decomp)) return usage();
+    if (comp && decomp) {
+        std::puts("compression and decompression options conflict");
+        return 0;
+    }
+    if (decomp) {
+        std::puts("decompression is not part of the B200 path yet: use the reference `curc -d`");
+        return 2;
+    }
+    struct stat st;
+    if (stat(wd.c_str(), &st) != 0) {
+        std::puts("invalid working dir");
+        return 0;
+    }
+    if (!(ratio > 0 && ratio <= 1)) {
+        std::puts("block ratio is a float number in the range (0,1]");
+        return 0;
+    }
+    std::vector<std::string> files;
+    size_t p = 0;
+    while (p <= input.size()) {
+        const size_t q = input.find(',', p);
+        files.push_back(input.substr(p, q == std::string::npos ? std::string::npos : q - p));
+        if (q == std::string::npos) break;
+        p = q + 1;
+    }
+    if (files.empty() || files.size() > 2) {
+        std::puts("invalid input path number");
+        return 0;
+    }
+    for (const auto& f : files) {
+        if (stat(f.c_str(), &st) != 0 || !has_ext(f, ".fastq", ".fq")) {
+            std::puts("please check the fastq path (filename extension is .fastq or .fq)");
+            return 0;
+        }
+    }
+    curc_ctx* ctx = nullptr;
+    if (curc_ctx_create(device, &ctx) != CURC_OK) {
+        std::fprintf(stderr, "GPU assert: %s\n", curc_last_error(nullptr));
+        return 1;
+    }
+    std::string tmp = wd + "/curc_tmp_XXXXXX";
+    if (!mkdtemp(&tmp[0])) {
+        std::puts("cannot create a working directory");
+        return 1;
+    }
+    const std::string archive = wd + "/" + output + ".curc";
+    const std::string bsc = self_dir() + "/bsc";
+    uint64_t reads = 0;
+    uint32_t blocks = 0;
+    const int rc = curc_compress_files(ctx, files[0].c_str(), files.size() > 1 ? files[1].c_str() : nullptr,
+                                       archive.c_str(), ratio, po, level, threads, bsc.c_str(), tmp.c_str(), &reads,
+                                       &blocks);
+    rmdir(tmp.c_str());
+    if (rc != CURC_OK) {
+        std::fprintf(stderr, "curc: %s\n", curc_last_error(ctx));
+        curc_ctx_destroy(ctx);
+        return 1;
+    }
+    curc_ctx_destroy(ctx);
+    struct stat ast;
+    stat(archive.c_str(), &ast);
+    std::printf("reads count : %llu \n", (unsigned long long)reads);
+    std::printf("block count : %u \n", blocks);
+    std::printf("archive size : %lld bytes \n", (long long)ast.st_size);
+    return 0;
+}

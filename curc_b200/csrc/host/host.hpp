@@ -1,0 +1,57 @@
+// Host side of the drop-in `curc -c`: FASTQ ingest with the reference's
+// block split, block stream coding, archive layout.  No CUDA types here.
+#pragma once
+#include <cstdint>
+#include <functional>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace curc {
+namespace host {
+
+struct Buf {
+    const uint8_t* ptr = nullptr;
+    size_t size = 0;
+};
+
+// The streams of one compressed block, by the names of curc_block_get.
+struct BlockView {
+    uint32_t reads_count = 0;
+    int read_len = 0;
+    bool preserve_order = false, paired_end = false;
+    std::map<std::string, Buf> streams;
+    const Buf& get(const char* name) const;
+};
+
+struct CoderParams {
+    int flzma2_level = 10;    // --flzma2_level
+    int flzma2_threads = 16;  // --flzma2_thread_num
+    std::string bsc_path;     // the bsc executable (strand stream)
+    std::string tmpdir;       // scratch files for bsc
+};
+
+// Block body in the reference layout (compress.cu:1364-2146).
+std::string encode_block(const BlockView& v, const CoderParams& cp);
+// Archive header (preprocess.cpp:261-266).
+std::string archive_header(bool po, bool pe, int read_len, int blocks);
+
+// FASTQ ingest.  Reads single-end (f2 empty) or paired-end files in the
+// reference's 50 MB windows (25 MB per mate) cut at record boundaries by its
+// header heuristic, and closes a block once the bytes read since the last
+// cut exceed block_ratio of the input (preprocess.cpp:66-254).  Each block
+// is handed over as n x L ASCII sequences in block order (mates
+// interleaved); `sink` returns false to stop.
+struct IngestResult {
+    int read_len = 0;
+    uint64_t reads = 0;
+    int blocks = 0;
+};
+IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double block_ratio,
+                          const std::function<void(std::vector<char>&& seqs, uint64_t n, int L)>& sink);
+
+// Read length of the first record (preprocess.cpp:286-300).
+int first_read_length(const std::string& f1);
+
+}  // namespace host
+}  // namespace curc

@@ -168,6 +168,7 @@ void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, cons
     for (int rc = 0; rc < 2; ++rc) {
         for (int q = 0; q < np; ++q) {
             auto mk = a.mark();
+            SubStage sp_index(rc ? "mapping.index_rc" : "mapping.index_fwd");
             const uint64_t count = parts[q].count;
             const uint32_t hs = hash_size_for(count);
             uint32_t* hv = a.alloc<uint32_t>(count);
@@ -184,6 +185,8 @@ void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, cons
             uint32_t* pos = a.alloc<uint32_t>(std::min<uint64_t>(count, uint64_t(hs) * 12) + 2);
             bucket_fill_kernel<<<grid_for(count, 256, 4), 256, 0, s>>>(hv, idx, count, kr, pos);
             CURC_LAUNCH_CHECK();
+            sp_index.stop();
+            SubStage sp_map(rc ? "mapping.map_rc" : "mapping.map_fwd");
             MapIndex ix{hs - 1, kr, pos, parts[q].start};
             const int g = grid_for(total, 128);
             if (rc)

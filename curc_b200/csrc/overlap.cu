@@ -230,6 +230,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     const uint32_t mp = hc[0];
     uint32_t ms = hc[1];
 
+    SubStage sp_index("overlap.index");
     // index: stable sort of prefixes by bucket (compress.cu:1440-1471)
     const uint32_t hs = hash_size_for(mp);
     OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, pre, nullptr, next, prev, offset};
@@ -256,16 +257,20 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     uint32_t* cidx = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* ckey = a.alloc<uint32_t>(ms ? ms : 1);
 
+    sp_index.stop();
     uint32_t passes = 0, contested_total = 0;
     for (int off = 1; off < p.max_off && ms > 0 && mp > 0; ++off) {
         ++passes;
         const int g = grid_for(ms, 256);
+        SubStage sp_probe("overlap.probe_resolve");
         probe_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim);
         CURC_LAUNCH_CHECK();
         resolve_solo_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim, flag);
         CURC_LAUNCH_CHECK();
         select_indices(flag, cidx, ms, counts + 2, a, s);
         const uint32_t nc = read_scalar(counts + 2, s);
+        sp_probe.stop();
+        SubStage sp_cont("overlap.contested");
         if (nc) {
             contested_total += nc;
             gather_cand_kernel<<<grid_for(nc, 256), 256, 0, s>>>(cidx, nc, cand, ckey);
@@ -274,6 +279,8 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
             resolve_group_kernel<<<grid_for(nc, 256), 256, 0, s>>>(c, suf, off, ckey, cidx, nc, cand_end, claim);
             CURC_LAUNCH_CHECK();
         }
+        sp_cont.stop();
+        SubStage sp_comp("overlap.compact");
         keep_unlinked_kernel<<<g, 256, 0, s>>>(suf, ms, next, flag);
         CURC_LAUNCH_CHECK();
         select_flagged(suf, flag, suf2, ms, counts + 3, a, s);

@@ -71,6 +71,67 @@ void Arena::release(const Mark& m) {
     if (cur_ < chunks_.size()) chunks_[cur_].used = m.used;
 }
 
+// ---------------------------------------------------------------- pinned arena
+
+PinnedArena::~PinnedArena() {
+    for (auto& c : chunks_) cudaFreeHost(c.base);
+}
+
+uint8_t* PinnedArena::alloc(size_t bytes) {
+    bytes = (bytes + 63) & ~size_t(63);
+    while (cur_ < chunks_.size()) {
+        Chunk& c = chunks_[cur_];
+        if (c.used + bytes <= c.size) {
+            uint8_t* p = c.base + c.used;
+            c.used += bytes;
+            return p;
+        }
+        ++cur_;
+    }
+    Chunk c{nullptr, std::max(bytes, size_t(256) << 20), 0};
+    CURC_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&c.base), c.size, cudaHostAllocPortable));
+    c.used = bytes;
+    chunks_.push_back(c);
+    cur_ = chunks_.size() - 1;
+    return c.base;
+}
+
+void PinnedArena::reset() {
+    for (auto& c : chunks_) c.used = 0;
+    cur_ = 0;
+}
+
+// ---------------------------------------------------------------- stage timer
+
+size_t StageTimer::begin_span(const std::string& name) {
+    Span sp{name, nullptr, nullptr};
+    CURC_CHECK(cudaEventCreate(&sp.a));
+    CURC_CHECK(cudaEventCreate(&sp.b));
+    CURC_CHECK(cudaEventRecord(sp.a, s));
+    ev.push_back(sp);
+    return ev.size() - 1;
+}
+
+void StageTimer::end_span(size_t i) { CURC_CHECK(cudaEventRecord(ev[i].b, s)); }
+
+void StageTimer::collect(std::map<std::string, float>& out) {
+    CURC_CHECK(cudaStreamSynchronize(s));
+    for (auto& e : ev) {
+        float ms = 0;
+        CURC_CHECK(cudaEventElapsedTime(&ms, e.a, e.b));
+        out[e.name] += ms;
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    ev.clear();
+    open.clear();
+}
+
+StageTimer*& active_timer() {
+    thread_local StageTimer* t = nullptr;
+    return t;
+}
+
 // ---------------------------------------------------------------- scan
 
 namespace {

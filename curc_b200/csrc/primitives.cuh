@@ -4,6 +4,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -40,6 +42,54 @@ private:
     size_t cur_ = 0;
     size_t chunk_;
     size_t high_water_ = 0;
+};
+
+// Growable pinned host memory, bump allocated, reset per block; results are
+// copied into it asynchronously and returned as views.
+class PinnedArena {
+public:
+    ~PinnedArena();
+    uint8_t* alloc(size_t bytes);
+    void reset();
+
+private:
+    struct Chunk { uint8_t* base; size_t size, used; };
+    std::vector<Chunk> chunks_;
+    size_t cur_ = 0;
+};
+
+// CUDA events around the stages of one block run (nested names allowed,
+// e.g. "refmatch" and "refmatch.probe"); collect() adds each span's time.
+struct StageTimer {
+    cudaStream_t s;
+    struct Span { std::string name; cudaEvent_t a, b; };
+    std::vector<Span> ev;
+    std::vector<size_t> open;
+    size_t begin_span(const std::string& name);
+    void end_span(size_t i);
+    void begin(const std::string& name) { open.push_back(begin_span(name)); }
+    void end() {
+        end_span(open.back());
+        open.pop_back();
+    }
+    void collect(std::map<std::string, float>& out);
+};
+
+// The timer of the block run in progress on this thread (or null).
+StageTimer*& active_timer();
+
+// Times a scope as a sub-stage of the running block, if any.
+struct SubStage {
+    StageTimer* t;
+    size_t i = 0;
+    explicit SubStage(const char* name) : t(active_timer()) {
+        if (t) i = t->begin_span(name);
+    }
+    void stop() {
+        if (t) t->end_span(i);
+        t = nullptr;
+    }
+    ~SubStage() { stop(); }
 };
 
 // out[i] = sum(in[0..i)); optionally *total = sum(in[0..n)) (device pointer).

@@ -400,25 +400,29 @@ inline int log2_ceil(uint32_t x) {
     return b;
 }
 
+// Device views of one destination's results (valid until the arena region
+// is reused: the caller copies them out before the next destination).
 struct RmResult {
-    std::vector<uint8_t> seq, map_off, map_len;
+    const uint8_t* seq = nullptr;
+    uint64_t seq_len = 0;
+    const uint8_t* map_off = nullptr;
+    uint64_t off_len = 0;
+    const uint8_t* map_len = nullptr;
+    uint64_t len_len = 0;
 };
 
 // One destination (compress.cu:856-993).  `dest` is the ASCII string on the
 // device (forward strand).
 void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_n, bool dest_is_ref, RmResult& r,
                   Arena& a, cudaStream_t s) {
-    r.map_off.clear();
-    r.map_len.clear();
-    r.seq.resize(dl);
-    if (dl) CURC_CHECK(cudaMemcpyAsync(r.seq.data(), dest, dl, cudaMemcpyDeviceToHost, s));
+    r = RmResult{};
+    r.seq = dest;  // unchanged unless spans are kept
+    r.seq_len = dl;
     const uint64_t dic = dl >= uint64_t(RM_K) ? (dl - RM_K + 1 + RM_DEST_STEP - 1) / RM_DEST_STEP : 0;
     const uint64_t cap = uint64_t(double(dic) * (dest_is_ref ? 0.2 : 0.21));
-    if (dic == 0 || ix.rl < uint64_t(RM_K)) {
-        CURC_CHECK(cudaStreamSynchronize(s));
-        return;
-    }
+    if (dic == 0 || ix.rl < uint64_t(RM_K)) return;
     auto mk = a.mark();
+    SubStage sp_probe(dest_is_ref ? "refmatch.probe_self" : "refmatch.probe_unmapped");
     uint8_t* rc = a.alloc<uint8_t>(dl + 64);
     rc_ascii_kernel<<<grid_for(dl, 256, 8), 256, 0, s>>>(dest, dl, rc);
     CURC_LAUNCH_CHECK();
@@ -442,12 +446,13 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
     uint32_t* sel = a.alloc<uint32_t>(nslots);
     select_indices(flag, sel, nslots, cnt, a, s);
     uint32_t c = read_scalar(cnt, s);
+    sp_probe.stop();
     if (c > cap) c = uint32_t(cap);  // capacity: the first hits in probe order
     if (c == 0) {
         a.release(mk);
-        CURC_CHECK(cudaStreamSynchronize(s));
         return;
     }
+    SubStage sp_sort("refmatch.sort_unique");
     Hit* hv = a.alloc<Hit>(c);
     gather_hits_kernel<<<grid_for(c, 256), 256, 0, s>>>(hits, sel, c, dl, dest_is_ref, hv);
     CURC_LAUNCH_CHECK();
@@ -470,6 +475,8 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
     Hit* uniq = a.alloc<Hit>(cu);
     compact_hits_kernel<<<grid_for(cu, 256), 256, 0, s>>>(sorted, sel2, cu, uniq);
     CURC_LAUNCH_CHECK();
+    sp_sort.stop();
+    SubStage sp_accept("refmatch.accept");
     uint8_t* keptf = a.alloc<uint8_t>(cu);
     uint64_t* adst = a.alloc<uint64_t>(cu);
     uint64_t* alen = a.alloc<uint64_t>(cu);
@@ -500,16 +507,16 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
     CURC_CHECK(cudaMemcpyAsync(&len_bytes, cnt + 3, 4, cudaMemcpyDeviceToHost, s));
     CURC_CHECK(cudaStreamSynchronize(s));
     uint64_t hi[4] = {K, uint64_t(K) * (std32 ? 4 : 8), 1 + uint64_t(len_bytes), dl - total_removed};
-    r.map_off.resize(hi[1]);
-    r.map_len.resize(hi[2]);
-    if (hi[1]) CURC_CHECK(cudaMemcpyAsync(r.map_off.data(), moff, hi[1], cudaMemcpyDeviceToHost, s));
-    if (hi[2]) CURC_CHECK(cudaMemcpyAsync(r.map_len.data(), mlen, hi[2], cudaMemcpyDeviceToHost, s));
+    r.map_off = moff;
+    r.off_len = hi[1];
+    r.map_len = mlen;
+    r.len_len = hi[2];
     uint8_t* out = a.alloc<uint8_t>(hi[3] + 1);
     compact_string_kernel<<<grid_for(dl, 256, 8), 256, 0, s>>>(dest, dl, sd, se, removed, hi[0], out);
     CURC_LAUNCH_CHECK();
-    r.seq.resize(hi[3]);
-    if (hi[3]) CURC_CHECK(cudaMemcpyAsync(r.seq.data(), out, hi[3], cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaStreamSynchronize(s));
+    r.seq = out;
+    r.seq_len = hi[3];
+    sp_accept.stop();
     a.release(mk);
 }
 
@@ -519,11 +526,12 @@ void Block::refmatch_all() {
     // compress.cu:2053-2069: index on the main pseudogenome, applied to the
     // unmapped, the unmapped-N and then the main pseudogenome itself.
     cudaStream_t s = stream;
-    RmResult main_r, un_r, unn_r;
+    RmResult r;
     auto mk = arena.mark();
     RmIndex ix{hq.packed, hq.len, 0, nullptr, nullptr};
     const bool usable = hq.len >= uint64_t(RM_K);
     if (usable) {
+        SubStage sub("refmatch.index");
         const uint64_t count = (hq.len - RM_K + 1 + RM_SRC_STEP - 1) / RM_SRC_STEP;
         if (count > (1ull << 30)) throw std::runtime_error("RefMatcher: pseudogenome above the 2^30-entry index");
         const uint32_t hs = hash_size_for(count);
@@ -543,41 +551,37 @@ void Block::refmatch_all() {
         CURC_LAUNCH_CHECK();
         ix.kr = kr;
         ix.pos = pos;
-    }
-    if (usable) {
-        if (lq.len) refmatch_one(ix, lq.seq, lq.len, false, false, un_r, arena, s);
-        if (lqn.len) refmatch_one(ix, lqn.seq, lqn.len, true, false, unn_r, arena, s);
-        refmatch_one(ix, hq.seq, hq.len, false, true, main_r, arena, s);
     } else {
-        // no index: every pseudogenome is kept as assembled
-        RmIndex none{hq.packed, 0, 0, nullptr, nullptr};
-        refmatch_one(none, lq.seq, lq.len, false, false, un_r, arena, s);
-        refmatch_one(none, lqn.seq, lqn.len, true, false, unn_r, arena, s);
-        refmatch_one(none, hq.seq, hq.len, false, true, main_r, arena, s);
+        ix.rl = 0;  // no index: every pseudogenome is kept as assembled
     }
+    // results are copied out right after each destination, before the next
+    // one reuses the scratch region
+    refmatch_one(ix, lq.seq, lq.len, false, false, r, arena, s);
+    keep("unmap_ref", r.seq, r.seq_len);
+    keep("unmap_ref_off", r.map_off, r.off_len);
+    keep("unmap_ref_len", r.map_len, r.len_len);
+    const uint64_t un_len = r.seq_len;
+    refmatch_one(ix, lqn.seq, lqn.len, true, false, r, arena, s);
+    keep("unmap_n_ref", r.seq, r.seq_len);
+    keep("unmap_n_ref_off", r.map_off, r.off_len);
+    keep("unmap_n_ref_len", r.map_len, r.len_len);
+    const uint64_t unn_len = r.seq_len;
+    refmatch_one(ix, hq.seq, hq.len, false, true, r, arena, s);
+    keep("ref", r.seq, r.seq_len);
+    keep("ref_off", r.map_off, r.off_len);
+    keep("ref_len_map", r.map_len, r.len_len);
+    const uint64_t main_len = r.seq_len;
     arena.release(mk);
-    host["ref"] = std::move(main_r.seq);
-    host["unmap_ref"] = std::move(un_r.seq);
-    host["unmap_n_ref"] = std::move(unn_r.seq);
-    host["ref_off"] = std::move(main_r.map_off);
-    host["ref_len_map"] = std::move(main_r.map_len);
-    host["unmap_ref_off"] = std::move(un_r.map_off);
-    host["unmap_ref_len"] = std::move(un_r.map_len);
-    host["unmap_n_ref_off"] = std::move(unn_r.map_off);
-    host["unmap_n_ref_len"] = std::move(unn_r.map_len);
-    const uint64_t sizes[6] = {hq.len, lq.len, lqn.len, host["ref"].size(), host["unmap_ref"].size(),
-                               host["unmap_n_ref"].size()};
-    auto& v = host["sizes"];
-    v.resize(sizeof(sizes));
-    std::memcpy(v.data(), sizes, sizeof(sizes));
+    const uint64_t sizes[6] = {hq.len, lq.len, lqn.len, main_len, un_len, unn_len};
+    put("sizes", std::vector<uint8_t>(reinterpret_cast<const uint8_t*>(sizes),
+                                      reinterpret_cast<const uint8_t*>(sizes) + sizeof(sizes)));
     // block statistics: reads, non-N reads, N reads, pseudogenome reads,
     // unmatched, mapped, unmapped (non-N, N), overlap passes, contested
     // suffixes, records, mismatches
     const uint64_t stats[12] = {n, m, NN, n_ref, U, n_map, n_ug, n_un, ostats.passes, ostats.contested, n_records,
                                 n_mis};
-    auto& st = host["stats"];
-    st.resize(sizeof(stats));
-    std::memcpy(st.data(), stats, sizeof(stats));
+    put("stats", std::vector<uint8_t>(reinterpret_cast<const uint8_t*>(stats),
+                                      reinterpret_cast<const uint8_t*>(stats) + sizeof(stats)));
 }
 
 }  // namespace curc

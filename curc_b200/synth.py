@@ -126,8 +126,8 @@ def sample_paired(rng, genome: np.ndarray, pairs: int, L: int, err, n_rate: floa
     return m1, m2
 
 
-def fastq_bytes(reads: np.ndarray, suffix: bytes = b"") -> bytes:
-    """FASTQ text: ``@r<i><suffix>`` / sequence / ``+`` / ``I`` * L."""
+def fastq_bytes(reads: np.ndarray, suffix: bytes = b"", name: bytes = b"r") -> bytes:
+    """FASTQ text: ``@<name><i><suffix>`` / sequence / ``+`` / ``I`` * L."""
     n, L = reads.shape
     out = []
     lo = 0
@@ -136,16 +136,18 @@ def fastq_bytes(reads: np.ndarray, suffix: bytes = b"") -> bytes:
         hi = min(n, 10 ** digits)
         if hi > lo:
             cnt = hi - lo
-            hl = 2 + digits + len(suffix)  # '@' 'r' digits suffix
+            hl = 1 + len(name) + digits + len(suffix)  # '@' name digits suffix
             rec = hl + 1 + L + 1 + 2 + L + 1
             buf = np.empty((cnt, rec), dtype=np.uint8)
             buf[:, 0] = ord("@")
-            buf[:, 1] = ord("r")
+            for j, ch in enumerate(name):
+                buf[:, 1 + j] = ch
             ids = np.arange(lo, hi, dtype=np.int64)
+            h0 = 1 + len(name)
             for d in range(digits):
-                buf[:, 2 + d] = ord("0") + (ids // 10 ** (digits - 1 - d)) % 10
+                buf[:, h0 + d] = ord("0") + (ids // 10 ** (digits - 1 - d)) % 10
             for j, ch in enumerate(suffix):
-                buf[:, 2 + digits + j] = ch
+                buf[:, h0 + digits + j] = ch
             buf[:, hl] = ord("\n")
             buf[:, hl + 1:hl + 1 + L] = reads[lo:hi]
             p = hl + 1 + L
@@ -183,17 +185,20 @@ class Workload:
         s[1::2] = self.mate2
         return s
 
-    def write(self, prefix: str) -> list[str]:
+    def write(self, prefix: str, name: bytes = b"r") -> list[str]:
+        """Writes the FASTQ file(s); headers are ``@<name><i>`` (``/1``, ``/2``
+        for mates).  Inputs above one 50 MB window need a header of at least 6
+        bytes for the block splitter's record-boundary test."""
         if self.mate2 is None:
             p = prefix + ".fastq"
             with open(p, "wb") as f:
-                f.write(fastq_bytes(self.mate1))
+                f.write(fastq_bytes(self.mate1, name=name))
             return [p]
         p1, p2 = prefix + "_1.fastq", prefix + "_2.fastq"
         with open(p1, "wb") as f:
-            f.write(fastq_bytes(self.mate1, b"/1"))
+            f.write(fastq_bytes(self.mate1, b"/1", name))
         with open(p2, "wb") as f:
-            f.write(fastq_bytes(self.mate2, b"/2"))
+            f.write(fastq_bytes(self.mate2, b"/2", name))
         return [p1, p2]
 
 

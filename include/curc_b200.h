@@ -85,6 +85,20 @@ int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint1
  * streams are always returned.  No reference counterpart. */
 int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep);
 
+/* Whole-file compression, the drop-in for `curc -c` (src/main.cpp:53-161,
+ * src/preprocess.cpp:66-283 and the coders of src/compress.cu:1923-2146):
+ * reads f1 (and f2 for paired end, else NULL) with the reference's block
+ * split, runs each block through the device path, codes its streams with
+ * the reference's coders (fast-lzma2 at `flzma2_level` with
+ * `flzma2_threads`, PPMd7/LZMA, CLR range coder, and the `bsc` executable at
+ * bsc_path, which writes scratch files in tmpdir) and writes the archive to
+ * archive_path in the reference's .curc layout.  Coding of a block overlaps
+ * the next block's ingest and device work.  *reads_out / *blocks_out (may be
+ * NULL) receive the totals. */
+int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2, const char* archive_path, double block_ratio,
+                        int preserve_order, int flzma2_level, int flzma2_threads, const char* bsc_path,
+                        const char* tmpdir, uint64_t* reads_out, uint32_t* blocks_out);
+
 /* Host view of a named result of the last block run ("strand", "mis_cnt",
  * "mis_base", "read_off", "ref", ... and the stage intermediates
  * "sorted_ids", "next", "prev", "offset", "hq_seq", ...).  The pointer stays

@@ -335,6 +335,8 @@ std::vector<RawBlock> split_fastq(const std::string& f1, const std::string& f2, 
                 }
                 ne--;
             }
+            // no boundary: the reference re-reads the same window forever
+            throw std::runtime_error("no record boundary found in a 50 MB window");
         cut:
             total -= (end - ne);
             end = ne;
