@@ -83,7 +83,8 @@ __device__ __forceinline__ void link_first_free(const OverlapCtx& c, uint32_t s,
 // bound of suffix[off, L) among the bucket's prefix[0, L-off).
 __global__ void probe_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uint32_t ms, int off,
                              uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
-                             uint32_t* __restrict__ claim) {
+                             uint32_t* __restrict__ claim, uint32_t* __restrict__ lead, uint32_t* __restrict__ ghead,
+                             uint32_t* __restrict__ gnext) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ms) return;
     const uint32_t s = suf[j];
@@ -105,50 +106,51 @@ __global__ void probe_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uin
     uint32_t r = INVALID;
     if (lo < e && cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) == 0) {
         r = lo;
+        // run membership: count, lowest list index, and a list of members
         atomicAdd(&claim[lo], 1u);
+        atomicMin(&lead[lo], j);
+        gnext[j] = atomicExch(&ghead[lo], j);
     }
     cand[j] = r;
     cand_end[j] = e;
 }
 
-__global__ void resolve_solo_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uint32_t ms, int off,
-                                    const uint32_t* __restrict__ cand, const uint32_t* __restrict__ cand_end,
-                                    uint32_t* __restrict__ claim, uint8_t* __restrict__ contested) {
+// A suffix alone on its run links directly.  A run claimed by several
+// suffixes is resolved by its lowest-index member, which visits the members
+// in list order (ascending index; runs are small, so repeated minimum
+// search) and gives each the first free non-self prefix, exactly the
+// sequential loop of compress.cu:1474.  The run's bookkeeping is reset for
+// the next pass by the thread that used it.
+__global__ void resolve_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uint32_t ms, int off,
+                               const uint32_t* __restrict__ cand, const uint32_t* __restrict__ cand_end,
+                               uint32_t* __restrict__ claim, uint32_t* __restrict__ lead, uint32_t* __restrict__ ghead,
+                               const uint32_t* __restrict__ gnext, uint32_t* __restrict__ contested) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ms) return;
     const uint32_t lo = cand[j];
-    uint8_t f = 0;
-    if (lo != INVALID) {
-        if (claim[lo] == 1) {
-            link_first_free(c, suf[j], lo, cand_end[j], off);
-            claim[lo] = 0;
-        } else {
-            f = 1;
-        }
-    }
-    contested[j] = f;
-}
-
-__global__ void gather_cand_kernel(const uint32_t* __restrict__ cidx, uint32_t nc, const uint32_t* __restrict__ cand,
-                                   uint32_t* __restrict__ ckey) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < nc) ckey[t] = cand[cidx[t]];
-}
-
-// One thread per contested run: its suffixes in list order, each taking the
-// first free non-self equal prefix (serial order of compress.cu:1474).
-__global__ void resolve_group_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, int off,
-                                     const uint32_t* __restrict__ ckey, const uint32_t* __restrict__ cidx, uint32_t nc,
-                                     const uint32_t* __restrict__ cand_end, uint32_t* __restrict__ claim) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nc) return;
-    const uint32_t lo = ckey[t];
-    if (t > 0 && ckey[t - 1] == lo) return;
-    for (uint32_t u = t; u < nc && ckey[u] == lo; ++u) {
-        const uint32_t j = cidx[u];
+    if (lo == INVALID) return;
+    const uint32_t n = claim[lo];
+    if (n == 1) {
         link_first_free(c, suf[j], lo, cand_end[j], off);
+    } else if (lead[lo] == j) {
+        atomicAdd(contested, n);
+        uint32_t last = 0;
+        bool first = true;
+        for (uint32_t k = 0; k < n; ++k) {
+            uint32_t best = INVALID;
+            for (uint32_t m = ghead[lo]; m != INVALID; m = gnext[m])
+                if ((first || m > last) && m < best) best = m;
+            if (best == INVALID) break;
+            link_first_free(c, suf[best], lo, cand_end[best], off);
+            last = best;
+            first = false;
+        }
+    } else {
+        return;  // the run's lowest member resolves it
     }
     claim[lo] = 0;
+    lead[lo] = INVALID;
+    ghead[lo] = INVALID;
 }
 
 __global__ void keep_unlinked_kernel(const uint32_t* __restrict__ suf, uint32_t ms, const uint32_t* __restrict__ next,
@@ -232,7 +234,12 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
 
     SubStage sp_index("overlap.index");
     // index: stable sort of prefixes by bucket (compress.cu:1440-1471)
-    const uint32_t hs = hash_size_for(mp);
+    // The table size does not change which prefixes a suffix meets: equal
+    // strings share a bucket whatever its size, and other bucket entries are
+    // rejected by the comparison.  The reference sizes it to the prefix count
+    // (get_hash_size); four times that keeps most probes of unlinkable
+    // suffixes at one empty bucket instead of a binary search.
+    const uint32_t hs = hash_size_for(uint64_t(mp) * 4);
     OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, pre, nullptr, next, prev, offset};
     uint32_t* keys = a.alloc<uint32_t>(mp ? mp : 1);
     if (mp) {
@@ -249,37 +256,29 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     exclusive_scan<uint32_t>(kr, kr, size_t(hs) + 2, nullptr, a, s);
     c.kr = kr;
 
+    // per prefix slot: run claim count, lowest claimer, member list head
     uint32_t* claim = a.alloc<uint32_t>(mp ? mp : 1);
+    uint32_t* lead = a.alloc<uint32_t>(mp ? mp : 1);
+    uint32_t* ghead = a.alloc<uint32_t>(mp ? mp : 1);
     CURC_CHECK(cudaMemsetAsync(claim, 0, size_t(mp ? mp : 1) * sizeof(uint32_t), s));
+    fill<uint32_t>(lead, INVALID, mp ? mp : 1, s);
+    fill<uint32_t>(ghead, INVALID, mp ? mp : 1, s);
     uint32_t* cand = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* cand_end = a.alloc<uint32_t>(ms ? ms : 1);
+    uint32_t* gnext = a.alloc<uint32_t>(ms ? ms : 1);
     uint8_t* flag = a.alloc<uint8_t>(ms ? ms : 1);
-    uint32_t* cidx = a.alloc<uint32_t>(ms ? ms : 1);
-    uint32_t* ckey = a.alloc<uint32_t>(ms ? ms : 1);
+    CURC_CHECK(cudaMemsetAsync(counts + 2, 0, 4, s));
 
-    sp_index.stop();
-    uint32_t passes = 0, contested_total = 0;
+    uint32_t passes = 0;
     for (int off = 1; off < p.max_off && ms > 0 && mp > 0; ++off) {
         ++passes;
         const int g = grid_for(ms, 256);
         SubStage sp_probe("overlap.probe_resolve");
-        probe_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim);
+        probe_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim, lead, ghead, gnext);
         CURC_LAUNCH_CHECK();
-        resolve_solo_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim, flag);
+        resolve_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim, lead, ghead, gnext, counts + 2);
         CURC_LAUNCH_CHECK();
-        select_indices(flag, cidx, ms, counts + 2, a, s);
-        const uint32_t nc = read_scalar(counts + 2, s);
         sp_probe.stop();
-        SubStage sp_cont("overlap.contested");
-        if (nc) {
-            contested_total += nc;
-            gather_cand_kernel<<<grid_for(nc, 256), 256, 0, s>>>(cidx, nc, cand, ckey);
-            CURC_LAUNCH_CHECK();
-            radix_sort_pairs<uint32_t, uint32_t>(ckey, cidx, nc, 0, 32, a, s);
-            resolve_group_kernel<<<grid_for(nc, 256), 256, 0, s>>>(c, suf, off, ckey, cidx, nc, cand_end, claim);
-            CURC_LAUNCH_CHECK();
-        }
-        sp_cont.stop();
         SubStage sp_comp("overlap.compact");
         keep_unlinked_kernel<<<g, 256, 0, s>>>(suf, ms, next, flag);
         CURC_LAUNCH_CHECK();
@@ -287,6 +286,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         std::swap(suf, suf2);
         ms = read_scalar(counts + 3, s);
     }
+    const uint32_t contested_total = read_scalar(counts + 2, s);
     if (st) {
         st->passes = passes;
         st->contested = contested_total;

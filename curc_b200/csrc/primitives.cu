@@ -484,20 +484,105 @@ void iota(uint32_t* p, size_t n, cudaStream_t s) {
     CURC_LAUNCH_CHECK();
 }
 
+namespace {
+// Marks elements that share their first word with a neighbour (tie runs).
+__global__ void tie_flags_kernel(const uint64_t* __restrict__ k0, size_t n, uint8_t* __restrict__ tie) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t v = k0[i];
+    tie[i] = (i > 0 && k0[i - 1] == v) || (i + 1 < n && k0[i + 1] == v);
+}
+
+// 1 where a tie element starts a new run (its predecessor in the tie list
+// is not its neighbour or has another first word).
+__global__ void run_starts_kernel(const uint32_t* __restrict__ pos, const uint64_t* __restrict__ k0, uint32_t m,
+                                  uint32_t* __restrict__ start) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    start[t] = t == 0 || pos[t - 1] + 1 != pos[t] || k0[pos[t - 1]] != k0[pos[t]];
+}
+
+// inclusive count of run starts: equal for all elements of one run
+__global__ void run_number_kernel(const uint32_t* __restrict__ excl, const uint32_t* __restrict__ start, uint32_t m,
+                                  uint64_t* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) out[t] = uint64_t(excl[t]) + start[t];
+}
+
+__global__ void gather_ids_kernel(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ pos, uint32_t m,
+                                  uint32_t* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) out[t] = ids[pos[t]];
+}
+
+__global__ void scatter_ids_kernel(const uint32_t* __restrict__ vals, const uint32_t* __restrict__ pos, uint32_t m,
+                                   uint32_t* __restrict__ ids) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < m) ids[pos[t]] = vals[t];
+}
+}  // namespace
+
 void sort_ids_by_reads(const uint64_t* db, int W, int L, uint32_t* ids, size_t n, Arena& a, cudaStream_t s) {
-    // LSD over whole words, last word first; each word sorted stably, so the
-    // final order is lexicographic with ties kept in input order
-    // (compress.cu:1400-1407 under a stable comparison sort).
+    // Stable lexicographic order of the reads (compress.cu:1400-1407 under a
+    // stable comparison sort; ties keep input order).  First by the first
+    // 32 bases; then only the runs of reads that share them are ordered by
+    // the remaining words, least significant first, and finally by run so
+    // that every run returns to its place.
     if (n <= 1) return;
-    auto m = a.mark();
-    uint64_t* keys = a.alloc<uint64_t>(n);
-    for (int w = W - 1; w >= 0; --w) {
-        gather_words(db, ids, n, W, w, keys, s);
-        int lo = 0;
-        if (w == W - 1) lo = 64 - 2 * (L - 32 * (W - 1));  // unused low bits are zero
-        radix_sort_pairs<uint64_t, uint32_t>(keys, ids, n, lo, 64, a, s);
+    auto mk = a.mark();
+    uint64_t* k0 = a.alloc<uint64_t>(n);
+    gather_words(db, ids, n, W, 0, k0, s);
+    const int lo0 = W == 1 ? 64 - 2 * L : 0;
+    radix_sort_pairs<uint64_t, uint32_t>(k0, ids, n, lo0, 64, a, s);
+    if (W > 1) {
+        uint8_t* tie = a.alloc<uint8_t>(n);
+        tie_flags_kernel<<<grid_for(n, 256), 256, 0, s>>>(k0, n, tie);
+        CURC_LAUNCH_CHECK();
+        uint32_t* pos = a.alloc<uint32_t>(n);
+        uint32_t* cnt = a.alloc<uint32_t>(1);
+        select_indices(tie, pos, n, cnt, a, s);
+        const uint32_t m = read_scalar(cnt, s);
+        if (m) {
+            uint32_t* sub = a.alloc<uint32_t>(m);
+            uint64_t* key = a.alloc<uint64_t>(m);
+            uint64_t* run = a.alloc<uint64_t>(m);
+            gather_ids_kernel<<<grid_for(m, 256), 256, 0, s>>>(ids, pos, m, sub);
+            CURC_LAUNCH_CHECK();
+            {
+                // run number = number of run starts before the element
+                uint32_t* st = a.alloc<uint32_t>(m);
+                uint32_t* ex = a.alloc<uint32_t>(m);
+                run_starts_kernel<<<grid_for(m, 256), 256, 0, s>>>(pos, k0, m, st);
+                CURC_LAUNCH_CHECK();
+                exclusive_scan<uint32_t>(st, ex, m, nullptr, a, s);
+                run_number_kernel<<<grid_for(m, 256), 256, 0, s>>>(ex, st, m, run);
+                CURC_LAUNCH_CHECK();
+            }
+            // the run numbers ride along as the sort moves the ids: sort pairs
+            // of (key, index into sub) and permute both at the end
+            uint32_t* perm = a.alloc<uint32_t>(m);
+            iota(perm, m, s);
+            uint32_t* tmp = a.alloc<uint32_t>(m);
+            for (int w = W - 1; w >= 1; --w) {
+                gather_ids_kernel<<<grid_for(m, 256), 256, 0, s>>>(sub, perm, m, tmp);  // current order's ids
+                CURC_LAUNCH_CHECK();
+                gather_words(db, tmp, m, W, w, key, s);
+                const int lo = w == W - 1 ? 64 - 2 * (L - 32 * (W - 1)) : 0;
+                radix_sort_pairs<uint64_t, uint32_t>(key, perm, m, lo, 64, a, s);
+            }
+            // stable by run number (ascending with position)
+            uint64_t* rk = a.alloc<uint64_t>(m);
+            gather_words(run, perm, m, 1, 0, rk, s);
+            int bits = 1;
+            while (bits < 64 && (1ull << bits) <= uint64_t(m) + 1) ++bits;
+            radix_sort_pairs<uint64_t, uint32_t>(rk, perm, m, 0, bits, a, s);
+            gather_ids_kernel<<<grid_for(m, 256), 256, 0, s>>>(sub, perm, m, tmp);
+            CURC_LAUNCH_CHECK();
+            scatter_ids_kernel<<<grid_for(m, 256), 256, 0, s>>>(tmp, pos, m, ids);
+            CURC_LAUNCH_CHECK();
+        }
     }
-    a.release(m);
+    a.release(mk);
 }
 
 }  // namespace curc
