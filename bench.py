@@ -190,7 +190,8 @@ def run_ours(a, rank, world):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         step_s, e2e_s = float(t[0]), float(t[1])
     stats = dict(zip(["reads", "non_n", "n_reads", "pseudogenome_reads", "unmatched", "mapped", "unmapped",
-                      "unmapped_n", "overlap_passes", "contested", "records", "mismatches"],
+                      "unmapped_n", "overlap_passes", "contested", "records", "mismatches",
+                      "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits"],
                      [int(x) for x in ctx.get("stats", np.uint64)]))
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     res = dict(bases=bases, n=n, L=L, step_s=step_s, e2e_s=e2e_s, wall=wall, launches=launches, stats=stats,

@@ -61,11 +61,12 @@ __global__ void rank_init_kernel(uint32_t n, const uint32_t* __restrict__ pv, co
     out[x] = st;
 }
 
-__global__ void rank_step_kernel(uint32_t n, const RankState* __restrict__ in, RankState* __restrict__ out,
-                                 uint32_t* __restrict__ active) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    bool still = false;
-    if (x < n) {
+// One jump for every read (grid-stride); *active counts the reads whose
+// ancestor pointer is still set afterwards.
+__global__ void __launch_bounds__(512) rank_step_kernel(uint32_t n, const RankState* __restrict__ in,
+                                                        RankState* __restrict__ out, uint32_t* __restrict__ active) {
+    uint32_t still = 0;
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
         RankState st = in[x];
         if (st.jump != INVALID) {
             const RankState a = in[st.jump];
@@ -74,12 +75,11 @@ __global__ void rank_step_kernel(uint32_t n, const RankState* __restrict__ in, R
             st.cnt += a.cnt;
             st.mn = min(st.mn, a.mn);
             st.jump = a.jump;
-            still = st.jump != INVALID;
+            still += st.jump != INVALID;
         }
         out[x] = st;
     }
-    const uint32_t b = __ballot_sync(0xFFFFFFFFu, still);
-    if (b && (threadIdx.x & 31) == 0) atomicAdd(active, uint32_t(__popc(b)));
+    block_tally<uint32_t>(still, active);
 }
 
 __global__ void cycle_flags_kernel(uint32_t n, const RankState* __restrict__ st, uint8_t* __restrict__ cyc) {
@@ -235,7 +235,7 @@ RankState* run_ranking(uint32_t n, uint32_t m, const uint32_t* pv, const uint16_
     *left = 0;
     for (int t = 0; t < R; ++t) {
         CURC_CHECK(cudaMemsetAsync(active, 0, 4, s));
-        rank_step_kernel<<<g, 256, 0, s>>>(n, A, B, active);
+        rank_step_kernel<<<resident_grid(rank_step_kernel, 512, n), 512, 0, s>>>(n, A, B, active);
         CURC_LAUNCH_CHECK();
         std::swap(A, B);
         *left = read_scalar(active, s);

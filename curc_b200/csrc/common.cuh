@@ -148,4 +148,29 @@ inline int grid_for(uint64_t n, int block, int per_thread = 1) {
     return int(g);
 }
 
+// Grid of a grid-stride kernel: as many blocks as stay resident on the
+// device at once, no more than the n items need.
+template <class K>
+inline int resident_grid(K kernel, int block, uint64_t n) {
+    int per_sm = 0;
+    CURC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0));
+    const uint64_t cap = uint64_t(SM_COUNT_B200) * uint64_t(per_sm < 1 ? 1 : per_sm);
+    const uint64_t need = div_up(n, uint64_t(block));
+    return int(need < 1 ? 1 : (need < cap ? need : cap));
+}
+
+// Sum of a per-thread count over the block, added to *out with one atomic:
+// a single global counter bumped by every warp serialises at the L2.  Every
+// thread of the block calls it, after any divergent work.
+template <class T>
+__device__ __forceinline__ void block_tally(uint32_t v, T* out) {
+    __shared__ uint32_t acc;
+    if (threadIdx.x == 0) acc = 0;
+    __syncthreads();
+    v = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&acc, v);
+    __syncthreads();
+    if (threadIdx.x == 0 && acc) atomicAdd(out, T(acc));
+}
+
 }  // namespace curc

@@ -76,9 +76,17 @@ __global__ void record_streams_kernel(const DevRecord* __restrict__ rec, uint32_
 
 __host__ __device__ inline uint32_t class_width(uint32_t m) { return m == 1 ? 2 : (m == 2 ? 3 : m + 2); }
 
-__global__ void class_hist_kernel(const uint8_t* __restrict__ mis, uint32_t T, uint32_t* __restrict__ hist) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < T && mis[i]) atomicAdd(&hist[mis[i]], 1u);
+// Records per mismatch count (bins 1..nb-1), counted in shared memory by a
+// resident grid and added to hist once per block.
+__global__ void __launch_bounds__(256) class_hist_kernel(const uint8_t* __restrict__ mis, uint32_t T, int nb,
+                                                         uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < T; i += gridDim.x * blockDim.x)
+        if (mis[i]) atomicAdd(&h[mis[i]], 1u);
+    __syncthreads();
+    if (int(threadIdx.x) < nb && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
 __global__ void class_keys_kernel(const uint32_t* __restrict__ sel, uint32_t c, const uint8_t* __restrict__ mis,
@@ -405,7 +413,7 @@ void Block::emit(StageTimer& T) {
     uint32_t* chist = arena.alloc<uint32_t>(maxm + 2);
     CURC_CHECK(cudaMemsetAsync(chist, 0, size_t(maxm + 2) * 4, s));
     if (Tn) {
-        class_hist_kernel<<<grid_for(Tn, 256), 256, 0, s>>>(smis, Tn, chist);
+        class_hist_kernel<<<resident_grid(class_hist_kernel, 256, Tn), 256, 0, s>>>(smis, Tn, maxm + 2, chist);
         CURC_LAUNCH_CHECK();
     }
     std::vector<uint32_t> hcls(maxm + 2);

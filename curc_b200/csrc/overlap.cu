@@ -41,10 +41,43 @@ __global__ void link_flags_kernel(const uint32_t* __restrict__ sorted, uint32_t 
 }
 
 __global__ void prefix_hash_kernel(const uint64_t* __restrict__ db, int W, int kip, int k, uint32_t mask,
-                                   const uint32_t* __restrict__ pre, uint32_t m, uint32_t* __restrict__ keys) {
+                                   uint32_t bmask, const uint32_t* __restrict__ pre, uint32_t m,
+                                   uint32_t* __restrict__ keys, uint32_t* __restrict__ present) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
-    keys[i] = uint32_t(murmur64(word_at(db + uint64_t(pre[i]) * W, kip, k)) & mask);
+    const uint64_t hv = murmur64(word_at(db + uint64_t(pre[i]) * W, kip, k));
+    keys[i] = uint32_t(hv & mask);
+    const uint32_t bit = uint32_t(hv >> 32) & bmask;
+    atomicOr(&present[bit >> 5], 1u << (bit & 31));
+}
+
+__global__ void gather_rows_kernel(const uint64_t* __restrict__ db, int W, const uint32_t* __restrict__ ids,
+                                   uint32_t m, uint64_t* __restrict__ out) {
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= uint64_t(m) * W) return;
+    const uint32_t i = uint32_t(t / W), w = uint32_t(t - uint64_t(i) * W);
+    out[t] = db[uint64_t(ids[i]) * W + w];
+}
+
+// keep flag of each suffix (not linked) as a 0/1 count for the scan
+__global__ void keep_count_kernel(const uint8_t* __restrict__ linked, uint32_t ms, uint32_t* __restrict__ keep) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < ms) keep[j] = !linked[j];
+}
+
+// moves the kept suffixes (id, packed words, offset mask) to their
+// compacted slots, preserving list order
+__global__ void compact_rows_kernel(const uint32_t* __restrict__ suf, const uint64_t* __restrict__ sufw, int W,
+                                    const uint32_t* __restrict__ mask, int mw, uint32_t ms, uint32_t ms2,
+                                    const uint32_t* __restrict__ keep, const uint32_t* __restrict__ pos,
+                                    uint32_t* __restrict__ suf2, uint64_t* __restrict__ sufw2,
+                                    uint32_t* __restrict__ mask2) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ms || !keep[j]) return;
+    const uint32_t q = pos[j];
+    for (int w = 0; w < W; ++w) sufw2[uint64_t(q) * W + w] = sufw[uint64_t(j) * W + w];
+    for (int w = 0; w < mw; ++w) mask2[uint64_t(w) * ms2 + q] = mask[uint64_t(w) * ms + j];
+    suf2[q] = suf[j];
 }
 
 __global__ void bucket_count_kernel(const uint32_t* __restrict__ keys, uint32_t m, uint32_t* __restrict__ kr) {
@@ -56,6 +89,8 @@ struct OverlapCtx {
     const uint64_t* db;
     int W, L, k, kip;
     uint32_t mask;
+    const uint32_t* present;  // bitmap of prefix k-mer hashes (high 32 bits)
+    uint32_t bmask;
     const uint32_t* va;  // prefix ids sorted by (bucket, read)
     const uint32_t* kr;  // bucket ranges
     uint32_t* next;
@@ -63,9 +98,10 @@ struct OverlapCtx {
     uint16_t* offset;
 };
 
-// First free non-self prefix of the equal run starting at lo, if equal.
-__device__ __forceinline__ void link_first_free(const OverlapCtx& c, uint32_t s, uint32_t lo, uint32_t e, int off) {
-    const uint64_t* sr = c.db + uint64_t(s) * c.W;
+// First free non-self prefix of the equal run starting at lo, if equal;
+// sr = the suffix read's packed words.
+__device__ __forceinline__ bool link_first_free(const OverlapCtx& c, uint32_t s, const uint64_t* sr, uint32_t lo,
+                                                uint32_t e, int off) {
     const int cl = c.L - off;
     for (uint32_t q = lo; q < e; ++q) {
         const uint32_t pr = c.va[q];
@@ -74,45 +110,89 @@ __device__ __forceinline__ void link_first_free(const OverlapCtx& c, uint32_t s,
             c.prev[pr] = s;
             c.next[s] = pr;
             c.offset[s] = uint16_t(off);
+            return true;
         }
-        return;
+        return false;
+    }
+    return false;
+}
+
+// Offsets at which a suffix can meet a prefix at all: bit off of the
+// suffix's mask (word off/32 of the list's masks, stored word-major so a
+// pass reads one coalesced u32 per suffix) is set when the k-mer at kmer_index_pos+off is in the
+// presence bitmap of prefix k-mers.  The prefix set is fixed for the whole
+// stage, so this is computed once, with the suffix's words in registers.
+__global__ void offset_mask_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw, uint32_t ms, int max_off,
+                                   uint32_t* __restrict__ mask) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ms) return;
+    const uint64_t* sr = sufw + uint64_t(j) * c.W;
+    uint32_t word = 0;
+    int wi = 0;
+    for (int off = 0; off < max_off; ++off) {
+        if (off > 0) {
+            const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
+            const uint32_t bit = uint32_t(hv >> 32) & c.bmask;
+            word |= ((c.present[bit >> 5] >> (bit & 31)) & 1u) << (off & 31);
+        }
+        if ((off & 31) == 31 || off == max_off - 1) {
+            mask[uint64_t(wi) * ms + j] = word;
+            ++wi;
+            word = 0;
+        }
     }
 }
 
 // compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
-// bound of suffix[off, L) among the bucket's prefix[0, L-off).
-__global__ void probe_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uint32_t ms, int off,
-                             uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
-                             uint32_t* __restrict__ claim, uint32_t* __restrict__ lead, uint32_t* __restrict__ ghead,
-                             uint32_t* __restrict__ gnext) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ms) return;
-    const uint32_t s = suf[j];
-    const uint64_t* sr = c.db + uint64_t(s) * c.W;
-    const uint32_t h = uint32_t(murmur64(word_at(sr, c.kip + off, c.k)) & c.mask);
-    uint32_t lo = c.kr[h];
-    const uint32_t e = c.kr[h + 1];
+// bound of suffix[off, L) among the bucket's prefix[0, L-off).  Suffixes
+// already linked or whose mask rules the offset out are skipped.  One
+// resident grid walks the list; tally[0] counts probes, tally[1] the
+// probes that met an equal prefix.
+__global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
+                                                    const uint32_t* __restrict__ mask,
+                                                    const uint8_t* __restrict__ linked, uint32_t ms, int off,
+                                                    uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
+                                                    uint32_t* __restrict__ claim, uint32_t* __restrict__ lead,
+                                                    uint32_t* __restrict__ ghead, uint32_t* __restrict__ gnext,
+                                                    unsigned long long* __restrict__ tally) {
+    uint32_t probes = 0, hits = 0;
     const int cl = c.L - off;
-    uint32_t count = e - lo;
-    while (count > 0) {
-        const uint32_t step = count / 2, it = lo + step;
-        if (cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl) < 0) {
-            lo = it + 1;
-            count -= step + 1;
-        } else {
-            count = step;
+    const uint32_t* mrow = mask + uint64_t(off >> 5) * ms;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ms; j += gridDim.x * blockDim.x) {
+        if (linked[j] || !((mrow[j] >> (off & 31)) & 1u)) {
+            cand[j] = INVALID;
+            continue;
         }
+        ++probes;
+        const uint64_t* sr = sufw + uint64_t(j) * c.W;
+        const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
+        const uint32_t h = uint32_t(hv & c.mask);
+        uint32_t lo = c.kr[h];
+        const uint32_t e = c.kr[h + 1];
+        uint32_t count = e - lo;
+        while (count > 0) {
+            const uint32_t step = count / 2, it = lo + step;
+            if (cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl) < 0) {
+                lo = it + 1;
+                count -= step + 1;
+            } else {
+                count = step;
+            }
+        }
+        uint32_t r = INVALID;
+        if (lo < e && cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) == 0) {
+            r = lo;
+            ++hits;
+            // run membership: count, lowest list index, and a list of members
+            atomicAdd(&claim[lo], 1u);
+            atomicMin(&lead[lo], j);
+            gnext[j] = atomicExch(&ghead[lo], j);
+        }
+        cand[j] = r;
+        cand_end[j] = e;
     }
-    uint32_t r = INVALID;
-    if (lo < e && cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) == 0) {
-        r = lo;
-        // run membership: count, lowest list index, and a list of members
-        atomicAdd(&claim[lo], 1u);
-        atomicMin(&lead[lo], j);
-        gnext[j] = atomicExch(&ghead[lo], j);
-    }
-    cand[j] = r;
-    cand_end[j] = e;
+    block_tally<unsigned long long>(probes, &tally[0]);
+    block_tally<unsigned long long>(hits, &tally[1]);
 }
 
 // A suffix alone on its run links directly.  A run claimed by several
@@ -120,43 +200,51 @@ __global__ void probe_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uin
 // in list order (ascending index; runs are small, so repeated minimum
 // search) and gives each the first free non-self prefix, exactly the
 // sequential loop of compress.cu:1474.  The run's bookkeeping is reset for
-// the next pass by the thread that used it.
-__global__ void resolve_kernel(OverlapCtx c, const uint32_t* __restrict__ suf, uint32_t ms, int off,
-                               const uint32_t* __restrict__ cand, const uint32_t* __restrict__ cand_end,
-                               uint32_t* __restrict__ claim, uint32_t* __restrict__ lead, uint32_t* __restrict__ ghead,
-                               const uint32_t* __restrict__ gnext, uint32_t* __restrict__ contested) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ms) return;
-    const uint32_t lo = cand[j];
-    if (lo == INVALID) return;
-    const uint32_t n = claim[lo];
-    if (n == 1) {
-        link_first_free(c, suf[j], lo, cand_end[j], off);
-    } else if (lead[lo] == j) {
-        atomicAdd(contested, n);
-        uint32_t last = 0;
-        bool first = true;
-        for (uint32_t k = 0; k < n; ++k) {
-            uint32_t best = INVALID;
-            for (uint32_t m = ghead[lo]; m != INVALID; m = gnext[m])
-                if ((first || m > last) && m < best) best = m;
-            if (best == INVALID) break;
-            link_first_free(c, suf[best], lo, cand_end[best], off);
-            last = best;
-            first = false;
+// the next pass by the thread that used it.  tally[2] counts links,
+// tally[3] the members of contested runs.
+__global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32_t* __restrict__ suf,
+                                                      const uint64_t* __restrict__ sufw, uint32_t ms, int off,
+                                                      const uint32_t* __restrict__ cand,
+                                                      const uint32_t* __restrict__ cand_end,
+                                                      uint32_t* __restrict__ claim, uint32_t* __restrict__ lead,
+                                                      uint32_t* __restrict__ ghead, const uint32_t* __restrict__ gnext,
+                                                      uint8_t* __restrict__ linked,
+                                                      unsigned long long* __restrict__ tally) {
+    uint32_t links = 0, contested = 0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ms; j += gridDim.x * blockDim.x) {
+        const uint32_t lo = cand[j];
+        if (lo == INVALID) continue;
+        const uint32_t n = claim[lo];
+        if (n == 1) {
+            if (link_first_free(c, suf[j], sufw + uint64_t(j) * c.W, lo, cand_end[j], off)) {
+                linked[j] = 1;
+                ++links;
+            }
+        } else if (lead[lo] == j) {
+            contested += n;
+            uint32_t last = 0;
+            bool first = true;
+            for (uint32_t k = 0; k < n; ++k) {
+                uint32_t best = INVALID;
+                for (uint32_t m = ghead[lo]; m != INVALID; m = gnext[m])
+                    if ((first || m > last) && m < best) best = m;
+                if (best == INVALID) break;
+                if (link_first_free(c, suf[best], sufw + uint64_t(best) * c.W, lo, cand_end[best], off)) {
+                    linked[best] = 1;
+                    ++links;
+                }
+                last = best;
+                first = false;
+            }
+        } else {
+            continue;  // the run's lowest member resolves it
         }
-    } else {
-        return;  // the run's lowest member resolves it
+        claim[lo] = 0;
+        lead[lo] = INVALID;
+        ghead[lo] = INVALID;
     }
-    claim[lo] = 0;
-    lead[lo] = INVALID;
-    ghead[lo] = INVALID;
-}
-
-__global__ void keep_unlinked_kernel(const uint32_t* __restrict__ suf, uint32_t ms, const uint32_t* __restrict__ next,
-                                     uint8_t* __restrict__ keep) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < ms) keep[j] = next[suf[j]] == INVALID;
+    block_tally<unsigned long long>(links, &tally[2]);
+    block_tally<unsigned long long>(contested, &tally[3]);
 }
 
 __global__ void chain_res_kernel(uint32_t n, const uint32_t* __restrict__ next, const uint32_t* __restrict__ prev,
@@ -240,10 +328,19 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     // (get_hash_size); four times that keeps most probes of unlinkable
     // suffixes at one empty bucket instead of a binary search.
     const uint32_t hs = hash_size_for(uint64_t(mp) * 4);
-    OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, pre, nullptr, next, prev, offset};
+    // presence bitmap, 16 bits per prefix (2^20..2^32 bits): a test that stays
+    // in L2 rejects most suffixes without touching the bucket table
+    int bbits = 20;
+    while (bbits < 32 && (1ull << bbits) < uint64_t(mp) * 16) ++bbits;
+    const uint64_t bwords = (1ull << bbits) / 32;
+    uint32_t* present = a.alloc<uint32_t>(bwords);
+    CURC_CHECK(cudaMemsetAsync(present, 0, bwords * 4, s));
+    OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, present, uint32_t((1ull << bbits) - 1), pre, nullptr,
+                 next, prev, offset};
     uint32_t* keys = a.alloc<uint32_t>(mp ? mp : 1);
     if (mp) {
-        prefix_hash_kernel<<<grid_for(mp, 256), 256, 0, s>>>(db, p.W, p.kip, p.k, c.mask, pre, mp, keys);
+        prefix_hash_kernel<<<grid_for(mp, 256), 256, 0, s>>>(db, p.W, p.kip, p.k, c.mask, c.bmask, pre, mp, keys,
+                                                             present);
         CURC_LAUNCH_CHECK();
         radix_sort_pairs<uint32_t, uint32_t>(keys, pre, mp, 0, log2_exact(hs), a, s);
     }
@@ -266,30 +363,75 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     uint32_t* cand = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* cand_end = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* gnext = a.alloc<uint32_t>(ms ? ms : 1);
-    uint8_t* flag = a.alloc<uint8_t>(ms ? ms : 1);
-    CURC_CHECK(cudaMemsetAsync(counts + 2, 0, 4, s));
+    uint32_t* keepc = a.alloc<uint32_t>(ms ? ms : 1);
+    uint32_t* kpos = a.alloc<uint32_t>(ms ? ms : 1);
+    // suffix reads and offset masks in list order
+    const int W = p.W, mw = (p.max_off + 31) / 32;
+    uint64_t* sufw = a.alloc<uint64_t>(size_t(ms ? ms : 1) * W);
+    uint64_t* sufw2 = a.alloc<uint64_t>(size_t(ms ? ms : 1) * W);
+    uint32_t* mask = a.alloc<uint32_t>(size_t(ms ? ms : 1) * mw);
+    uint32_t* mask2 = a.alloc<uint32_t>(size_t(ms ? ms : 1) * mw);
+    uint8_t* linked = a.alloc<uint8_t>(ms ? ms : 1);
+    CURC_CHECK(cudaMemsetAsync(linked, 0, ms ? ms : 1, s));
+    if (ms) {
+        gather_rows_kernel<<<grid_for(uint64_t(ms) * W, 256), 256, 0, s>>>(db, W, suf, ms, sufw);
+        CURC_LAUNCH_CHECK();
+        if (mp) {
+            offset_mask_kernel<<<grid_for(ms, 256), 256, 0, s>>>(c, sufw, ms, p.max_off, mask);
+            CURC_LAUNCH_CHECK();
+        }
+    }
+    // probes, probes that met a prefix, links, contested members
+    unsigned long long* tally = a.alloc<unsigned long long>(4);
+    CURC_CHECK(cudaMemsetAsync(tally, 0, 32, s));
+    sp_index.stop();
 
-    uint32_t passes = 0;
-    for (int off = 1; off < p.max_off && ms > 0 && mp > 0; ++off) {
+    // list of size ms, of which `active` are unlinked; compacted once half
+    // of it has linked
+    uint32_t passes = 0, active = ms;
+    uint64_t links_seen = 0;
+    const uint32_t ms0 = ms;
+    uint64_t active_sum = 0;
+    for (int off = 1; off < p.max_off && active > 0 && mp > 0; ++off) {
         ++passes;
+        active_sum += active;
         const int g = grid_for(ms, 256);
         SubStage sp_probe("overlap.probe_resolve");
-        probe_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim, lead, ghead, gnext);
+        probe_kernel<<<resident_grid(probe_kernel, 512, ms), 512, 0, s>>>(c, sufw, mask, linked, ms, off, cand, cand_end, claim, lead, ghead, gnext,
+                                        tally);
         CURC_LAUNCH_CHECK();
-        resolve_kernel<<<g, 256, 0, s>>>(c, suf, ms, off, cand, cand_end, claim, lead, ghead, gnext, counts + 2);
+        resolve_kernel<<<resident_grid(resolve_kernel, 512, ms), 512, 0, s>>>(c, suf, sufw, ms, off, cand, cand_end, claim, lead, ghead, gnext, linked,
+                                          tally);
         CURC_LAUNCH_CHECK();
+        const uint64_t links = read_scalar(tally + 2, s);
+        active -= uint32_t(links - links_seen);
+        links_seen = links;
         sp_probe.stop();
-        SubStage sp_comp("overlap.compact");
-        keep_unlinked_kernel<<<g, 256, 0, s>>>(suf, ms, next, flag);
-        CURC_LAUNCH_CHECK();
-        select_flagged(suf, flag, suf2, ms, counts + 3, a, s);
-        std::swap(suf, suf2);
-        ms = read_scalar(counts + 3, s);
+        if (active * 2 < ms) {
+            SubStage sp_comp("overlap.compact");
+            keep_count_kernel<<<g, 256, 0, s>>>(linked, ms, keepc);
+            CURC_LAUNCH_CHECK();
+            exclusive_scan<uint32_t>(keepc, kpos, ms, nullptr, a, s);
+            compact_rows_kernel<<<g, 256, 0, s>>>(suf, sufw, W, mask, mw, ms, active, keepc, kpos, suf2, sufw2, mask2);
+            CURC_LAUNCH_CHECK();
+            std::swap(suf, suf2);
+            std::swap(sufw, sufw2);
+            std::swap(mask, mask2);
+            ms = active;
+            CURC_CHECK(cudaMemsetAsync(linked, 0, ms ? ms : 1, s));
+        }
     }
-    const uint32_t contested_total = read_scalar(counts + 2, s);
     if (st) {
+        unsigned long long t[4];
+        CURC_CHECK(cudaMemcpyAsync(t, tally, 32, cudaMemcpyDeviceToHost, s));
+        CURC_CHECK(cudaStreamSynchronize(s));
         st->passes = passes;
-        st->contested = contested_total;
+        st->links = uint32_t(t[2]);
+        st->contested = uint32_t(t[3]);
+        st->suffixes = ms0;
+        st->active_sum = active_sum;
+        st->probes = t[0];
+        st->hits = t[1];
     }
     a.release(mk);
 }
