@@ -9,12 +9,17 @@
 // largest offset (first maximum met walking from the successor of the
 // cycle's first listed member), which becomes the tail.
 //
-// B200 design: list ranking by pointer jumping (at most log2 rounds, double
-// buffered, 32-byte state per read so a jump is one sector) gives each read
-// its chain head, base offset and rank; cycles are found as reads whose
-// ancestor pointer never clears and are cut in parallel (below); chains are
-// ordered by (min list index) with a radix sort and placed by exclusive
-// scans; every read then writes its bases independently.
+// B200 design: list ranking with a sparse ruling set.  Every chain head and
+// one member in 16 (by a hash of its id) is a ruler; one thread per ruler
+// walks its sublist up to the next ruler, giving every read its offset
+// within the sublist; the rulers (about a sixteenth of the reads, resident
+// in L2) are then ranked by pointer jumping, and one pass over the members
+// adds the two.  Each read is touched a constant number of times instead of
+// once per jumping round.  Cycles show up as ruler lists whose pointers never
+// clear (a cycle without any ruler gets one: its member of smallest list
+// index) and are cut in parallel (below); chains are ordered by their first
+// list index with a radix sort and placed by exclusive scans; every read
+// then writes its bases independently.
 #include "stages.cuh"
 
 namespace curc {
@@ -26,43 +31,156 @@ __global__ void scatter_index_kernel(const uint32_t* __restrict__ ids, uint32_t 
     if (i < m) pos_in_ids[ids[i]] = i;
 }
 
-// Pointer-jumping state of one read, 32 bytes so that one jump gathers one
-// sector.
+constexpr uint32_t RULER_SPACING = 16;  // one sampled ruler per 16 members (power of two)
+
+// Pointer-jumping state, 32 bytes so that one jump gathers one sector.  For
+// a ruler: acc / cnt = bases / reads of the sublists before its own, mn = the
+// smallest list index over its own and the preceding sublists, far = the
+// chain's head ruler.  The final per-member state (indexed by list index)
+// has the same fields for the read itself: far = the head read, acc = its
+// base offset in the chain, cnt = its rank, and mn, which covers at least
+// the read's predecessors and is the chain's (or cycle's) minimum at the
+// tail (or on a cycle).
 struct __align__(32) RankState {
-    uint64_t acc;     // bases contributed by the reads before this one (so far)
-    uint32_t jump;    // ancestor 2^t links back, INVALID once past the head
-    uint32_t far;     // farthest ancestor reached (the head at convergence)
-    uint32_t cnt;     // reads before this one (so far)
-    uint32_t mn;      // smallest list index over the reads covered
-    uint32_t member;  // read belongs to this assembly
-    uint32_t pad;
+    uint64_t acc;
+    uint32_t jump;    // ruler 2^t sublists back, INVALID once past the head
+    uint32_t far;
+    uint32_t cnt;
+    uint32_t mn;
+    uint32_t pad0, pad1;
 };
 
-// Reads are processed in id order so that a read's own state is read and
-// written coalesced; only the ancestor's state is a random gather.
-__global__ void rank_init_kernel(uint32_t n, const uint32_t* __restrict__ pv, const uint16_t* __restrict__ offset,
-                                 const uint32_t* __restrict__ pos_in_ids, const uint8_t* __restrict__ redo,
-                                 const RankState* __restrict__ keep, RankState* __restrict__ out) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= n) return;
-    if (redo && !redo[x]) {
-        out[x] = keep[x];
-        return;
-    }
-    RankState st;
-    st.pad = 0;
-    st.member = pos_in_ids[x] != INVALID;
-    const uint32_t p = st.member ? pv[x] : INVALID;
-    st.jump = p;
-    st.far = p == INVALID ? x : p;
-    st.acc = p == INVALID ? 0 : offset[p];
-    st.cnt = p == INVALID ? 0 : 1;
-    st.mn = pos_in_ids[x];
-    out[x] = st;
+// The links of one read in one 16-byte gather: successor, the read's own
+// offset to it, list index, ruler index (INVALID unless a ruler).
+struct __align__(16) ChainNode {
+    uint32_t nx, off, pos, rix;
+};
+
+// Position of a read within its ruler's sublist (indexed by list index).
+struct __align__(32) SubPos {
+    uint64_t la;     // bases from the ruler's first base to this read's
+    uint32_t owner;  // ruler index, INVALID while no walk has reached it
+    uint32_t lc;     // reads between the ruler and this read
+    uint32_t lm;     // smallest list index from the ruler to this read
+    uint32_t pad0, pad1, pad2;
+};
+
+// Totals of one ruler's sublist.
+struct __align__(16) SubTotal {
+    uint64_t acc;   // bases from the ruler's first base to the next ruler's
+    uint32_t cnt;   // reads in the sublist
+    uint32_t mn;    // smallest list index in the sublist
+};
+
+__global__ void ruler_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ pv,
+                                   const uint8_t* __restrict__ promote, uint8_t* __restrict__ f) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t x = ids[i];
+    f[i] = pv[x] == INVALID || (murmur64(x) & (RULER_SPACING - 1)) == 0 || (promote && promote[i]);
 }
 
-// One jump for every read (grid-stride); *active counts the reads whose
-// ancestor pointer is still set afterwards.
+__global__ void chain_nodes_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ nx,
+                                   const uint16_t* __restrict__ offset, ChainNode* __restrict__ node,
+                                   SubPos* __restrict__ loc) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t x = ids[i];
+    const uint32_t n = nx[x];
+    node[x] = ChainNode{n, n == INVALID ? 0u : uint32_t(offset[x]), i, INVALID};
+    loc[i].owner = INVALID;
+}
+
+__global__ void ruler_index_kernel(const uint32_t* __restrict__ rul, uint32_t nr, ChainNode* __restrict__ node) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nr) node[rul[t]].rix = t;
+}
+
+// One thread per ruler walks its sublist; the walk ends at the next ruler
+// or the chain's tail (a walk that comes back to a ruler on a cycle ends
+// there too), at most m steps.
+__global__ void ruler_walk_kernel(const uint32_t* __restrict__ rul, uint32_t nr, uint32_t m, uint32_t n,
+                                  const ChainNode* __restrict__ node, SubPos* __restrict__ loc,
+                                  SubTotal* __restrict__ tot, uint32_t* __restrict__ err) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nr; t += gridDim.x * blockDim.x) {
+        ChainNode c = node[rul[t]];
+        uint64_t la = 0;
+        uint32_t lc = 0, lm = c.pos;
+        loc[c.pos] = SubPos{0, t, 0, lm, 0, 0, 0};
+        for (uint32_t step = 0; step < m && c.nx != INVALID; ++step) {
+            if (c.nx >= n || node[c.nx].pos >= m) {  // a link out of the member set
+                atomicExch(err, 1u);
+                break;
+            }
+            const ChainNode d = node[c.nx];
+            la += c.off;
+            ++lc;
+            if (d.rix != INVALID) break;
+            lm = min(lm, d.pos);
+            loc[d.pos] = SubPos{la, t, lc, lm, 0, 0, 0};
+            c = d;
+        }
+        tot[t] = SubTotal{la, lc, lm};
+    }
+}
+
+// Members that no walk reached (cycles without a ruler).
+__global__ void __launch_bounds__(256) unreached_kernel(uint32_t m, const SubPos* __restrict__ loc,
+                                                        uint8_t* __restrict__ flag, uint32_t* __restrict__ count) {
+    uint32_t c = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const bool u = loc[i].owner == INVALID;
+        flag[i] = u;
+        c += u;
+    }
+    block_tally<uint32_t>(c, count);
+}
+
+// On a cycle without a ruler, its member of smallest list index becomes
+// one: each member walks the cycle (bounded by m steps) for the minimum.
+__global__ void promote_kernel(const uint32_t* __restrict__ ids, uint32_t m, uint32_t n,
+                               const uint8_t* __restrict__ unreached,
+                               const uint32_t* __restrict__ nx, const uint32_t* __restrict__ pos_in_ids,
+                               uint8_t* __restrict__ promote) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !unreached[i]) return;
+    const uint32_t x = ids[i];
+    uint32_t y = nx[x];
+    bool smallest = true;
+    for (uint32_t step = 0; step < m && y != x && y < n; ++step) {
+        if (pos_in_ids[y] < i) {  // non-members hold INVALID
+            smallest = false;
+            break;
+        }
+        y = nx[y];
+    }
+    promote[i] = smallest;
+}
+
+// Ruler ranking state: the predecessor ruler owns the read before this
+// ruler's first read.
+__global__ void ruler_init_kernel(const uint32_t* __restrict__ rul, uint32_t nr, uint32_t m,
+                                  const uint32_t* __restrict__ pv,
+                                  const uint32_t* __restrict__ pos_in_ids, const SubPos* __restrict__ loc,
+                                  const SubTotal* __restrict__ tot, RankState* __restrict__ st) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nr) return;
+    const uint32_t p = pv[rul[t]];
+    const uint32_t pi = p == INVALID ? INVALID : pos_in_ids[p];
+    const uint32_t pr = pi < m ? loc[pi].owner : INVALID;
+    RankState r;
+    r.jump = pr;
+    r.far = pr == INVALID ? t : pr;
+    r.acc = pr == INVALID ? 0 : tot[pr].acc;
+    r.cnt = pr == INVALID ? 0 : tot[pr].cnt;
+    r.mn = tot[t].mn;
+    if (pr != INVALID) r.mn = min(r.mn, tot[pr].mn);
+    r.pad0 = r.pad1 = 0;
+    st[t] = r;
+}
+
+// One jump for every ruler (grid-stride); *active counts the rulers whose
+// pointer is still set afterwards.
 __global__ void __launch_bounds__(512) rank_step_kernel(uint32_t n, const RankState* __restrict__ in,
                                                         RankState* __restrict__ out, uint32_t* __restrict__ active) {
     uint32_t still = 0;
@@ -82,25 +200,45 @@ __global__ void __launch_bounds__(512) rank_step_kernel(uint32_t n, const RankSt
     block_tally<uint32_t>(still, active);
 }
 
-__global__ void cycle_flags_kernel(uint32_t n, const RankState* __restrict__ st, uint8_t* __restrict__ cyc) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x < n) cyc[x] = st[x].member && st[x].jump != INVALID;
+// Member state = its ruler's + its place in the sublist.  jump stays set for
+// members of a cycle.
+__global__ void member_state_kernel(uint32_t m, const uint32_t* __restrict__ rul, const SubPos* __restrict__ loc,
+                                    const RankState* __restrict__ rs, RankState* __restrict__ st) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const SubPos l = loc[i];
+    const RankState r = rs[l.owner];
+    RankState o;
+    o.acc = r.acc + l.la;
+    o.jump = r.jump;
+    o.far = rul[r.far];
+    o.cnt = r.cnt + l.lc;
+    o.mn = min(r.mn, l.lm);
+    o.pad0 = o.pad1 = 0;
+    st[i] = o;
+}
+
+__global__ void cycle_flags_kernel(uint32_t m, const RankState* __restrict__ st, uint8_t* __restrict__ cyc) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) cyc[i] = st[i].jump != INVALID;
 }
 
 // Cycles are cut in parallel.  The reference walks each cycle from the
 // successor h of its first listed read r (the read visited first) round to
 // r, and cuts after the first read of largest offset met on the way.  Here:
-// (1) a temporary cut before h makes each cycle a chain h .. r;
+// (1) a temporary cut between r and h makes each cycle a chain h .. r;
 // (2) ranking that chain gives every read its walk position;
 // (3) the largest (offset, -position) over the chain picks the cut read;
 // (4) the temporary cut is undone and the real one made.
 
-// (1) r = the cycle read whose list index is the cycle's minimum.
-__global__ void cycle_open_kernel(uint32_t n, const RankState* __restrict__ st, const uint8_t* __restrict__ cyc,
-                                  const uint32_t* __restrict__ pos_in_ids, const uint32_t* __restrict__ nx,
-                                  uint32_t* pv, uint32_t* __restrict__ leader_of_head, uint32_t* __restrict__ err) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= n || !cyc[x] || st[x].mn != pos_in_ids[x]) return;
+// (1) r = the cycle member whose list index is the cycle's minimum (mn on a
+// cycle covers the whole cycle).
+__global__ void cycle_open_kernel(const uint32_t* __restrict__ ids, uint32_t m, const RankState* __restrict__ st,
+                                  const uint8_t* __restrict__ cyc, uint32_t* nx, uint32_t* pv,
+                                  uint32_t* __restrict__ leader_of_head, uint32_t* __restrict__ err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !cyc[i] || st[i].mn != i) return;
+    const uint32_t x = ids[i];
     const uint32_t h = nx[x];
     if (h == INVALID || pv[h] != x) {
         atomicExch(err, 1u);
@@ -108,37 +246,42 @@ __global__ void cycle_open_kernel(uint32_t n, const RankState* __restrict__ st, 
     }
     leader_of_head[h] = x;
     pv[h] = INVALID;
+    nx[x] = INVALID;
 }
 
 // (3) per chain head: max of (offset << 32 | ~position)
-__global__ void cycle_max_kernel(uint32_t n, const RankState* __restrict__ st, const uint8_t* __restrict__ cyc,
-                                 const uint16_t* __restrict__ offset, unsigned long long* __restrict__ best) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= n || !cyc[x]) return;
-    const unsigned long long key = (unsigned long long)offset[x] << 32 | (0xFFFFFFFFu - st[x].cnt);
-    atomicMax(&best[st[x].far], key);
+__global__ void cycle_max_kernel(const uint32_t* __restrict__ ids, uint32_t m, const RankState* __restrict__ st,
+                                 const uint8_t* __restrict__ cyc, const uint16_t* __restrict__ offset,
+                                 unsigned long long* __restrict__ best) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !cyc[i]) return;
+    const unsigned long long key = (unsigned long long)offset[ids[i]] << 32 | (0xFFFFFFFFu - st[i].cnt);
+    atomicMax(&best[st[i].far], key);
 }
 
 // (4) the read that holds its chain's maximum restores the temporary cut and
 // makes the real one after itself.
-__global__ void cycle_cut_kernel(uint32_t n, const RankState* __restrict__ st, const uint8_t* __restrict__ cyc,
-                                 const unsigned long long* __restrict__ best,
+__global__ void cycle_cut_kernel(const uint32_t* __restrict__ ids, uint32_t m, const RankState* __restrict__ st,
+                                 const uint8_t* __restrict__ cyc, const unsigned long long* __restrict__ best,
                                  const uint32_t* __restrict__ leader_of_head, uint32_t* nx, uint32_t* pv) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= n || !cyc[x]) return;
-    const uint32_t h = st[x].far;
-    if ((0xFFFFFFFFu - uint32_t(best[h] & 0xFFFFFFFFull)) != st[x].cnt) return;
-    pv[h] = leader_of_head[h];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !cyc[i]) return;
+    const uint32_t h = st[i].far;
+    if ((0xFFFFFFFFu - uint32_t(best[h] & 0xFFFFFFFFull)) != st[i].cnt) return;
+    const uint32_t r = leader_of_head[h];
+    pv[h] = r;
+    nx[r] = h;
+    const uint32_t x = ids[i];
     const uint32_t nh = nx[x];
     nx[x] = INVALID;
     pv[nh] = INVALID;
 }
 
-__global__ void chain_key_kernel(uint32_t n, const RankState* __restrict__ st, uint32_t* __restrict__ key) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    // mn covers the read and its predecessors, so the minimum over the
-    // chain's reads is the chain's first list index
-    if (x < n && st[x].member) atomicMin(&key[st[x].far], st[x].mn);
+// The chain's first list index, from its tail (whose mn covers the chain).
+__global__ void chain_key_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ nx,
+                                 const RankState* __restrict__ st, uint32_t* __restrict__ key) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m && nx[ids[i]] == INVALID) key[st[i].far] = st[i].mn;
 }
 
 __global__ void head_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ pv,
@@ -147,12 +290,13 @@ __global__ void head_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, 
     if (i < m) f[i] = pv[ids[i]] == INVALID;
 }
 
-__global__ void tail_sizes_kernel(uint32_t n, const uint32_t* __restrict__ nx, const RankState* __restrict__ st,
-                                  int L, uint64_t* __restrict__ chain_bases, uint32_t* __restrict__ chain_members) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= n || !st[x].member || nx[x] != INVALID) return;
-    chain_bases[st[x].far] = st[x].acc + uint64_t(L);
-    chain_members[st[x].far] = st[x].cnt + 1;
+__global__ void tail_sizes_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ nx,
+                                  const RankState* __restrict__ st, int L, uint64_t* __restrict__ chain_bases,
+                                  uint32_t* __restrict__ chain_members) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || nx[ids[i]] != INVALID) return;
+    chain_bases[st[i].far] = st[i].acc + uint64_t(L);
+    chain_members[st[i].far] = st[i].cnt + 1;
 }
 
 __global__ void gather_heads_kernel(const uint32_t* __restrict__ heads, uint32_t nh, const uint32_t* __restrict__ key,
@@ -182,7 +326,7 @@ __global__ void place_kernel(const uint32_t* __restrict__ ids, uint32_t m, const
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     const uint32_t x = ids[i];
-    const RankState r = st[x];
+    const RankState r = st[i];
     const uint32_t c = slot[r.far];
     const uint64_t pos = cpos[c] + r.acc;
     DevRecord d;
@@ -222,26 +366,72 @@ inline int rounds_for(uint32_t m) {
     return r + 1;
 }
 
-// Pointer jumping to convergence (early exit when no pointer is left, at
-// most enough rounds for a chain of every member).  Returns the final state
-// and, in *left, the number of reads whose pointer never cleared (cycles).
-RankState* run_ranking(uint32_t n, uint32_t m, const uint32_t* pv, const uint16_t* offset, const uint32_t* pos_in_ids,
-                       const uint8_t* redo, const RankState* keep, RankState* A, RankState* B, uint32_t* active,
-                       uint32_t* left, cudaStream_t s) {
-    const int g = grid_for(n, 256);
-    rank_init_kernel<<<g, 256, 0, s>>>(n, pv, offset, pos_in_ids, redo, keep, A);
+// Scratch of one ranking, sized for m members of n reads.
+struct RankScratch {
+    ChainNode* node;
+    SubPos* loc;
+    uint8_t* flags;
+    uint8_t* promote;
+    uint32_t* rul;
+    SubTotal* tot;
+    RankState* A;
+    RankState* B;
+    uint32_t* counts;  // [0] rulers, [1] unreached, [2] active
+};
+
+// Ranks every member: st[i] for list index i.  Returns the number of members
+// on cycles (jump still set).
+uint32_t rank_members(const uint32_t* ids, uint32_t m, uint32_t n, const uint32_t* nx, const uint32_t* pv,
+                      const uint16_t* offset, const uint32_t* pos_in_ids, RankScratch& k, RankState* st,
+                      Arena& a, cudaStream_t s) {
+    const int g = grid_for(m, 256);
+    const uint8_t* promote = nullptr;
+    uint32_t nr = 0;
+    CURC_CHECK(cudaMemsetAsync(k.node, 0xFF, size_t(n) * sizeof(ChainNode), s));
+    CURC_CHECK(cudaMemsetAsync(k.counts + 3, 0, 4, s));
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        ruler_flags_kernel<<<g, 256, 0, s>>>(ids, m, pv, promote, k.flags);
+        CURC_LAUNCH_CHECK();
+        select_flagged(ids, k.flags, k.rul, m, k.counts, a, s);
+        chain_nodes_kernel<<<g, 256, 0, s>>>(ids, m, nx, offset, k.node, k.loc);
+        CURC_LAUNCH_CHECK();
+        CURC_CHECK(cudaMemsetAsync(k.counts + 1, 0, 4, s));
+        nr = read_scalar(k.counts, s);
+        ruler_index_kernel<<<grid_for(nr, 256), 256, 0, s>>>(k.rul, nr, k.node);
+        CURC_LAUNCH_CHECK();
+        ruler_walk_kernel<<<resident_grid(ruler_walk_kernel, 256, nr), 256, 0, s>>>(k.rul, nr, m, n, k.node, k.loc,
+                                                                                    k.tot, k.counts + 3);
+        CURC_LAUNCH_CHECK();
+        unreached_kernel<<<resident_grid(unreached_kernel, 256, m), 256, 0, s>>>(m, k.loc, k.flags, k.counts + 1);
+        CURC_LAUNCH_CHECK();
+        uint32_t hc[4];
+        CURC_CHECK(cudaMemcpyAsync(hc, k.counts, 16, cudaMemcpyDeviceToHost, s));
+        CURC_CHECK(cudaStreamSynchronize(s));
+        if (hc[3]) throw std::runtime_error("assemble: a chain link leaves the member set");
+        if (hc[1] == 0) break;
+        if (attempt == 1) throw std::runtime_error("assemble: reads left unranked after promoting cycle rulers");
+        CURC_CHECK(cudaMemsetAsync(k.promote, 0, m, s));
+        promote_kernel<<<g, 256, 0, s>>>(ids, m, n, k.flags, nx, pos_in_ids, k.promote);
+        CURC_LAUNCH_CHECK();
+        promote = k.promote;
+    }
+    ruler_init_kernel<<<grid_for(nr, 256), 256, 0, s>>>(k.rul, nr, m, pv, pos_in_ids, k.loc, k.tot, k.A);
     CURC_LAUNCH_CHECK();
-    const int R = rounds_for(m);
-    *left = 0;
+    RankState* A = k.A;
+    RankState* B = k.B;
+    uint32_t left = 0;
+    const int R = rounds_for(nr);
     for (int t = 0; t < R; ++t) {
-        CURC_CHECK(cudaMemsetAsync(active, 0, 4, s));
-        rank_step_kernel<<<resident_grid(rank_step_kernel, 512, n), 512, 0, s>>>(n, A, B, active);
+        CURC_CHECK(cudaMemsetAsync(k.counts + 2, 0, 4, s));
+        rank_step_kernel<<<resident_grid(rank_step_kernel, 512, nr), 512, 0, s>>>(nr, A, B, k.counts + 2);
         CURC_LAUNCH_CHECK();
         std::swap(A, B);
-        *left = read_scalar(active, s);
-        if (*left == 0) break;
+        left = read_scalar(k.counts + 2, s);
+        if (left == 0) break;
     }
-    return A;
+    member_state_kernel<<<g, 256, 0, s>>>(m, k.rul, k.loc, A, st);
+    CURC_LAUNCH_CHECK();
+    return left;
 }
 
 }  // namespace
@@ -274,44 +464,46 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
     fill<uint32_t>(pos_in_ids, INVALID, n, s);
     scatter_index_kernel<<<g, 256, 0, s>>>(ids, m, pos_in_ids);
     CURC_LAUNCH_CHECK();
-    RankState* A = a.alloc<RankState>(n);
-    RankState* B = a.alloc<RankState>(n);
-    uint32_t* active = a.alloc<uint32_t>(4);
-    uint32_t left = 0;
     SubStage sp_rank("assembly.ranking");
-    RankState* R = run_ranking(n_total, m, pv, offset, pos_in_ids, nullptr, nullptr, A, B, active, &left, s);
+    RankScratch k;
+    k.node = a.alloc<ChainNode>(n);
+    k.loc = a.alloc<SubPos>(m);
+    k.flags = a.alloc<uint8_t>(m);
+    k.promote = a.alloc<uint8_t>(m);
+    k.rul = a.alloc<uint32_t>(m);
+    k.tot = a.alloc<SubTotal>(m);
+    k.A = a.alloc<RankState>(m);
+    k.B = a.alloc<RankState>(m);
+    k.counts = a.alloc<uint32_t>(4);
+    RankState* R = a.alloc<RankState>(m);
+    uint32_t left = rank_members(ids, m, n_total, nx, pv, offset, pos_in_ids, k, R, a, s);
     if (left) {
-        // cycles: cut each in parallel, then rank its reads again (the other
-        // reads keep their final state from the first ranking)
-        const int gn = grid_for(n, 256);
-        uint8_t* cyc = a.alloc<uint8_t>(n);
-        cycle_flags_kernel<<<gn, 256, 0, s>>>(n_total, R, cyc);
+        // cycles: cut each in parallel, then rank again
+        uint8_t* cyc = a.alloc<uint8_t>(m);
+        cycle_flags_kernel<<<g, 256, 0, s>>>(m, R, cyc);
         CURC_LAUNCH_CHECK();
         uint32_t* leader_of_head = a.alloc<uint32_t>(n);
         unsigned long long* best = a.alloc<unsigned long long>(n);
         CURC_CHECK(cudaMemsetAsync(best, 0, n * sizeof(unsigned long long), s));
-        CURC_CHECK(cudaMemsetAsync(active + 1, 0, 4, s));
-        cycle_open_kernel<<<gn, 256, 0, s>>>(n_total, R, cyc, pos_in_ids, nx, pv, leader_of_head, active + 1);
+        CURC_CHECK(cudaMemsetAsync(k.counts + 3, 0, 4, s));
+        cycle_open_kernel<<<g, 256, 0, s>>>(ids, m, R, cyc, nx, pv, leader_of_head, k.counts + 3);
         CURC_LAUNCH_CHECK();
-        if (read_scalar(active + 1, s)) throw std::runtime_error("assemble: broken cycle");
-        RankState* keep = R;
-        RankState* X = keep == A ? B : A;
-        RankState* Y = a.alloc<RankState>(n);
-        RankState* T = run_ranking(n_total, m, pv, offset, pos_in_ids, cyc, keep, X, Y, active, &left, s);
-        if (left) throw std::runtime_error("assemble: cycle still closed after its temporary cut");
-        cycle_max_kernel<<<gn, 256, 0, s>>>(n_total, T, cyc, offset, best);
+        if (read_scalar(k.counts + 3, s)) throw std::runtime_error("assemble: broken cycle");
+        RankState* T = a.alloc<RankState>(m);
+        if (rank_members(ids, m, n_total, nx, pv, offset, pos_in_ids, k, T, a, s))
+            throw std::runtime_error("assemble: cycle still closed after its temporary cut");
+        cycle_max_kernel<<<g, 256, 0, s>>>(ids, m, T, cyc, offset, best);
         CURC_LAUNCH_CHECK();
-        cycle_cut_kernel<<<gn, 256, 0, s>>>(n_total, T, cyc, best, leader_of_head, nx, pv);
+        cycle_cut_kernel<<<g, 256, 0, s>>>(ids, m, T, cyc, best, leader_of_head, nx, pv);
         CURC_LAUNCH_CHECK();
-        R = run_ranking(n_total, m, pv, offset, pos_in_ids, cyc, keep, X, Y, active, &left, s);
-        if (left) throw std::runtime_error("assemble: unresolved chain links after cutting cycles");
+        if (rank_members(ids, m, n_total, nx, pv, offset, pos_in_ids, k, R, a, s))
+            throw std::runtime_error("assemble: unresolved chain links after cutting cycles");
     }
     sp_rank.stop();
     SubStage sp_place("assembly.order_place");
     // chain order: first member in list order
     uint32_t* key = a.alloc<uint32_t>(n);
-    fill<uint32_t>(key, INVALID, n, s);
-    chain_key_kernel<<<grid_for(n, 256), 256, 0, s>>>(n_total, R, key);
+    chain_key_kernel<<<g, 256, 0, s>>>(ids, m, nx, R, key);
     CURC_LAUNCH_CHECK();
     uint8_t* hf = a.alloc<uint8_t>(m);
     head_flags_kernel<<<g, 256, 0, s>>>(ids, m, pv, hf);
@@ -326,7 +518,7 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
     radix_sort_pairs<uint32_t, uint32_t>(hkey, heads, nh, 0, 32, a, s);
     uint64_t* chain_bases = a.alloc<uint64_t>(n);
     uint32_t* chain_members = a.alloc<uint32_t>(n);
-    tail_sizes_kernel<<<grid_for(n, 256), 256, 0, s>>>(n_total, nx, R, L, chain_bases, chain_members);
+    tail_sizes_kernel<<<g, 256, 0, s>>>(ids, m, nx, R, L, chain_bases, chain_members);
     CURC_LAUNCH_CHECK();
     uint64_t* cpos = a.alloc<uint64_t>(nh + 1);
     uint32_t* crec = a.alloc<uint32_t>(nh + 1);

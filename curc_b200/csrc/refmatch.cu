@@ -36,23 +36,28 @@ struct Hit {
     uint64_t src, len, dst;
 };
 
-__device__ __forceinline__ uint32_t sym_word(const uint64_t* bits, uint64_t pos) {
-    // four symbols as ASCII bytes, little endian (memcpy of 4 chars)
-    uint32_t v = 0;
-#pragma unroll
-    for (int t = 0; t < 4; ++t) v |= uint32_t(uint8_t("ACGT"[code_at(bits, pos + t)])) << (8 * t);
-    return v;
+// The four bases of one byte of a packed word (first base in the top two
+// bits) as ASCII bytes, first base lowest: byte c of 'A','C','G','T' for each
+// code, selected with one byte permute.
+__device__ __forceinline__ uint32_t ascii4(uint32_t b) {
+    const uint32_t sel = (b >> 6) | ((b >> 4) & 3u) << 4 | ((b >> 2) & 3u) << 8 | (b & 3u) << 12;
+    return __byte_perm(0x54474341u, 0u, sel);
 }
 
-// maRushPrime1HashBinary<36> (compress.cu:597-615)
+// maRushPrime1HashBinary<36> (compress.cu:597-615): the 36 bases as nine
+// little-endian words of four ASCII characters, each plus its index, folded
+// by xor and multiply.
 __device__ __forceinline__ uint32_t marush_packed(const uint64_t* bits, uint64_t pos) {
+    const uint64_t x = word_unaligned(bits, pos, 32);
+    const uint32_t t = uint32_t(word_unaligned(bits, pos + 32, 4));
     uint64_t h = RM_K;
 #pragma unroll
-    for (uint32_t j = 0; j < RM_K / 4; ++j) {
-        uint32_t v = sym_word(bits, pos + 4 * j) + j;
-        h ^= v;
+    for (uint32_t j = 0; j < 8; ++j) {
+        h ^= ascii4(uint32_t(x >> (56 - 8 * j)) & 0xFFu) + j;
         h *= 171717;
     }
+    h ^= ascii4(t) + 8u;
+    h *= 171717;
     return uint32_t(h);
 }
 
@@ -119,53 +124,94 @@ __device__ __forceinline__ uint64_t match_left(const uint64_t* a, uint64_t ao, c
 }
 
 // Packed destination (reverse complemented, dl bases, zero padded): the
-// reference's probe of one destination position against one bucket.
-__device__ bool probe_packed(const RmIndex& ix, const uint64_t* dest, uint64_t dl, uint64_t dpad, uint64_t dpos,
-                             bool dest_is_ref, Hit* hit) {
+// reference's probe of one destination position against one bucket
+// (compress.cu:758-802).  A bucket entry is taken when the match through it
+// spans more than 50 bases and its whole 36-mer is equal; both tests are
+// required, so the 36-mer is compared first, and the span test needs at most
+// 15 bases of extension on each side (36 + right + left + 1 > 50).  Returns
+// the source position of the first entry taken.
+__device__ bool probe_candidate(const RmIndex& ix, const uint64_t* dest, uint64_t dl, uint64_t dpad, uint64_t dpos,
+                                bool dest_is_ref, uint64_t* spos_out) {
     const uint32_t h = marush_packed(dest, dpos) & ix.mask;
     const uint32_t b = ix.kr[h], e = ix.kr[h + 1];
+    if (b == e) return false;
+    const uint64_t k32 = word_unaligned(dest, dpos, 32), k4 = word_unaligned(dest, dpos + 32, 4);
+    const uint64_t d0 = dpos + RM_K;
+    const uint64_t dlim = d0 <= dl ? dl - d0 : dpad - d0;  // bases readable on the dest side
     for (uint32_t j = b; j < e; ++j) {
         const uint64_t spos = uint64_t(ix.pos[j]) * RM_SRC_STEP;
         if (dest_is_ref && (dl - spos < dpos)) continue;
-        // right: p1 from dpos+36 (never equal to dl when it starts beyond it)
-        const uint64_t d0 = dpos + RM_K, s0 = spos + RM_K;
-        uint64_t dlim = d0 <= dl ? dl - d0 : dpad - d0;  // bases readable on the dest side
+        if (word_unaligned(ix.ref, spos, 32) != k32 || word_unaligned(ix.ref, spos + 32, 4) != k4) continue;
+        const uint64_t s0 = spos + RM_K;
         const uint64_t slim = s0 <= ix.rl ? ix.rl - s0 : 0;
-        const uint64_t run = match_right(dest, d0, ix.ref, s0, min(dlim, slim));
-        const uint64_t right = d0 + run;
-        // left
+        const uint64_t run = match_right(dest, d0, ix.ref, s0, min(min(dlim, slim), uint64_t(15)));
         const uint64_t lmax = min(dpos, spos);
-        const uint64_t k = match_left(dest, dpos, ix.ref, spos, lmax);
-        const uint64_t p1 = k < lmax ? dpos - 1 - k : dpos - k;
-        const uint64_t p2 = k < lmax ? spos - 1 - k : spos - k;
-        if (right - p1 > uint64_t(RM_MIN)) {
-            if (word_unaligned(dest, dpos, 32) != word_unaligned(ix.ref, spos, 32)) continue;
-            if (word_unaligned(dest, dpos + 32, 4) == word_unaligned(ix.ref, spos + 32, 4)) {
-                hit->src = p2 + 1;
-                hit->len = right - p1 - 1;
-                hit->dst = p1 + 1;
-                return true;
-            }
+        const uint64_t k = match_left(dest, dpos, ix.ref, spos, min(lmax, uint64_t(15)));
+        if (run + k + (k < lmax ? 1 : 0) + RM_K > uint64_t(RM_MIN)) {
+            *spos_out = spos;
+            return true;
         }
     }
     return false;
 }
 
-__global__ void probe_segments_kernel(RmIndex ix, const uint64_t* __restrict__ dest, uint64_t dl, uint64_t dpad,
-                                      uint64_t dic, uint64_t segs, bool dest_is_ref, uint8_t* __restrict__ flag,
-                                      Hit* __restrict__ hits) {
-    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < segs; i += uint64_t(gridDim.x) * blockDim.x) {
-        uint8_t f = 0;
-        for (uint64_t s = 0; s < 4; ++s) {
-            Hit h;
-            if (probe_packed(ix, dest, dl, dpad, (i * 4 + s) * RM_DEST_STEP, dest_is_ref, &h)) {
-                hits[i] = h;
-                f = 1;
-                break;
-            }
+// The maximal match through an accepted probe: extended right from the end
+// of the 36-mer and left from its start, as the reference does.
+__device__ Hit extend_full(const RmIndex& ix, const uint64_t* dest, uint64_t dl, uint64_t dpad, uint64_t dpos,
+                           uint64_t spos) {
+    const uint64_t d0 = dpos + RM_K, s0 = spos + RM_K;
+    const uint64_t dlim = d0 <= dl ? dl - d0 : dpad - d0;
+    const uint64_t slim = s0 <= ix.rl ? ix.rl - s0 : 0;
+    const uint64_t right = d0 + match_right(dest, d0, ix.ref, s0, min(dlim, slim));
+    const uint64_t lmax = min(dpos, spos);
+    const uint64_t k = match_left(dest, dpos, ix.ref, spos, lmax);
+    const uint64_t p1 = k < lmax ? dpos - 1 - k : dpos - k;
+    const uint64_t p2 = k < lmax ? spos - 1 - k : spos - k;
+    return Hit{p2 + 1, right - p1 - 1, p1 + 1};
+}
+
+// One thread per probe; the four probes of a segment sit in four adjacent
+// lanes and the segment takes its first accepting probe (the reference's
+// segment stops at its first hit, compress.cu:746-807).  cand[seg] = (dest, source) position.
+__global__ void __launch_bounds__(256) probe_segments_kernel(RmIndex ix, const uint64_t* __restrict__ dest, uint64_t dl,
+                                                             uint64_t dpad, uint64_t segs, bool dest_is_ref,
+                                                             uint8_t* __restrict__ flag,
+                                                             ulonglong2* __restrict__ cand) {
+    const uint64_t P = segs * 4;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    // lanes of a warp share i - lane, so the warp stays converged for the ballot
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i - lane < P; i += stride) {
+        uint64_t sp = 0;
+        const bool hit = i < P && probe_candidate(ix, dest, dl, dpad, i * RM_DEST_STEP, dest_is_ref, &sp);
+        const uint32_t g = (__ballot_sync(0xFFFFFFFFu, hit) >> (lane & ~3u)) & 0xFu;
+        if (i < P) {
+            if ((lane & 3u) == 0) flag[i >> 2] = g != 0;
+            if (g && (lane & 3u) == uint32_t(__ffs(g) - 1)) cand[i >> 2] = make_ulonglong2(i * RM_DEST_STEP, sp);
         }
-        flag[i] = f;
-        (void)dic;
+    }
+}
+
+// Segment j lies in the same maximal match as segment j-1: both accepted a
+// probe on the same diagonal (source - dest), and their 36-mers, at most 21
+// bases apart, overlap, so extending either gives the same span (both right
+// limits are the destination end).
+__device__ __forceinline__ bool rm_follows(const uint8_t* flag, const ulonglong2* cand, uint64_t j, uint64_t dl) {
+    if (j == 0 || !flag[j - 1]) return false;
+    const ulonglong2 c = cand[j], p = cand[j - 1];
+    return c.x + RM_K <= dl && c.y - c.x == p.y - p.x;
+}
+
+// The first segment of each run extends its match once and writes the hit
+// for the whole run.
+__global__ void extend_runs_kernel(RmIndex ix, const uint64_t* __restrict__ dest, uint64_t dl, uint64_t dpad,
+                                   uint64_t segs, const uint8_t* __restrict__ flag,
+                                   const ulonglong2* __restrict__ cand, Hit* __restrict__ hits) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < segs; i += uint64_t(gridDim.x) * blockDim.x) {
+        if (!flag[i] || rm_follows(flag, cand, i, dl)) continue;
+        const Hit h = extend_full(ix, dest, dl, dpad, cand[i].x, cand[i].y);
+        hits[i] = h;
+        for (uint64_t j = i + 1; j < segs && flag[j] && rm_follows(flag, cand, j, dl); ++j) hits[j] = h;
     }
 }
 
@@ -435,8 +481,11 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
         CURC_CHECK(cudaMemsetAsync(packed, 0, words * 8, s));
         pack_ascii_ref(rc, dl, packed, s);
         const uint64_t dpad = (words - 1) * 32;
-        probe_segments_kernel<<<grid_for(nslots, 128), 128, 0, s>>>(ix, packed, dl, dpad, dic, nslots, dest_is_ref,
-                                                                    flag, hits);
+        ulonglong2* cand = a.alloc<ulonglong2>(nslots);
+        probe_segments_kernel<<<resident_grid(probe_segments_kernel, 256, nslots * 4), 256, 0, s>>>(
+            ix, packed, dl, dpad, nslots, dest_is_ref, flag, cand);
+        CURC_LAUNCH_CHECK();
+        extend_runs_kernel<<<grid_for(nslots, 256), 256, 0, s>>>(ix, packed, dl, dpad, nslots, flag, cand, hits);
     } else {
         CURC_CHECK(cudaMemsetAsync(rc + dl, 0, 64, s));
         probe_ascii_kernel<<<grid_for(nslots, 128), 128, 0, s>>>(ix, rc, dl, dic, flag, hits);
