@@ -15,6 +15,7 @@
 // (1) is done as a parallel stable merge of the per-symbol runs: each
 // element's output position is its rank in its run plus, for every other
 // run, the number of elements that precede it (binary search).
+#include "compact.cuh"
 #include "stages.cuh"
 
 namespace curc {
@@ -55,11 +56,12 @@ struct AsciiAcc {
 };
 
 template <class Acc>
-__global__ void run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf, uint32_t m, int off,
-                                  uint32_t* __restrict__ bounds) {
+__global__ void run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf, const uint32_t* __restrict__ m_dev,
+                                  int off, uint32_t* __restrict__ bounds) {
     // bounds[c] = first index whose symbol at off-1 is >= c
     const int c = threadIdx.x;
     if (c > Acc::ALPHA) return;
+    const uint32_t m = *m_dev;
     uint32_t lo = 0, count = m;
     while (count > 0) {
         uint32_t step = count / 2, it = lo + step;
@@ -73,15 +75,12 @@ __global__ void run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf, uin
     bounds[c] = c == Acc::ALPHA ? m : lo;
 }
 
-// Stable merge of the symbol runs by read[off, L).
+// Output position of element i: its rank in its symbol run plus, for every
+// other run, the number of that run's elements that precede it.
 template <class Acc>
-__global__ void merge_runs_kernel(Acc acc, const uint32_t* __restrict__ suf, uint32_t m, int off,
-                                  const uint32_t* __restrict__ bounds, uint32_t* __restrict__ out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    uint32_t bd[Acc::ALPHA + 1];
-#pragma unroll
-    for (int c = 0; c <= Acc::ALPHA; ++c) bd[c] = bounds[c];
+__device__ __forceinline__ void merge_one(const Acc& acc, const uint32_t* __restrict__ suf, int off,
+                                          const uint32_t (&bd)[Acc::ALPHA + 1], uint32_t i,
+                                          uint32_t* __restrict__ out) {
     int x = 0;
     while (x + 1 <= Acc::ALPHA && bd[x + 1] <= i) ++x;
     const uint32_t me = suf[i];
@@ -107,13 +106,24 @@ __global__ void merge_runs_kernel(Acc acc, const uint32_t* __restrict__ suf, uin
     out[pos] = me;
 }
 
+// Stable merge of the symbol runs by read[off, L).
+template <class Acc>
+__global__ void merge_runs_kernel(Acc acc, const uint32_t* __restrict__ suf, const uint32_t* __restrict__ m_dev,
+                                  int off, const uint32_t* __restrict__ bounds, uint32_t* __restrict__ out) {
+    const uint32_t m = *m_dev;
+    uint32_t bd[Acc::ALPHA + 1];
+#pragma unroll
+    for (int c = 0; c <= Acc::ALPHA; ++c) bd[c] = bounds[c];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+        merge_one(acc, suf, off, bd, i, out);
+}
+
 // One thread per run of equal suffix strings: the reference's bucket merge
 // restricted to that run (compress.cu:1089-1160 / 1297-1336).
 template <class Acc>
-__global__ void merge_groups_kernel(Acc acc, uint32_t* pre, uint32_t mp, const uint32_t* __restrict__ suf,
-                                    uint32_t ms, int off, uint32_t* next, uint32_t* prev, uint16_t* offset) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ms) return;
+__device__ __forceinline__ void group_one(const Acc& acc, uint32_t* pre, uint32_t mp,
+                                          const uint32_t* __restrict__ suf, uint32_t ms, int off, uint32_t j,
+                                          uint32_t* next, uint32_t* prev, uint16_t* offset) {
     const int len = acc.L - off;
     const uint32_t s0 = suf[j];
     if (j > 0 && acc.cmp(suf[j - 1], off, s0, off, len) == 0) return;
@@ -167,12 +177,32 @@ __global__ void merge_groups_kernel(Acc acc, uint32_t* pre, uint32_t mp, const u
     }
 }
 
-__global__ void keep_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ link,
-                                  uint8_t* __restrict__ keep) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) keep[i] = link[ids[i]] == INVALID;
+template <class Acc>
+__global__ void merge_groups_kernel(Acc acc, uint32_t* pre, const uint32_t* __restrict__ mp_dev,
+                                    const uint32_t* __restrict__ suf, const uint32_t* __restrict__ ms_dev, int off,
+                                    uint32_t* next, uint32_t* prev, uint16_t* offset) {
+    const uint32_t mp = *mp_dev, ms = *ms_dev;
+    if (mp == 0) return;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ms; j += gridDim.x * blockDim.x)
+        group_one(acc, pre, mp, suf, ms, off, j, next, prev, offset);
 }
 
+// Compaction functors: keep the list entries whose link is still free.
+struct FreeLink {
+    const uint32_t* ids;
+    const uint32_t* link;
+    __device__ bool operator()(uint32_t i) const { return link[ids[i]] == INVALID; }
+};
+struct MoveId {
+    const uint32_t* in;
+    uint32_t* out;
+    __device__ void operator()(uint32_t i, uint32_t d) const { out[d] = in[i]; }
+};
+
+// The passes are queued without a host round trip: list lengths stay on
+// the device (two slots per list, read by one pass and written by its
+// compaction), kernels walk them with resident grids, and the host looks at
+// the lengths only every few passes to stop early once a list is empty.
 template <class Acc>
 void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt, uint32_t* next, uint32_t* prev,
                      uint16_t* offset, Arena& a, cudaStream_t s) {
@@ -180,35 +210,43 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     auto mk = a.mark();
     uint32_t* suf2 = a.alloc<uint32_t>(cnt);
     uint32_t* tmp = a.alloc<uint32_t>(cnt);
-    uint8_t* keep = a.alloc<uint8_t>(cnt);
     uint32_t* bounds = a.alloc<uint32_t>(8);
-    uint32_t* counts = a.alloc<uint32_t>(2);
-    uint32_t mp = cnt, ms = cnt;
-    for (int off = 1; off < acc.L && mp > 0 && ms > 0; ++off) {
+    uint32_t* len = a.alloc<uint32_t>(4);  // mp, ms for even passes, then for odd passes
+    const uint32_t init[4] = {cnt, cnt, 0, 0};
+    CURC_CHECK(cudaMemcpyAsync(len, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    Compactor cp(cnt, a, s);
+    const int gm = resident_grid(merge_runs_kernel<Acc>, 256, cnt);
+    const int gg = resident_grid(merge_groups_kernel<Acc>, 128, cnt);
+    constexpr int CHECK_EVERY = 8;
+    int par = 0;
+    for (int off = 1; off < acc.L; ++off, par ^= 1) {
+        uint32_t* mp_in = len + 2 * par;
+        uint32_t* ms_in = mp_in + 1;
+        uint32_t* mp_out = len + 2 * (par ^ 1);
+        uint32_t* ms_out = mp_out + 1;
         SubStage sp_merge("full_match.resort");
-        run_bounds_kernel<Acc><<<1, 32, 0, s>>>(acc, suf, ms, off, bounds);
+        run_bounds_kernel<Acc><<<1, 32, 0, s>>>(acc, suf, ms_in, off, bounds);
         CURC_LAUNCH_CHECK();
-        merge_runs_kernel<Acc><<<grid_for(ms, 256), 256, 0, s>>>(acc, suf, ms, off, bounds, suf2);
+        merge_runs_kernel<Acc><<<gm, 256, 0, s>>>(acc, suf, ms_in, off, bounds, suf2);
         CURC_LAUNCH_CHECK();
         sp_merge.stop();
         SubStage sp_groups("full_match.groups");
-        merge_groups_kernel<Acc><<<grid_for(ms, 128), 128, 0, s>>>(acc, pre, mp, suf2, ms, off, next, prev, offset);
+        merge_groups_kernel<Acc><<<gg, 128, 0, s>>>(acc, pre, mp_in, suf2, ms_in, off, next, prev, offset);
+        CURC_LAUNCH_CHECK();
         sp_groups.stop();
         SubStage sp_comp("full_match.compact");
-        CURC_LAUNCH_CHECK();
-        keep_flags_kernel<<<grid_for(mp, 256), 256, 0, s>>>(pre, mp, prev, keep);
-        CURC_LAUNCH_CHECK();
-        select_flagged(pre, keep, tmp, mp, counts + 0, a, s);
-        CURC_CHECK(cudaMemcpyAsync(pre, tmp, size_t(mp) * 4, cudaMemcpyDeviceToDevice, s));
-        keep_flags_kernel<<<grid_for(ms, 256), 256, 0, s>>>(suf2, ms, next, keep);
-        CURC_LAUNCH_CHECK();
-        select_flagged(suf2, keep, suf, ms, counts + 1, a, s);
-        uint32_t hc[2];
-        CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
-        CURC_CHECK(cudaStreamSynchronize(s));
-        mp = hc[0];
-        ms = hc[1];
+        cp.run(mp_in, cnt, mp_out, FreeLink{pre, prev}, MoveId{pre, tmp});
+        std::swap(pre, tmp);
+        cp.run(ms_in, cnt, ms_out, FreeLink{suf2, next}, MoveId{suf2, suf});
+        sp_comp.stop();
+        if (off % CHECK_EVERY == 0) {
+            uint32_t h[2];
+            CURC_CHECK(cudaMemcpyAsync(h, mp_out, 8, cudaMemcpyDeviceToHost, s));
+            CURC_CHECK(cudaStreamSynchronize(s));
+            if (h[0] == 0 || h[1] == 0) break;
+        }
     }
+    cp.check();
     a.release(mk);
 }
 

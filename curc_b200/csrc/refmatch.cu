@@ -15,13 +15,15 @@
 // first `capacity` in probe order.  The index buckets hold the first 12
 // positions (as in mapper.cu).
 //
-// B200 design: one thread per segment (packed) or per probe (ASCII); the
+// B200 design: one thread per probe, the four probes of a segment in
+// adjacent lanes; the 36-mer is compared before the match is extended, and
+// a maximal match met by a run of consecutive segments is extended once; the
 // extensions compare 32 bases per step with XOR and count-leading-zeros
 // instead of one base per step; the triples are ordered with three stable
-// radix passes; the acceptance decisions (each depends on the end of the
-// previous kept span) are taken by one thread reading shared-memory tiles,
-// and the map streams and the string compaction are built in parallel from
-// scans over the kept spans.
+// radix passes; the acceptance walk (each decision depends on the end of the
+// previous kept span) is rewritten as a successor chain followed by binary
+// lifting; the map streams and the string compaction are built in parallel
+// from scans over the kept spans.
 #include <cstring>
 
 #include "block.cuh"
@@ -296,56 +298,84 @@ __global__ void compact_hits_kernel(const Hit* __restrict__ in, const uint32_t* 
 }
 
 // compress.cu:946-992, the acceptance walk over the sorted distinct hits:
-// a hit starting before the end of the last kept span is trimmed (or
-// dropped when covered); it is kept when 50 or more bases remain.  The walk
-// carries one value (the end of the last kept span) from hit to hit, so one
-// thread decides; the block stages 2048 hits at a time in shared memory so
-// that thread reads only shared memory.  Everything else is parallel.
-constexpr int ACCEPT_CHUNK = 2048;
+// a hit starting before the end `pos` of the last kept span is trimmed to
+// start there (or dropped when covered), and kept when 50 or more bases
+// remain; a kept hit sets pos to its end.  Trimming keeps the end, so with
+// end_i = dst_i + len_i, hit i is kept iff len_i >= 50 and end_i >= pos + 50,
+// and then pos = end_i.  The kept hits are therefore the chain
+//   start -> nxt(start) -> nxt(nxt(start)) -> ...
+// where nxt(j) is the first i > j with len_i >= 50 and end_i >= end_j + 50
+// (the start has end 0).  nxt is found for every hit at once by descending
+// a sparse table of range maxima of the eligible ends, and the chain is
+// followed by binary lifting, so no step is sequential.  Node c is the
+// start and c + 1 the end of the chain.
 
-__global__ void __launch_bounds__(1024) accept_decide_kernel(const Hit* __restrict__ h, uint32_t c,
-                                                             uint8_t* __restrict__ kept, uint64_t* __restrict__ adst,
-                                                             uint64_t* __restrict__ alen) {
-    __shared__ uint64_t sdst[ACCEPT_CHUNK], slen[ACCEPT_CHUNK];
-    __shared__ uint8_t skept[ACCEPT_CHUNK];
-    uint64_t pos = 0;  // meaningful in thread 0 only
-    for (uint32_t base = 0; base < c; base += ACCEPT_CHUNK) {
-        const uint32_t cnt = min(uint32_t(ACCEPT_CHUNK), c - base);
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-            sdst[i] = h[base + i].dst;
-            slen[i] = h[base + i].len;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (uint32_t i = 0; i < cnt; ++i) {
-                uint64_t d = sdst[i], l = slen[i];
-                uint8_t k = 0;
-                if (d < pos) {
-                    const uint64_t ov = pos - d;
-                    if (ov >= l) {
-                        l = 0;
-                    } else {
-                        l -= ov;
-                        d += ov;
-                    }
-                }
-                if (l >= uint64_t(RM_MIN)) {
-                    k = 1;
-                    pos = d + l;
-                }
-                sdst[i] = d;
-                slen[i] = l;
-                skept[i] = k;
-            }
-        }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-            kept[base + i] = skept[i];
-            adst[base + i] = sdst[i];
-            alen[base + i] = slen[i];
-        }
-        __syncthreads();
+// eligible ends: level 0 of the range-maximum table
+__global__ void accept_ends_kernel(const Hit* __restrict__ h, uint32_t c, uint64_t* __restrict__ m0) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c) m0[i] = h[i].len >= uint64_t(RM_MIN) ? h[i].dst + h[i].len : 0;
+}
+
+// level k from level k-1: maxima of [i, i + 2^k), valid where i + 2^k <= c
+__global__ void range_max_kernel(const uint64_t* __restrict__ prev, uint32_t c, uint32_t half,
+                                 uint64_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c) out[i] = i + half < c ? max(prev[i], prev[i + half]) : prev[i];
+}
+
+__global__ void accept_next_kernel(const Hit* __restrict__ h, const uint64_t* __restrict__ M, uint32_t c, int levels,
+                                   uint32_t* __restrict__ J0) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u > c + 1) return;
+    if (u == c + 1) {
+        J0[u] = c + 1;
+        return;
     }
+    uint32_t p;
+    uint64_t T;
+    if (u == c) {
+        p = 0;
+        T = RM_MIN;
+    } else if (h[u].len < uint64_t(RM_MIN)) {
+        J0[u] = c + 1;  // never kept, never followed
+        return;
+    } else {
+        p = u + 1;
+        T = h[u].dst + h[u].len + RM_MIN;
+    }
+    // skip the longest run of ends below T: its length bit by bit
+    for (int k = levels - 1; k >= 0; --k)
+        if (uint64_t(p) + (1ull << k) <= c && M[uint64_t(k) * c + p] < T) p += 1u << k;
+    J0[u] = p < c ? p : c + 1;
+}
+
+__global__ void lift_square_kernel(const uint32_t* __restrict__ Jk, uint32_t nodes, uint32_t* __restrict__ Jn) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < nodes) Jn[u] = Jk[Jk[u]];
+}
+
+__device__ __forceinline__ uint32_t lift(const uint32_t* J, uint32_t nodes, uint32_t u, uint32_t t) {
+    for (int k = 0; t; ++k, t >>= 1)
+        if (t & 1u) u = J[uint64_t(k) * nodes + u];
+    return u;
+}
+
+// The t-th kept hit (t >= 1) and its trimmed start.
+__global__ void accept_chain_kernel(const Hit* __restrict__ h, uint32_t c, const uint32_t* __restrict__ J,
+                                    uint8_t* __restrict__ kept, uint64_t* __restrict__ adst,
+                                    uint64_t* __restrict__ alen) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (t > c) return;
+    const uint32_t nodes = c + 2;
+    const uint32_t i = lift(J, nodes, c, t);
+    if (i >= c) return;  // the chain is shorter than t
+    const uint32_t pr = lift(J, nodes, c, t - 1);
+    const uint64_t pos = pr == c ? 0 : h[pr].dst + h[pr].len;
+    const uint64_t end = h[i].dst + h[i].len;
+    const uint64_t d = max(h[i].dst, pos);
+    kept[i] = 1;
+    adst[i] = d;
+    alen[i] = end - d;
 }
 
 __device__ __forceinline__ uint32_t frugal_size(uint64_t v) {
@@ -529,8 +559,31 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
     uint8_t* keptf = a.alloc<uint8_t>(cu);
     uint64_t* adst = a.alloc<uint64_t>(cu);
     uint64_t* alen = a.alloc<uint64_t>(cu);
-    accept_decide_kernel<<<1, 1024, 0, s>>>(uniq, cu, keptf, adst, alen);
-    CURC_LAUNCH_CHECK();
+    {
+        int levels = 1;  // range-maximum levels: 2^(levels-1) <= cu
+        while ((2ull << (levels - 1)) <= cu) ++levels;
+        int lifts = 1;   // lifting levels: 2^lifts > cu
+        while ((1ull << lifts) <= cu) ++lifts;
+        const uint32_t nodes = cu + 2;
+        uint64_t* M = a.alloc<uint64_t>(uint64_t(levels) * cu);
+        uint32_t* J = a.alloc<uint32_t>(uint64_t(lifts) * nodes);
+        const int gc = grid_for(cu, 256), gn = grid_for(nodes, 256);
+        accept_ends_kernel<<<gc, 256, 0, s>>>(uniq, cu, M);
+        CURC_LAUNCH_CHECK();
+        for (int k = 1; k < levels; ++k) {
+            range_max_kernel<<<gc, 256, 0, s>>>(M + uint64_t(k - 1) * cu, cu, 1u << (k - 1), M + uint64_t(k) * cu);
+            CURC_LAUNCH_CHECK();
+        }
+        accept_next_kernel<<<gn, 256, 0, s>>>(uniq, M, cu, levels, J);
+        CURC_LAUNCH_CHECK();
+        for (int k = 1; k < lifts; ++k) {
+            lift_square_kernel<<<gn, 256, 0, s>>>(J + uint64_t(k - 1) * nodes, nodes, J + uint64_t(k) * nodes);
+            CURC_LAUNCH_CHECK();
+        }
+        CURC_CHECK(cudaMemsetAsync(keptf, 0, cu, s));
+        accept_chain_kernel<<<gc, 256, 0, s>>>(uniq, cu, J, keptf, adst, alen);
+        CURC_LAUNCH_CHECK();
+    }
     uint32_t* ksel = a.alloc<uint32_t>(cu);
     select_indices(keptf, ksel, cu, cnt + 2, a, s);
     const uint32_t K = read_scalar(cnt + 2, s);
