@@ -145,8 +145,9 @@ def run_ours(a, rank, world):
         dev_step()
     stage_names = ["pack", "sort_dedupe", "overlap", "chain_filter", "full_match", "assembly", "mapping", "emit",
                    "unmapped_refs", "refmatch"]
-    sub_names = ["sort_dedupe.radix", "overlap.index", "overlap.probe_resolve", "overlap.contested", "overlap.compact",
-                 "full_match.resort", "full_match.groups", "full_match.compact", "assembly.ranking",
+    sub_names = ["sort_dedupe.radix", "overlap.index", "overlap.index_sort", "overlap.index_mask",
+                 "overlap.probe_resolve", "overlap.filter", "overlap.probe", "overlap.resolve", "overlap.compact",
+                 "full_match.resort", "full_match.groups", "full_match.compact", "assembly.ranking", "assembly.walk", "assembly.jump",
                  "assembly.order_place", "mapping.index_fwd", "mapping.map_fwd", "mapping.index_rc", "mapping.map_rc",
                  "refmatch.index", "refmatch.probe_unmapped", "refmatch.probe_self", "refmatch.sort_unique",
                  "refmatch.accept"]

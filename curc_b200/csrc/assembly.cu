@@ -387,6 +387,7 @@ uint32_t rank_members(const uint32_t* ids, uint32_t m, uint32_t n, const uint32_
     const int g = grid_for(m, 256);
     const uint8_t* promote = nullptr;
     uint32_t nr = 0;
+    SubStage sp_walk("assembly.walk");
     CURC_CHECK(cudaMemsetAsync(k.node, 0xFF, size_t(n) * sizeof(ChainNode), s));
     CURC_CHECK(cudaMemsetAsync(k.counts + 3, 0, 4, s));
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -415,6 +416,8 @@ uint32_t rank_members(const uint32_t* ids, uint32_t m, uint32_t n, const uint32_
         CURC_LAUNCH_CHECK();
         promote = k.promote;
     }
+    sp_walk.stop();
+    SubStage sp_jump("assembly.jump");
     ruler_init_kernel<<<grid_for(nr, 256), 256, 0, s>>>(k.rul, nr, m, pv, pos_in_ids, k.loc, k.tot, k.A);
     CURC_LAUNCH_CHECK();
     RankState* A = k.A;

@@ -1,7 +1,7 @@
 // Stable compaction in one launch, with the item count read on the device.
 //
 // Tiles of CP_TILE items are taken in order from an atomic counter; each
-// tile ranks its kept items with warp ballots, publishes its count, and
+// tile ranks its kept items with one block scan, publishes its count, and
 // finds its output offset by looking back over the tiles before it
 // (decoupled look-back: a predecessor publishes its own count at once and
 // its inclusive offset as soon as it knows it).  Because the count is read
@@ -30,6 +30,8 @@ __device__ __forceinline__ uint64_t cp_pack(uint32_t epoch, uint32_t flag, uint3
 }
 
 // keep(i) -> bool for item i < n; move(i, dst) places kept item i at dst.
+// Each thread takes CP_ITEMS consecutive items; one block scan ranks them;
+// warp 0 looks back over 32 predecessor tiles per step.
 template <class Keep, class Move>
 __global__ void __launch_bounds__(CP_THREADS) compact_kernel(const uint32_t* __restrict__ n_dev,
                                                              uint32_t* __restrict__ n_out, Keep keep, Move move,
@@ -46,67 +48,83 @@ __global__ void __launch_bounds__(CP_THREADS) compact_kernel(const uint32_t* __r
     const uint64_t start = uint64_t(tile) * CP_TILE;
     if (start >= n && tile != 0) return;  // beyond the items; nobody looks back at it
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t rank[CP_ITEMS];
-    uint32_t kept = 0;  // bit r: item r of this thread is kept
-    uint32_t local = 0;
+    const uint64_t first = start + uint64_t(threadIdx.x) * CP_ITEMS;
+    uint32_t kept = 0;  // bit r: item first + r is kept
 #pragma unroll
     for (int r = 0; r < CP_ITEMS; ++r) {
-        const uint64_t i = start + uint64_t(r) * CP_THREADS + threadIdx.x;
-        const bool k = i < n && keep(uint32_t(i));
-        const uint32_t b = __ballot_sync(0xFFFFFFFFu, k);
-        if (lane == 0) s_warp[warp] = __popc(b);
-        __syncthreads();
-        uint32_t before = 0, total = 0;
-#pragma unroll
-        for (int w = 0; w < CP_THREADS / 32; ++w) {
-            const uint32_t c = s_warp[w];
-            before += w < int(warp) ? c : 0;
-            total += c;
-        }
-        rank[r] = local + before + __popc(b & ((1u << lane) - 1u));
-        kept |= uint32_t(k) << r;
-        local += total;
-        __syncthreads();
+        const uint64_t i = first + r;
+        if (i < n && keep(uint32_t(i))) kept |= 1u << r;
     }
-    if (threadIdx.x == 0) {
+    // block-wide exclusive scan of the per-thread counts
+    const uint32_t mine = __popc(kept);
+    uint32_t incl = mine;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= uint32_t(d)) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0, local = 0;
+#pragma unroll
+    for (int w = 0; w < CP_THREADS / 32; ++w) {
+        const uint32_t c = s_warp[w];
+        before += w < int(warp) ? c : 0;
+        local += c;
+    }
+    const uint32_t rank = before + incl - mine;
+    if (warp == 0) {
         uint32_t excl = 0;
+        const uint32_t ep = epoch & 0x3FFFFFFFu;
         if (tile == 0) {
-            atomicExch(&tiles[0], cp_pack(epoch, 2, local));
+            if (lane == 0) atomicExch(&tiles[0], cp_pack(epoch, 2, local));
         } else {
-            atomicExch(&tiles[tile], cp_pack(epoch, 1, local));
-            uint32_t j = tile - 1;
+            if (lane == 0) atomicExch(&tiles[tile], cp_pack(epoch, 1, local));
+            // window of up to 32 predecessors: lane l reads tile (top - l)
+            int64_t top = int64_t(tile) - 1;
             bool ok = true;
             while (true) {
-                uint64_t v = 0;
+                const int64_t j = top - int64_t(lane);
+                uint64_t v = cp_pack(epoch, 2, 0);  // lanes past tile 0 add nothing
                 uint32_t spins = 0;
-                for (;;) {
-                    v = *reinterpret_cast<volatile unsigned long long*>(&tiles[j]);
-                    if ((v >> 34) == (epoch & 0x3FFFFFFFu) && ((v >> 32) & 3u) != 0) break;
-                    if (++spins >= CP_WAIT_LIMIT) break;
-                    __nanosleep(64);
+                if (j >= 0) {
+                    for (;;) {
+                        v = *reinterpret_cast<volatile unsigned long long*>(&tiles[j]);
+                        if ((v >> 34) == ep && ((v >> 32) & 3u) != 0) break;
+                        if (++spins >= CP_WAIT_LIMIT) break;
+                        __nanosleep(64);
+                    }
                 }
-                if (spins >= CP_WAIT_LIMIT) {
-                    atomicExch(err, 1u);
+                if (__any_sync(0xFFFFFFFFu, spins >= CP_WAIT_LIMIT)) {
                     ok = false;
                     break;
                 }
-                excl += uint32_t(v);
-                if (((v >> 32) & 3u) == 2u || j == 0) break;
-                --j;
+                // nearest lane holding an inclusive offset; sum the lanes
+                // before it and itself
+                const uint32_t inc = __ballot_sync(0xFFFFFFFFu, ((v >> 32) & 3u) == 2u);
+                const int stop = inc ? __ffs(inc) - 1 : 32;
+                uint32_t add = int(lane) <= stop ? uint32_t(v) : 0u;
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) add += __shfl_xor_sync(0xFFFFFFFFu, add, d);
+                excl += add;
+                if (inc) break;
+                top -= 32;
             }
+            if (!ok && lane == 0) atomicExch(err, 1u);
             // published even after a wait ran out, so that no later tile waits
             // in turn (the result is then void and *err tells the host)
-            (void)ok;
-            atomicExch(&tiles[tile], cp_pack(epoch, 2, excl + local));
+            if (lane == 0) atomicExch(&tiles[tile], cp_pack(epoch, 2, excl + local));
         }
-        s_excl = excl;
-        if (start + CP_TILE >= n) *n_out = excl + local;
+        if (lane == 0) {
+            s_excl = excl;
+            if (start + CP_TILE >= n) *n_out = excl + local;
+        }
     }
     __syncthreads();
-    const uint32_t excl = s_excl;
+    uint32_t d = s_excl + rank;
 #pragma unroll
     for (int r = 0; r < CP_ITEMS; ++r)
-        if ((kept >> r) & 1u) move(uint32_t(start + uint64_t(r) * CP_THREADS + threadIdx.x), excl + rank[r]);
+        if ((kept >> r) & 1u) move(uint32_t(first + r), d++);
 }
 
 // Owns the tile states of a sequence of compactions on one stream.

@@ -10,6 +10,7 @@
 // exactly: every suffix whose equal-prefix run is claimed by it alone links
 // directly (runs of different suffix strings are disjoint); suffixes that
 // share a run are resolved by one thread per run, in list order.
+#include "compact.cuh"
 #include "stages.cuh"
 
 namespace curc {
@@ -127,42 +128,53 @@ __global__ void offset_mask_kernel(OverlapCtx c, const uint64_t* __restrict__ su
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ms) return;
     const uint64_t* sr = sufw + uint64_t(j) * c.W;
-    uint32_t word = 0;
-    int wi = 0;
-    for (int off = 0; off < max_off; ++off) {
-        if (off > 0) {
-            const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
-            const uint32_t bit = uint32_t(hv >> 32) & c.bmask;
-            word |= ((c.present[bit >> 5] >> (bit & 31)) & 1u) << (off & 31);
+    for (int wi = 0; wi * 32 < max_off; ++wi) {
+        // 32 independent bitmap lookups in flight per thread
+        uint32_t word = 0;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+            const int off = wi * 32 + b;
+            if (off > 0 && off < max_off) {
+                const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
+                const uint32_t bit = uint32_t(hv >> 32) & c.bmask;
+                word |= ((c.present[bit >> 5] >> (bit & 31)) & 1u) << b;
+            }
         }
-        if ((off & 31) == 31 || off == max_off - 1) {
-            mask[uint64_t(wi) * ms + j] = word;
-            ++wi;
-            word = 0;
-        }
+        mask[uint64_t(wi) * ms + j] = word;
     }
 }
 
+// The suffixes probed in a pass: not yet linked, and with a prefix k-mer
+// present at this offset (mask bit).  Listing them first lets the probe and
+// resolve kernels give every thread real work, instead of warps that wait on
+// the few lanes whose suffix probes.
+struct ProbeFilter {
+    const uint8_t* linked;
+    const uint32_t* mrow;  // mask word off/32 of every suffix
+    uint32_t bit;
+    __device__ bool operator()(uint32_t j) const { return !linked[j] && ((mrow[j] >> bit) & 1u); }
+};
+struct ProbeListMove {
+    uint32_t* plist;
+    __device__ void operator()(uint32_t j, uint32_t d) const { plist[d] = j; }
+};
+
 // compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
-// bound of suffix[off, L) among the bucket's prefix[0, L-off).  Suffixes
-// already linked or whose mask rules the offset out are skipped.  One
-// resident grid walks the list; tally[0] counts probes, tally[1] the
-// probes that met an equal prefix.
+// bound of suffix[off, L) among the bucket's prefix[0, L-off), for every
+// listed suffix.  tally[0] counts probes, tally[1] the probes that met an
+// equal prefix.
 __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
-                                                    const uint32_t* __restrict__ mask,
-                                                    const uint8_t* __restrict__ linked, uint32_t ms, int off,
+                                                    const uint32_t* __restrict__ plist,
+                                                    const uint32_t* __restrict__ pcount, int off,
                                                     uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
                                                     uint32_t* __restrict__ claim, uint32_t* __restrict__ lead,
                                                     uint32_t* __restrict__ ghead, uint32_t* __restrict__ gnext,
                                                     unsigned long long* __restrict__ tally) {
     uint32_t probes = 0, hits = 0;
     const int cl = c.L - off;
-    const uint32_t* mrow = mask + uint64_t(off >> 5) * ms;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ms; j += gridDim.x * blockDim.x) {
-        if (linked[j] || !((mrow[j] >> (off & 31)) & 1u)) {
-            cand[j] = INVALID;
-            continue;
-        }
+    const uint32_t np = *pcount;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
+        const uint32_t j = plist[q];
         ++probes;
         const uint64_t* sr = sufw + uint64_t(j) * c.W;
         const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
@@ -203,7 +215,9 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
 // the next pass by the thread that used it.  tally[2] counts links,
 // tally[3] the members of contested runs.
 __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32_t* __restrict__ suf,
-                                                      const uint64_t* __restrict__ sufw, uint32_t ms, int off,
+                                                      const uint64_t* __restrict__ sufw,
+                                                      const uint32_t* __restrict__ plist,
+                                                      const uint32_t* __restrict__ pcount, int off,
                                                       const uint32_t* __restrict__ cand,
                                                       const uint32_t* __restrict__ cand_end,
                                                       uint32_t* __restrict__ claim, uint32_t* __restrict__ lead,
@@ -211,7 +225,9 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
                                                       uint8_t* __restrict__ linked,
                                                       unsigned long long* __restrict__ tally) {
     uint32_t links = 0, contested = 0;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ms; j += gridDim.x * blockDim.x) {
+    const uint32_t np = *pcount;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
+        const uint32_t j = plist[q];
         const uint32_t lo = cand[j];
         if (lo == INVALID) continue;
         const uint32_t n = claim[lo];
@@ -246,6 +262,8 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
     block_tally<unsigned long long>(links, &tally[2]);
     block_tally<unsigned long long>(contested, &tally[3]);
 }
+
+__global__ void set_u32_kernel(uint32_t* p, uint32_t v) { *p = v; }
 
 __global__ void chain_res_kernel(uint32_t n, const uint32_t* __restrict__ next, const uint32_t* __restrict__ prev,
                                  const uint16_t* __restrict__ offset, uint8_t* __restrict__ res) {
@@ -338,6 +356,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, present, uint32_t((1ull << bbits) - 1), pre, nullptr,
                  next, prev, offset};
     uint32_t* keys = a.alloc<uint32_t>(mp ? mp : 1);
+    SubStage sp_sort("overlap.index_sort");
     if (mp) {
         prefix_hash_kernel<<<grid_for(mp, 256), 256, 0, s>>>(db, p.W, p.kip, p.k, c.mask, c.bmask, pre, mp, keys,
                                                              present);
@@ -352,6 +371,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     }
     exclusive_scan<uint32_t>(kr, kr, size_t(hs) + 2, nullptr, a, s);
     c.kr = kr;
+    sp_sort.stop();
 
     // per prefix slot: run claim count, lowest claimer, member list head
     uint32_t* claim = a.alloc<uint32_t>(mp ? mp : 1);
@@ -373,6 +393,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     uint32_t* mask2 = a.alloc<uint32_t>(size_t(ms ? ms : 1) * mw);
     uint8_t* linked = a.alloc<uint8_t>(ms ? ms : 1);
     CURC_CHECK(cudaMemsetAsync(linked, 0, ms ? ms : 1, s));
+    SubStage sp_mask("overlap.index_mask");
     if (ms) {
         gather_rows_kernel<<<grid_for(uint64_t(ms) * W, 256), 256, 0, s>>>(db, W, suf, ms, sufw);
         CURC_LAUNCH_CHECK();
@@ -381,34 +402,52 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
             CURC_LAUNCH_CHECK();
         }
     }
+    sp_mask.stop();
     // probes, probes that met a prefix, links, contested members
     unsigned long long* tally = a.alloc<unsigned long long>(4);
     CURC_CHECK(cudaMemsetAsync(tally, 0, 32, s));
     sp_index.stop();
 
-    // list of size ms, of which `active` are unlinked; compacted once half
-    // of it has linked
+    // List of size ms, of which `active` are unlinked; compacted once half
+    // of it has linked.  Passes are queued without a host round trip; the
+    // host reads the link count every few passes to compact or stop.
+    uint32_t* plist = a.alloc<uint32_t>(ms ? ms : 1);
+    uint32_t* dcount = a.alloc<uint32_t>(2);  // [0] list size, [1] listed probes
+    set_u32_kernel<<<1, 1, 0, s>>>(dcount, ms);
+    CURC_LAUNCH_CHECK();
+    Compactor cp(ms, a, s);
+    const int gp = resident_grid(probe_kernel, 512, ms ? ms : 1);
+    const int gr = resident_grid(resolve_kernel, 512, ms ? ms : 1);
+    constexpr int CHECK_EVERY = 8;
     uint32_t passes = 0, active = ms;
-    uint64_t links_seen = 0;
+    uint64_t links_seen = 0, active_sum = 0;
     const uint32_t ms0 = ms;
-    uint64_t active_sum = 0;
     for (int off = 1; off < p.max_off && active > 0 && mp > 0; ++off) {
         ++passes;
-        active_sum += active;
-        const int g = grid_for(ms, 256);
+        active_sum += active;  // as of the last check
         SubStage sp_probe("overlap.probe_resolve");
-        probe_kernel<<<resident_grid(probe_kernel, 512, ms), 512, 0, s>>>(c, sufw, mask, linked, ms, off, cand, cand_end, claim, lead, ghead, gnext,
+        SubStage sp_filter("overlap.filter");
+        cp.run(dcount, ms, dcount + 1,
+               ProbeFilter{linked, mask + uint64_t(off >> 5) * ms, uint32_t(off & 31)}, ProbeListMove{plist});
+        sp_filter.stop();
+        SubStage sp_pk("overlap.probe");
+        probe_kernel<<<gp, 512, 0, s>>>(c, sufw, plist, dcount + 1, off, cand, cand_end, claim, lead, ghead, gnext,
                                         tally);
         CURC_LAUNCH_CHECK();
-        resolve_kernel<<<resident_grid(resolve_kernel, 512, ms), 512, 0, s>>>(c, suf, sufw, ms, off, cand, cand_end, claim, lead, ghead, gnext, linked,
-                                          tally);
+        sp_pk.stop();
+        SubStage sp_rk("overlap.resolve");
+        resolve_kernel<<<gr, 512, 0, s>>>(c, suf, sufw, plist, dcount + 1, off, cand, cand_end, claim, lead, ghead,
+                                          gnext, linked, tally);
         CURC_LAUNCH_CHECK();
+        sp_rk.stop();
+        sp_probe.stop();
+        if (off % CHECK_EVERY != 0 && off + 1 < p.max_off) continue;
         const uint64_t links = read_scalar(tally + 2, s);
         active -= uint32_t(links - links_seen);
         links_seen = links;
-        sp_probe.stop();
         if (active * 2 < ms) {
             SubStage sp_comp("overlap.compact");
+            const int g = grid_for(ms, 256);
             keep_count_kernel<<<g, 256, 0, s>>>(linked, ms, keepc);
             CURC_LAUNCH_CHECK();
             exclusive_scan<uint32_t>(keepc, kpos, ms, nullptr, a, s);
@@ -419,8 +458,11 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
             std::swap(mask, mask2);
             ms = active;
             CURC_CHECK(cudaMemsetAsync(linked, 0, ms ? ms : 1, s));
+            set_u32_kernel<<<1, 1, 0, s>>>(dcount, ms);
+            CURC_LAUNCH_CHECK();
         }
     }
+    cp.check();
     if (st) {
         unsigned long long t[4];
         CURC_CHECK(cudaMemcpyAsync(t, tally, 32, cudaMemcpyDeviceToHost, s));
