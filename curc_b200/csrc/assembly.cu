@@ -10,9 +10,9 @@
 // cycle's first listed member), which becomes the tail.
 //
 // B200 design: list ranking with a sparse ruling set.  Every chain head and
-// one member in 16 (by a hash of its id) is a ruler; one thread per ruler
+// one member in 8 (by a hash of its id) is a ruler; one thread per ruler
 // walks its sublist up to the next ruler, giving every read its offset
-// within the sublist; the rulers (about a sixteenth of the reads, resident
+// within the sublist; the rulers (about an eighth of the reads, resident
 // in L2) are then ranked by pointer jumping, and one pass over the members
 // adds the two.  Each read is touched a constant number of times instead of
 // once per jumping round.  Cycles show up as ruler lists whose pointers never
@@ -31,7 +31,7 @@ __global__ void scatter_index_kernel(const uint32_t* __restrict__ ids, uint32_t 
     if (i < m) pos_in_ids[ids[i]] = i;
 }
 
-constexpr uint32_t RULER_SPACING = 16;  // one sampled ruler per 16 members (power of two)
+constexpr uint32_t RULER_SPACING = 8;  // one sampled ruler per 8 members (power of two)
 
 // Pointer-jumping state, 32 bytes so that one jump gathers one sector.  For
 // a ruler: acc / cnt = bases / reads of the sublists before its own, mn = the
@@ -59,10 +59,11 @@ struct __align__(16) ChainNode {
 // Position of a read within its ruler's sublist (indexed by list index).
 struct __align__(32) SubPos {
     uint64_t la;     // bases from the ruler's first base to this read's
-    uint32_t owner;  // ruler index, INVALID while no walk has reached it
+    uint32_t owner;  // ruler index
     uint32_t lc;     // reads between the ruler and this read
     uint32_t lm;     // smallest list index from the ruler to this read
-    uint32_t pad0, pad1, pad2;
+    uint32_t epoch;  // walk that wrote the entry; older entries mean "not reached"
+    uint32_t pad1, pad2;
 };
 
 // Totals of one ruler's sublist.
@@ -80,15 +81,20 @@ __global__ void ruler_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m,
     f[i] = pv[x] == INVALID || (murmur64(x) & (RULER_SPACING - 1)) == 0 || (promote && promote[i]);
 }
 
-__global__ void chain_nodes_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ nx,
-                                   const uint16_t* __restrict__ offset, ChainNode* __restrict__ node,
-                                   SubPos* __restrict__ loc) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    const uint32_t x = ids[i];
-    const uint32_t n = nx[x];
-    node[x] = ChainNode{n, n == INVALID ? 0u : uint32_t(offset[x]), i, INVALID};
-    loc[i].owner = INVALID;
+// One node per read, written in read order (non-members get INVALID
+// fields, so a link out of the member set is caught by the walk).
+__global__ void chain_nodes_kernel(uint32_t n, const uint32_t* __restrict__ pos_in_ids,
+                                   const uint32_t* __restrict__ nx, const uint16_t* __restrict__ offset,
+                                   ChainNode* __restrict__ node) {
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+        const uint32_t i = pos_in_ids[x];
+        if (i == INVALID) {
+            node[x] = ChainNode{INVALID, 0u, INVALID, INVALID};
+        } else {
+            const uint32_t nn = nx[x];
+            node[x] = ChainNode{nn, nn == INVALID ? 0u : uint32_t(offset[x]), i, INVALID};
+        }
+    }
 }
 
 __global__ void ruler_index_kernel(const uint32_t* __restrict__ rul, uint32_t nr, ChainNode* __restrict__ node) {
@@ -100,13 +106,13 @@ __global__ void ruler_index_kernel(const uint32_t* __restrict__ rul, uint32_t nr
 // or the chain's tail (a walk that comes back to a ruler on a cycle ends
 // there too), at most m steps.
 __global__ void ruler_walk_kernel(const uint32_t* __restrict__ rul, uint32_t nr, uint32_t m, uint32_t n,
-                                  const ChainNode* __restrict__ node, SubPos* __restrict__ loc,
+                                  uint32_t epoch, const ChainNode* __restrict__ node, SubPos* __restrict__ loc,
                                   SubTotal* __restrict__ tot, uint32_t* __restrict__ err) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nr; t += gridDim.x * blockDim.x) {
         ChainNode c = node[rul[t]];
         uint64_t la = 0;
         uint32_t lc = 0, lm = c.pos;
-        loc[c.pos] = SubPos{0, t, 0, lm, 0, 0, 0};
+        loc[c.pos] = SubPos{0, t, 0, lm, epoch, 0, 0};
         for (uint32_t step = 0; step < m && c.nx != INVALID; ++step) {
             if (c.nx >= n || node[c.nx].pos >= m) {  // a link out of the member set
                 atomicExch(err, 1u);
@@ -117,7 +123,7 @@ __global__ void ruler_walk_kernel(const uint32_t* __restrict__ rul, uint32_t nr,
             ++lc;
             if (d.rix != INVALID) break;
             lm = min(lm, d.pos);
-            loc[d.pos] = SubPos{la, t, lc, lm, 0, 0, 0};
+            loc[d.pos] = SubPos{la, t, lc, lm, epoch, 0, 0};
             c = d;
         }
         tot[t] = SubTotal{la, lc, lm};
@@ -125,11 +131,11 @@ __global__ void ruler_walk_kernel(const uint32_t* __restrict__ rul, uint32_t nr,
 }
 
 // Members that no walk reached (cycles without a ruler).
-__global__ void __launch_bounds__(256) unreached_kernel(uint32_t m, const SubPos* __restrict__ loc,
+__global__ void __launch_bounds__(256) unreached_kernel(uint32_t m, uint32_t epoch, const SubPos* __restrict__ loc,
                                                         uint8_t* __restrict__ flag, uint32_t* __restrict__ count) {
     uint32_t c = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        const bool u = loc[i].owner == INVALID;
+        const bool u = loc[i].epoch != epoch;
         flag[i] = u;
         c += u;
     }
@@ -377,6 +383,7 @@ struct RankScratch {
     RankState* A;
     RankState* B;
     uint32_t* counts;  // [0] rulers, [1] unreached, [2] active
+    uint32_t epoch;    // walks so far (loc is zeroed once, so 0 is never current)
 };
 
 // Ranks every member: st[i] for list index i.  Returns the number of members
@@ -388,22 +395,28 @@ uint32_t rank_members(const uint32_t* ids, uint32_t m, uint32_t n, const uint32_
     const uint8_t* promote = nullptr;
     uint32_t nr = 0;
     SubStage sp_walk("assembly.walk");
-    CURC_CHECK(cudaMemsetAsync(k.node, 0xFF, size_t(n) * sizeof(ChainNode), s));
     CURC_CHECK(cudaMemsetAsync(k.counts + 3, 0, 4, s));
+    chain_nodes_kernel<<<resident_grid(chain_nodes_kernel, 256, n), 256, 0, s>>>(n, pos_in_ids, nx, offset, k.node);
+    CURC_LAUNCH_CHECK();
     for (int attempt = 0; attempt < 2; ++attempt) {
+        const uint32_t epoch = ++k.epoch;
         ruler_flags_kernel<<<g, 256, 0, s>>>(ids, m, pv, promote, k.flags);
         CURC_LAUNCH_CHECK();
         select_flagged(ids, k.flags, k.rul, m, k.counts, a, s);
-        chain_nodes_kernel<<<g, 256, 0, s>>>(ids, m, nx, offset, k.node, k.loc);
-        CURC_LAUNCH_CHECK();
+        if (attempt) {  // clear the ruler marks of the first attempt
+            chain_nodes_kernel<<<resident_grid(chain_nodes_kernel, 256, n), 256, 0, s>>>(n, pos_in_ids, nx, offset,
+                                                                                          k.node);
+            CURC_LAUNCH_CHECK();
+        }
         CURC_CHECK(cudaMemsetAsync(k.counts + 1, 0, 4, s));
         nr = read_scalar(k.counts, s);
         ruler_index_kernel<<<grid_for(nr, 256), 256, 0, s>>>(k.rul, nr, k.node);
         CURC_LAUNCH_CHECK();
-        ruler_walk_kernel<<<resident_grid(ruler_walk_kernel, 256, nr), 256, 0, s>>>(k.rul, nr, m, n, k.node, k.loc,
-                                                                                    k.tot, k.counts + 3);
+        ruler_walk_kernel<<<resident_grid(ruler_walk_kernel, 256, nr), 256, 0, s>>>(k.rul, nr, m, n, epoch, k.node,
+                                                                                    k.loc, k.tot, k.counts + 3);
         CURC_LAUNCH_CHECK();
-        unreached_kernel<<<resident_grid(unreached_kernel, 256, m), 256, 0, s>>>(m, k.loc, k.flags, k.counts + 1);
+        unreached_kernel<<<resident_grid(unreached_kernel, 256, m), 256, 0, s>>>(m, epoch, k.loc, k.flags,
+                                                                                  k.counts + 1);
         CURC_LAUNCH_CHECK();
         uint32_t hc[4];
         CURC_CHECK(cudaMemcpyAsync(hc, k.counts, 16, cudaMemcpyDeviceToHost, s));
@@ -471,6 +484,8 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
     RankScratch k;
     k.node = a.alloc<ChainNode>(n);
     k.loc = a.alloc<SubPos>(m);
+    CURC_CHECK(cudaMemsetAsync(k.loc, 0, size_t(m) * sizeof(SubPos), s));
+    k.epoch = 0;
     k.flags = a.alloc<uint8_t>(m);
     k.promote = a.alloc<uint8_t>(m);
     k.rul = a.alloc<uint32_t>(m);

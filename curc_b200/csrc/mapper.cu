@@ -87,53 +87,109 @@ __device__ __forceinline__ int ascii_mismatches(const uint64_t* __restrict__ ref
     return c;
 }
 
+// One warp per read.  The reference's loop visits the candidates of the
+// read's probes in order (probe offset, then bucket slot), takes each that
+// strictly improves the mismatch count, and stops at the first count
+// <= target.  So its result is the first candidate with count <= target,
+// or else the first candidate with the smallest count (when that improves
+// on the read's count so far).  The warp lists the candidates of 32 probes
+// at a time, evaluates them 32 at a time in that order, and stops after the
+// chunk in which a count <= target appears.  A candidate's count is exact
+// below the read's starting count (the bound of the early exit), which is
+// all the comparison needs.
 template <bool RC>
-__global__ void map_kernel(MapIndex ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
-                           const uint64_t* __restrict__ udb, uint32_t U, const uint8_t* __restrict__ ndb, uint32_t NN,
-                           int L, int W, int k, int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
-                           uint64_t* __restrict__ pos) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= U + NN) return;
-    int best = mm[i];
-    if (best <= BlockParams::target_mm) return;
+__global__ void __launch_bounds__(128) map_kernel(MapIndex ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
+                                                  const uint64_t* __restrict__ udb, uint32_t U,
+                                                  const uint8_t* __restrict__ ndb, uint32_t NN, int L, int W, int k,
+                                                  int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
+                                                  uint64_t* __restrict__ pos) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (i >= U + NN) return;  // whole warp
+    const int init = mm[i];
+    if (init <= BlockParams::target_mm) return;
     const bool isn = i >= U;
     const uint64_t* rd = isn ? nullptr : udb + uint64_t(i) * W;
     const uint8_t* nd = isn ? ndb + uint64_t(i - U) * L : nullptr;
-    bool found = false;
-    uint64_t bpos = 0;
-    for (int j = 0; j + k <= L; j += BlockParams::read_step) {
-        uint64_t key;
-        if (!isn) {
-            key = word_at(rd, j, k);
-        } else {
-            key = 0;
-            for (int t = 0; t < k; ++t) key = (key << 2) | uint64_t(ascii_code(nd[j + t]));
+    const int probes = (L - k) / BlockParams::read_step + 1;
+    int best = init;  // smallest count met so far (the same in every lane)
+    uint64_t best_pos = 0;
+    bool done = false;
+    for (int p0 = 0; p0 < probes && !done; p0 += 32) {
+        // this lane's probe: bucket range of its k-mer
+        const int pj = p0 + int(lane);
+        const int j = pj * BlockParams::read_step;
+        uint32_t b = 0, cnt = 0;
+        if (pj < probes) {
+            uint64_t key;
+            if (!isn) {
+                key = word_at(rd, j, k);
+            } else {
+                key = 0;
+                for (int t = 0; t < k; ++t) key = (key << 2) | uint64_t(ascii_code(nd[j + t]));
+            }
+            const uint32_t h = uint32_t(murmur64(key) & ix.mask);
+            b = ix.kr[h];
+            const uint32_t e = ix.kr[h + 1];
+            cnt = min(e - b, uint32_t(BlockParams::bucket_limit));
         }
-        const uint32_t h = uint32_t(murmur64(key) & ix.mask);
-        const uint32_t b = ix.kr[h];
-        uint32_t e = ix.kr[h + 1];
-        if (b == e) continue;
-        e = min(b + 12u, e);
-        const uint64_t shift = RC ? uint64_t(L - k - j) : uint64_t(j);
-        for (uint32_t q = b; q < e; ++q) {
-            const uint64_t refpos = ix.start + uint64_t(ix.pos[q]) * step;
-            if (refpos < shift) continue;
-            const uint64_t mp = refpos - shift;
-            if (mp + L > ref_len) continue;
-            const int c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best) : packed_mismatches<RC>(ref, mp, rd, L, best);
-            if (c < best) {
-                best = c;
-                bpos = mp;
-                found = true;
-                if (best <= BlockParams::target_mm) goto done;
+        // inclusive scan of the candidate counts over the lanes
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= uint32_t(d)) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        for (uint32_t cs = 0; cs < total; cs += 32) {
+            const uint32_t ci = cs + lane;
+            int c = 0x7FFF;
+            uint64_t mp = 0;
+            // owner lane: the first lane whose inclusive count exceeds ci
+            uint32_t owner = 0;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, owner + d - 1);
+                if (v <= ci) owner += d;
+            }
+            const uint32_t ob = __shfl_sync(0xFFFFFFFFu, b, owner);
+            const uint32_t oex = __shfl_sync(0xFFFFFFFFu, incl - cnt, owner);
+            if (ci < total) {
+                const int oj = (p0 + int(owner)) * BlockParams::read_step;
+                const uint32_t q = ob + (ci - oex);
+                const uint64_t refpos = ix.start + uint64_t(ix.pos[q]) * step;
+                const uint64_t shift = RC ? uint64_t(L - k - oj) : uint64_t(oj);
+                if (refpos >= shift && refpos - shift + L <= ref_len) {
+                    mp = refpos - shift;
+                    c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, init) : packed_mismatches<RC>(ref, mp, rd, L, init);
+                }
+            }
+            // the loop stops at the first count <= target
+            const uint32_t stop = __ballot_sync(0xFFFFFFFFu, c <= BlockParams::target_mm);
+            if (stop) {
+                const int first = __ffs(stop) - 1;
+                best = __shfl_sync(0xFFFFFFFFu, c, first);
+                best_pos = __shfl_sync(0xFFFFFFFFu, mp, first);
+                done = true;
+                break;
+            }
+            // otherwise the earliest candidate of the chunk with the smallest
+            // count, kept only if it strictly improves
+            int cmin = c;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) cmin = min(cmin, __shfl_xor_sync(0xFFFFFFFFu, cmin, d));
+            const int first = __ffs(__ballot_sync(0xFFFFFFFFu, c == cmin)) - 1;
+            const uint64_t fpos = __shfl_sync(0xFFFFFFFFu, mp, first);
+            if (cmin < best) {
+                best = cmin;
+                best_pos = fpos;
             }
         }
     }
-done:
-    if (found) {
+    if (lane == 0 && best < init) {
         mm[i] = uint8_t(best);
         strand[i] = RC ? 1 : 0;
-        pos[i] = bpos;
+        pos[i] = best_pos;
     }
 }
 
@@ -188,7 +244,7 @@ void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, cons
             sp_index.stop();
             SubStage sp_map(rc ? "mapping.map_rc" : "mapping.map_fwd");
             MapIndex ix{hs - 1, kr, pos, parts[q].start};
-            const int g = grid_for(total, 128);
+            const int g = grid_for(uint64_t(total) * 32, 128);
             if (rc)
                 map_kernel<true><<<g, 128, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
                                                    out.strand, out.pos);

@@ -51,6 +51,23 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+// Four ASCII bases (a little-endian word, first base in the low byte) to
+// eight bits, first base in the top two: bits 1-3 of the letters give
+// A/a 0, C/c 1, G/g 2, T/t 3 as ((c >> 1) ^ (c >> 2)) & 3, and one multiply
+// gathers the four 2-bit codes into the top byte.
+__device__ __forceinline__ uint32_t pack4(uint32_t x) {
+    const uint32_t t = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
+    return (t * 0x40100401u) >> 24;
+}
+
+// The four bytes are all uppercase A, C, G or T (the common case, where
+// pack4 is exact and no N is present): rebuild them from their codes.
+__device__ __forceinline__ bool plain4(uint32_t x) {
+    const uint32_t t = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
+    const uint32_t sel = (t & 3u) | ((t >> 4) & 0x30u) | ((t >> 8) & 0x300u) | ((t >> 12) & 0x3000u);
+    return __byte_perm(0x54474341u, 0u, sel) == x;
+}
+
 __global__ void __launch_bounds__(PACK_THREADS) pack_kernel(const uint8_t* __restrict__ seq, uint64_t n, int L, int W,
                                                              uint32_t tile_bytes, bool use_tma,
                                                              uint64_t* __restrict__ packed, uint8_t* __restrict__ has_n,
@@ -59,7 +76,8 @@ __global__ void __launch_bounds__(PACK_THREADS) pack_kernel(const uint8_t* __res
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint8_t nflag[PACK_READS];
     const uint64_t tiles = div_up(n, PACK_READS);
-    const uint32_t stride_bytes = (tile_bytes + 127u) & ~127u;
+    // a word's loads may run 36 bytes past its row: keep them in the buffer
+    const uint32_t stride_bytes = (tile_bytes + 64u + 127u) & ~127u;
     auto full = [&](uint64_t t) { return (t + 1) * PACK_READS <= n; };
     auto issue = [&](uint64_t t, int stage) {
         mbar_expect_tx(&bar[stage], tile_bytes);
@@ -104,18 +122,41 @@ __global__ void __launch_bounds__(PACK_THREADS) pack_kernel(const uint8_t* __res
         __syncthreads();
         for (uint32_t item = threadIdx.x; item < nr * uint32_t(W); item += PACK_THREADS) {
             const uint32_t r = item / W, w = item - r * W;
-            const uint8_t* s = buf + r * L + w * 32;
+            const uint32_t a = r * uint32_t(L) + w * 32;
             const int nb = min(32, L - int(w) * 32);
+            // eight 4-byte groups from aligned shared-memory words; bytes past
+            // the read's end are replaced by 'A' (code 0, the zero padding)
+            const uint32_t* b32 = reinterpret_cast<const uint32_t*>(buf + (a & ~3u));
+            const uint32_t sh = (a & 3u) * 8u;
+            uint32_t lo = b32[0];
             uint64_t v = 0;
-            bool hn = false;
-            for (int j = 0; j < nb; ++j) {
-                const uint8_t c = s[j];
-                hn |= (c == 'N');
-                v = (v << 2) | uint64_t(ascii_code(c));
+            bool plain = true;
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                const uint32_t hi = b32[g + 1];
+                uint32_t x = __funnelshift_r(lo, hi, sh);
+                lo = hi;
+                const int vb = nb - 4 * g;
+                if (vb < 4) {
+                    const uint32_t keep = vb <= 0 ? 0u : (1u << (8 * vb)) - 1u;
+                    x = (x & keep) | (0x41414141u & ~keep);
+                }
+                v = (v << 8) | pack4(x);
+                plain &= plain4(x);
             }
-            v <<= 2 * (32 - nb);
+            if (!plain) {  // N, lower case or other letters: byte by byte
+                const uint8_t* sb = buf + a;
+                bool hn = false;
+                v = 0;
+                for (int j = 0; j < nb; ++j) {
+                    const uint8_t c = sb[j];
+                    hn |= (c == 'N');
+                    v = (v << 2) | uint64_t(ascii_code(c));
+                }
+                v <<= 2 * (32 - nb);
+                if (hn) nflag[r] = 1;
+            }
             packed[(t * PACK_READS + r) * W + w] = v;
-            if (hn) nflag[r] = 1;
         }
         __syncthreads();
         if (threadIdx.x < nr) has_n[t * PACK_READS + threadIdx.x] = nflag[threadIdx.x];
@@ -148,14 +189,15 @@ void pack_reads(const uint8_t* seq, uint64_t n, int L, uint64_t* packed, uint8_t
     const int W = (L + 31) / 32;
     const uint32_t tile_bytes = uint32_t(PACK_READS) * uint32_t(L);
     const bool aligned = (reinterpret_cast<uintptr_t>(seq) & 15u) == 0;
-    const size_t smem = 2 * ((tile_bytes + 127u) & ~127u);
+    const size_t smem = 2 * ((tile_bytes + 64u + 127u) & ~127u);
     static bool attr_set = false;
     if (!attr_set) {
-        CURC_CHECK(cudaFuncSetAttribute(pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 64 * 512 + 256));
+        CURC_CHECK(cudaFuncSetAttribute(pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        2 * (64 * 512 + 64 + 128)));
         attr_set = true;
     }
     const uint64_t tiles = div_up(n, PACK_READS);
-    const int grid = int(std::min<uint64_t>(tiles, uint64_t(SM_COUNT_B200) * 4));
+    const int grid = int(std::min<uint64_t>(tiles, uint64_t(SM_COUNT_B200) * 8));
     pack_kernel<<<grid, PACK_THREADS, smem, s>>>(seq, n, L, W, tile_bytes, aligned, packed, has_n, err);
     CURC_LAUNCH_CHECK();
 }
