@@ -86,6 +86,21 @@ __global__ void bucket_count_kernel(const uint32_t* __restrict__ keys, uint32_t 
     if (i < m) atomicAdd(&kr[keys[i]], 1u);
 }
 
+// bit h of bfree: bucket h still holds a prefix without a predecessor
+__global__ void bucket_free_bits_kernel(const uint32_t* __restrict__ cnt, uint32_t words, uint32_t* __restrict__ bfree) {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+        uint32_t v = 0;
+        const uint4* c4 = reinterpret_cast<const uint4*>(cnt + uint64_t(w) * 32);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint4 c = c4[q];
+            v |= uint32_t(c.x != 0) << (4 * q) | uint32_t(c.y != 0) << (4 * q + 1) | uint32_t(c.z != 0) << (4 * q + 2) |
+                 uint32_t(c.w != 0) << (4 * q + 3);
+        }
+        bfree[w] = v;
+    }
+}
+
 struct OverlapCtx {
     const uint64_t* db;
     int W, L, k, kip;
@@ -94,6 +109,8 @@ struct OverlapCtx {
     uint32_t bmask;
     const uint32_t* va;  // prefix ids sorted by (bucket, read)
     const uint32_t* kr;  // bucket ranges
+    uint32_t* free_cnt;  // per bucket: prefixes without a predecessor
+    uint32_t* bfree;     // per bucket: free_cnt != 0 (one bit, stays in L2)
     uint32_t* next;
     uint32_t* prev;
     uint16_t* offset;
@@ -116,6 +133,12 @@ __device__ __forceinline__ bool link_first_free(const OverlapCtx& c, uint32_t s,
         return false;
     }
     return false;
+}
+
+// A prefix of bucket h got its predecessor: the bucket's free count drops,
+// and its bit clears with the last one.
+__device__ __forceinline__ void take_from_bucket(const OverlapCtx& c, uint32_t h) {
+    if (atomicSub(&c.free_cnt[h], 1u) == 1u) atomicAnd(&c.bfree[h >> 5], ~(1u << (h & 31)));
 }
 
 // Offsets at which a suffix can meet a prefix at all: bit off of the
@@ -179,6 +202,12 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
         const uint64_t* sr = sufw + uint64_t(j) * c.W;
         const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
         const uint32_t h = uint32_t(hv & c.mask);
+        // every prefix of the bucket has a predecessor already: no link is
+        // possible for any suffix that meets it, so none needs to claim it
+        if (!((c.bfree[h >> 5] >> (h & 31)) & 1u)) {
+            cand[j] = INVALID;
+            continue;
+        }
         uint32_t lo = c.kr[h];
         const uint32_t e = c.kr[h + 1];
         uint32_t count = e - lo;
@@ -231,10 +260,13 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
         const uint32_t lo = cand[j];
         if (lo == INVALID) continue;
         const uint32_t n = claim[lo];
+        // the run's bucket (the same for every member)
+        const uint32_t h = uint32_t(murmur64(word_at(sufw + uint64_t(j) * c.W, c.kip + off, c.k)) & c.mask);
         if (n == 1) {
             if (link_first_free(c, suf[j], sufw + uint64_t(j) * c.W, lo, cand_end[j], off)) {
                 linked[j] = 1;
                 ++links;
+                take_from_bucket(c, h);
             }
         } else if (lead[lo] == j) {
             contested += n;
@@ -248,6 +280,7 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
                 if (link_first_free(c, suf[best], sufw + uint64_t(best) * c.W, lo, cand_end[best], off)) {
                     linked[best] = 1;
                     ++links;
+                    take_from_bucket(c, h);
                 }
                 last = best;
                 first = false;
@@ -353,8 +386,8 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     const uint64_t bwords = (1ull << bbits) / 32;
     uint32_t* present = a.alloc<uint32_t>(bwords);
     CURC_CHECK(cudaMemsetAsync(present, 0, bwords * 4, s));
-    OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, present, uint32_t((1ull << bbits) - 1), pre, nullptr,
-                 next, prev, offset};
+    OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, present, uint32_t((1ull << bbits) - 1), pre, nullptr, nullptr,
+                 nullptr, next, prev, offset};
     uint32_t* keys = a.alloc<uint32_t>(mp ? mp : 1);
     SubStage sp_sort("overlap.index_sort");
     if (mp) {
@@ -369,6 +402,13 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         bucket_count_kernel<<<grid_for(mp, 256), 256, 0, s>>>(keys, mp, kr);
         CURC_LAUNCH_CHECK();
     }
+    uint32_t* free_cnt = a.alloc<uint32_t>(size_t(hs) + 32);
+    uint32_t* bfree = a.alloc<uint32_t>(hs / 32 + 1);
+    CURC_CHECK(cudaMemcpyAsync(free_cnt, kr, size_t(hs) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    bucket_free_bits_kernel<<<grid_for(hs / 32, 256), 256, 0, s>>>(free_cnt, hs / 32, bfree);
+    CURC_LAUNCH_CHECK();
+    c.free_cnt = free_cnt;
+    c.bfree = bfree;
     exclusive_scan<uint32_t>(kr, kr, size_t(hs) + 2, nullptr, a, s);
     c.kr = kr;
     sp_sort.stop();
