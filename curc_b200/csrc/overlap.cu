@@ -101,6 +101,13 @@ __global__ void bucket_free_bits_kernel(const uint32_t* __restrict__ cnt, uint32
     }
 }
 
+// Per prefix slot, while a pass runs: how many suffixes met the run that
+// starts there, the lowest of their list indices, and the head of the list
+// of their indices (one sector for the three).
+struct __align__(16) RunSlot {
+    uint32_t claim, lead, head, pad;
+};
+
 struct OverlapCtx {
     const uint64_t* db;
     int W, L, k, kip;
@@ -124,7 +131,8 @@ __device__ __forceinline__ bool link_first_free(const OverlapCtx& c, uint32_t s,
     for (uint32_t q = lo; q < e; ++q) {
         const uint32_t pr = c.va[q];
         if (pr == s || c.prev[pr] != INVALID) continue;
-        if (cmp_span(c.db + uint64_t(pr) * c.W, 0, sr, off, cl) == 0) {
+        // the probe found prefix lo equal; later entries need the comparison
+        if (q == lo || cmp_span(c.db + uint64_t(pr) * c.W, 0, sr, off, cl) == 0) {
             c.prev[pr] = s;
             c.next[s] = pr;
             c.offset[s] = uint16_t(off);
@@ -183,54 +191,73 @@ struct ProbeListMove {
 };
 
 // compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
-// bound of suffix[off, L) among the bucket's prefix[0, L-off), for every
-// listed suffix.  tally[0] counts probes, tally[1] the probes that met an
-// equal prefix.
+// bound of suffix[off, L) among the bucket's prefix[0, L-off).  Returns
+// whether an equal prefix exists; then its run start and bucket end are
+// stored and the suffix joins the run's claimers.
+__device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* __restrict__ sufw, uint32_t j, int off,
+                                          uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
+                                          RunSlot* __restrict__ run, uint32_t* __restrict__ gnext) {
+    const int cl = c.L - off;
+    const uint64_t* sr = sufw + uint64_t(j) * c.W;
+    const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
+    const uint32_t h = uint32_t(hv & c.mask);
+    // every prefix of the bucket has a predecessor already: no link is
+    // possible for any suffix that meets it, so none needs to claim it
+    if (!((c.bfree[h >> 5] >> (h & 31)) & 1u)) return false;
+    uint32_t lo = c.kr[h];
+    const uint32_t e = c.kr[h + 1];
+    uint32_t count = e - lo;
+    while (count > 0) {
+        const uint32_t step = count / 2, it = lo + step;
+        if (cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl) < 0) {
+            lo = it + 1;
+            count -= step + 1;
+        } else {
+            count = step;
+        }
+    }
+    if (lo >= e || cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) != 0) return false;
+    // run membership: count, lowest list index, and a list of members
+    atomicAdd(&run[lo].claim, 1u);
+    atomicMin(&run[lo].lead, j);
+    gnext[j] = atomicExch(&run[lo].head, j);
+    cand[j] = lo;
+    cand_end[j] = e;
+    return true;
+}
+
+// Probes every listed suffix and lists the ones that met an equal prefix
+// (hlist, *hcount; order is immaterial to the resolution).  tally[0] counts
+// probes, tally[1] hits.
 __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
                                                     const uint32_t* __restrict__ plist,
                                                     const uint32_t* __restrict__ pcount, int off,
                                                     uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
-                                                    uint32_t* __restrict__ claim, uint32_t* __restrict__ lead,
-                                                    uint32_t* __restrict__ ghead, uint32_t* __restrict__ gnext,
+                                                    RunSlot* __restrict__ run, uint32_t* __restrict__ gnext,
+                                                    uint32_t* __restrict__ hlist, uint32_t* __restrict__ hcount,
                                                     unsigned long long* __restrict__ tally) {
+    __shared__ uint32_t s_hits[512];
+    __shared__ uint32_t s_n, s_base;
     uint32_t probes = 0, hits = 0;
-    const int cl = c.L - off;
     const uint32_t np = *pcount;
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
-        const uint32_t j = plist[q];
-        ++probes;
-        const uint64_t* sr = sufw + uint64_t(j) * c.W;
-        const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
-        const uint32_t h = uint32_t(hv & c.mask);
-        // every prefix of the bucket has a predecessor already: no link is
-        // possible for any suffix that meets it, so none needs to claim it
-        if (!((c.bfree[h >> 5] >> (h & 31)) & 1u)) {
-            cand[j] = INVALID;
-            continue;
+    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < np; b0 += gridDim.x * blockDim.x) {
+        const uint32_t q = b0 + threadIdx.x;
+        bool hit = false;
+        uint32_t j = 0;
+        if (q < np) {
+            j = plist[q];
+            ++probes;
+            hit = probe_one(c, sufw, j, off, cand, cand_end, run, gnext);
+            hits += hit;
         }
-        uint32_t lo = c.kr[h];
-        const uint32_t e = c.kr[h + 1];
-        uint32_t count = e - lo;
-        while (count > 0) {
-            const uint32_t step = count / 2, it = lo + step;
-            if (cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl) < 0) {
-                lo = it + 1;
-                count -= step + 1;
-            } else {
-                count = step;
-            }
-        }
-        uint32_t r = INVALID;
-        if (lo < e && cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) == 0) {
-            r = lo;
-            ++hits;
-            // run membership: count, lowest list index, and a list of members
-            atomicAdd(&claim[lo], 1u);
-            atomicMin(&lead[lo], j);
-            gnext[j] = atomicExch(&ghead[lo], j);
-        }
-        cand[j] = r;
-        cand_end[j] = e;
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        if (hit) s_hits[atomicAdd(&s_n, 1u)] = j;
+        __syncthreads();
+        if (threadIdx.x == 0 && s_n) s_base = atomicAdd(hcount, s_n);
+        __syncthreads();
+        if (threadIdx.x < s_n) hlist[s_base + threadIdx.x] = s_hits[threadIdx.x];
+        __syncthreads();
     }
     block_tally<unsigned long long>(probes, &tally[0]);
     block_tally<unsigned long long>(hits, &tally[1]);
@@ -245,21 +272,20 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
 // tally[3] the members of contested runs.
 __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32_t* __restrict__ suf,
                                                       const uint64_t* __restrict__ sufw,
-                                                      const uint32_t* __restrict__ plist,
-                                                      const uint32_t* __restrict__ pcount, int off,
+                                                      const uint32_t* __restrict__ hlist,
+                                                      const uint32_t* __restrict__ hcount, int off,
                                                       const uint32_t* __restrict__ cand,
                                                       const uint32_t* __restrict__ cand_end,
-                                                      uint32_t* __restrict__ claim, uint32_t* __restrict__ lead,
-                                                      uint32_t* __restrict__ ghead, const uint32_t* __restrict__ gnext,
+                                                      RunSlot* __restrict__ run, const uint32_t* __restrict__ gnext,
                                                       uint8_t* __restrict__ linked,
                                                       unsigned long long* __restrict__ tally) {
     uint32_t links = 0, contested = 0;
-    const uint32_t np = *pcount;
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
-        const uint32_t j = plist[q];
+    const uint32_t nh = *hcount;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nh; q += gridDim.x * blockDim.x) {
+        const uint32_t j = hlist[q];
         const uint32_t lo = cand[j];
-        if (lo == INVALID) continue;
-        const uint32_t n = claim[lo];
+        const RunSlot rs = run[lo];
+        const uint32_t n = rs.claim;
         // the run's bucket (the same for every member)
         const uint32_t h = uint32_t(murmur64(word_at(sufw + uint64_t(j) * c.W, c.kip + off, c.k)) & c.mask);
         if (n == 1) {
@@ -268,13 +294,13 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
                 ++links;
                 take_from_bucket(c, h);
             }
-        } else if (lead[lo] == j) {
+        } else if (rs.lead == j) {
             contested += n;
             uint32_t last = 0;
             bool first = true;
             for (uint32_t k = 0; k < n; ++k) {
                 uint32_t best = INVALID;
-                for (uint32_t m = ghead[lo]; m != INVALID; m = gnext[m])
+                for (uint32_t m = rs.head; m != INVALID; m = gnext[m])
                     if ((first || m > last) && m < best) best = m;
                 if (best == INVALID) break;
                 if (link_first_free(c, suf[best], sufw + uint64_t(best) * c.W, lo, cand_end[best], off)) {
@@ -288,15 +314,18 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
         } else {
             continue;  // the run's lowest member resolves it
         }
-        claim[lo] = 0;
-        lead[lo] = INVALID;
-        ghead[lo] = INVALID;
+        run[lo] = RunSlot{0, INVALID, INVALID, 0};
     }
     block_tally<unsigned long long>(links, &tally[2]);
     block_tally<unsigned long long>(contested, &tally[3]);
 }
 
 __global__ void set_u32_kernel(uint32_t* p, uint32_t v) { *p = v; }
+
+__global__ void run_slots_init_kernel(RunSlot* run, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) run[i] = RunSlot{0, INVALID, INVALID, 0};
+}
 
 __global__ void chain_res_kernel(uint32_t n, const uint32_t* __restrict__ next, const uint32_t* __restrict__ prev,
                                  const uint16_t* __restrict__ offset, uint8_t* __restrict__ res) {
@@ -414,12 +443,9 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     sp_sort.stop();
 
     // per prefix slot: run claim count, lowest claimer, member list head
-    uint32_t* claim = a.alloc<uint32_t>(mp ? mp : 1);
-    uint32_t* lead = a.alloc<uint32_t>(mp ? mp : 1);
-    uint32_t* ghead = a.alloc<uint32_t>(mp ? mp : 1);
-    CURC_CHECK(cudaMemsetAsync(claim, 0, size_t(mp ? mp : 1) * sizeof(uint32_t), s));
-    fill<uint32_t>(lead, INVALID, mp ? mp : 1, s);
-    fill<uint32_t>(ghead, INVALID, mp ? mp : 1, s);
+    RunSlot* run = a.alloc<RunSlot>(mp ? mp : 1);
+    run_slots_init_kernel<<<grid_for(mp ? mp : 1, 256), 256, 0, s>>>(run, mp ? mp : 1);
+    CURC_LAUNCH_CHECK();
     uint32_t* cand = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* cand_end = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* gnext = a.alloc<uint32_t>(ms ? ms : 1);
@@ -452,6 +478,9 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     // of it has linked.  Passes are queued without a host round trip; the
     // host reads the link count every few passes to compact or stop.
     uint32_t* plist = a.alloc<uint32_t>(ms ? ms : 1);
+    uint32_t* hlist = a.alloc<uint32_t>(ms ? ms : 1);
+    uint32_t* hcount = a.alloc<uint32_t>(p.max_off + 1);  // one per pass
+    CURC_CHECK(cudaMemsetAsync(hcount, 0, size_t(p.max_off + 1) * 4, s));
     uint32_t* dcount = a.alloc<uint32_t>(2);  // [0] list size, [1] listed probes
     set_u32_kernel<<<1, 1, 0, s>>>(dcount, ms);
     CURC_LAUNCH_CHECK();
@@ -471,12 +500,12 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
                ProbeFilter{linked, mask + uint64_t(off >> 5) * ms, uint32_t(off & 31)}, ProbeListMove{plist});
         sp_filter.stop();
         SubStage sp_pk("overlap.probe");
-        probe_kernel<<<gp, 512, 0, s>>>(c, sufw, plist, dcount + 1, off, cand, cand_end, claim, lead, ghead, gnext,
-                                        tally);
+        probe_kernel<<<gp, 512, 0, s>>>(c, sufw, plist, dcount + 1, off, cand, cand_end, run, gnext,
+                                        hlist, hcount + off, tally);
         CURC_LAUNCH_CHECK();
         sp_pk.stop();
         SubStage sp_rk("overlap.resolve");
-        resolve_kernel<<<gr, 512, 0, s>>>(c, suf, sufw, plist, dcount + 1, off, cand, cand_end, claim, lead, ghead,
+        resolve_kernel<<<gr, 512, 0, s>>>(c, suf, sufw, hlist, hcount + off, off, cand, cand_end, run,
                                           gnext, linked, tally);
         CURC_LAUNCH_CHECK();
         sp_rk.stop();
