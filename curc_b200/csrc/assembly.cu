@@ -283,6 +283,26 @@ __global__ void cycle_cut_kernel(const uint32_t* __restrict__ ids, uint32_t m, c
     pv[nh] = INVALID;
 }
 
+// The cycle members as a list of their own (in list order).
+__global__ void cycle_list_kernel(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ cidx, uint32_t mc,
+                                  uint32_t* __restrict__ cids, uint32_t* __restrict__ pos_in_cyc) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mc) return;
+    const uint32_t x = ids[cidx[t]];
+    cids[t] = x;
+    pos_in_cyc[x] = t;
+}
+
+// States of the cut cycles back into the full list (mn to a list index).
+__global__ void cycle_merge_kernel(const uint32_t* __restrict__ cidx, uint32_t mc, const RankState* __restrict__ T,
+                                   RankState* __restrict__ R) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mc) return;
+    RankState r = T[t];
+    r.mn = cidx[r.mn];
+    R[cidx[t]] = r;
+}
+
 // The chain's first list index, from its tail (whose mn covers the chain).
 __global__ void chain_key_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint32_t* __restrict__ nx,
                                  const RankState* __restrict__ st, uint32_t* __restrict__ key) {
@@ -436,12 +456,16 @@ uint32_t rank_members(const uint32_t* ids, uint32_t m, uint32_t n, const uint32_
     RankState* A = k.A;
     RankState* B = k.B;
     uint32_t left = 0;
+    // the count of pointers left is read every few rounds (a round on
+    // converged states changes nothing)
     const int R = rounds_for(nr);
+    const int gs = resident_grid(rank_step_kernel, 512, nr);
     for (int t = 0; t < R; ++t) {
         CURC_CHECK(cudaMemsetAsync(k.counts + 2, 0, 4, s));
-        rank_step_kernel<<<resident_grid(rank_step_kernel, 512, nr), 512, 0, s>>>(nr, A, B, k.counts + 2);
+        rank_step_kernel<<<gs, 512, 0, s>>>(nr, A, B, k.counts + 2);
         CURC_LAUNCH_CHECK();
         std::swap(A, B);
+        if (t % 4 != 3 && t + 1 < R) continue;
         left = read_scalar(k.counts + 2, s);
         if (left == 0) break;
     }
@@ -496,7 +520,9 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
     RankState* R = a.alloc<RankState>(m);
     uint32_t left = rank_members(ids, m, n_total, nx, pv, offset, pos_in_ids, k, R, a, s);
     if (left) {
-        // cycles: cut each in parallel, then rank again
+        // Cycles: cut each in parallel.  Only their members are ranked again
+        // (a cut cycle is a chain of exactly its members), as a list of its
+        // own in list order, and their states are then written back.
         uint8_t* cyc = a.alloc<uint8_t>(m);
         cycle_flags_kernel<<<g, 256, 0, s>>>(m, R, cyc);
         CURC_LAUNCH_CHECK();
@@ -506,16 +532,44 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
         CURC_CHECK(cudaMemsetAsync(k.counts + 3, 0, 4, s));
         cycle_open_kernel<<<g, 256, 0, s>>>(ids, m, R, cyc, nx, pv, leader_of_head, k.counts + 3);
         CURC_LAUNCH_CHECK();
-        if (read_scalar(k.counts + 3, s)) throw std::runtime_error("assemble: broken cycle");
-        RankState* T = a.alloc<RankState>(m);
-        if (rank_members(ids, m, n_total, nx, pv, offset, pos_in_ids, k, T, a, s))
+        uint32_t* cidx = a.alloc<uint32_t>(m);
+        select_indices(cyc, cidx, m, k.counts + 2, a, s);
+        uint32_t hc[2];
+        CURC_CHECK(cudaMemcpyAsync(hc, k.counts + 2, 8, cudaMemcpyDeviceToHost, s));
+        CURC_CHECK(cudaStreamSynchronize(s));
+        if (hc[1]) throw std::runtime_error("assemble: broken cycle");
+        const uint32_t mc = hc[0];
+        const int gc = grid_for(mc, 256);
+        uint32_t* cids = a.alloc<uint32_t>(mc);
+        uint32_t* pos_in_cyc = a.alloc<uint32_t>(n);
+        fill<uint32_t>(pos_in_cyc, INVALID, n, s);
+        cycle_list_kernel<<<gc, 256, 0, s>>>(ids, cidx, mc, cids, pos_in_cyc);
+        CURC_LAUNCH_CHECK();
+        uint8_t* all = a.alloc<uint8_t>(mc);
+        CURC_CHECK(cudaMemsetAsync(all, 1, mc, s));
+        RankScratch kc;
+        kc.node = k.node;
+        kc.loc = a.alloc<SubPos>(mc);
+        CURC_CHECK(cudaMemsetAsync(kc.loc, 0, size_t(mc) * sizeof(SubPos), s));
+        kc.epoch = 0;
+        kc.flags = a.alloc<uint8_t>(mc);
+        kc.promote = a.alloc<uint8_t>(mc);
+        kc.rul = a.alloc<uint32_t>(mc);
+        kc.tot = a.alloc<SubTotal>(mc);
+        kc.A = a.alloc<RankState>(mc);
+        kc.B = a.alloc<RankState>(mc);
+        kc.counts = a.alloc<uint32_t>(4);
+        RankState* T = a.alloc<RankState>(mc);
+        if (rank_members(cids, mc, n_total, nx, pv, offset, pos_in_cyc, kc, T, a, s))
             throw std::runtime_error("assemble: cycle still closed after its temporary cut");
-        cycle_max_kernel<<<g, 256, 0, s>>>(ids, m, T, cyc, offset, best);
+        cycle_max_kernel<<<gc, 256, 0, s>>>(cids, mc, T, all, offset, best);
         CURC_LAUNCH_CHECK();
-        cycle_cut_kernel<<<g, 256, 0, s>>>(ids, m, T, cyc, best, leader_of_head, nx, pv);
+        cycle_cut_kernel<<<gc, 256, 0, s>>>(cids, mc, T, all, best, leader_of_head, nx, pv);
         CURC_LAUNCH_CHECK();
-        if (rank_members(ids, m, n_total, nx, pv, offset, pos_in_ids, k, R, a, s))
+        if (rank_members(cids, mc, n_total, nx, pv, offset, pos_in_cyc, kc, T, a, s))
             throw std::runtime_error("assemble: unresolved chain links after cutting cycles");
+        cycle_merge_kernel<<<gc, 256, 0, s>>>(cidx, mc, T, R);
+        CURC_LAUNCH_CHECK();
     }
     sp_rank.stop();
     SubStage sp_place("assembly.order_place");
