@@ -46,8 +46,9 @@ def parse():
     ap.add_argument("--pairs", type=int, default=10_000_000)
     ap.add_argument("--genome", type=int, default=50_000_000)
     ap.add_argument("--cpu-sample-pairs", type=int, default=100_000)
-    ap.add_argument("--ref-sample-pairs", type=int, default=500_000)
+    ap.add_argument("--ref-sample-pairs", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cli", action="store_true", help="skip the whole-file `curc -c` measurement")
     return ap.parse_args()
 
 
@@ -185,6 +186,17 @@ def run_ours(a, rank, world):
                                            "unmap_n_ref", "ref_off", "ref_len_map", "unmap_ref_off", "unmap_ref_len",
                                            "unmap_n_ref_off", "unmap_n_ref_len"])
     d2h += sum(ctx.get(f"mis_off_{m}").nbytes for m in range(1, L // 5 + 1))
+    cli = None
+    if not a.no_cli and rank == 0:
+        with tempfile.TemporaryDirectory() as td:
+            v_full, t_full, sz_full = cli_run(ctx, w, td, "full")
+            ws = workload(a.ref_sample_pairs, a.genome, seed=1)
+            v_s, t_s, sz_s = cli_run(ctx, ws, td, "sample")
+        cli = {"value": v_full, "unit": "Mbases/s", "s": t_full, "archive_bytes": sz_full,
+               "sample_value": v_s, "sample": f"{a.ref_sample_pairs} pairs of the same generator (the reference "
+                                               f"arm's sample), {t_s:.2f} s, archive {sz_s} bytes",
+               "includes": "FASTQ parse and block split, device path, host stream coders, archive write "
+                           "(in-process call; files in page cache)"}
     step_s = dev_ms / 1000.0 / a.steps
     if world > 1:
         t = torch.tensor([step_s, e2e_s], dtype=torch.float64, device=f"cuda:{dev}")
@@ -198,7 +210,7 @@ def run_ours(a, rank, world):
     res = dict(bases=bases, n=n, L=L, step_s=step_s, e2e_s=e2e_s, wall=wall, launches=launches, stats=stats,
                stage_ms={k: v / a.steps for k, v in stage_tot.items()},
                substage_ms={k: round(v / a.steps, 3) for k, v in sub_tot.items()}, clocks=clocks.summary(),
-               h2d=int(seqs.size), d2h=int(d2h))
+               h2d=int(seqs.size), d2h=int(d2h), cli=cli)
     ctx.close()
     return res
 
@@ -218,6 +230,25 @@ def cpu_baseline(a):
                       f"block streams without the entropy coders, {dt:.1f} s"}
 
 
+# Record headers long enough for the reference's block-boundary heuristic
+# (it matches more than 5 bytes of the first header at a line start).
+FASTQ_NAME = b"synthetic_read_"
+
+
+def cli_run(ctx, w, td, tag):
+    """`curc -c` of a workload through the library (FASTQ files on disk to a
+    .curc archive), timed from the call to the archive's close."""
+    files = w.write(os.path.join(td, tag), name=FASTQ_NAME)
+    t = time.perf_counter()
+    ctx.compress_files(files, os.path.join(td, tag + ".curc"), 1.0, True, os.path.join(ROOT, "curc_b200", "_build", "bsc"),
+                       td)
+    dt = time.perf_counter() - t
+    size = os.path.getsize(os.path.join(td, tag + ".curc"))
+    for f in files + [os.path.join(td, tag + ".curc")]:
+        os.remove(f)
+    return w.bases / dt / 1e6, dt, size
+
+
 def run_reference(a):
     """The reference `curc -c` (built from its sources, oracle/_ref) end to
     end on a bounded sample of the workload, on this box."""
@@ -228,13 +259,13 @@ def run_reference(a):
     w = workload(a.ref_sample_pairs, a.genome, seed=1)
     times = []
     with tempfile.TemporaryDirectory() as td:
-        files = w.write(os.path.join(td, "in"))
+        files = w.write(os.path.join(td, "in"), name=FASTQ_NAME)
         env = dict(os.environ, LD_PRELOAD=os.path.join(ref_dir, "libzero_alloc.so"))
         for i in range(a.warmup + a.steps):
             t = time.perf_counter()
             r = subprocess.run([exe, "-c", "-i", ",".join(files), "-o", f"out{i}", "--working_dir", td,
                                 "--preserve_order"], cwd=ref_dir, env=env, capture_output=True, text=True,
-                               timeout=900)
+                               timeout=300)
             dt = time.perf_counter() - t
             if r.returncode != 0:
                 return None, f"reference exited {r.returncode}: {r.stdout[-200:]} {r.stderr[-200:]}"
@@ -309,6 +340,8 @@ def main():
         "clocks": r["clocks"],
         "gpu_launches": r["launches"],
     }
+    if r["cli"]:
+        out["cli_e2e"] = r["cli"]
     if not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(a)
     print(json.dumps(out))

@@ -36,6 +36,9 @@ def lib() -> ctypes.CDLL:
         L.curc_block_stage_ms.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
         L.curc_ctx_keep_intermediates.argtypes = [c_p, c_int]
         L.curc_kernel_launches.argtypes = []
+        L.curc_compress_files.argtypes = [c_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                          c_int, c_int, c_int, ctypes.c_char_p, ctypes.c_char_p,
+                                          ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
         L.curc_kernel_launches.restype = ctypes.c_uint64
         _lib = L
     return _lib
@@ -110,6 +113,18 @@ class Context:
         v = ctypes.c_float()
         self._check(lib().curc_block_stage_ms(self._h, stage.encode(), ctypes.byref(v)), "curc_block_stage_ms")
         return float(v.value)
+
+    def compress_files(self, files, archive: str, block_ratio: float = 1.0, preserve_order: bool = False,
+                       bsc: str = "", tmpdir: str = "/tmp", flzma2_level: int = 10, flzma2_threads: int = 16):
+        """`curc -c` through the library: FASTQ file(s) to a .curc archive.
+        Returns (reads, blocks)."""
+        reads, blocks = ctypes.c_uint64(), ctypes.c_uint32()
+        f2 = files[1].encode() if len(files) > 1 else None
+        self._check(lib().curc_compress_files(self._h, files[0].encode(), f2, archive.encode(), block_ratio,
+                                              int(preserve_order), flzma2_level, flzma2_threads, bsc.encode(),
+                                              tmpdir.encode(), ctypes.byref(reads), ctypes.byref(blocks)),
+                    "curc_compress_files")
+        return reads.value, blocks.value
 
     def pack_device(self, seqs_ptr: int, n: int, L: int, packed_ptr: int, has_n_ptr: int, stream: int = 0):
         self._check(lib().curc_pack_device(self._h, ctypes.c_void_p(seqs_ptr), n, L, ctypes.c_void_p(packed_ptr),

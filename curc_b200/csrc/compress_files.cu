@@ -4,7 +4,9 @@
 // (the reference's process() + block_compress(), preprocess.cpp:66-283).
 #include <unistd.h>
 
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <future>
 #include <memory>
 #include <string>
@@ -38,6 +40,93 @@ std::shared_ptr<Snapshot> snapshot(const Block& b) {
     }
     return s;
 }
+
+// Ingest sink that streams each window's sequences to the device: parsed
+// into one of two pinned staging buffers, copied asynchronously into the
+// block's device input while the next window is read and parsed; the block
+// then runs and its streams are coded on a host thread.
+class DeviceSink : public host::IngestSink {
+public:
+    DeviceSink(Block& blk, bool po, bool pe, const host::CoderParams& cp, bool verbose)
+        : blk_(blk), po_(po), pe_(pe), cp_(cp), verbose_(verbose) {
+        for (auto& e : ev_) CURC_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    ~DeviceSink() override {
+        for (auto& e : ev_) cudaEventSynchronize(e);
+        for (auto& e : ev_) cudaEventDestroy(e);
+        for (auto& b : stage_)
+            if (b.ptr) cudaFreeHost(b.ptr);
+    }
+    void begin_block(size_t max_bytes, int L) override {
+        t_begin_ = clk::now();
+        L_ = L;
+        blk_.arena.reset();
+        dev_ = blk_.arena.alloc<uint8_t>(max_bytes + 16);
+        cap_ = max_bytes;
+        off_ = 0;
+        reads_ = 0;
+    }
+    char* window_buffer(size_t bytes) override {
+        cur_ ^= 1;
+        Stage& st = stage_[cur_];
+        CURC_CHECK(cudaEventSynchronize(ev_[cur_]));  // its last copy is done
+        if (st.size < bytes) {
+            if (st.ptr) CURC_CHECK(cudaFreeHost(st.ptr));
+            st.ptr = nullptr;
+            CURC_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&st.ptr), bytes, cudaHostAllocDefault));
+            st.size = bytes;
+        }
+        return st.ptr;
+    }
+    void window_done(uint64_t reads) override {
+        const size_t bytes = size_t(reads) * size_t(L_);
+        if (off_ + bytes > cap_) throw std::runtime_error("ingest: block larger than its bound");
+        if (bytes)
+            CURC_CHECK(cudaMemcpyAsync(dev_ + off_, stage_[cur_].ptr, bytes, cudaMemcpyHostToDevice, blk_.stream));
+        CURC_CHECK(cudaEventRecord(ev_[cur_], blk_.stream));
+        off_ += bytes;
+        reads_ += reads;
+    }
+    void end_block() override {
+        const auto ta = clk::now();
+        blk_.run(dev_, reads_, L_, po_, pe_);
+        const auto tb = clk::now();
+        auto snap = snapshot(blk_);
+        const auto tc = clk::now();
+        const size_t bi = bodies.size();
+        const bool verbose = verbose_;
+        const host::CoderParams cp = cp_;
+        bodies.push_back(std::async(std::launch::async, [snap, cp, verbose, bi] {
+            const auto e0 = clk::now();
+            std::string body = host::encode_block(snap->view, cp);
+            if (verbose) std::fprintf(stderr, "curc: block %zu coders %.3f s\n", bi, secs(e0, clk::now()));
+            return body;
+        }));
+        if (verbose_)
+            std::fprintf(stderr, "curc: block %zu ingest and copy %.3f s, device %.3f s, snapshot %.3f s (%llu reads)\n",
+                         bi, secs(t_begin_, ta), secs(ta, tb), secs(tb, tc), (unsigned long long)reads_);
+    }
+    std::vector<std::future<std::string>> bodies;
+
+private:
+    using clk = std::chrono::steady_clock;
+    static double secs(clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); }
+    struct Stage {
+        char* ptr = nullptr;
+        size_t size = 0;
+    };
+    Block& blk_;
+    bool po_, pe_;
+    host::CoderParams cp_;
+    bool verbose_;
+    Stage stage_[2];
+    cudaEvent_t ev_[2];
+    int cur_ = 0, L_ = 0;
+    uint8_t* dev_ = nullptr;
+    size_t cap_ = 0, off_ = 0;
+    uint64_t reads_ = 0;
+    clk::time_point t_begin_;
+};
 
 }  // namespace
 
@@ -73,18 +162,13 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
         cp.bsc_path = bsc_path;
         cp.tmpdir = tmpdir;
         const std::string s2 = f2 ? f2 : "";
-        std::vector<std::future<std::string>> bodies;
-        int L = 0;
-        auto res = curc::host::ingest_fastq(f1, s2, block_ratio, [&](std::vector<char>&& seqs, uint64_t n, int len) {
-            L = len;
-            blk.arena.reset();
-            const size_t bytes = size_t(n) * len;
-            uint8_t* d = blk.arena.alloc<uint8_t>(bytes + 16);
-            if (bytes) CURC_CHECK(cudaMemcpyAsync(d, seqs.data(), bytes, cudaMemcpyHostToDevice, blk.stream));
-            blk.run(d, n, len, preserve_order != 0, !s2.empty());
-            auto snap = curc::snapshot(blk);
-            bodies.push_back(std::async(std::launch::async, [snap, cp] { return curc::host::encode_block(snap->view, cp); }));
-        });
+        // CURC_VERBOSE=1 prints host-side stage times to stderr
+        const bool verbose = std::getenv("CURC_VERBOSE") != nullptr;
+        const auto t0 = std::chrono::steady_clock::now();
+        curc::DeviceSink sink(blk, preserve_order != 0, !s2.empty(), cp, verbose);
+        const auto res = curc::host::ingest_fastq(f1, s2, block_ratio, sink);
+        const int L = res.read_len;
+        auto& bodies = sink.bodies;
         blk.keep_intermediates = keep_inter;
         FILE* out = std::fopen(archive_path, "wb");
         if (!out) throw std::runtime_error(std::string("cannot write ") + archive_path);
@@ -95,6 +179,9 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
             std::fwrite(b.data(), 1, b.size(), out);
         }
         std::fclose(out);
+        if (verbose)
+            std::fprintf(stderr, "curc: total %.3f s\n",
+                         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
         if (reads_out) *reads_out = res.reads;
         if (blocks_out) *blocks_out = uint32_t(res.blocks);
         return CURC_OK;

@@ -206,7 +206,8 @@ struct MoveId {
 template <class Acc>
 void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt, uint32_t* next, uint32_t* prev,
                      uint16_t* offset, Arena& a, cudaStream_t s) {
-    if (cnt == 0) return;
+    // one read cannot follow itself: with fewer than two ends nothing links
+    if (cnt < 2) return;
     auto mk = a.mark();
     uint32_t* suf2 = a.alloc<uint32_t>(cnt);
     uint32_t* tmp = a.alloc<uint32_t>(cnt);

@@ -17,7 +17,9 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <future>
@@ -266,6 +268,18 @@ std::string pe_order(const uint32_t* order, size_t n, int level, int thr) {
 
 }  // namespace
 
+// CURC_VERBOSE=1: time of each coder on stderr.
+template <class F>
+std::string timed(const char* what, F&& f) {
+    static const bool verbose = std::getenv("CURC_VERBOSE") != nullptr;
+    if (!verbose) return f();
+    const auto t0 = std::chrono::steady_clock::now();
+    std::string r = f();
+    std::fprintf(stderr, "curc:   coder %-16s %.3f s, %zu bytes\n", what,
+                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), r.size());
+    return r;
+}
+
 std::string encode_block(const BlockView& v, const CoderParams& cp) {
     const int L = v.read_len;
     const auto& S = [&](const char* name) -> const Buf& { return v.get(name); };
@@ -284,7 +298,7 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
     // concurrent coders
     std::future<std::string> f_idpos, f_strand, f_ref, f_peorder;
     if (v.preserve_order) {
-        f_idpos = std::async(std::launch::async, [&] {
+        f_idpos = std::async(std::launch::async, [&] { return timed("id_pos", [&] {
             const Buf& b = S("id_to_pos");
             const uint64_t* p = reinterpret_cast<const uint64_t*>(b.ptr);
             const size_t n = b.size / 8;
@@ -296,13 +310,13 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
                 return fl2(p, n * 8, lvl, thr);
             }
             return join_std ? pe_id_to_pos<uint32_t>(p, n, lvl, thr) : pe_id_to_pos<uint64_t>(p, n, lvl, thr);
-        });
+        }); });
     }
-    f_strand = std::async(std::launch::async, [&] {
+    f_strand = std::async(std::launch::async, [&] { return timed("strand", [&] {
         const Buf& b = S("strand");
         return bsc_strand(cp.bsc_path, cp.tmpdir, b.ptr, b.size);
-    });
-    f_ref = std::async(std::launch::async, [&] {
+    }); });
+    f_ref = std::async(std::launch::async, [&] { return timed("ref", [&] {
         std::string joined_ref;
         joined_ref.reserve(S("ref").size + S("unmap_ref").size + S("unmap_n_ref").size);
         for (const char* nm : {"ref", "unmap_ref", "unmap_n_ref"})
@@ -320,7 +334,7 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
         std::string r = fl2(enc, clen, lvl, thr);
         delete[] enc;
         return r;
-    });
+    }); });
     if (!v.preserve_order && v.paired_end) {
         f_peorder = std::async(std::launch::async, [&] {
             const Buf& b = S("pe_order");
@@ -349,14 +363,18 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
     }
     const double est = simpleUintCompressionEstimate(S("ref").size, ref_std ? 0xFFFFFFFFull : ~0ull);
     const int period = ref_std ? 2 : 3;
+    std::string maps = timed("maps", [&] {
     std::string maps;
     for (auto pr : {std::make_pair("ref_off", "ref_len_map"), std::make_pair("unmap_ref_off", "unmap_ref_len"),
                     std::make_pair("unmap_n_ref_off", "unmap_n_ref_len")}) {
         maps += blob(plain(pr.first, LZMA_CODER, period, est));
         maps += blob(plain(pr.second, LZMA_CODER, 0, 1));
     }
-    const std::string mis_cnt = plain("mis_cnt", PPMD7_CODER, 2, 1);
-    const std::string mis_base = plain("mis_base", PPMD7_CODER, 2, COMPRESSION_ESTIMATION_MIS_SYM);
+    return maps;
+    });
+    const std::string mis_cnt = timed("mis_cnt", [&] { return plain("mis_cnt", PPMD7_CODER, 2, 1); });
+    const std::string mis_base =
+        timed("mis_base", [&] { return plain("mis_base", PPMD7_CODER, 2, COMPRESSION_ESTIMATION_MIS_SYM); });
 
     std::string out = hdr;
     if (v.preserve_order) out += blob(f_idpos.get());

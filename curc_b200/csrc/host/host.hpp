@@ -39,16 +39,25 @@ std::string archive_header(bool po, bool pe, int read_len, int blocks);
 // FASTQ ingest.  Reads single-end (f2 empty) or paired-end files in the
 // reference's 50 MB windows (25 MB per mate) cut at record boundaries by its
 // header heuristic, and closes a block once the bytes read since the last
-// cut exceed block_ratio of the input (preprocess.cpp:66-254).  Each block
-// is handed over as n x L ASCII sequences in block order (mates
-// interleaved); `sink` returns false to stop.
+// cut exceed block_ratio of the input (preprocess.cpp:66-254).  The
+// sequences go to the sink window by window, n x L ASCII bytes in block
+// order (mates interleaved).
+struct IngestSink {
+    virtual ~IngestSink() = default;
+    // a block starts; its sequences take at most max_bytes
+    virtual void begin_block(size_t max_bytes, int L) = 0;
+    // where the next window's sequences go (at most `bytes`)
+    virtual char* window_buffer(size_t bytes) = 0;
+    // the window's `reads` sequences are in the buffer
+    virtual void window_done(uint64_t reads) = 0;
+    virtual void end_block() = 0;
+};
 struct IngestResult {
     int read_len = 0;
     uint64_t reads = 0;
     int blocks = 0;
 };
-IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double block_ratio,
-                          const std::function<void(std::vector<char>&& seqs, uint64_t n, int L)>& sink);
+IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double block_ratio, IngestSink& sink);
 
 // Read length of the first record (preprocess.cpp:286-300).
 int first_read_length(const std::string& f1);

@@ -1,11 +1,23 @@
 // FASTQ ingest with the reference's block split (preprocess.cpp:66-254).
+//
+// The windows and block boundaries are the reference's; inside a window the
+// work is spread over host threads: the window is read with parallel preads,
+// its newlines are counted per chunk, and every chunk then copies the
+// sequence lines (line 1 of each 4-line record) it starts to their slots in
+// the caller's buffer (mates interleaved).
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
+#include <thread>
 
 #include "host.hpp"
 
@@ -13,6 +25,95 @@ namespace curc {
 namespace host {
 
 namespace {
+
+// Fixed team of threads running one indexed job at a time.  Tasks are
+// claimed from a (generation, index) word by compare-and-swap, so a thread
+// still finishing one job never claims a task of the next.
+class Team {
+public:
+    explicit Team(int n) : size_(n) {
+        for (int i = 1; i < n; ++i) workers_.emplace_back([this] { loop(); });
+    }
+    ~Team() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    int size() const { return size_; }
+    // Runs f(0..tasks-1) on the team and the caller; rethrows the first error.
+    void run(int tasks, const std::function<void(int)>& f) {
+        uint32_t g0;
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            job_ = &f;
+            tasks_ = tasks;
+            left_ = tasks;
+            err_ = nullptr;
+            g0 = uint32_t(++gen_);
+            claim_.store(uint64_t(g0) << 32);
+        }
+        cv_.notify_all();
+        work(g0, &f, tasks);
+        std::unique_lock<std::mutex> g(mu_);
+        done_.wait(g, [&] { return left_ == 0; });
+        job_ = nullptr;
+        if (err_) std::rethrow_exception(err_);
+    }
+
+private:
+    void work(uint32_t gen, const std::function<void(int)>* job, int tasks) {
+        for (;;) {
+            uint64_t v = claim_.load();
+            int t;
+            for (;;) {
+                if (uint32_t(v >> 32) != gen || int(v & 0xFFFFFFFFu) >= tasks) return;
+                if (claim_.compare_exchange_weak(v, v + 1)) break;
+            }
+            t = int(v & 0xFFFFFFFFu);
+            try {
+                (*job)(t);
+            } catch (...) {
+                std::lock_guard<std::mutex> g(mu_);
+                if (!err_) err_ = std::current_exception();
+            }
+            std::lock_guard<std::mutex> g(mu_);
+            if (--left_ == 0) done_.notify_all();
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(int)>* job;
+            int tasks;
+            uint32_t gen;
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cv_.wait(g, [&] { return gen_ != seen; });
+                seen = gen_;
+                if (stop_) return;
+                if (!job_) continue;
+                job = job_;
+                tasks = tasks_;
+                gen = uint32_t(gen_);
+            }
+            work(gen, job, tasks);
+        }
+    }
+    int size_;
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int)>* job_ = nullptr;
+    int tasks_ = 0, left_ = 0;
+    std::atomic<uint64_t> claim_{0};
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+    std::exception_ptr err_;
+};
 
 struct File {
     int fd = -1;
@@ -27,14 +128,23 @@ struct File {
     ~File() {
         if (fd >= 0) ::close(fd);
     }
-    void read_at(uint64_t off, size_t n, std::vector<char>& buf) const {
-        buf.resize(n + 1);
+    void read_range(uint64_t off, size_t n, char* dst) const {
         size_t got = 0;
         while (got < n) {
-            const ssize_t k = ::pread(fd, buf.data() + got, n - got, off_t(off + got));
+            const ssize_t k = ::pread(fd, dst + got, n - got, off_t(off + got));
             if (k <= 0) throw std::runtime_error("short read");
             got += size_t(k);
         }
+    }
+    // n bytes at off into buf (plus a terminating zero), in parallel pieces
+    void read_at(uint64_t off, size_t n, std::vector<char>& buf, Team& team) const {
+        buf.resize(n + 1);
+        const int T = team.size();
+        const size_t piece = (n + T - 1) / T;
+        team.run(T, [&](int t) {
+            const size_t a = std::min(n, size_t(t) * piece), b = std::min(n, a + piece);
+            if (b > a) read_range(off + a, b - a, buf.data() + a);
+        });
         buf[n] = '\0';
     }
 };
@@ -64,39 +174,64 @@ size_t cut_window(const std::vector<char>& b, size_t end) {
     throw std::runtime_error("no record boundary found in a 50 MB window");
 }
 
-// One record's sequence line (preprocess.cpp:147-160); `lim` bounds the
-// scan (a record cut off by the end of the data is an error).
-inline const char* next_sequence(const std::vector<char>& b, size_t lim, size_t& i, int L) {
-    auto line_end = [&](size_t k) {
-        while (k < lim && b[k] != '\n') ++k;
-        if (k >= lim) throw std::runtime_error("truncated FASTQ record");
-        return k;
-    };
-    i = line_end(i) + 1;
-    const size_t st = i;
-    i = line_end(i);
-    if (long(i - st) != L) throw std::runtime_error("read length isn't fix");
-    i = line_end(i + 1) + 1;
-    i = line_end(i) + 1;
-    return b.data() + st;
+// Sequence lines of the records in b[0, end) (which starts at a record and
+// ends after a newline) to dst + record * stride; returns the record count.
+// Every sequence line must hold L bases (preprocess.cpp:147-160).
+uint64_t parse_window(const std::vector<char>& b, size_t end, int L, char* dst, size_t stride, Team& team) {
+    if (end == 0) return 0;
+    if (b[end - 1] != '\n') throw std::runtime_error("truncated FASTQ record");
+    const int T = std::max(1, std::min(team.size() * 4, int(end / 65536) + 1));
+    const size_t piece = (end + T - 1) / T;
+    std::vector<uint64_t> nl(T + 1, 0);
+    team.run(T, [&](int t) {
+        const size_t a = std::min(end, size_t(t) * piece), e = std::min(end, a + piece);
+        nl[t + 1] = uint64_t(std::count(b.data() + a, b.data() + e, '\n'));
+    });
+    for (int t = 0; t < T; ++t) nl[t + 1] += nl[t];
+    const uint64_t lines = nl[T];
+    if (lines % 4) throw std::runtime_error("truncated FASTQ record");
+    team.run(T, [&](int t) {
+        const size_t a = std::min(end, size_t(t) * piece), e = std::min(end, a + piece);
+        // lines starting in [a, e): at a (if a line starts there) and after
+        // every newline before e - 1
+        uint64_t li = nl[t];
+        size_t p = a;
+        if (a > 0 && b[a - 1] != '\n') {
+            const char* q = static_cast<const char*>(std::memchr(b.data() + a, '\n', e - a));
+            if (!q) return;
+            p = size_t(q - b.data()) + 1;
+            ++li;
+        }
+        while (p < e && p < end) {
+            const char* q = static_cast<const char*>(std::memchr(b.data() + p, '\n', end - p));
+            const size_t le = size_t(q - b.data());
+            if ((li & 3) == 1) {
+                if (le - p != size_t(L)) throw std::runtime_error("read length isn't fix");
+                std::memcpy(dst + (li >> 2) * stride, b.data() + p, size_t(L));
+            }
+            ++li;
+            p = le + 1;
+        }
+    });
+    return lines / 4;
 }
 
 }  // namespace
 
 int first_read_length(const std::string& f1) {
     File f(f1);
-    std::vector<char> b;
-    f.read_at(0, size_t(std::min<uint64_t>(f.size, 1 << 16)), b);
+    std::vector<char> b(size_t(std::min<uint64_t>(f.size, 1 << 16)) + 1);
+    f.read_range(0, b.size() - 1, b.data());
+    b.back() = '\0';
     size_t e1 = 0;
-    while (e1 < b.size() && b[e1] != '\n') ++e1;
+    while (e1 + 1 < b.size() && b[e1] != '\n') ++e1;
     size_t e2 = e1 + 1;
-    while (e2 < b.size() && b[e2] != '\n') ++e2;
-    if (e2 >= b.size()) throw std::runtime_error("cannot read the first record of " + f1);
+    while (e2 + 1 < b.size() && b[e2] != '\n') ++e2;
+    if (e2 + 1 >= b.size()) throw std::runtime_error("cannot read the first record of " + f1);
     return int(e2 - e1 - 1);
 }
 
-IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double ratio,
-                          const std::function<void(std::vector<char>&&, uint64_t, int)>& sink) {
+IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double ratio, IngestSink& sink) {
     IngestResult res;
     const bool pe = !f2.empty();
     File a(f1);
@@ -111,47 +246,49 @@ IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double r
     const uint64_t fq = a.size;
     const uint64_t block_bytes = pe ? uint64_t(2 * double(fq) * ratio) : uint64_t(double(fq) * ratio);
     const uint64_t win = pe ? 25000000 : 50000000;
+    const int mates = pe ? 2 : 1;
+    Team team(int(std::max(1u, std::min(32u, std::thread::hardware_concurrency()))));
     uint64_t total = 0, last_total = 0;
-    std::vector<char> wa, wb, seqs;
-    uint64_t n = 0;
-    auto flush = [&] {
-        sink(std::move(seqs), n, L);
-        seqs = std::vector<char>();
-        res.reads += n;
-        n = 0;
-        ++res.blocks;
-        if (res.blocks >= 255) throw std::runtime_error("too many blocks");
+    std::vector<char> wa, wb;
+    bool open = false;
+    auto begin_block = [&] {
+        // sequence bytes of the block are at most its FASTQ bytes
+        const uint64_t rest = (fq - total) * mates;
+        sink.begin_block(size_t(std::min(rest, block_bytes + 2 * win * mates)), L);
+        open = true;
     };
     while (total < fq) {
+        if (!open) begin_block();
         size_t end = size_t(std::min(win, fq - total));
-        a.read_at(total, end, wa);
-        if (pe) b->read_at(total, end, wb);
+        a.read_at(total, end, wa, team);
+        if (pe) b->read_at(total, end, wb, team);
         total += end;
         if (total < fq) {
             const size_t ne = cut_window(wa, end);
             total -= (end - ne);
             end = ne;
         }
-        size_t i = 0, j = 0;
-        const size_t lim_b = pe ? wb.size() - 1 : 0;
-        while (i < end) {
-            const char* s1 = next_sequence(wa, wa.size() - 1, i, L);
-            seqs.insert(seqs.end(), s1, s1 + L);
-            ++n;
-            if (pe) {
-                const char* s2 = next_sequence(wb, lim_b, j, L);
-                seqs.insert(seqs.end(), s2, s2 + L);
-                ++n;
-            }
-        }
+        char* dst = sink.window_buffer(end * mates);
+        const uint64_t n = parse_window(wa, end, L, dst, size_t(L) * mates, team);
+        if (pe && parse_window(wb, end, L, dst + L, size_t(L) * mates, team) != n)
+            throw std::runtime_error("paired-end files hold different record counts");
+        sink.window_done(n * mates);
+        res.reads += n * mates;
         uint64_t brb = total - last_total;
         if (pe) brb *= 2;
         if (brb > block_bytes) {
-            flush();
+            sink.end_block();
+            open = false;
+            ++res.blocks;
+            if (res.blocks >= 255) throw std::runtime_error("too many blocks");
             last_total = total;
         }
     }
-    if (total - last_total > 0) flush();
+    if (open) {
+        sink.end_block();
+        ++res.blocks;
+        if (res.blocks >= 255) throw std::runtime_error("too many blocks");
+    }
     return res;
 }
 
