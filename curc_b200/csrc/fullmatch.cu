@@ -12,9 +12,8 @@
 // organised per run of equal suffix strings instead: no fixed 4^10 cost,
 // and one thread per run executes the reference's merge steps for that run.
 //
-// (1) is done as a parallel stable merge of the per-symbol runs: each
-// element's output position is its rank in its run plus, for every other
-// run, the number of elements that precede it (binary search).
+// (1) is done as a tree of parallel stable pairwise merges of the
+// per-symbol runs (merge path).
 #include "compact.cuh"
 #include "stages.cuh"
 
@@ -75,47 +74,56 @@ __global__ void run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf, con
     bounds[c] = c == Acc::ALPHA ? m : lo;
 }
 
-// Output position of element i: its rank in its symbol run plus, for every
-// other run, the number of that run's elements that precede it.
-template <class Acc>
-__device__ __forceinline__ void merge_one(const Acc& acc, const uint32_t* __restrict__ suf, int off,
-                                          const uint32_t (&bd)[Acc::ALPHA + 1], uint32_t i,
-                                          uint32_t* __restrict__ out) {
-    int x = 0;
-    while (x + 1 <= Acc::ALPHA && bd[x + 1] <= i) ++x;
-    const uint32_t me = suf[i];
-    const int len = acc.L - off;
-    uint32_t pos = i - bd[x];
-#pragma unroll
-    for (int y = 0; y < Acc::ALPHA; ++y) {
-        if (y == x) continue;
-        uint32_t lo = bd[y], count = bd[y + 1] - bd[y];
-        // y < x: elements <= me precede; y > x: elements < me precede
-        while (count > 0) {
-            uint32_t step = count / 2, it = lo + step;
-            const int c = acc.cmp(suf[it], off, me, off, len);
-            if (c < 0 || (c == 0 && y < x)) {
-                lo = it + 1;
-                count -= step + 1;
-            } else {
-                count = step;
-            }
-        }
-        pos += lo - bd[y];
-    }
-    out[pos] = me;
-}
+// Stable merge of the symbol runs by read[off, L), as a tree of pairwise
+// merges of adjacent runs (level l merges groups of 2^l runs; ties go to the
+// lower run, as in the reference's stable merges), each
+// output element placed by merge path: a thread takes MP_ITEMS consecutive
+// outputs, finds by bisection how many of them precede in each of the two
+// inputs, and then merges sequentially.  About log2(n) / MP_ITEMS + 1
+// comparisons per output and level, instead of a binary search per run.
+constexpr int MP_ITEMS = 8;
 
-// Stable merge of the symbol runs by read[off, L).
 template <class Acc>
-__global__ void merge_runs_kernel(Acc acc, const uint32_t* __restrict__ suf, const uint32_t* __restrict__ m_dev,
-                                  int off, const uint32_t* __restrict__ bounds, uint32_t* __restrict__ out) {
+__global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                   const uint32_t* __restrict__ bounds, const uint32_t* __restrict__ m_dev,
+                                   int width) {
     const uint32_t m = *m_dev;
     uint32_t bd[Acc::ALPHA + 1];
 #pragma unroll
     for (int c = 0; c <= Acc::ALPHA; ++c) bd[c] = bounds[c];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-        merge_one(acc, suf, off, bd, i, out);
+    const int len = acc.L - off;
+    auto run_at = [&](int r) { return bd[r < Acc::ALPHA ? r : Acc::ALPHA]; };
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x * MP_ITEMS;
+    for (uint64_t d0 = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * MP_ITEMS; d0 < m; d0 += stride) {
+        const uint32_t dend = uint32_t(min(uint64_t(m), d0 + MP_ITEMS));
+        uint32_t d = uint32_t(d0);
+        int k = 0;
+        while (d < dend) {
+            // the pair of run groups that holds output d
+            uint32_t a0 = run_at(2 * k * width), a1 = run_at((2 * k + 1) * width), a2 = run_at((2 * k + 2) * width);
+            while (d >= a2) {
+                ++k;
+                a0 = run_at(2 * k * width);
+                a1 = run_at((2 * k + 1) * width);
+                a2 = run_at((2 * k + 2) * width);
+            }
+            const uint32_t na = a1 - a0, nb = a2 - a1, dd = d - a0;
+            uint32_t lo = dd > nb ? dd - nb : 0, hi = dd < na ? dd : na;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) / 2;
+                if (acc.cmp(in[a0 + mid], off, in[a1 + dd - mid - 1], off, len) <= 0)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            uint32_t i = lo, j = dd - lo;
+            const uint32_t stop = dend < a2 ? dend : a2;
+            for (; d < stop; ++d) {
+                const bool take_a = j >= nb || (i < na && acc.cmp(in[a0 + i], off, in[a1 + j], off, len) <= 0);
+                out[d] = take_a ? in[a0 + i++] : in[a1 + j++];
+            }
+        }
+    }
 }
 
 // One thread per run of equal suffix strings: the reference's bucket merge
@@ -211,12 +219,13 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     auto mk = a.mark();
     uint32_t* suf2 = a.alloc<uint32_t>(cnt);
     uint32_t* tmp = a.alloc<uint32_t>(cnt);
+    uint32_t* mtmp = a.alloc<uint32_t>(cnt);
     uint32_t* bounds = a.alloc<uint32_t>(8);
     uint32_t* len = a.alloc<uint32_t>(4);  // mp, ms for even passes, then for odd passes
     const uint32_t init[4] = {cnt, cnt, 0, 0};
     CURC_CHECK(cudaMemcpyAsync(len, init, sizeof(init), cudaMemcpyHostToDevice, s));
     Compactor cp(cnt, a, s);
-    const int gm = resident_grid(merge_runs_kernel<Acc>, 256, cnt);
+    const int gm = resident_grid(merge_level_kernel<Acc>, 256, div_up(cnt, MP_ITEMS));
     const int gg = resident_grid(merge_groups_kernel<Acc>, 128, cnt);
     constexpr int CHECK_EVERY = 8;
     int par = 0;
@@ -228,8 +237,19 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
         SubStage sp_merge("full_match.resort");
         run_bounds_kernel<Acc><<<1, 32, 0, s>>>(acc, suf, ms_in, off, bounds);
         CURC_LAUNCH_CHECK();
-        merge_runs_kernel<Acc><<<gm, 256, 0, s>>>(acc, suf, ms_in, off, bounds, suf2);
-        CURC_LAUNCH_CHECK();
+        {
+            // levels: runs merged in pairs, then pairs of pairs, ...; the last
+            // level writes suf2 (suf itself is free after the first level)
+            int levels = 0;
+            while ((1 << levels) < Acc::ALPHA) ++levels;
+            const uint32_t* src = suf;
+            for (int l = 0; l < levels; ++l) {
+                uint32_t* dst = l + 1 == levels ? suf2 : (l % 2 == 0 ? mtmp : suf);
+                merge_level_kernel<Acc><<<gm, 256, 0, s>>>(acc, off, src, dst, bounds, ms_in, 1 << l);
+                CURC_LAUNCH_CHECK();
+                src = dst;
+            }
+        }
         sp_merge.stop();
         SubStage sp_groups("full_match.groups");
         merge_groups_kernel<Acc><<<gg, 128, 0, s>>>(acc, pre, mp_in, suf2, ms_in, off, next, prev, offset);

@@ -154,25 +154,26 @@ __device__ __forceinline__ void take_from_bucket(const OverlapCtx& c, uint32_t h
 // pass reads one coalesced u32 per suffix) is set when the k-mer at kmer_index_pos+off is in the
 // presence bitmap of prefix k-mers.  The prefix set is fixed for the whole
 // stage, so this is computed once, with the suffix's words in registers.
-__global__ void offset_mask_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw, uint32_t ms, int max_off,
+// Word wi of the masks (offsets 32 wi .. 32 wi + 31).  Words after the
+// first are computed only when the passes reach them, for the suffixes
+// still unlinked then.
+__global__ void offset_mask_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw, uint32_t ms, int max_off, int wi,
                                    uint32_t* __restrict__ mask) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ms) return;
     const uint64_t* sr = sufw + uint64_t(j) * c.W;
-    for (int wi = 0; wi * 32 < max_off; ++wi) {
-        // 32 independent bitmap lookups in flight per thread
-        uint32_t word = 0;
+    // 32 independent bitmap lookups in flight per thread
+    uint32_t word = 0;
 #pragma unroll
-        for (int b = 0; b < 32; ++b) {
-            const int off = wi * 32 + b;
-            if (off > 0 && off < max_off) {
-                const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
-                const uint32_t bit = uint32_t(hv >> 32) & c.bmask;
-                word |= ((c.present[bit >> 5] >> (bit & 31)) & 1u) << b;
-            }
+    for (int b = 0; b < 32; ++b) {
+        const int off = wi * 32 + b;
+        if (off > 0 && off < max_off) {
+            const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
+            const uint32_t bit = uint32_t(hv >> 32) & c.bmask;
+            word |= ((c.present[bit >> 5] >> (bit & 31)) & 1u) << b;
         }
-        mask[uint64_t(wi) * ms + j] = word;
     }
+    mask[uint64_t(wi) * ms + j] = word;
 }
 
 // The suffixes probed in a pass: not yet linked, and with a prefix k-mer
@@ -464,7 +465,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         gather_rows_kernel<<<grid_for(uint64_t(ms) * W, 256), 256, 0, s>>>(db, W, suf, ms, sufw);
         CURC_LAUNCH_CHECK();
         if (mp) {
-            offset_mask_kernel<<<grid_for(ms, 256), 256, 0, s>>>(c, sufw, ms, p.max_off, mask);
+            offset_mask_kernel<<<grid_for(ms, 256), 256, 0, s>>>(c, sufw, ms, p.max_off, 0, mask);
             CURC_LAUNCH_CHECK();
         }
     }
@@ -491,7 +492,37 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     uint32_t passes = 0, active = ms;
     uint64_t links_seen = 0, active_sum = 0;
     const uint32_t ms0 = ms;
+    int words = 1;  // mask words computed so far
+    auto compact = [&] {
+        SubStage sp_comp("overlap.compact");
+        const int g = grid_for(ms, 256);
+        keep_count_kernel<<<g, 256, 0, s>>>(linked, ms, keepc);
+        CURC_LAUNCH_CHECK();
+        exclusive_scan<uint32_t>(keepc, kpos, ms, nullptr, a, s);
+        compact_rows_kernel<<<g, 256, 0, s>>>(suf, sufw, W, mask, words, ms, active, keepc, kpos, suf2, sufw2, mask2);
+        CURC_LAUNCH_CHECK();
+        std::swap(suf, suf2);
+        std::swap(sufw, sufw2);
+        std::swap(mask, mask2);
+        ms = active;
+        CURC_CHECK(cudaMemsetAsync(linked, 0, ms ? ms : 1, s));
+        set_u32_kernel<<<1, 1, 0, s>>>(dcount, ms);
+        CURC_LAUNCH_CHECK();
+    };
     for (int off = 1; off < p.max_off && active > 0 && mp > 0; ++off) {
+        if ((off >> 5) >= words) {  // next mask word, for the unlinked suffixes only
+            const uint64_t links = read_scalar(tally + 2, s);
+            active -= uint32_t(links - links_seen);
+            links_seen = links;
+            if (active < ms) compact();
+            if (ms) {
+                SubStage sp_mw("overlap.index_mask");
+                offset_mask_kernel<<<grid_for(ms, 256), 256, 0, s>>>(c, sufw, ms, p.max_off, words, mask);
+                CURC_LAUNCH_CHECK();
+            }
+            ++words;
+            if (active == 0) break;
+        }
         ++passes;
         active_sum += active;  // as of the last check
         SubStage sp_probe("overlap.probe_resolve");
@@ -514,22 +545,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         const uint64_t links = read_scalar(tally + 2, s);
         active -= uint32_t(links - links_seen);
         links_seen = links;
-        if (active * 2 < ms) {
-            SubStage sp_comp("overlap.compact");
-            const int g = grid_for(ms, 256);
-            keep_count_kernel<<<g, 256, 0, s>>>(linked, ms, keepc);
-            CURC_LAUNCH_CHECK();
-            exclusive_scan<uint32_t>(keepc, kpos, ms, nullptr, a, s);
-            compact_rows_kernel<<<g, 256, 0, s>>>(suf, sufw, W, mask, mw, ms, active, keepc, kpos, suf2, sufw2, mask2);
-            CURC_LAUNCH_CHECK();
-            std::swap(suf, suf2);
-            std::swap(sufw, sufw2);
-            std::swap(mask, mask2);
-            ms = active;
-            CURC_CHECK(cudaMemsetAsync(linked, 0, ms ? ms : 1, s));
-            set_u32_kernel<<<1, 1, 0, s>>>(dcount, ms);
-            CURC_LAUNCH_CHECK();
-        }
+        if (active * 2 < ms) compact();
     }
     cp.check();
     if (st) {
