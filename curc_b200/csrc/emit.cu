@@ -112,6 +112,7 @@ struct EmitCtx {
     const uint64_t* db;
     const uint8_t* nreads;
     const uint8_t* ref;          // ASCII pseudogenome
+    const uint64_t* packed;      // its 2-bit copy (one zero pad word)
     int L, W;
     uint8_t* ctx;
     uint8_t* base;
@@ -129,21 +130,44 @@ __global__ void mismatch_kernel(EmitCtx e, uint32_t T) {
     const int L = e.L;
     uint16_t mo[104];
     uint32_t found = 0, bi = e.base_idx[i];
-    const uint64_t* rd = r.is_n ? nullptr : e.db + uint64_t(r.read_id) * e.W;
-    const uint8_t* nd = r.is_n ? e.nreads + uint64_t(r.read_id) * L : nullptr;
-    const uint8_t* g = e.ref + r.pos;
-    for (int p = 0; p < L; ++p) {
-        const int src = r.strand == 0 ? p : L - 1 - p;
-        char rb = r.is_n ? char(nd[src]) : "ACGT"[code_at(rd, src)];
-        if (r.strand == 1) rb = comp_char(rb);
-        const char gb = char(g[p]);
-        if (gb != rb) {
-            if (found < m) {
-                e.ctx[bi + found] = uint8_t(gb);
-                e.base[bi + found] = uint8_t(rb);
-                if (found < 104) mo[found] = uint16_t(p);
+    if (!r.is_n) {
+        // packed read against the packed pseudogenome, 32 bases per step: the
+        // differing 2-bit groups give the mismatch positions in order
+        const uint64_t* rd = e.db + uint64_t(r.read_id) * e.W;
+        for (int p0 = 0; p0 < L; p0 += 32) {
+            const int nb = L - p0 < 32 ? L - p0 : 32;
+            const uint64_t gw = word_unaligned(e.packed, r.pos + p0, nb);
+            const uint64_t rw = r.strand == 0 ? word_at(rd, p0, nb) : revcomp_kmer(word_at(rd, L - p0 - nb, nb), nb);
+            const uint64_t x = gw ^ rw;
+            uint64_t y = (x | (x >> 1)) & 0x5555555555555555ull;  // low bit of each differing group
+            while (y) {
+                const int bit = 63 - __clzll(y);
+                y &= ~(1ull << bit);
+                const int t = nb - 1 - bit / 2;  // group index from the first base
+                if (found < m) {
+                    e.ctx[bi + found] = uint8_t("ACGT"[(gw >> (2 * (nb - 1 - t))) & 3u]);
+                    e.base[bi + found] = uint8_t("ACGT"[(rw >> (2 * (nb - 1 - t))) & 3u]);
+                    if (found < 104) mo[found] = uint16_t(p0 + t);
+                }
+                ++found;
             }
-            ++found;
+        }
+    } else {
+        const uint8_t* nd = e.nreads + uint64_t(r.read_id) * L;
+        const uint8_t* g = e.ref + r.pos;
+        for (int p = 0; p < L; ++p) {
+            const int src = r.strand == 0 ? p : L - 1 - p;
+            char rb = char(nd[src]);
+            if (r.strand == 1) rb = comp_char(rb);
+            const char gb = char(g[p]);
+            if (gb != rb) {
+                if (found < m) {
+                    e.ctx[bi + found] = uint8_t(gb);
+                    e.base[bi + found] = uint8_t(rb);
+                    if (found < 104) mo[found] = uint16_t(p);
+                }
+                ++found;
+            }
         }
     }
     if (found != m || m > 104) {
@@ -451,7 +475,7 @@ void Block::emit(StageTimer& T) {
         class_rank_kernel<<<grid_for(acc, 256), 256, 0, s>>>(key, sel, acc, d_first, crank);
         CURC_LAUNCH_CHECK();
         arena.release(mk);
-        EmitCtx e{srec, smis, base_idx, crank, d_cbase, db, nreads, hq.seq, L, W, mctx, mbase, off_all, err};
+        EmitCtx e{srec, smis, base_idx, crank, d_cbase, db, nreads, hq.seq, hq.packed, L, W, mctx, mbase, off_all, err};
         mismatch_kernel<<<grid_for(Tn, 128), 128, 0, s>>>(e, Tn);
         CURC_LAUNCH_CHECK();
     }

@@ -54,24 +54,53 @@ struct AsciiAcc {
     }
 };
 
+// bounds[c] = first index whose symbol at off-1 is >= c (the list is
+// sorted by read[off-1, L), so symbols are nondecreasing).  One block
+// narrows all boundaries at once, 64 threads each: every round samples 64
+// evenly spaced positions of the boundary's interval, so a few rounds of
+// independent loads replace a chain of ~log2(m) dependent ones.
 template <class Acc>
-__global__ void run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf, const uint32_t* __restrict__ m_dev,
-                                  int off, uint32_t* __restrict__ bounds) {
-    // bounds[c] = first index whose symbol at off-1 is >= c
-    const int c = threadIdx.x;
-    if (c > Acc::ALPHA) return;
+__global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf,
+                                                         const uint32_t* __restrict__ m_dev, int off,
+                                                         uint32_t* __restrict__ bounds) {
+    constexpr int NB = Acc::ALPHA - 1;  // boundaries to find: symbols 1 .. ALPHA-1 (at most 4)
+    constexpr uint32_t S = 64;          // samples per boundary and round
+    __shared__ uint32_t lo_s[4], hi_s[4];
+    __shared__ uint8_t sym_s[4][S];
     const uint32_t m = *m_dev;
-    uint32_t lo = 0, count = m;
-    while (count > 0) {
-        uint32_t step = count / 2, it = lo + step;
-        if (acc.sym(suf[it], off - 1) < c) {
-            lo = it + 1;
-            count -= step + 1;
-        } else {
-            count = step;
-        }
+    const int b = int(threadIdx.x / S);
+    const uint32_t t = threadIdx.x % S;
+    // invariant for boundary b: indices < lo have symbol < b+1, indices >= hi
+    // have symbol >= b+1
+    if (threadIdx.x < 4) {
+        lo_s[threadIdx.x] = 0;
+        hi_s[threadIdx.x] = m;
     }
-    bounds[c] = c == Acc::ALPHA ? m : lo;
+    __syncthreads();
+    for (;;) {
+        bool open = false;
+#pragma unroll
+        for (int q = 0; q < NB; ++q) open |= lo_s[q] < hi_s[q];
+        if (!open) break;
+        const uint32_t lo = b < NB ? lo_s[b] : 0, hi = b < NB ? hi_s[b] : 0;
+        const uint32_t span = hi - lo, k = span < S ? span : S;
+        if (b < NB && t < k) sym_s[b][t] = uint8_t(acc.sym(suf[lo + uint32_t((uint64_t(span) * t) / k)], off - 1));
+        __syncthreads();
+        if (b < NB && t == 0 && lo < hi) {
+            uint32_t f = 0;  // first sample with symbol >= b+1
+            while (f < k && sym_s[b][f] < uint32_t(b + 1)) ++f;
+            const uint32_t pf = f < k ? lo + uint32_t((uint64_t(span) * f) / k) : hi;
+            const uint32_t pp = f > 0 ? lo + uint32_t((uint64_t(span) * (f - 1)) / k) + 1 : lo;
+            lo_s[b] = k == span ? pf : pp;  // all positions sampled: exact
+            hi_s[b] = pf;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        bounds[0] = 0;
+        bounds[Acc::ALPHA] = m;
+    }
+    if (threadIdx.x < NB) bounds[threadIdx.x + 1] = lo_s[threadIdx.x];
 }
 
 // Stable merge of the symbol runs by read[off, L), as a tree of pairwise
@@ -235,7 +264,7 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
         uint32_t* mp_out = len + 2 * (par ^ 1);
         uint32_t* ms_out = mp_out + 1;
         SubStage sp_merge("full_match.resort");
-        run_bounds_kernel<Acc><<<1, 32, 0, s>>>(acc, suf, ms_in, off, bounds);
+        run_bounds_kernel<Acc><<<1, 256, 0, s>>>(acc, suf, ms_in, off, bounds);
         CURC_LAUNCH_CHECK();
         {
             // levels: runs merged in pairs, then pairs of pairs, ...; the last

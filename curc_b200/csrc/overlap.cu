@@ -193,11 +193,10 @@ struct ProbeListMove {
 
 // compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
 // bound of suffix[off, L) among the bucket's prefix[0, L-off).  Returns
-// whether an equal prefix exists; then its run start and bucket end are
-// stored and the suffix joins the run's claimers.
+// whether an equal prefix exists; then the hit (list index, run start,
+// bucket end, bucket) is set and the suffix joins the run's claimers.
 __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* __restrict__ sufw, uint32_t j, int off,
-                                          uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
-                                          RunSlot* __restrict__ run, uint32_t* __restrict__ gnext) {
+                                          RunSlot* __restrict__ run, uint32_t* __restrict__ gnext, uint4& hitrec) {
     const int cl = c.L - off;
     const uint64_t* sr = sufw + uint64_t(j) * c.W;
     const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
@@ -222,38 +221,35 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
     atomicAdd(&run[lo].claim, 1u);
     atomicMin(&run[lo].lead, j);
     gnext[j] = atomicExch(&run[lo].head, j);
-    cand[j] = lo;
-    cand_end[j] = e;
+    hitrec = make_uint4(j, lo, e, h);
     return true;
 }
 
-// Probes every listed suffix and lists the ones that met an equal prefix
-// (hlist, *hcount; order is immaterial to the resolution).  tally[0] counts
-// probes, tally[1] hits.
+// Probes every listed suffix and lists the hits (hlist, *hcount; their
+// order is immaterial to the resolution).  tally[0] counts probes,
+// tally[1] hits.
 __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
                                                     const uint32_t* __restrict__ plist,
                                                     const uint32_t* __restrict__ pcount, int off,
-                                                    uint32_t* __restrict__ cand, uint32_t* __restrict__ cand_end,
                                                     RunSlot* __restrict__ run, uint32_t* __restrict__ gnext,
-                                                    uint32_t* __restrict__ hlist, uint32_t* __restrict__ hcount,
+                                                    uint4* __restrict__ hlist, uint32_t* __restrict__ hcount,
                                                     unsigned long long* __restrict__ tally) {
-    __shared__ uint32_t s_hits[512];
+    __shared__ uint4 s_hits[512];
     __shared__ uint32_t s_n, s_base;
     uint32_t probes = 0, hits = 0;
     const uint32_t np = *pcount;
     for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < np; b0 += gridDim.x * blockDim.x) {
         const uint32_t q = b0 + threadIdx.x;
         bool hit = false;
-        uint32_t j = 0;
+        uint4 rec;
         if (q < np) {
-            j = plist[q];
             ++probes;
-            hit = probe_one(c, sufw, j, off, cand, cand_end, run, gnext);
+            hit = probe_one(c, sufw, plist[q], off, run, gnext, rec);
             hits += hit;
         }
         if (threadIdx.x == 0) s_n = 0;
         __syncthreads();
-        if (hit) s_hits[atomicAdd(&s_n, 1u)] = j;
+        if (hit) s_hits[atomicAdd(&s_n, 1u)] = rec;
         __syncthreads();
         if (threadIdx.x == 0 && s_n) s_base = atomicAdd(hcount, s_n);
         __syncthreads();
@@ -273,24 +269,21 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
 // tally[3] the members of contested runs.
 __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32_t* __restrict__ suf,
                                                       const uint64_t* __restrict__ sufw,
-                                                      const uint32_t* __restrict__ hlist,
+                                                      const uint4* __restrict__ hlist,
                                                       const uint32_t* __restrict__ hcount, int off,
-                                                      const uint32_t* __restrict__ cand,
-                                                      const uint32_t* __restrict__ cand_end,
                                                       RunSlot* __restrict__ run, const uint32_t* __restrict__ gnext,
                                                       uint8_t* __restrict__ linked,
                                                       unsigned long long* __restrict__ tally) {
     uint32_t links = 0, contested = 0;
     const uint32_t nh = *hcount;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nh; q += gridDim.x * blockDim.x) {
-        const uint32_t j = hlist[q];
-        const uint32_t lo = cand[j];
+        // members of a run share its start, bucket end and bucket
+        const uint4 hr = hlist[q];
+        const uint32_t j = hr.x, lo = hr.y, e = hr.z, h = hr.w;
         const RunSlot rs = run[lo];
         const uint32_t n = rs.claim;
-        // the run's bucket (the same for every member)
-        const uint32_t h = uint32_t(murmur64(word_at(sufw + uint64_t(j) * c.W, c.kip + off, c.k)) & c.mask);
         if (n == 1) {
-            if (link_first_free(c, suf[j], sufw + uint64_t(j) * c.W, lo, cand_end[j], off)) {
+            if (link_first_free(c, suf[j], sufw + uint64_t(j) * c.W, lo, e, off)) {
                 linked[j] = 1;
                 ++links;
                 take_from_bucket(c, h);
@@ -304,7 +297,7 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
                 for (uint32_t m = rs.head; m != INVALID; m = gnext[m])
                     if ((first || m > last) && m < best) best = m;
                 if (best == INVALID) break;
-                if (link_first_free(c, suf[best], sufw + uint64_t(best) * c.W, lo, cand_end[best], off)) {
+                if (link_first_free(c, suf[best], sufw + uint64_t(best) * c.W, lo, e, off)) {
                     linked[best] = 1;
                     ++links;
                     take_from_bucket(c, h);
@@ -447,8 +440,6 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     RunSlot* run = a.alloc<RunSlot>(mp ? mp : 1);
     run_slots_init_kernel<<<grid_for(mp ? mp : 1, 256), 256, 0, s>>>(run, mp ? mp : 1);
     CURC_LAUNCH_CHECK();
-    uint32_t* cand = a.alloc<uint32_t>(ms ? ms : 1);
-    uint32_t* cand_end = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* gnext = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* keepc = a.alloc<uint32_t>(ms ? ms : 1);
     uint32_t* kpos = a.alloc<uint32_t>(ms ? ms : 1);
@@ -479,7 +470,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     // of it has linked.  Passes are queued without a host round trip; the
     // host reads the link count every few passes to compact or stop.
     uint32_t* plist = a.alloc<uint32_t>(ms ? ms : 1);
-    uint32_t* hlist = a.alloc<uint32_t>(ms ? ms : 1);
+    uint4* hlist = a.alloc<uint4>(ms ? ms : 1);
     uint32_t* hcount = a.alloc<uint32_t>(p.max_off + 1);  // one per pass
     CURC_CHECK(cudaMemsetAsync(hcount, 0, size_t(p.max_off + 1) * 4, s));
     uint32_t* dcount = a.alloc<uint32_t>(2);  // [0] list size, [1] listed probes
@@ -531,12 +522,12 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
                ProbeFilter{linked, mask + uint64_t(off >> 5) * ms, uint32_t(off & 31)}, ProbeListMove{plist});
         sp_filter.stop();
         SubStage sp_pk("overlap.probe");
-        probe_kernel<<<gp, 512, 0, s>>>(c, sufw, plist, dcount + 1, off, cand, cand_end, run, gnext,
+        probe_kernel<<<gp, 512, 0, s>>>(c, sufw, plist, dcount + 1, off, run, gnext,
                                         hlist, hcount + off, tally);
         CURC_LAUNCH_CHECK();
         sp_pk.stop();
         SubStage sp_rk("overlap.resolve");
-        resolve_kernel<<<gr, 512, 0, s>>>(c, suf, sufw, hlist, hcount + off, off, cand, cand_end, run,
+        resolve_kernel<<<gr, 512, 0, s>>>(c, suf, sufw, hlist, hcount + off, off, run,
                                           gnext, linked, tally);
         CURC_LAUNCH_CHECK();
         sp_rk.stop();
