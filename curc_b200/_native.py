@@ -16,6 +16,9 @@ LIB_PATH = os.path.join(_HERE, "libcurc_b200.so")
 _lib = None
 
 
+BLOCK_DONE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32)
+
+
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
@@ -36,6 +39,10 @@ def lib() -> ctypes.CDLL:
         L.curc_block_stage_ms.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
         L.curc_ctx_keep_intermediates.argtypes = [c_p, c_int]
         L.curc_kernel_launches.argtypes = []
+        L.curc_batch_submit.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_int, c_int,
+                                        ctypes.POINTER(ctypes.c_uint32)]
+        L.curc_batch_drain.argtypes = [c_p, BLOCK_DONE, c_p]
+        L.curc_batch_workers.argtypes = [c_p, c_int]
         L.curc_compress_files.argtypes = [c_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
                                           c_int, c_int, c_int, ctypes.c_char_p, ctypes.c_char_p,
                                           ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
@@ -113,6 +120,39 @@ class Context:
         v = ctypes.c_float()
         self._check(lib().curc_block_stage_ms(self._h, stage.encode(), ctypes.byref(v)), "curc_block_stage_ms")
         return float(v.value)
+
+    def batch_submit(self, seqs: np.ndarray, preserve_order: bool = False, paired_end: bool = False) -> int:
+        """Queue a block ((n, L) uint8 ASCII, host memory kept alive by the
+        caller until the drain returns); returns its ticket."""
+        assert seqs.flags["C_CONTIGUOUS"] and seqs.dtype == np.uint8
+        n, L = seqs.shape
+        t = ctypes.c_uint32()
+        self._check(lib().curc_batch_submit(self._h, ctypes.c_void_p(seqs.ctypes.data), n, L, int(preserve_order),
+                                            int(paired_end), ctypes.byref(t)), "curc_batch_submit")
+        return t.value
+
+    def batch_workers(self, workers: int):
+        self._check(lib().curc_batch_workers(self._h, workers), "curc_batch_workers")
+
+    def batch_drain(self, on_block=None):
+        """Run the queued blocks; on_block(ticket) is called after each, while
+        get() returns that block's results."""
+        err = []
+
+        def cb(_user, ticket):
+            try:
+                if on_block:
+                    on_block(ticket)
+                return 0
+            except Exception as e:  # stop the drain, re-raised below
+                err.append(e)
+                return 1
+
+        fn = BLOCK_DONE(cb)
+        rc = lib().curc_batch_drain(self._h, fn, None)
+        if err:
+            raise err[0]
+        self._check(rc, "curc_batch_drain")
 
     def compress_files(self, files, archive: str, block_ratio: float = 1.0, preserve_order: bool = False,
                        bsc: str = "", tmpdir: str = "/tmp", flzma2_level: int = 10, flzma2_threads: int = 16):

@@ -285,8 +285,9 @@ int curc_block_run(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read_le
 
 int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* bytes) {
     if (!ctx || !name || !ptr || !bytes) return CURC_ERR_ARG;
-    auto it = ctx->block->host.find(name);
-    if (it == ctx->block->host.end()) {
+    const curc::Block* blk = curc::batch_current() ? curc::batch_current() : ctx->block.get();
+    auto it = blk->host.find(name);
+    if (it == blk->host.end()) {
         ctx->err = std::string("unknown result: ") + name;
         return CURC_ERR_ARG;
     }

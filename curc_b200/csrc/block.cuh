@@ -84,9 +84,45 @@ struct Block {
 
 }  // namespace curc
 
+namespace curc {
+
+// Blocks queued for curc_batch_drain: the caller's host reads (valid until
+// the drain returns).  The drain runs them on several block pipelines at
+// once (each a Block with its own stream, arena and input slot), so one
+// block's copies and host round trips overlap another's kernels.
+struct BatchItem {
+    const char* seqs;
+    uint64_t n;
+    int L;
+    bool po, pe;
+    uint32_t ticket;
+};
+struct BatchWorker {
+    Block* blk = nullptr;               // the context's own block, or `own`
+    std::unique_ptr<Block> own;
+    uint8_t* dev = nullptr;             // device input slot
+    size_t dev_cap = 0;
+    uint8_t* pin = nullptr;             // pinned staging for pageable input
+    size_t pin_cap = 0;
+    ~BatchWorker();
+};
+struct BatchQueue {
+    std::vector<BatchItem> items;
+    uint32_t next_ticket = 0;
+    int workers = 2;
+    std::vector<std::unique_ptr<BatchWorker>> pool;
+};
+
+// The block whose results curc_block_get returns on this thread while a
+// drain callback runs (null otherwise).
+Block*& batch_current();
+
+}  // namespace curc
+
 // The C-ABI context (include/curc_b200.h): one device, one block pipeline.
 struct curc_ctx {
     int device = 0;
     std::unique_ptr<curc::Block> block;
+    std::unique_ptr<curc::BatchQueue> batch;
     std::string err;
 };

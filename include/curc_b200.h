@@ -106,6 +106,26 @@ int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2, const cha
  * name. */
 int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* bytes);
 
+/* Batched path: blocks queued on a context and run by several block
+ * pipelines at once (the context's own and curc_batch_workers - 1 more, each
+ * with its own stream and device memory), so that one block's copies and
+ * host round trips overlap another's kernels.  Replaces the reference's
+ * one-thread-per-block scheduling of process() (preprocess.cpp:195-242) and
+ * its GPU mutexes (compress.cu:52-65) on one device.
+ *
+ * curc_batch_submit queues n x read_len ASCII reads (host memory that must
+ * stay valid until the drain returns) and returns a ticket.  curc_batch_drain
+ * runs every queued block; after each one it calls done(user, ticket) (one
+ * call at a time, in completion order, from the thread that ran the block),
+ * during which curc_block_get on that thread returns that block's results.
+ * A non-zero return from done stops the drain with CURC_ERR_STATE.
+ * curc_batch_workers sets the number of pipelines (1..16, default 2). */
+typedef int (*curc_block_done_fn)(void* user, uint32_t ticket);
+int curc_batch_submit(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read_len, int preserve_order,
+                      int paired_end, uint32_t* ticket);
+int curc_batch_workers(curc_ctx* ctx, int workers);
+int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user);
+
 /* Number of kernels the library has launched in this process (no
  * reference counterpart; used to report launches per benchmark step). */
 uint64_t curc_kernel_launches(void);
