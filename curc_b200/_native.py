@@ -43,6 +43,22 @@ def lib() -> ctypes.CDLL:
                                         ctypes.POINTER(ctypes.c_uint32)]
         L.curc_batch_drain.argtypes = [c_p, BLOCK_DONE, c_p]
         L.curc_batch_workers.argtypes = [c_p, c_int]
+        L.curc_learn_create.argtypes = [c_int, ctypes.POINTER(c_p)]
+        L.curc_learn_destroy.argtypes = [c_p]
+        L.curc_learn_error.argtypes = [c_p]
+        L.curc_learn_error.restype = ctypes.c_char_p
+        L.curc_learn_add_block.argtypes = [c_p, c_p]
+        L.curc_learn_anchors.argtypes = [c_p]
+        L.curc_learn_anchors.restype = c_u64
+        L.curc_learn_train.argtypes = [c_p, c_int, c_int, ctypes.c_float, c_u64, ctypes.POINTER(ctypes.c_float)]
+        L.curc_learn_model.argtypes = [c_p, ctypes.POINTER(c_p), ctypes.POINTER(c_u64)]
+        L.curc_learn_set_model.argtypes = [c_p, c_p, c_u64]
+        L.curc_learn_encode.argtypes = [c_p, c_p, ctypes.POINTER(c_p), ctypes.POINTER(c_u64)]
+        L.curc_learn_decode_check.argtypes = [c_p, c_p, c_p, c_u64, ctypes.POINTER(c_int)]
+        L.curc_learn_param_count.argtypes = []
+        L.curc_learn_param_count.restype = c_u64
+        L.curc_learn_grad.argtypes = [c_p, c_p, c_p, c_p, c_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), c_p]
+        L.curc_plain_mismatch_bytes.argtypes = [c_p, c_p]
         L.curc_compress_files.argtypes = [c_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
                                           c_int, c_int, c_int, ctypes.c_char_p, ctypes.c_char_p,
                                           ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
@@ -169,3 +185,86 @@ class Context:
     def pack_device(self, seqs_ptr: int, n: int, L: int, packed_ptr: int, has_n_ptr: int, stream: int = 0):
         self._check(lib().curc_pack_device(self._h, ctypes.c_void_p(seqs_ptr), n, L, ctypes.c_void_p(packed_ptr),
                                            ctypes.c_void_p(has_n_ptr), ctypes.c_void_p(stream)), "curc_pack_device")
+
+
+class Learner:
+    """The learned mismatch coder (curc_learn_* in include/curc_b200.h)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        rc = lib().curc_learn_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise CurcError(f"curc_learn_create: {lib().curc_last_error(None).decode()}")
+        self._h = h
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise CurcError(f"{what}: {lib().curc_learn_error(self._h).decode()}")
+
+    def close(self):
+        if self._h:
+            lib().curc_learn_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_block(self, ctx: "Context"):
+        self._check(lib().curc_learn_add_block(self._h, ctx.handle), "curc_learn_add_block")
+
+    @property
+    def anchors(self) -> int:
+        return int(lib().curc_learn_anchors(self._h))
+
+    def train(self, epochs=2, batch=4096, lr=2e-3, seed=1) -> float:
+        loss = ctypes.c_float()
+        self._check(lib().curc_learn_train(self._h, epochs, batch, lr, seed, ctypes.byref(loss)), "curc_learn_train")
+        return float(loss.value)
+
+    def model(self) -> bytes:
+        p, n = ctypes.c_void_p(), ctypes.c_uint64()
+        self._check(lib().curc_learn_model(self._h, ctypes.byref(p), ctypes.byref(n)), "curc_learn_model")
+        return ctypes.string_at(p.value, n.value)
+
+    def set_model(self, blob: bytes):
+        self._check(lib().curc_learn_set_model(self._h, blob, len(blob)), "curc_learn_set_model")
+
+    def encode(self, ctx: "Context") -> bytes:
+        p, n = ctypes.c_void_p(), ctypes.c_uint64()
+        self._check(lib().curc_learn_encode(self._h, ctx.handle, ctypes.byref(p), ctypes.byref(n)),
+                    "curc_learn_encode")
+        return ctypes.string_at(p.value, n.value)
+
+    def decode_check(self, ctx: "Context", stream: bytes) -> bool:
+        ok = ctypes.c_int()
+        self._check(lib().curc_learn_decode_check(self._h, ctx.handle, stream, len(stream), ctypes.byref(ok)),
+                    "curc_learn_decode_check")
+        return ok.value == 1
+
+    def grad(self, params: np.ndarray, x: np.ndarray, tb: np.ndarray, tg: np.ndarray):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        tb = np.ascontiguousarray(tb, dtype=np.int8)
+        tg = np.ascontiguousarray(tg, dtype=np.int8)
+        g = np.zeros_like(params)
+        loss = ctypes.c_float()
+        self._check(lib().curc_learn_grad(self._h, params.ctypes.data, x.ctypes.data, tb.ctypes.data, tg.ctypes.data,
+                                          x.shape[0], ctypes.byref(loss), g.ctypes.data), "curc_learn_grad")
+        return float(loss.value), g
+
+
+def learn_param_count() -> int:
+    return int(lib().curc_learn_param_count())
+
+
+def plain_mismatch_bytes(ctx: "Context"):
+    """Coded sizes (counts, bases, offsets) of the last block's mismatch
+    streams with the plain coders."""
+    out = (ctypes.c_uint64 * 3)()
+    rc = lib().curc_plain_mismatch_bytes(ctx.handle, out)
+    if rc != 0:
+        raise CurcError(f"curc_plain_mismatch_bytes: {lib().curc_last_error(ctx.handle).decode()}")
+    return tuple(int(v) for v in out)

@@ -395,6 +395,19 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
     return out;
 }
 
+void plain_mismatch_bytes(const BlockView& v, uint64_t out[3]) {
+    const int L = v.read_len;
+    out[0] = container(v.get("mis_cnt").ptr, v.get("mis_cnt").size, PPMD7_CODER, 2, 1).size();
+    out[1] = container(v.get("mis_base").ptr, v.get("mis_base").size, PPMD7_CODER, 2,
+                       COMPRESSION_ESTIMATION_MIS_SYM).size();
+    uint64_t o = 0;
+    for (int m = 1; m <= L / 5; ++m) {
+        const Buf& b = v.get(("mis_off_" + std::to_string(m)).c_str());
+        o += offsets(L, reinterpret_cast<const uint16_t*>(b.ptr), b.size / 2, size_t(m)).size();
+    }
+    out[2] = o;
+}
+
 std::string archive_header(bool po, bool pe, int read_len, int blocks) {
     std::string h(5, '\0');
     h[0] = char(po);

@@ -33,6 +33,9 @@ struct CoderParams {
 
 // Block body in the reference layout (compress.cu:1364-2146).
 std::string encode_block(const BlockView& v, const CoderParams& cp);
+// Coded sizes of a block's mismatch streams with the plain coders (the
+// same calls as encode_block): counts, bases, offsets.
+void plain_mismatch_bytes(const BlockView& v, uint64_t out[3]);
 // Archive header (preprocess.cpp:261-266).
 std::string archive_header(bool po, bool pe, int read_len, int blocks);
 

@@ -1,0 +1,247 @@
+// Learned mismatch coder: the integer model shared by the GPU encoder and the
+// host decoder, and the range coder.  Everything that decides a probability
+// is integer arithmetic (int8 weights, int32 accumulation, fixed-point
+// requantisation, a table for the exponential), so both sides derive
+// bit-identical 12-bit frequencies.
+//
+// What is coded, per record with mismatches (its count comes from the plain
+// mismatch-count stream): walking the read in pseudogenome order from an
+// anchor before its first base, the gap to the next mismatch (16 bins, the
+// offset inside a bin uniform), then at that mismatch the read's base (one
+// of the three other bases or N), and so on.  The network sees, at an
+// anchor: the 16 pseudogenome bases around it, the position along the
+// sequenced read (16 bins), whether it is the start anchor, and the previous
+// mismatch's read base.
+#pragma once
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifdef __CUDACC__
+#define LM_HD __host__ __device__ __forceinline__
+#else
+#define LM_HD inline
+#endif
+
+namespace curc {
+namespace learned {
+
+constexpr int IN = 96;       // input features (one-hots, zero padded)
+constexpr int HID = 128;     // hidden units per layer
+constexpr int NB = 4;        // base outcomes: the three other bases, then N
+constexpr int NG = 16;       // gap bins
+constexpr int OUT = NB + NG;
+constexpr int CTX = 16;      // pseudogenome bases around an anchor
+constexpr int LUTN = 256;    // exponential table entries
+constexpr uint32_t TOTAL = 4096;  // frequency total (12 bits)
+
+// Gap bins: [lo, lo + width) with widths 1,1,1,1,2,2,4,4,8,8,16,16,32,32,64,320.
+LM_HD int gap_bin_lo(int b) {
+    constexpr int lo[NG + 1] = {0, 1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 512};
+    return lo[b];
+}
+LM_HD int gap_bin(int g) {
+    int b = 0;
+    while (b + 1 < NG && g >= gap_bin_lo(b + 1)) ++b;
+    return b;
+}
+
+// Base outcome of read base rb at pseudogenome base gb (ASCII): index among
+// the three other bases in A<C<G<T order, or 3 for N; -1 if not a mismatch.
+LM_HD int base_outcome(char gb, char rb) {
+    if (rb == 'N') return 3;
+    const char order[4] = {'A', 'C', 'G', 'T'};
+    int k = 0;
+    for (int t = 0; t < 4; ++t) {
+        if (order[t] == gb) continue;
+        if (order[t] == rb) return k;
+        ++k;
+    }
+    return -1;
+}
+LM_HD char outcome_base(char gb, int o) {
+    if (o == 3) return 'N';
+    const char order[4] = {'A', 'C', 'G', 'T'};
+    int k = 0;
+    for (int t = 0; t < 4; ++t) {
+        if (order[t] == gb) continue;
+        if (k == o) return order[t];
+        ++k;
+    }
+    return '?';
+}
+
+LM_HD int code_of(char c) {
+    switch (c) {
+        case 'A': return 0;
+        case 'C': return 1;
+        case 'G': return 2;
+        case 'T': return 3;
+        default: return -1;
+    }
+}
+
+// Active input features of an anchor (indices of the ones), at most 19.
+// ref/rl: pseudogenome (ASCII) and its length; rpos: the record's position;
+// q: anchor offset in pseudogenome order (-1 for the start anchor); L, strand;
+// prev: previous mismatch's read base (0 if none).
+LM_HD int anchor_features(const uint8_t* ref, uint64_t rl, uint64_t rpos, int q, int L, int strand, char prev,
+                          int* idx) {
+    int n = 0;
+    for (int t = 0; t < CTX; ++t) {
+        const int64_t p = int64_t(rpos) + q - CTX / 2 + t;
+        if (p < 0 || uint64_t(p) >= rl) continue;
+        const int c = code_of(char(ref[p]));
+        if (c >= 0) idx[n++] = 4 * t + c;
+    }
+    if (q < 0) {
+        idx[n++] = 80;  // start anchor
+    } else {
+        const int rq = strand ? L - 1 - q : q;  // position along the sequenced read
+        idx[n++] = 64 + (rq * 16) / L;
+    }
+    const int pc = prev == 'N' ? 4 : code_of(prev);
+    if (pc >= 0) idx[n++] = 81 + pc;
+    return n;
+}
+
+// Integer model.  acc1 = W1[:, active] summed + b1; a1 = clamp((acc1*m1 +
+// round) >> sh1, 0, 127); the same for layer 2; z = W3 a2 + b3.
+struct Model {
+    int8_t w1[HID][IN];
+    int32_t b1[HID];
+    int8_t w2[HID][HID];
+    int32_t b2[HID];
+    int8_t w3[OUT][HID];
+    int32_t b3[OUT];
+    int32_t m1, sh1, m2, sh2;   // requantisation multipliers and shifts
+    int32_t zmul;               // logit difference -> table index (16.16)
+    uint32_t lut[LUTN];         // exp(-i/16) * 2^16, at least 1
+};
+
+LM_HD int32_t requant(int32_t acc, int32_t m, int32_t sh) {
+    if (acc <= 0) return 0;
+    const int64_t v = (int64_t(acc) * m + (int64_t(1) << (sh - 1))) >> sh;
+    return v > 127 ? 127 : int32_t(v);
+}
+
+// Frequencies (total TOTAL, each >= 1) of `k` outcomes from their logits.
+LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, uint32_t* f) {
+    int32_t mx = z[0];
+    int am = 0;
+    for (int j = 1; j < k; ++j)
+        if (z[j] > mx) {
+            mx = z[j];
+            am = j;
+        }
+    uint64_t tot = 0;
+    uint32_t e[NG];
+    for (int j = 0; j < k; ++j) {
+        const int64_t d = int64_t(mx) - z[j];
+        int64_t i = (d * M.zmul) >> 16;
+        if (i > LUTN - 1) i = LUTN - 1;
+        e[j] = M.lut[i];
+        tot += e[j];
+    }
+    uint32_t sum = 0;
+    for (int j = 0; j < k; ++j) {
+        f[j] = 1 + uint32_t((uint64_t(e[j]) * (TOTAL - uint32_t(k))) / tot);
+        sum += f[j];
+    }
+    f[am] += TOTAL - sum;
+}
+
+// The network at one anchor: base and gap frequencies.
+LM_HD void model_freqs(const Model& M, const int* idx, int nidx, uint32_t* fb, uint32_t* fg) {
+    int32_t a1[HID], a2[HID];
+    for (int h = 0; h < HID; ++h) {
+        int32_t acc = M.b1[h];
+        for (int t = 0; t < nidx; ++t) acc += M.w1[h][idx[t]];
+        a1[h] = requant(acc, M.m1, M.sh1);
+    }
+    for (int h = 0; h < HID; ++h) {
+        int32_t acc = M.b2[h];
+        for (int t = 0; t < HID; ++t) acc += int32_t(M.w2[h][t]) * a1[t];
+        a2[h] = requant(acc, M.m2, M.sh2);
+    }
+    int32_t z[OUT];
+    for (int o = 0; o < OUT; ++o) {
+        int32_t acc = M.b3[o];
+        for (int t = 0; t < HID; ++t) acc += int32_t(M.w3[o][t]) * a2[t];
+        z[o] = acc;
+    }
+    logits_to_freq(M, z, NB, fb);
+    logits_to_freq(M, z + NB, NG, fg);
+}
+
+// ------------------------------------------------------------ range coder
+// Carry-propagating range coder (32-bit range, 64-bit low with a cached
+// byte, as in LZMA's), symbols given as (cumulative, frequency, total).
+class RangeEncoder {
+public:
+    void encode(uint32_t cum, uint32_t freq, uint32_t total) {
+        const uint32_t r = range_ / total;
+        low_ += uint64_t(r) * cum;
+        range_ = r * freq;
+        while (range_ < (1u << 24)) {
+            range_ <<= 8;
+            shift_low();
+        }
+    }
+    std::string finish() {
+        for (int i = 0; i < 5; ++i) shift_low();
+        return out_;
+    }
+
+private:
+    void shift_low() {
+        if (uint32_t(low_) < 0xFF000000u || (low_ >> 32) != 0) {
+            const uint8_t carry = uint8_t(low_ >> 32);
+            if (have_cache_) out_.push_back(char(uint8_t(cache_ + carry)));
+            for (; pending_ > 0; --pending_) out_.push_back(char(uint8_t(0xFF + carry)));
+            cache_ = uint8_t(low_ >> 24);
+            have_cache_ = true;
+        } else {
+            ++pending_;
+        }
+        low_ = (low_ & 0x00FFFFFFu) << 8;
+    }
+    uint64_t low_ = 0;
+    uint32_t range_ = 0xFFFFFFFFu;
+    uint8_t cache_ = 0;
+    bool have_cache_ = false;
+    uint64_t pending_ = 0;
+    std::string out_;
+};
+
+class RangeDecoder {
+public:
+    RangeDecoder(const uint8_t* p, size_t n) : p_(p), n_(n) {
+        for (int i = 0; i < 4; ++i) code_ = (code_ << 8) | next();
+    }
+    // the cumulative count the next symbol falls in
+    uint32_t peek(uint32_t total) {
+        r_ = range_ / total;
+        const uint32_t v = code_ / r_;
+        return v < total ? v : total - 1;
+    }
+    void consume(uint32_t cum, uint32_t freq) {
+        code_ -= r_ * cum;
+        range_ = r_ * freq;
+        while (range_ < (1u << 24)) {
+            range_ <<= 8;
+            code_ = (code_ << 8) | next();
+        }
+    }
+
+private:
+    uint8_t next() { return i_ < n_ ? p_[i_++] : 0; }
+    const uint8_t* p_;
+    size_t n_, i_ = 0;
+    uint32_t code_ = 0, range_ = 0xFFFFFFFFu, r_ = 1;
+};
+
+}  // namespace learned
+}  // namespace curc

@@ -126,6 +126,39 @@ int curc_batch_submit(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read
 int curc_batch_workers(curc_ctx* ctx, int workers);
 int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user);
 
+/* Learned coder of the mismatch streams (no counterpart in the reference,
+ * whose plain method codes bases and counts with PPMd7, compress.cu:1931-1933,
+ * and offsets with the CLR range coder, util.cuh:307-343).  A small network
+ * (int8 weights, int32 accumulation, integer frequencies) predicts, walking
+ * each read with mismatches, the gap to the next mismatch and the read's base
+ * there from the surrounding pseudogenome; a range coder uses its 12-bit
+ * frequencies.  Training (FP32 forward, backward and Adam on the GPU) uses the
+ * anchors of blocks added with curc_learn_add_block; curc_learn_train also
+ * quantises.  curc_learn_encode codes the mismatch gaps and bases of the
+ * context's last block; curc_learn_decode_check decodes a stream on the host
+ * and compares it with that block (*ok = 1 when lossless). */
+typedef struct curc_learn curc_learn;
+int curc_learn_create(int device, curc_learn** out);
+void curc_learn_destroy(curc_learn* l);
+const char* curc_learn_error(const curc_learn* l);
+int curc_learn_add_block(curc_learn* l, curc_ctx* ctx);
+uint64_t curc_learn_anchors(const curc_learn* l);
+int curc_learn_train(curc_learn* l, int epochs, int batch, float lr, uint64_t seed, float* final_loss);
+int curc_learn_model(curc_learn* l, const void** ptr, uint64_t* bytes);
+int curc_learn_set_model(curc_learn* l, const void* ptr, uint64_t bytes);
+int curc_learn_encode(curc_learn* l, curc_ctx* ctx, const void** out, uint64_t* bytes);
+int curc_learn_decode_check(curc_learn* l, curc_ctx* ctx, const void* data, uint64_t bytes, int* ok);
+/* Test support: loss and gradients of one FP32 forward/backward pass over n
+ * dense inputs (n x 96) with base / gap targets (-1: none), for the parameter
+ * vector `params` (curc_learn_param_count floats: W1 128x96, b1, W2 128x128,
+ * b2, W3 20x128, b3). */
+uint64_t curc_learn_param_count(void);
+int curc_learn_grad(curc_learn* l, const float* params, const float* x, const int8_t* tb, const int8_t* tg,
+                    uint32_t n, float* loss, float* grads);
+/* Coded sizes, with the reference's plain coders, of the context's last
+ * block's mismatch streams: out[0] counts, out[1] bases, out[2] offsets. */
+int curc_plain_mismatch_bytes(curc_ctx* ctx, uint64_t* out);
+
 /* Number of kernels the library has launched in this process (no
  * reference counterpart; used to report launches per benchmark step). */
 uint64_t curc_kernel_launches(void);

@@ -1,0 +1,15 @@
+"""The learned coder's host parts, no GPU: the range coder round trip
+(compiled from tests/helpers/rc_roundtrip.cpp against learned_model.hpp)."""
+import os
+import subprocess
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_range_coder_round_trip(tmp_path):
+    exe = str(tmp_path / "rc")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "curc_b200", "csrc"), "-o", exe,
+                    os.path.join(ROOT, "tests", "helpers", "rc_roundtrip.cpp")], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "round trips ok" in r.stdout
