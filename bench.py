@@ -40,7 +40,7 @@ METRIC = "Mbases/s on 1 B200, batched vs plain; bits/base learned vs plain; loss
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--pairs", type=int, default=10_000_000)
@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cli", action="store_true", help="skip the whole-file `curc -c` measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain measurement")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-coder evaluation")
+    ap.add_argument("--learned-pairs", type=int, default=200_000)
     ap.add_argument("--batched-blocks", type=int, default=16)
     ap.add_argument("--batched-scale", type=float, default=0.1)
     return ap.parse_args()
@@ -70,6 +72,13 @@ class ClockSampler:
         self.samples = []
         self._stop = threading.Event()
         self._proc = None
+
+    def wait_first(self, timeout=5.0):
+        """Block until the first sample has arrived (nvidia-smi takes a moment
+        to start), so that the timed region is sampled."""
+        t = time.perf_counter()
+        while self._proc and not self.samples and time.perf_counter() - t < timeout:
+            time.sleep(0.02)
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -121,6 +130,24 @@ def pack_bytes(n, L):
     return n * (L + 8 * ((L + 31) // 32) + 1)
 
 
+# Algorithmic bytes of the overlap probe kernel (its launches over all
+# passes), with one 32-byte sector per random access: per listed suffix its
+# k-mer (32); per bucket searched the bucket range (32); per prefix
+# comparison the prefix id (32) and row (32 * ceil(8W/32)); per hit the run
+# slot (32).  Counts come from the kernel's own counters.
+def probe_bytes(st, L):
+    row = 32 * -(-8 * ((L + 31) // 32) // 32)
+    return (32 * st["overlap_probes"] + 32 * st["overlap_searched"] + (32 + row) * st["overlap_compares"]
+            + 32 * st["overlap_hits"])
+
+
+# DRAM bytes per listed suffix of the probe kernel, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum over its 96 launches) on the
+# 2M-pair case of the same generator: 5.662e9 bytes / 20.21e6 probes.  The
+# traffic of a launch at full size is this times its probes.
+PROBE_DRAM_BYTES_PER_PROBE = 5.662e9 / 20.207e6
+
+
 def run_ours(a, rank, world):
     import torch
     from curc_b200 import Context, kernel_launches
@@ -159,6 +186,7 @@ def run_ours(a, rank, world):
     sub_tot = {}
     l0 = kernel_launches()
     with ClockSampler(dev) as clocks:
+        clocks.wait_first()
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
@@ -205,7 +233,8 @@ def run_ours(a, rank, world):
     d2h += sum(ctx.get(f"mis_off_{m}").nbytes for m in range(1, L // 5 + 1))
     stats = dict(zip(["reads", "non_n", "n_reads", "pseudogenome_reads", "unmatched", "mapped", "unmapped",
                       "unmapped_n", "overlap_passes", "contested", "records", "mismatches",
-                      "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits"],
+                      "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits",
+                      "overlap_searched", "overlap_compares"],
                      [int(x) for x in ctx.get("stats", np.uint64)]))
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     step_s = dev_ms / 1000.0 / a.steps
@@ -298,6 +327,24 @@ def batched_vs_plain(ctx, a):
             "unit": "Mbases/s", "includes": "host reads to host streams (copies and device work), no coders"}
 
 
+def learned_eval(a):
+    """Bits/base of the mismatch streams, learned vs plain coders, on the
+    position-dependent-error workload: 8 training seeds, 2 disjoint
+    evaluation seeds (paired-end 150 bp, error rising 0.1% -> 1.0% along the
+    read, transitions 2:1), every learned stream decoded back and checked."""
+    from curc_b200.learned import train_and_evaluate
+    t = time.perf_counter()
+    r = train_and_evaluate(train_seeds=list(range(301, 309)), eval_seeds=[401, 402], pairs=a.learned_pairs,
+                           genome_len=4_000_000, epochs=2, batch=4096)
+    return {"workload": f"paired-end 150 bp, {a.learned_pairs} pairs per seed from 4 Mbp genomes, substitutions "
+                        "0.1% -> 1.0% along the read, Ti:Tv 2:1; 8 training seeds, 2 evaluation seeds",
+            "plain_bits_per_base": r["plain_bits_per_base"], "learned_bits_per_base": r["learned_bits_per_base"],
+            "plain_bytes": {"counts": r["plain"][0], "bases": r["plain"][1], "offsets": r["plain"][2]},
+            "learned_bytes": {"counts (plain)": r["plain"][0], "gaps and bases": r["learned"]},
+            "gaps_and_bases_vs_plain": r["gaps_and_bases_ratio"], "lossless": r["lossless"],
+            "train_anchors": r["train_anchors"], "final_loss": r["loss"], "s": time.perf_counter() - t}
+
+
 def run_reference(a):
     """The reference `curc -c` (built from its sources, oracle/_ref) end to
     end on a bounded sample of the workload, on this box."""
@@ -363,6 +410,10 @@ def main():
     pack_ms = r["stage_ms"]["pack"]
     dominant = max(r["stage_ms"], key=r["stage_ms"].get)
     achieved = pack_bytes(r["n"], r["L"]) / (pack_ms / 1000.0) / 1e9 if pack_ms > 0 else None
+    st = r["stats"]
+    probe_ms = r["substage_ms"].get("overlap.probe", 0.0)
+    passes = max(1, st["overlap_passes"])
+    probe_ach = probe_bytes(st, r["L"]) / (probe_ms / 1000.0) / 1e9 if probe_ms > 0 else None
     out = {
         "metric": METRIC,
         "value": r["bases"] * world / r["step_s"] / 1e6,
@@ -381,9 +432,16 @@ def main():
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "api": "curc_batch_submit/curc_batch_drain, one block per step from pinned host memory",
                 "one_call_per_step": r["bases"] * world / r["e2e_plain_s"] / 1e6},
-        "roofline": {"kernel": "pack (stage a1)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                     "traffic": None},
+        "roofline": {"kernel": "probe_kernel (overlap passes, stage a4; the largest share of the launch list)",
+                     "bound": "hbm", "achieved": probe_ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": probe_ach / peak if probe_ach else None,
+                     "traffic": PROBE_DRAM_BYTES_PER_PROBE * st["overlap_probes"] / passes,
+                     "algorithmic_bytes_per_launch": probe_bytes(st, r["L"]) / passes, "launches": passes,
+                     "ms_per_launch": probe_ms / passes,
+                     "traffic_source": "ncu dram bytes per probe on the 2M-pair case, times this launch's probes"},
+        "roofline_pack": {"kernel": "pack_kernel (stage a1)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                          "traffic": None},
         "stage_ms": r["stage_ms"],
         "substage_ms": r["substage_ms"],
         "block_stats": r["stats"],
@@ -395,6 +453,8 @@ def main():
         out["cli_e2e"] = r["cli"]
     if r["batched"]:
         out["batched"] = r["batched"]
+    if not a.no_learned and rank == 0:
+        out["learned_coder"] = learned_eval(a)
     if not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(a)
     print(json.dumps(out))

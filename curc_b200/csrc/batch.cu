@@ -55,26 +55,32 @@ void parallel_copy(void* dst, const void* src, size_t bytes) {
     for (auto& x : th) x.join();
 }
 
-// One block on one worker: reads to the worker's device slot on its stream,
-// then the block pipeline.
-void run_item(BatchWorker& w, const BatchItem& it) {
-    Block& blk = *w.blk;
-    const size_t bytes = size_t(it.n) * size_t(it.L);
+// Input slot (and pinned staging, for pageable input) of at least `bytes`.
+void reserve(BatchWorker& w, size_t bytes, bool staging) {
     if (w.dev_cap < bytes + 16) {
-        CURC_CHECK(cudaStreamSynchronize(blk.stream));
+        CURC_CHECK(cudaStreamSynchronize(w.blk->stream));
         if (w.dev) CURC_CHECK(cudaFree(w.dev));
         w.dev = nullptr;
         CURC_CHECK(cudaMalloc(&w.dev, bytes + 16));
         w.dev_cap = bytes + 16;
     }
+    if (staging && w.pin_cap < bytes) {
+        if (w.pin) CURC_CHECK(cudaFreeHost(w.pin));
+        w.pin = nullptr;
+        CURC_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&w.pin), bytes, cudaHostAllocDefault));
+        w.pin_cap = bytes;
+    }
+}
+
+// One block on one worker: reads to the worker's device slot on its stream,
+// then the block pipeline.
+void run_item(BatchWorker& w, const BatchItem& it) {
+    Block& blk = *w.blk;
+    const size_t bytes = size_t(it.n) * size_t(it.L);
+    const bool pageable = bytes && !is_pinned(it.seqs);
+    reserve(w, bytes, pageable);
     const void* src = it.seqs;
-    if (bytes && !is_pinned(it.seqs)) {
-        if (w.pin_cap < bytes) {
-            if (w.pin) CURC_CHECK(cudaFreeHost(w.pin));
-            w.pin = nullptr;
-            CURC_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&w.pin), bytes, cudaHostAllocDefault));
-            w.pin_cap = bytes;
-        }
+    if (pageable) {
         parallel_copy(w.pin, it.seqs, bytes);
         src = w.pin;
     }
@@ -146,6 +152,15 @@ int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user) {
             q.pool.push_back(std::move(w));
         }
         for (auto& w : q.pool) w->blk->keep_intermediates = ctx->block->keep_intermediates;
+        // every pipeline sized for the largest queued block up front: growing a
+        // slot later would allocate (and synchronise) in the middle of the drain
+        size_t most = 0;
+        bool pageable = false;
+        for (const auto& it : items) {
+            most = std::max(most, size_t(it.n) * size_t(it.L));
+            pageable |= it.n && !curc::is_pinned(it.seqs);
+        }
+        for (int i = 0; i < W; ++i) curc::reserve(*q.pool[i], most, pageable);
         std::atomic<size_t> next{0};
         std::atomic<bool> stop{false};
         std::mutex cb_mu;

@@ -18,6 +18,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <random>
 
@@ -112,7 +114,7 @@ __global__ void anchors_kernel(const DevRecord* __restrict__ rec, const uint8_t*
         const int q = j == 0 ? -1 : pos[j - 1];
         const char pv = j >= 2 ? rb[j - 2] : 0;
         int idx[20];
-        const int n = anchor_features(ref, rl, r.pos, q, L, r.strand, pv, idx);
+        const int n = anchor_features(ref, rl, r.pos, q, L, r.strand, pv, m - j, idx);
         Anchor x;
         for (int t = 0; t < 20; ++t) x.idx[t] = t < n ? uint8_t(idx[t]) : 255;
         x.nidx = uint8_t(n);
@@ -130,7 +132,8 @@ __global__ void anchors_kernel(const DevRecord* __restrict__ rec, const uint8_t*
             x.gap = 0;
             x.tgap = -1;
         }
-        x.gmax = uint16_t(L - 2 - q);
+        // the next mismatch leaves room for the m - j - 1 after it
+        x.gmax = uint16_t(j < m ? L - 1 - q - (m - j) : 0);
         x.pad0 = 0;
         x.rec = i;
         a[j] = x;
@@ -703,9 +706,12 @@ int curc_learn_encode(curc_learn* L, curc_ctx* ctx, const void** out, uint64_t* 
         cut.push_back(na);
         const int nc = int(cut.size()) - 1;
         std::vector<std::string> chunks(nc);
+        double bits[3] = {0, 0, 0};  // bases, gap bins, offsets inside bins
 #pragma omp parallel for schedule(dynamic)
         for (int c = 0; c < nc; ++c) {
             RangeEncoder enc;
+            BinModels bins;
+            double cb[3] = {0, 0, 0};
             for (size_t k = cut[c]; k < cut[c + 1]; ++k) {
                 const Anchor& x = ha[k];
                 const uint16_t* f = &hf[k * OUT];
@@ -713,18 +719,29 @@ int curc_learn_encode(curc_learn* L, curc_ctx* ctx, const void** out, uint64_t* 
                     uint32_t cum = 0;
                     for (int j = 0; j < x.tbase; ++j) cum += f[j];
                     enc.encode(cum, f[x.tbase], TOTAL);
+                    cb[0] -= std::log2(double(f[x.tbase]) / TOTAL);
                 }
                 if (x.tgap >= 0) {
                     uint32_t cum = 0;
                     for (int j = 0; j < x.tgap; ++j) cum += f[NB + j];
                     enc.encode(cum, f[NB + x.tgap], TOTAL);
+                    cb[1] -= std::log2(double(f[NB + x.tgap]) / TOTAL);
                     const int lo = gap_bin_lo(x.tgap);
                     const int hi = std::min(gap_bin_lo(x.tgap + 1), int(x.gmax) + 1);
-                    enc.encode(uint32_t(x.gap - lo), 1, uint32_t(hi - lo));
+                    uint32_t oc, of, ot;
+                    bins.lookup(x.tgap, x.gap - lo, hi - lo, oc, of, ot);
+                    enc.encode(oc, of, ot);
+                    cb[2] -= std::log2(double(of) / ot);
+                    bins.update(x.tgap, x.gap - lo);
                 }
             }
             chunks[c] = enc.finish();
+#pragma omp critical
+            for (int q = 0; q < 3; ++q) bits[q] += cb[q];
         }
+        if (std::getenv("CURC_VERBOSE"))
+            std::fprintf(stderr, "curc: learned bytes: bases %.0f, gap bins %.0f, offsets in bins %.0f (%u anchors)\n",
+                         bits[0] / 8, bits[1] / 8, bits[2] / 8, na);
         std::string s;
         const uint32_t ncu = uint32_t(nc);
         s.append(reinterpret_cast<const char*>(&ncu), 4);
@@ -788,6 +805,7 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
 #pragma omp parallel for schedule(dynamic) reduction(+ : bad)
         for (int c = 0; c < int(nc); ++c) {
             RangeDecoder dec(p + coff[c], size_t(coff[c + 1] - coff[c]));
+            BinModels bins;
             const size_t r0 = size_t(c) * CHUNK_RECORDS, r1 = std::min(rlist.size(), r0 + CHUNK_RECORDS);
             for (size_t ri = r0; ri < r1; ++ri) {
                 const DevRecord& r = rec[rlist[ri]];
@@ -796,7 +814,7 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
                 char prev = 0;  // read base decoded at the previous anchor
                 for (int j = 0; j <= m; ++j) {
                     int idx[20];
-                    const int n = anchor_features(ref.data(), ref.size(), r.pos, q, Lr, r.strand, prev, idx);
+                    const int n = anchor_features(ref.data(), ref.size(), r.pos, q, Lr, r.strand, prev, m - j, idx);
                     uint32_t fb[NB], fg[NG];
                     model_freqs(T.model, idx, n, fb, fg);
                     const Anchor& truth = ha[first[ri] + j];
@@ -814,11 +832,14 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
                         int gb = 0;
                         while (cum + fg[gb] <= v) cum += fg[gb++];
                         dec.consume(cum, fg[gb]);
-                        const int lo = gap_bin_lo(gb), hi = std::min(gap_bin_lo(gb + 1), Lr - 2 - q + 1);
-                        const uint32_t w = uint32_t(std::max(1, hi - lo));
-                        const uint32_t o = dec.peek(w);
-                        dec.consume(o, 1);
-                        const int g = lo + int(o);
+                        const int lo = gap_bin_lo(gb), hi = std::min(gap_bin_lo(gb + 1), Lr - 1 - q - (m - j) + 1);
+                        const int w = std::max(1, hi - lo);
+                        uint32_t oc, of;
+                        const uint32_t ov = dec.peek(bins.total(gb, w));
+                        const int o = bins.find(gb, w, ov, oc, of);
+                        dec.consume(oc, of);
+                        bins.update(gb, o);
+                        const int g = lo + o;
                         if (g != truth.gap) ++bad;
                         q = q + 1 + g;
                     }

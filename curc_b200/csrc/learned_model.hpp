@@ -6,12 +6,14 @@
 //
 // What is coded, per record with mismatches (its count comes from the plain
 // mismatch-count stream): walking the read in pseudogenome order from an
-// anchor before its first base, the gap to the next mismatch (16 bins, the
-// offset inside a bin uniform), then at that mismatch the read's base (one
+// anchor before its first base, the gap to the next mismatch (one of 16
+// bins, then the offset inside the bin), then at that mismatch the read's base (one
 // of the three other bases or N), and so on.  The network sees, at an
 // anchor: the 16 pseudogenome bases around it, the position along the
 // sequenced read (16 bins), whether it is the start anchor, and the previous
-// mismatch's read base.
+// mismatch's read base, and how many mismatches of the read are still to
+// come.  The offset inside a gap bin is coded with adaptive per-bin
+// frequencies.
 #pragma once
 #include <cstdint>
 #include <cstring>
@@ -83,12 +85,14 @@ LM_HD int code_of(char c) {
     }
 }
 
-// Active input features of an anchor (indices of the ones), at most 19.
+// Active input features of an anchor (indices of the ones), at most 20.
 // ref/rl: pseudogenome (ASCII) and its length; rpos: the record's position;
 // q: anchor offset in pseudogenome order (-1 for the start anchor); L, strand;
-// prev: previous mismatch's read base (0 if none).
+// prev: previous mismatch's read base (0 if none); remaining: mismatches of
+// the read still to come after this anchor (its count is known to both
+// sides from the mismatch-count stream).
 LM_HD int anchor_features(const uint8_t* ref, uint64_t rl, uint64_t rpos, int q, int L, int strand, char prev,
-                          int* idx) {
+                          int remaining, int* idx) {
     int n = 0;
     for (int t = 0; t < CTX; ++t) {
         const int64_t p = int64_t(rpos) + q - CTX / 2 + t;
@@ -104,6 +108,7 @@ LM_HD int anchor_features(const uint8_t* ref, uint64_t rl, uint64_t rpos, int q,
     }
     const int pc = prev == 'N' ? 4 : code_of(prev);
     if (pc >= 0) idx[n++] = 81 + pc;
+    idx[n++] = 86 + (remaining < 4 ? remaining : 4);
     return n;
 }
 
@@ -175,6 +180,58 @@ LM_HD void model_freqs(const Model& M, const int* idx, int nidx, uint32_t* fb, u
     logits_to_freq(M, z, NB, fb);
     logits_to_freq(M, z + NB, NG, fg);
 }
+
+// Adaptive frequencies of the offset inside each gap bin (the network gives
+// the bin): reset at the start of each independently coded chunk, updated
+// after every coded gap in the same way by the encoder and the decoder.
+class BinModels {
+public:
+    static constexpr uint32_t INC = 24, LIMIT = 1u << 15;
+    BinModels() {
+        for (int b = 0; b < NG; ++b) {
+            f_[b].assign(size_t(gap_bin_lo(b + 1) - gap_bin_lo(b)), 1);
+            tot_[b] = uint32_t(f_[b].size());
+        }
+    }
+    // cumulative count, count and total of offset o among the first w offsets
+    void lookup(int b, int o, int w, uint32_t& cum, uint32_t& freq, uint32_t& total) const {
+        cum = 0;
+        total = 0;
+        for (int j = 0; j < w; ++j) {
+            if (j < o) cum += f_[b][j];
+            total += f_[b][j];
+        }
+        freq = f_[b][o];
+    }
+    // offset whose cumulative range holds v, among the first w offsets
+    int find(int b, int w, uint32_t v, uint32_t& cum, uint32_t& freq) const {
+        cum = 0;
+        int o = 0;
+        while (o + 1 < w && cum + f_[b][o] <= v) cum += f_[b][o++];
+        freq = f_[b][o];
+        return o;
+    }
+    uint32_t total(int b, int w) const {
+        uint32_t t = 0;
+        for (int j = 0; j < w; ++j) t += f_[b][j];
+        return t;
+    }
+    void update(int b, int o) {
+        f_[b][o] += INC;
+        tot_[b] += INC;
+        if (tot_[b] > LIMIT) {
+            tot_[b] = 0;
+            for (auto& x : f_[b]) {
+                x = (x + 1) / 2;
+                tot_[b] += x;
+            }
+        }
+    }
+
+private:
+    std::vector<uint32_t> f_[NG];
+    uint32_t tot_[NG];
+};
 
 // ------------------------------------------------------------ range coder
 // Carry-propagating range coder (32-bit range, 64-bit low with a cached

@@ -196,7 +196,8 @@ struct ProbeListMove {
 // whether an equal prefix exists; then the hit (list index, run start,
 // bucket end, bucket) is set and the suffix joins the run's claimers.
 __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* __restrict__ sufw, uint32_t j, int off,
-                                          RunSlot* __restrict__ run, uint32_t* __restrict__ gnext, uint4& hitrec) {
+                                          RunSlot* __restrict__ run, uint32_t* __restrict__ gnext, uint4& hitrec,
+                                          uint32_t& searched, uint32_t& compares) {
     const int cl = c.L - off;
     const uint64_t* sr = sufw + uint64_t(j) * c.W;
     const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
@@ -207,7 +208,9 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
     uint32_t lo = c.kr[h];
     const uint32_t e = c.kr[h + 1];
     uint32_t count = e - lo;
+    ++searched;
     while (count > 0) {
+        ++compares;
         const uint32_t step = count / 2, it = lo + step;
         if (cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl) < 0) {
             lo = it + 1;
@@ -216,7 +219,9 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
             count = step;
         }
     }
-    if (lo >= e || cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) != 0) return false;
+    if (lo >= e) return false;
+    ++compares;
+    if (cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) != 0) return false;
     // run membership: count, lowest list index, and a list of members
     atomicAdd(&run[lo].claim, 1u);
     atomicMin(&run[lo].lead, j);
@@ -227,7 +232,8 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
 
 // Probes every listed suffix and lists the hits (hlist, *hcount; their
 // order is immaterial to the resolution).  tally[0] counts probes,
-// tally[1] hits.
+// tally[1] hits, tally[4] probes that searched a bucket, tally[5] prefix
+// comparisons (for the algorithmic bytes of the pass).
 __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
                                                     const uint32_t* __restrict__ plist,
                                                     const uint32_t* __restrict__ pcount, int off,
@@ -236,7 +242,7 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
                                                     unsigned long long* __restrict__ tally) {
     __shared__ uint4 s_hits[512];
     __shared__ uint32_t s_n, s_base;
-    uint32_t probes = 0, hits = 0;
+    uint32_t probes = 0, hits = 0, searched = 0, compares = 0;
     const uint32_t np = *pcount;
     for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < np; b0 += gridDim.x * blockDim.x) {
         const uint32_t q = b0 + threadIdx.x;
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
         uint4 rec;
         if (q < np) {
             ++probes;
-            hit = probe_one(c, sufw, plist[q], off, run, gnext, rec);
+            hit = probe_one(c, sufw, plist[q], off, run, gnext, rec, searched, compares);
             hits += hit;
         }
         if (threadIdx.x == 0) s_n = 0;
@@ -258,6 +264,8 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
     }
     block_tally<unsigned long long>(probes, &tally[0]);
     block_tally<unsigned long long>(hits, &tally[1]);
+    block_tally<unsigned long long>(searched, &tally[4]);
+    block_tally<unsigned long long>(compares, &tally[5]);
 }
 
 // A suffix alone on its run links directly.  A run claimed by several
@@ -462,8 +470,8 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     }
     sp_mask.stop();
     // probes, probes that met a prefix, links, contested members
-    unsigned long long* tally = a.alloc<unsigned long long>(4);
-    CURC_CHECK(cudaMemsetAsync(tally, 0, 32, s));
+    unsigned long long* tally = a.alloc<unsigned long long>(6);
+    CURC_CHECK(cudaMemsetAsync(tally, 0, 48, s));
     sp_index.stop();
 
     // List of size ms, of which `active` are unlinked; compacted once half
@@ -540,8 +548,8 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     }
     cp.check();
     if (st) {
-        unsigned long long t[4];
-        CURC_CHECK(cudaMemcpyAsync(t, tally, 32, cudaMemcpyDeviceToHost, s));
+        unsigned long long t[6];
+        CURC_CHECK(cudaMemcpyAsync(t, tally, 48, cudaMemcpyDeviceToHost, s));
         CURC_CHECK(cudaStreamSynchronize(s));
         st->passes = passes;
         st->links = uint32_t(t[2]);
@@ -550,6 +558,8 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         st->active_sum = active_sum;
         st->probes = t[0];
         st->hits = t[1];
+        st->searched = t[4];
+        st->compares = t[5];
     }
     a.release(mk);
 }

@@ -680,9 +680,12 @@ void Block::refmatch_all() {
     // block statistics: reads, non-N reads, N reads, pseudogenome reads,
     // unmatched, mapped, unmapped (non-N, N), overlap passes, contested
     // suffixes, records, mismatches; overlap suffixes, and summed over the
-    // passes: unlinked suffixes, suffixes probed, probes that met a prefix
-    const uint64_t stats[16] = {n, m, NN, n_ref, U, n_map, n_ug, n_un, ostats.passes, ostats.contested, n_records,
-                                n_mis, ostats.suffixes, ostats.active_sum, ostats.probes, ostats.hits};
+    // passes: unlinked suffixes, suffixes probed, probes that met a prefix,
+    // probes that searched a bucket, prefix comparisons
+    const uint64_t stats[18] = {n,          m,           NN,         n_ref,         U,           n_map,
+                                n_ug,       n_un,        ostats.passes, ostats.contested, n_records, n_mis,
+                                ostats.suffixes, ostats.active_sum, ostats.probes, ostats.hits, ostats.searched,
+                                ostats.compares};
     put("stats", std::vector<uint8_t>(reinterpret_cast<const uint8_t*>(stats),
                                       reinterpret_cast<const uint8_t*>(stats) + sizeof(stats)));
 }
