@@ -114,7 +114,8 @@ __global__ void anchors_kernel(const DevRecord* __restrict__ rec, const uint8_t*
         const int q = j == 0 ? -1 : pos[j - 1];
         const char pv = j >= 2 ? rb[j - 2] : 0;
         int idx[20];
-        const int n = anchor_features(ref, rl, r.pos, q, L, r.strand, pv, m - j, idx);
+        const int gmx = j < m ? L - 1 - q - (m - j) : 0;
+        const int n = anchor_features(ref, rl, r.pos, q, L, r.strand, pv, m - j, gmx, idx);
         Anchor x;
         for (int t = 0; t < 20; ++t) x.idx[t] = t < n ? uint8_t(idx[t]) : 255;
         x.nidx = uint8_t(n);
@@ -133,7 +134,7 @@ __global__ void anchors_kernel(const DevRecord* __restrict__ rec, const uint8_t*
             x.tgap = -1;
         }
         // the next mismatch leaves room for the m - j - 1 after it
-        x.gmax = uint16_t(j < m ? L - 1 - q - (m - j) : 0);
+        x.gmax = uint16_t(gmx);
         x.pad0 = 0;
         x.rec = i;
         a[j] = x;
@@ -298,8 +299,8 @@ __global__ void __launch_bounds__(128) infer_kernel(const Model* __restrict__ gm
         z[o] = acc;
     }
     uint32_t fb[NB], fg[NG];
-    logits_to_freq(M, z, NB, fb);
-    logits_to_freq(M, z + NB, NG, fg);
+    logits_to_freq(M, z, NB, NB, fb);
+    logits_to_freq(M, z + NB, gap_bin(an.gmax) + 1, NG, fg);
     uint16_t* f = freq + size_t(k) * OUT;
     for (int j = 0; j < NB; ++j) f[j] = uint16_t(fb[j]);
     for (int j = 0; j < NG; ++j) f[NB + j] = uint16_t(fg[j]);
@@ -814,9 +815,11 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
                 char prev = 0;  // read base decoded at the previous anchor
                 for (int j = 0; j <= m; ++j) {
                     int idx[20];
-                    const int n = anchor_features(ref.data(), ref.size(), r.pos, q, Lr, r.strand, prev, m - j, idx);
+                    const int gmx = j < m ? Lr - 1 - q - (m - j) : 0;
+                    const int n =
+                        anchor_features(ref.data(), ref.size(), r.pos, q, Lr, r.strand, prev, m - j, gmx, idx);
                     uint32_t fb[NB], fg[NG];
-                    model_freqs(T.model, idx, n, fb, fg);
+                    model_freqs(T.model, idx, n, gmx, fb, fg);
                     const Anchor& truth = ha[first[ri] + j];
                     if (j > 0) {
                         const uint32_t v = dec.peek(TOTAL);
@@ -832,7 +835,7 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
                         int gb = 0;
                         while (cum + fg[gb] <= v) cum += fg[gb++];
                         dec.consume(cum, fg[gb]);
-                        const int lo = gap_bin_lo(gb), hi = std::min(gap_bin_lo(gb + 1), Lr - 1 - q - (m - j) + 1);
+                        const int lo = gap_bin_lo(gb), hi = std::min(gap_bin_lo(gb + 1), gmx + 1);
                         const int w = std::max(1, hi - lo);
                         uint32_t oc, of;
                         const uint32_t ov = dec.peek(bins.total(gb, w));

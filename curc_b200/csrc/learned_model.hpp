@@ -30,7 +30,7 @@
 namespace curc {
 namespace learned {
 
-constexpr int IN = 96;       // input features (one-hots, zero padded)
+constexpr int IN = 128;      // input features (one-hots, zero padded)
 constexpr int HID = 128;     // hidden units per layer
 constexpr int NB = 4;        // base outcomes: the three other bases, then N
 constexpr int NG = 16;       // gap bins
@@ -86,13 +86,15 @@ LM_HD int code_of(char c) {
 }
 
 // Active input features of an anchor (indices of the ones), at most 20.
+// gmax: largest gap that can follow the anchor (when a mismatch is still to
+// come).
 // ref/rl: pseudogenome (ASCII) and its length; rpos: the record's position;
 // q: anchor offset in pseudogenome order (-1 for the start anchor); L, strand;
 // prev: previous mismatch's read base (0 if none); remaining: mismatches of
 // the read still to come after this anchor (its count is known to both
 // sides from the mismatch-count stream).
 LM_HD int anchor_features(const uint8_t* ref, uint64_t rl, uint64_t rpos, int q, int L, int strand, char prev,
-                          int remaining, int* idx) {
+                          int remaining, int gmax, int* idx) {
     int n = 0;
     for (int t = 0; t < CTX; ++t) {
         const int64_t p = int64_t(rpos) + q - CTX / 2 + t;
@@ -109,6 +111,7 @@ LM_HD int anchor_features(const uint8_t* ref, uint64_t rl, uint64_t rpos, int q,
     const int pc = prev == 'N' ? 4 : code_of(prev);
     if (pc >= 0) idx[n++] = 81 + pc;
     idx[n++] = 86 + (remaining < 4 ? remaining : 4);
+    if (remaining > 0) idx[n++] = 96 + gap_bin(gmax);  // the last gap bin that can occur
     return n;
 }
 
@@ -132,8 +135,10 @@ LM_HD int32_t requant(int32_t acc, int32_t m, int32_t sh) {
     return v > 127 ? 127 : int32_t(v);
 }
 
-// Frequencies (total TOTAL, each >= 1) of `k` outcomes from their logits.
-LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, uint32_t* f) {
+// Frequencies (total TOTAL) of the first `k` outcomes from their logits,
+// each >= 1; outcomes k .. n-1 cannot occur and get 0.
+LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, int n, uint32_t* f) {
+    for (int j = k; j < n; ++j) f[j] = 0;
     int32_t mx = z[0];
     int am = 0;
     for (int j = 1; j < k; ++j)
@@ -158,8 +163,9 @@ LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, uint32_t* f) 
     f[am] += TOTAL - sum;
 }
 
-// The network at one anchor: base and gap frequencies.
-LM_HD void model_freqs(const Model& M, const int* idx, int nidx, uint32_t* fb, uint32_t* fg) {
+// The network at one anchor: base and gap frequencies (gap bins beyond the
+// one holding gmax get 0).
+LM_HD void model_freqs(const Model& M, const int* idx, int nidx, int gmax, uint32_t* fb, uint32_t* fg) {
     int32_t a1[HID], a2[HID];
     for (int h = 0; h < HID; ++h) {
         int32_t acc = M.b1[h];
@@ -177,8 +183,8 @@ LM_HD void model_freqs(const Model& M, const int* idx, int nidx, uint32_t* fb, u
         for (int t = 0; t < HID; ++t) acc += int32_t(M.w3[o][t]) * a2[t];
         z[o] = acc;
     }
-    logits_to_freq(M, z, NB, fb);
-    logits_to_freq(M, z + NB, NG, fg);
+    logits_to_freq(M, z, NB, NB, fb);
+    logits_to_freq(M, z + NB, gap_bin(gmax < 0 ? 0 : gmax) + 1, NG, fg);
 }
 
 // Adaptive frequencies of the offset inside each gap bin (the network gives

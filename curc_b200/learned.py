@@ -15,7 +15,7 @@ def workload(seed: int, pairs: int, genome_len: int):
                                 err=synth.position_ramp(150, 0.001, 0.010), ti_tv=2.0, preserve_order=True)
 
 
-def train_and_evaluate(train_seeds, eval_seeds, pairs=200_000, genome_len=2_000_000, epochs=2, batch=4096,
+def train_and_evaluate(train_seeds, eval_seeds, pairs=200_000, genome_len=2_000_000, epochs=3, batch=4096,
                        lr=2e-3, device=0):
     """Trains on blocks of the training seeds and codes the mismatch streams of
     the evaluation seeds both ways.  Returns a dict with bytes and bits/base of

@@ -149,8 +149,8 @@ int curc_learn_set_model(curc_learn* l, const void* ptr, uint64_t bytes);
 int curc_learn_encode(curc_learn* l, curc_ctx* ctx, const void** out, uint64_t* bytes);
 int curc_learn_decode_check(curc_learn* l, curc_ctx* ctx, const void* data, uint64_t bytes, int* ok);
 /* Test support: loss and gradients of one FP32 forward/backward pass over n
- * dense inputs (n x 96) with base / gap targets (-1: none), for the parameter
- * vector `params` (curc_learn_param_count floats: W1 128x96, b1, W2 128x128,
+ * dense inputs (n x 128) with base / gap targets (-1: none), for the parameter
+ * vector `params` (curc_learn_param_count floats: W1 128x128, b1, W2 128x128,
  * b2, W3 20x128, b3). */
 uint64_t curc_learn_param_count(void);
 int curc_learn_grad(curc_learn* l, const float* params, const float* x, const int8_t* tb, const int8_t* tg,

@@ -8,7 +8,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-IN, HID, OUT, NB = 96, 128, 20, 4
+IN, HID, OUT, NB = 128, 128, 20, 4
 
 
 def _unpack(p):
