@@ -29,6 +29,12 @@ struct PackedAcc {
         return cmp_span(db + uint64_t(a) * W, aoff, db + uint64_t(b) * W, boff, len);
     }
     __device__ __forceinline__ int sym(uint32_t a, int pos) const { return code_at(db + uint64_t(a) * W, pos); }
+    // key: the first KS symbols of read a from pos, left-aligned, zero padded
+    static constexpr int KS = 32, SB = 2;
+    __device__ __forceinline__ uint64_t key(uint32_t a, int pos) const {
+        const int nb = L - pos < KS ? L - pos : KS;
+        return word_at(db + uint64_t(a) * W, uint32_t(pos), nb) << (64 - SB * nb);
+    }
 };
 
 struct AsciiAcc {
@@ -52,7 +58,39 @@ struct AsciiAcc {
             default: return 4;
         }
     }
+    static constexpr int KS = 8, SB = 8;
+    __device__ __forceinline__ uint64_t key(uint32_t a, int pos) const {
+        const uint8_t* x = r + uint64_t(a) * L;
+        uint64_t v = 0;
+        for (int b = 0; b < KS; ++b) v = (v << 8) | (pos + b < L ? x[pos + b] : 0);
+        return v;
+    }
 };
+
+// Comparison of read a from aoff with read b from boff over len symbols,
+// given their keys at those offsets (the key comparison decides unless the
+// first KS symbols are equal and more follow).
+template <class Acc>
+__device__ __forceinline__ int cmp_keyed(const Acc& acc, uint64_t ka, uint32_t a, int aoff, uint64_t kb, uint32_t b,
+                                         int boff, int len) {
+    if (len < Acc::KS) {
+        const uint64_t mask = ~0ull << (64 - Acc::SB * len);
+        ka &= mask;
+        kb &= mask;
+    }
+    if (ka != kb) return ka < kb ? -1 : 1;
+    if (len <= Acc::KS) return 0;
+    return acc.cmp(a, aoff + Acc::KS, b, boff + Acc::KS, len - Acc::KS);
+}
+
+// keys of the list entries at offset off
+template <class Acc>
+__global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, const uint32_t* __restrict__ m_dev, int off,
+                                 uint64_t* __restrict__ key) {
+    const uint32_t m = *m_dev;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+        key[i] = acc.key(ids[i], off);
+}
 
 // bounds[c] = first index whose symbol at off-1 is >= c (the list is
 // sorted by read[off-1, L), so symbols are nondecreasing).  One block
@@ -110,10 +148,13 @@ __global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t
 // outputs, finds by bisection how many of them precede in each of the two
 // inputs, and then merges sequentially.  About log2(n) / MP_ITEMS + 1
 // comparisons per output and level, instead of a binary search per run.
+// The entries' keys at off travel with them, so a comparison reads the
+// reads themselves only when the first key symbols are equal.
 constexpr int MP_ITEMS = 8;
 
 template <class Acc>
-__global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+__global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict__ in, const uint64_t* __restrict__ ink,
+                                   uint32_t* __restrict__ out, uint64_t* __restrict__ outk,
                                    const uint32_t* __restrict__ bounds, const uint32_t* __restrict__ m_dev,
                                    int width) {
     const uint32_t m = *m_dev;
@@ -122,6 +163,10 @@ __global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict_
     for (int c = 0; c <= Acc::ALPHA; ++c) bd[c] = bounds[c];
     const int len = acc.L - off;
     auto run_at = [&](int r) { return bd[r < Acc::ALPHA ? r : Acc::ALPHA]; };
+    // entry x against entry y (positions in the input)
+    auto cmp_at = [&](uint32_t x, uint32_t y) {
+        return cmp_keyed(acc, ink[x], in[x], off, ink[y], in[y], off, len);
+    };
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x * MP_ITEMS;
     for (uint64_t d0 = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * MP_ITEMS; d0 < m; d0 += stride) {
         const uint32_t dend = uint32_t(min(uint64_t(m), d0 + MP_ITEMS));
@@ -140,7 +185,7 @@ __global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict_
             uint32_t lo = dd > nb ? dd - nb : 0, hi = dd < na ? dd : na;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) / 2;
-                if (acc.cmp(in[a0 + mid], off, in[a1 + dd - mid - 1], off, len) <= 0)
+                if (cmp_at(a0 + mid, a1 + dd - mid - 1) <= 0)
                     lo = mid + 1;
                 else
                     hi = mid;
@@ -148,27 +193,33 @@ __global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict_
             uint32_t i = lo, j = dd - lo;
             const uint32_t stop = dend < a2 ? dend : a2;
             for (; d < stop; ++d) {
-                const bool take_a = j >= nb || (i < na && acc.cmp(in[a0 + i], off, in[a1 + j], off, len) <= 0);
-                out[d] = take_a ? in[a0 + i++] : in[a1 + j++];
+                const bool take_a = j >= nb || (i < na && cmp_at(a0 + i, a1 + j) <= 0);
+                const uint32_t x = take_a ? a0 + i++ : a1 + j++;
+                out[d] = in[x];
+                outk[d] = ink[x];
             }
         }
     }
 }
 
 // One thread per run of equal suffix strings: the reference's bucket merge
-// restricted to that run (compress.cu:1089-1160 / 1297-1336).
+// restricted to that run (compress.cu:1089-1160 / 1297-1336).  Prefix keys
+// (at offset 0) and suffix keys (at off) decide most comparisons.
 template <class Acc>
-__device__ __forceinline__ void group_one(const Acc& acc, uint32_t* pre, uint32_t mp,
-                                          const uint32_t* __restrict__ suf, uint32_t ms, int off, uint32_t j,
-                                          uint32_t* next, uint32_t* prev, uint16_t* offset) {
+__device__ __forceinline__ void group_one(const Acc& acc, uint32_t* pre, uint64_t* pk, uint32_t mp,
+                                          const uint32_t* __restrict__ suf, const uint64_t* __restrict__ sk,
+                                          uint32_t ms, int off, uint32_t j, uint32_t* next, uint32_t* prev,
+                                          uint16_t* offset) {
     const int len = acc.L - off;
     const uint32_t s0 = suf[j];
-    if (j > 0 && acc.cmp(suf[j - 1], off, s0, off, len) == 0) return;
+    const uint64_t k0 = sk[j];
+    if (j > 0 && cmp_keyed(acc, sk[j - 1], suf[j - 1], off, k0, s0, off, len) == 0) return;
     // prefixes P with P[0, len) == s0[off, L)
+    auto pcmp = [&](uint32_t i) { return cmp_keyed(acc, pk[i], pre[i], 0, k0, s0, off, len); };
     uint32_t lo = 0, count = mp;
     while (count > 0) {
         uint32_t step = count / 2, it = lo + step;
-        if (acc.cmp(pre[it], 0, s0, off, len) < 0) {
+        if (pcmp(it) < 0) {
             lo = it + 1;
             count -= step + 1;
         } else {
@@ -176,10 +227,10 @@ __device__ __forceinline__ void group_one(const Acc& acc, uint32_t* pre, uint32_
         }
     }
     uint32_t hi = lo;
-    while (hi < mp && acc.cmp(pre[hi], 0, s0, off, len) == 0) ++hi;
+    while (hi < mp && pcmp(hi) == 0) ++hi;
     if (hi == lo) return;
     uint32_t se = j + 1;
-    while (se < ms && acc.cmp(suf[se], off, s0, off, len) == 0) ++se;
+    while (se < ms && cmp_keyed(acc, sk[se], suf[se], off, k0, s0, off, len) == 0) ++se;
     uint32_t pi = lo, si = j;
     while (pi < hi && si < se) {
         uint32_t P = pre[pi];
@@ -199,12 +250,16 @@ __device__ __forceinline__ void group_one(const Acc& acc, uint32_t* pre, uint32_
                 ++si;
                 continue;
             }
+            // rotate P to the front of [cur, pi], keys alongside
             P = pre[pi];
+            const uint64_t K = pk[pi];
             while (pi > cur) {
                 pre[pi] = pre[pi - 1];
+                pk[pi] = pk[pi - 1];
                 --pi;
             }
             pre[pi] = P;
+            pk[pi] = K;
         }
         next[S] = P;
         prev[P] = S;
@@ -215,13 +270,14 @@ __device__ __forceinline__ void group_one(const Acc& acc, uint32_t* pre, uint32_
 }
 
 template <class Acc>
-__global__ void merge_groups_kernel(Acc acc, uint32_t* pre, const uint32_t* __restrict__ mp_dev,
-                                    const uint32_t* __restrict__ suf, const uint32_t* __restrict__ ms_dev, int off,
-                                    uint32_t* next, uint32_t* prev, uint16_t* offset) {
+__global__ void merge_groups_kernel(Acc acc, uint32_t* pre, uint64_t* pk, const uint32_t* __restrict__ mp_dev,
+                                    const uint32_t* __restrict__ suf, const uint64_t* __restrict__ sk,
+                                    const uint32_t* __restrict__ ms_dev, int off, uint32_t* next, uint32_t* prev,
+                                    uint16_t* offset) {
     const uint32_t mp = *mp_dev, ms = *ms_dev;
     if (mp == 0) return;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ms; j += gridDim.x * blockDim.x)
-        group_one(acc, pre, mp, suf, ms, off, j, next, prev, offset);
+        group_one(acc, pre, pk, mp, suf, sk, ms, off, j, next, prev, offset);
 }
 
 // Compaction functors: keep the list entries whose link is still free.
@@ -234,6 +290,16 @@ struct MoveId {
     const uint32_t* in;
     uint32_t* out;
     __device__ void operator()(uint32_t i, uint32_t d) const { out[d] = in[i]; }
+};
+struct MoveIdKey {
+    const uint32_t* in;
+    const uint64_t* ink;
+    uint32_t* out;
+    uint64_t* outk;
+    __device__ void operator()(uint32_t i, uint32_t d) const {
+        out[d] = in[i];
+        outk[d] = ink[i];
+    }
 };
 
 // The passes are queued without a host round trip: list lengths stay on
@@ -249,13 +315,23 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     uint32_t* suf2 = a.alloc<uint32_t>(cnt);
     uint32_t* tmp = a.alloc<uint32_t>(cnt);
     uint32_t* mtmp = a.alloc<uint32_t>(cnt);
+    // keys: prefixes at offset 0 (kept with the prefix list), suffixes at
+    // the pass's offset (taken at the start of each pass)
+    uint64_t* pk = a.alloc<uint64_t>(cnt);
+    uint64_t* tk = a.alloc<uint64_t>(cnt);
+    uint64_t* sk = a.alloc<uint64_t>(cnt);
+    uint64_t* sk2 = a.alloc<uint64_t>(cnt);
+    uint64_t* mk2 = a.alloc<uint64_t>(cnt);
     uint32_t* bounds = a.alloc<uint32_t>(8);
     uint32_t* len = a.alloc<uint32_t>(4);  // mp, ms for even passes, then for odd passes
     const uint32_t init[4] = {cnt, cnt, 0, 0};
     CURC_CHECK(cudaMemcpyAsync(len, init, sizeof(init), cudaMemcpyHostToDevice, s));
     Compactor cp(cnt, a, s);
+    const int gk = resident_grid(list_keys_kernel<Acc>, 256, cnt);
     const int gm = resident_grid(merge_level_kernel<Acc>, 256, div_up(cnt, MP_ITEMS));
     const int gg = resident_grid(merge_groups_kernel<Acc>, 128, cnt);
+    list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, pre, len, 0, pk);
+    CURC_LAUNCH_CHECK();
     constexpr int CHECK_EVERY = 8;
     int par = 0;
     for (int off = 1; off < acc.L; ++off, par ^= 1) {
@@ -266,27 +342,34 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
         SubStage sp_merge("full_match.resort");
         run_bounds_kernel<Acc><<<1, 256, 0, s>>>(acc, suf, ms_in, off, bounds);
         CURC_LAUNCH_CHECK();
+        list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, suf, ms_in, off, sk);
+        CURC_LAUNCH_CHECK();
         {
             // levels: runs merged in pairs, then pairs of pairs, ...; the last
-            // level writes suf2 (suf itself is free after the first level)
+            // level writes suf2/sk2 (suf/sk are free after the first level)
             int levels = 0;
             while ((1 << levels) < Acc::ALPHA) ++levels;
             const uint32_t* src = suf;
+            const uint64_t* srck = sk;
             for (int l = 0; l < levels; ++l) {
-                uint32_t* dst = l + 1 == levels ? suf2 : (l % 2 == 0 ? mtmp : suf);
-                merge_level_kernel<Acc><<<gm, 256, 0, s>>>(acc, off, src, dst, bounds, ms_in, 1 << l);
+                const bool last = l + 1 == levels;
+                uint32_t* dst = last ? suf2 : (l % 2 == 0 ? mtmp : suf);
+                uint64_t* dstk = last ? sk2 : (l % 2 == 0 ? mk2 : sk);
+                merge_level_kernel<Acc><<<gm, 256, 0, s>>>(acc, off, src, srck, dst, dstk, bounds, ms_in, 1 << l);
                 CURC_LAUNCH_CHECK();
                 src = dst;
+                srck = dstk;
             }
         }
         sp_merge.stop();
         SubStage sp_groups("full_match.groups");
-        merge_groups_kernel<Acc><<<gg, 128, 0, s>>>(acc, pre, mp_in, suf2, ms_in, off, next, prev, offset);
+        merge_groups_kernel<Acc><<<gg, 128, 0, s>>>(acc, pre, pk, mp_in, suf2, sk2, ms_in, off, next, prev, offset);
         CURC_LAUNCH_CHECK();
         sp_groups.stop();
         SubStage sp_comp("full_match.compact");
-        cp.run(mp_in, cnt, mp_out, FreeLink{pre, prev}, MoveId{pre, tmp});
+        cp.run(mp_in, cnt, mp_out, FreeLink{pre, prev}, MoveIdKey{pre, pk, tmp, tk});
         std::swap(pre, tmp);
+        std::swap(pk, tk);
         cp.run(ms_in, cnt, ms_out, FreeLink{suf2, next}, MoveId{suf2, suf});
         sp_comp.stop();
         if (off % CHECK_EVERY == 0) {

@@ -509,6 +509,57 @@ __global__ void run_number_kernel(const uint32_t* __restrict__ excl, const uint3
     if (t < m) out[t] = uint64_t(excl[t]) + start[t];
 }
 
+__global__ void run_starts8_kernel(const uint32_t* __restrict__ pos, const uint64_t* __restrict__ k0, uint32_t m,
+                                   uint8_t* __restrict__ start) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    start[t] = t == 0 || pos[t - 1] + 1 != pos[t] || k0[pos[t - 1]] != k0[pos[t]];
+}
+
+// One warp per run of reads sharing their first word: runs of up to 32
+// reads are ordered in place by their remaining words, ties by position
+// (stable), each lane ranking its read against the others' words by
+// shuffles.  Longer runs are flagged for the radix path.
+__global__ void small_runs_kernel(const uint64_t* __restrict__ db, int W, uint32_t* __restrict__ ids,
+                                  const uint32_t* __restrict__ pos, const uint32_t* __restrict__ rb, uint32_t R,
+                                  uint32_t m, uint8_t* __restrict__ large) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < R; r += warps) {
+        const uint32_t b = rb[r], e = r + 1 < R ? rb[r + 1] : m, len = e - b;
+        if (len > 32) {
+            for (uint32_t k = lane; k < len; k += 32) large[b + k] = 1;
+            continue;
+        }
+        const uint32_t p0 = pos[b];
+        uint32_t id = 0;
+        uint64_t w[15];
+#pragma unroll
+        for (int k = 0; k < 15; ++k) w[k] = 0;
+        if (lane < len) {
+            id = ids[p0 + lane];
+#pragma unroll
+            for (int k = 0; k < 15; ++k)
+                if (k + 1 < W) w[k] = db[uint64_t(id) * W + k + 1];
+        }
+        uint32_t rank = 0;
+        for (uint32_t j = 0; j < len; ++j) {
+            int c = 0;  // lane j's read against mine
+#pragma unroll
+            for (int k = 0; k < 15; ++k) {
+                if (k + 1 < W) {
+                    const uint64_t o = __shfl_sync(0xFFFFFFFFu, w[k], int(j));
+                    if (c == 0 && o != w[k]) c = o < w[k] ? -1 : 1;
+                }
+            }
+            rank += (c < 0 || (c == 0 && j < lane)) ? 1u : 0u;
+        }
+        __syncwarp();
+        if (lane < len) ids[p0 + rank] = id;
+        __syncwarp();
+    }
+}
+
 __global__ void gather_ids_kernel(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ pos, uint32_t m,
                                   uint32_t* __restrict__ out) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -526,8 +577,9 @@ void sort_ids_by_reads(const uint64_t* db, int W, int L, uint32_t* ids, size_t n
     // Stable lexicographic order of the reads (compress.cu:1400-1407 under a
     // stable comparison sort; ties keep input order).  First by the first
     // 32 bases; then only the runs of reads that share them are ordered by
-    // the remaining words, least significant first, and finally by run so
-    // that every run returns to its place.
+    // the remaining words: runs of up to 32 reads by one warp each, longer
+    // runs by radix passes over the remaining words, least significant first,
+    // and finally by run so that every run returns to its place.
     if (n <= 1) return;
     auto mk = a.mark();
     uint64_t* k0 = a.alloc<uint64_t>(n);
@@ -541,7 +593,31 @@ void sort_ids_by_reads(const uint64_t* db, int W, int L, uint32_t* ids, size_t n
         uint32_t* pos = a.alloc<uint32_t>(n);
         uint32_t* cnt = a.alloc<uint32_t>(1);
         select_indices(tie, pos, n, cnt, a, s);
-        const uint32_t m = read_scalar(cnt, s);
+        const uint32_t m0 = read_scalar(cnt, s);
+        uint32_t m = 0;
+        if (m0) {
+            // runs of up to 32 reads: one warp each; longer runs: radix below
+            uint8_t* st8 = a.alloc<uint8_t>(m0);
+            run_starts8_kernel<<<grid_for(m0, 256), 256, 0, s>>>(pos, k0, m0, st8);
+            CURC_LAUNCH_CHECK();
+            uint32_t* rb = a.alloc<uint32_t>(m0);
+            uint32_t* rc = a.alloc<uint32_t>(2);
+            select_indices(st8, rb, m0, rc, a, s);
+            const uint32_t R = read_scalar(rc, s);
+            uint8_t* large = a.alloc<uint8_t>(m0);
+            CURC_CHECK(cudaMemsetAsync(large, 0, m0, s));
+            small_runs_kernel<<<grid_for(uint64_t(R) * 32, 256), 256, 0, s>>>(db, W, ids, pos, rb, R, m0, large);
+            CURC_LAUNCH_CHECK();
+            uint32_t* li = a.alloc<uint32_t>(m0);
+            select_indices(large, li, m0, rc + 1, a, s);
+            m = read_scalar(rc + 1, s);
+            if (m) {
+                uint32_t* lp = a.alloc<uint32_t>(m);
+                gather_ids_kernel<<<grid_for(m, 256), 256, 0, s>>>(pos, li, m, lp);
+                CURC_LAUNCH_CHECK();
+                pos = lp;
+            }
+        }
         if (m) {
             uint32_t* sub = a.alloc<uint32_t>(m);
             uint64_t* key = a.alloc<uint64_t>(m);
