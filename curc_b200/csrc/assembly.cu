@@ -439,8 +439,7 @@ uint32_t rank_members(const uint32_t* ids, uint32_t m, uint32_t n, const uint32_
                                                                                   k.counts + 1);
         CURC_LAUNCH_CHECK();
         uint32_t hc[4];
-        CURC_CHECK(cudaMemcpyAsync(hc, k.counts, 16, cudaMemcpyDeviceToHost, s));
-        CURC_CHECK(cudaStreamSynchronize(s));
+        read_small(hc, k.counts, 16, s);
         if (hc[3]) throw std::runtime_error("assemble: a chain link leaves the member set");
         if (hc[1] == 0) break;
         if (attempt == 1) throw std::runtime_error("assemble: reads left unranked after promoting cycle rulers");
@@ -535,8 +534,7 @@ void assemble(const uint64_t* db, const uint8_t* ascii, int L, int W, const uint
         uint32_t* cidx = a.alloc<uint32_t>(m);
         select_indices(cyc, cidx, m, k.counts + 2, a, s);
         uint32_t hc[2];
-        CURC_CHECK(cudaMemcpyAsync(hc, k.counts + 2, 8, cudaMemcpyDeviceToHost, s));
-        CURC_CHECK(cudaStreamSynchronize(s));
+        read_small(hc, k.counts + 2, 8, s);
         if (hc[1]) throw std::runtime_error("assemble: broken cycle");
         const uint32_t mc = hc[0];
         const int gc = grid_for(mc, 256);

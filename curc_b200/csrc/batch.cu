@@ -6,6 +6,9 @@
 // mutex spin, compress.cu:52-65) on one device.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <mutex>
@@ -25,6 +28,7 @@ Block*& batch_current() {
 BatchWorker::~BatchWorker() {
     if (dev) cudaFree(dev);
     if (pin) cudaFreeHost(pin);
+    if (landed) cudaEventDestroy(landed);
 }
 
 namespace {
@@ -72,21 +76,54 @@ void reserve(BatchWorker& w, size_t bytes, bool staging) {
     }
 }
 
-// One block on one worker: reads to the worker's device slot on its stream,
-// then the block pipeline.
-void run_item(BatchWorker& w, const BatchItem& it) {
-    Block& blk = *w.blk;
+// Blocks of at least this many bases fill the device on their own: they run
+// one at a time from the draining thread, double-buffered over two
+// pipelines, instead of on concurrent workers.  (Measured on B200: while one
+// worker thread's multi-gigabyte input copy was in flight, the other worker
+// thread's block did not start until the copy had landed, so concurrent
+// workers hid none of a 3 GB block's 54 ms copy.)
+constexpr size_t LARGE_BYTES = size_t(1) << 28;
+
+// CURC_VERBOSE=1: when each block's copy was queued and its run ended.
+bool batch_verbose() {
+    static const bool v = std::getenv("CURC_VERBOSE") != nullptr;
+    return v;
+}
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Queues the block's reads to the worker's input slot on the queue's copy
+// stream (pageable input goes through the worker's pinned staging first).
+// The copies have a stream of their own: measured on B200, a 3 GB copy
+// queued on one block pipeline's stream held back the kernels of the block
+// running on the other pipeline's stream until it had landed, while the same
+// copy on a separate stream overlapped them.
+void stage_in(BatchQueue& q, BatchWorker& w, const BatchItem& it) {
     const size_t bytes = size_t(it.n) * size_t(it.L);
     const bool pageable = bytes && !is_pinned(it.seqs);
     reserve(w, bytes, pageable);
+    if (!w.landed) CURC_CHECK(cudaEventCreateWithFlags(&w.landed, cudaEventDisableTiming));
     const void* src = it.seqs;
     if (pageable) {
+        CURC_CHECK(cudaEventSynchronize(w.landed));  // the staging buffer's previous copy
         parallel_copy(w.pin, it.seqs, bytes);
         src = w.pin;
     }
-    if (bytes) CURC_CHECK(cudaMemcpyAsync(w.dev, src, bytes, cudaMemcpyHostToDevice, blk.stream));
+    if (bytes) CURC_CHECK(cudaMemcpyAsync(w.dev, src, bytes, cudaMemcpyHostToDevice, q.copy_stream));
+    CURC_CHECK(cudaEventRecord(w.landed, q.copy_stream));
+}
+
+// The block pipeline over the worker's input slot, once its copy has landed.
+void run_staged(BatchWorker& w, const BatchItem& it, int wi, std::chrono::steady_clock::time_point t0) {
+    Block& blk = *w.blk;
+    CURC_CHECK(cudaEventSynchronize(w.landed));
+    const double tl = batch_verbose() ? ms_since(t0) : 0;
     blk.arena.reset();
     blk.run(w.dev, it.n, it.L, it.po, it.pe);
+    if (batch_verbose())
+        std::fprintf(stderr, "curc: batch block %u pipeline %d: reads landed %.1f, done %.1f ms (device %.1f)\n",
+                     it.ticket, wi, tl, ms_since(t0), blk.stage_ms.count("total") ? blk.stage_ms["total"] : -1.f);
 }
 
 template <class F>
@@ -161,27 +198,59 @@ int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user) {
             pageable |= it.n && !curc::is_pinned(it.seqs);
         }
         for (int i = 0; i < W; ++i) curc::reserve(*q.pool[i], most, pageable);
+        if (!q.copy_stream) CURC_CHECK(cudaStreamCreateWithFlags(&q.copy_stream, cudaStreamNonBlocking));
+        std::vector<size_t> large, small;
+        for (size_t k = 0; k < items.size(); ++k)
+            (size_t(items[k].n) * size_t(items[k].L) >= curc::LARGE_BYTES ? large : small).push_back(k);
+        const auto t0 = std::chrono::steady_clock::now();
+        auto callback = [&](curc::BatchWorker& w, size_t k) {
+            if (!done) return;
+            curc::batch_current() = w.blk;
+            const int rc = done(user, items[k].ticket);
+            curc::batch_current() = nullptr;
+            if (rc != 0) throw std::runtime_error("batch drain stopped by the callback");
+        };
+        // large blocks first, from this thread: while one pipeline runs a
+        // block, the next block's reads are already queued on the other's stream
+        if (!large.empty()) {
+            const int P = std::min(W, 2);
+            try {
+                curc::stage_in(q, *q.pool[0], items[large[0]]);
+                for (size_t i = 0; i < large.size(); ++i) {
+                    curc::BatchWorker& w = *q.pool[i % P];
+                    const bool more = i + 1 < large.size();
+                    if (more && P > 1) curc::stage_in(q, *q.pool[(i + 1) % P], items[large[i + 1]]);
+                    curc::run_staged(w, items[large[i]], int(i % P), t0);
+                    callback(w, large[i]);
+                    if (more && P == 1) curc::stage_in(q, w, items[large[i + 1]]);
+                }
+            } catch (...) {
+                curc::batch_current() = nullptr;
+                // a queued copy may still read the caller's memory: let it land
+                if (q.copy_stream) cudaStreamSynchronize(q.copy_stream);
+                throw;
+            }
+        }
+        // smaller blocks on concurrent pipelines, one host thread each, so one
+        // block's host round trips overlap another's kernels
         std::atomic<size_t> next{0};
         std::atomic<bool> stop{false};
         std::mutex cb_mu;
         std::exception_ptr err;
-        auto work = [&](curc::BatchWorker& w) {
+        auto work = [&](curc::BatchWorker& w, int wi) {
             try {
                 CURC_CHECK(cudaSetDevice(ctx->device));
                 for (;;) {
                     if (stop.load()) return;
-                    const size_t k = next.fetch_add(1);
-                    if (k >= items.size()) return;
-                    curc::run_item(w, items[k]);
+                    const size_t j = next.fetch_add(1);
+                    if (j >= small.size()) return;
+                    const size_t k = small[j];
+                    curc::stage_in(q, w, items[k]);
+                    curc::run_staged(w, items[k], wi, t0);
                     // callbacks one at a time, on this thread, with this block's results
                     std::lock_guard<std::mutex> g(cb_mu);
                     if (stop.load()) return;
-                    if (done) {
-                        curc::batch_current() = w.blk;
-                        const int rc = done(user, items[k].ticket);
-                        curc::batch_current() = nullptr;
-                        if (rc != 0) throw std::runtime_error("batch drain stopped by the callback");
-                    }
+                    callback(w, k);
                 }
             } catch (...) {
                 curc::batch_current() = nullptr;
@@ -190,10 +259,13 @@ int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user) {
                 stop.store(true);
             }
         };
-        std::vector<std::thread> th;
-        for (int i = 1; i < W; ++i) th.emplace_back([&, i] { work(*q.pool[i]); });
-        work(*q.pool[0]);
-        for (auto& t : th) t.join();
+        if (!small.empty()) {
+            const int Ws = int(std::min<size_t>(size_t(W), small.size()));
+            std::vector<std::thread> th;
+            for (int i = 1; i < Ws; ++i) th.emplace_back([&, i] { work(*q.pool[i], i); });
+            work(*q.pool[0], 0);
+            for (auto& t : th) t.join();
+        }
         if (err) std::rethrow_exception(err);
         return int(CURC_OK);
     });

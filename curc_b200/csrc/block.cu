@@ -66,8 +66,7 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     n_ids = arena.alloc<uint32_t>(n ? n : 1);
     split_n_reads(has_n, n, reads_id, n_ids, counts, arena, s);
     uint32_t hc[2];
-    CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaStreamSynchronize(s));
+    read_small(hc, counts, 8, s);
     m = hc[0];
     NN = hc[1];
     nreads = arena.alloc<uint8_t>(size_t(NN) * L + 16);
@@ -107,8 +106,7 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     ref_ids = arena.alloc<uint32_t>(m ? m : 1);
     unmatch_ids = arena.alloc<uint32_t>(m ? m : 1);
     chain_filter(n, sorted, m, next, prev, offset, ref_ids, unmatch_ids, counts, arena, s);
-    CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaStreamSynchronize(s));
+    read_small(hc, counts, 8, s);
     n_ref = hc[0];
     U = hc[1];
     T.end();

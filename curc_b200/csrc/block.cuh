@@ -104,6 +104,7 @@ struct BatchWorker {
     size_t dev_cap = 0;
     uint8_t* pin = nullptr;             // pinned staging for pageable input
     size_t pin_cap = 0;
+    cudaEvent_t landed = nullptr;       // the last copy into `dev` has completed
     ~BatchWorker();
 };
 struct BatchQueue {
@@ -111,6 +112,10 @@ struct BatchQueue {
     uint32_t next_ticket = 0;
     int workers = 2;
     std::vector<std::unique_ptr<BatchWorker>> pool;
+    cudaStream_t copy_stream = nullptr;  // every input copy of the drains
+    ~BatchQueue() {
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+    }
 };
 
 // The block whose results curc_block_get returns on this thread while a

@@ -384,8 +384,7 @@ void Block::emit(StageTimer& T) {
     select_indices(unm_n, un, NN, counts + 2, arena, s);
     {
         uint32_t hc[2];
-        CURC_CHECK(cudaMemcpyAsync(hc, counts + 1, 8, cudaMemcpyDeviceToHost, s));
-        CURC_CHECK(cudaStreamSynchronize(s));
+        read_small(hc, counts + 1, 8, s);
         n_ug = hc[0];
         n_un = hc[1];
     }
@@ -441,8 +440,7 @@ void Block::emit(StageTimer& T) {
         CURC_LAUNCH_CHECK();
     }
     std::vector<uint32_t> hcls(maxm + 2);
-    CURC_CHECK(cudaMemcpyAsync(hcls.data(), chist, size_t(maxm + 2) * 4, cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaStreamSynchronize(s));
+    read_small(hcls.data(), chist, size_t(maxm + 2) * 4, s);
     class_count.assign(maxm + 1, 0);
     std::vector<uint32_t> first(maxm + 2, 0);
     std::vector<uint64_t> cbase(maxm + 2, 0);
@@ -496,8 +494,7 @@ void Block::emit(StageTimer& T) {
     }
     {
         uint32_t he[2];
-        CURC_CHECK(cudaMemcpyAsync(he, err, 8, cudaMemcpyDeviceToHost, s));
-        CURC_CHECK(cudaStreamSynchronize(s));
+        read_small(he, err, 8, s);
         if (he[0]) throw std::runtime_error("emit: mismatch count disagrees with mapping");
         if (he[1]) throw std::runtime_error("emit: unexpected symbol in a mismatch");
     }

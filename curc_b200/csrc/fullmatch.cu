@@ -374,8 +374,7 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
         sp_comp.stop();
         if (off % CHECK_EVERY == 0) {
             uint32_t h[2];
-            CURC_CHECK(cudaMemcpyAsync(h, mp_out, 8, cudaMemcpyDeviceToHost, s));
-            CURC_CHECK(cudaStreamSynchronize(s));
+            read_small(h, mp_out, 8, s);
             if (h[0] == 0 || h[1] == 0) break;
         }
     }

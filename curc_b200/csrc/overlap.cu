@@ -397,8 +397,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     select_flagged(sorted, pre_f, pre, m, counts + 0, a, s);
     select_flagged(sorted, suf_f, suf, m, counts + 1, a, s);
     uint32_t hc[2];
-    CURC_CHECK(cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaStreamSynchronize(s));
+    read_small(hc, counts, 8, s);
     const uint32_t mp = hc[0];
     uint32_t ms = hc[1];
 
@@ -549,8 +548,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     cp.check();
     if (st) {
         unsigned long long t[6];
-        CURC_CHECK(cudaMemcpyAsync(t, tally, 48, cudaMemcpyDeviceToHost, s));
-        CURC_CHECK(cudaStreamSynchronize(s));
+        read_small(t, tally, 48, s);
         st->passes = passes;
         st->links = uint32_t(t[2]);
         st->contested = uint32_t(t[3]);

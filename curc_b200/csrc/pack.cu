@@ -5,17 +5,21 @@
 //
 // B200 design: a persistent grid walks tiles of 64 reads.  Each tile is
 // 64*L contiguous bytes, moved into shared memory by a 1D TMA bulk copy
-// (cp.async.bulk + mbarrier) two tiles ahead of the compute, so HBM reads
-// are full-line and overlap the packing.  Each thread then packs one output
-// word (32 bases) from shared memory; packed words of a tile are contiguous
-// in HBM, so stores coalesce.  Bytes per read: L in, 8*W + 1 out.
+// (cp.async.bulk + mbarrier) one tile ahead of the compute, so HBM reads
+// are full-line and overlap the packing.  The block then works in two
+// conflict-free passes: every thread turns 16-byte groups of the tile into
+// 32 bits of codes (one 16-byte shared-memory load each), giving the tile's
+// bases as one contiguous 2-bit string, and then every thread cuts one
+// output word (32 bases) per read of its column out of that string.  A
+// block has 32*W threads, so both passes keep every thread busy; packed
+// words of a tile are contiguous in HBM, so stores coalesce.  Bytes per
+// read: L in, 8*W + 1 out.
 #include "stages.cuh"
 
 namespace curc {
 
 namespace {
 constexpr int PACK_READS = 64;
-constexpr int PACK_THREADS = 256;
 constexpr uint32_t WAIT_LIMIT = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -60,38 +64,53 @@ __device__ __forceinline__ uint32_t pack4(uint32_t x) {
     return (t * 0x40100401u) >> 24;
 }
 
-// The four bytes are all uppercase A, C, G or T (the common case, where
-// pack4 is exact and no N is present): rebuild them from their codes.
-__device__ __forceinline__ bool plain4(uint32_t x) {
+// The four bytes are all A, C, G or T in either case (the common case,
+// where pack4 is exact and no N is present): rebuild them, in lower case,
+// from their codes.
+__device__ __forceinline__ bool acgt4(uint32_t x) {
     const uint32_t t = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
     const uint32_t sel = (t & 3u) | ((t >> 4) & 0x30u) | ((t >> 8) & 0x300u) | ((t >> 12) & 0x3000u);
-    return __byte_perm(0x54474341u, 0u, sel) == x;
+    return __byte_perm(0x74676361u, 0u, sel) == (x | 0x20202020u);
 }
 
-__global__ void __launch_bounds__(PACK_THREADS) pack_kernel(const uint8_t* __restrict__ seq, uint64_t n, int L, int W,
-                                                             uint32_t tile_bytes, bool use_tma,
-                                                             uint64_t* __restrict__ packed, uint8_t* __restrict__ has_n,
-                                                             uint32_t* __restrict__ err) {
+// Shared memory of one stage: the tile's bytes (a multiple of 128), then
+// its codes (4*L words of 16 bases, and 4 zero words after them).
+__host__ __device__ inline uint32_t pack_tile_stride(int L) { return (uint32_t(PACK_READS) * L + 127u) & ~127u; }
+__host__ __device__ inline uint32_t pack_code_words(int L) { return 4u * uint32_t(L) + 4u; }
+inline size_t pack_smem_bytes(int L) { return 2 * (size_t(pack_tile_stride(L)) + 4 * size_t(pack_code_words(L))); }
+
+__global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ seq, uint64_t n, int L, int W,
+                                                   bool use_tma, uint64_t* __restrict__ packed,
+                                                   uint8_t* __restrict__ has_n, uint32_t* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar[2];
-    __shared__ uint8_t nflag[PACK_READS];
+    __shared__ uint8_t nflag[2][PACK_READS];
+    const uint32_t tile_bytes = uint32_t(PACK_READS) * uint32_t(L);
+    const uint32_t groups = tile_bytes / 16;  // 4*L
+    const uint32_t stride = pack_tile_stride(L);
+    uint32_t* codes_base = reinterpret_cast<uint32_t*>(smem + 2 * stride);
+    const uint32_t cw = pack_code_words(L);
     const uint64_t tiles = div_up(n, PACK_READS);
-    // a word's loads may run 36 bytes past its row: keep them in the buffer
-    const uint32_t stride_bytes = (tile_bytes + 64u + 127u) & ~127u;
     auto full = [&](uint64_t t) { return (t + 1) * PACK_READS <= n; };
     auto issue = [&](uint64_t t, int stage) {
         mbar_expect_tx(&bar[stage], tile_bytes);
-        bulk_g2s(smem + stage * stride_bytes, seq + t * uint64_t(PACK_READS) * L, tile_bytes, &bar[stage]);
+        bulk_g2s(smem + stage * stride, seq + t * uint64_t(PACK_READS) * L, tile_bytes, &bar[stage]);
     };
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (uint32_t i = threadIdx.x; i < 2 * PACK_READS; i += blockDim.x) nflag[i / PACK_READS][i % PACK_READS] = 0;
+    if (threadIdx.x < 8) codes_base[(threadIdx.x / 4) * cw + groups + threadIdx.x % 4] = 0;
     __syncthreads();
+    // this thread's output column: word w0 of reads r0, r0 + 32, ...
+    const uint32_t r0 = threadIdx.x / uint32_t(W), w0 = threadIdx.x - r0 * uint32_t(W);
+    const int nb = min(32, L - int(w0) * 32);
+    const uint64_t tail_mask = nb < 32 ? ~0ull << (64 - 2 * nb) : ~0ull;
     uint64_t t = blockIdx.x;
     if (use_tma && threadIdx.x == 0 && t < tiles && full(t)) issue(t, 0);
-    bool pending[2] = {use_tma && t < tiles && full(t), false};
+    uint32_t pending = (use_tma && t < tiles && full(t)) ? 1u : 0u;  // bit s: a copy into stage s is in flight
     for (uint32_t it = 0; t < tiles; t += gridDim.x, ++it) {
         const int stage = it & 1;
         const uint64_t nt = t + gridDim.x;
@@ -100,12 +119,14 @@ __global__ void __launch_bounds__(PACK_THREADS) pack_kernel(const uint8_t* __res
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 issue(nt, stage ^ 1);
             }
-            pending[stage ^ 1] = true;
+            pending |= 1u << (stage ^ 1);
         }
-        uint8_t* buf = smem + stage * stride_bytes;
+        uint8_t* buf = smem + stage * stride;
+        uint32_t* codes = codes_base + stage * cw;
+        uint8_t* nf = nflag[stage];
         const uint64_t rem = n - t * PACK_READS;
         const uint32_t nr = rem < uint64_t(PACK_READS) ? uint32_t(rem) : uint32_t(PACK_READS);
-        if (pending[stage]) {
+        if (pending >> stage & 1u) {
             uint32_t spins = 0;
             while (!mbar_try_wait(&bar[stage], (it >> 1) & 1)) {
                 if (++spins > WAIT_LIMIT) {  // never expected: report and stop cleanly
@@ -113,57 +134,43 @@ __global__ void __launch_bounds__(PACK_THREADS) pack_kernel(const uint8_t* __res
                     break;
                 }
             }
-            pending[stage] = false;
+            pending &= ~(1u << stage);
         } else {
+            // the last, partial tile: plain loads, the rest of the tile 'A'
             const uint8_t* src = seq + t * uint64_t(PACK_READS) * L;
-            for (uint32_t b = threadIdx.x; b < nr * uint32_t(L); b += PACK_THREADS) buf[b] = src[b];
-        }
-        if (threadIdx.x < PACK_READS) nflag[threadIdx.x] = 0;
-        __syncthreads();
-        for (uint32_t item = threadIdx.x; item < nr * uint32_t(W); item += PACK_THREADS) {
-            const uint32_t r = item / W, w = item - r * W;
-            const uint32_t a = r * uint32_t(L) + w * 32;
-            const int nb = min(32, L - int(w) * 32);
-            // eight 4-byte groups from aligned shared-memory words; bytes past
-            // the read's end are replaced by 'A' (code 0, the zero padding)
-            const uint32_t* b32 = reinterpret_cast<const uint32_t*>(buf + (a & ~3u));
-            const uint32_t sh = (a & 3u) * 8u;
-            uint32_t lo = b32[0];
-            uint64_t v = 0;
-            bool plain = true;
-#pragma unroll
-            for (int g = 0; g < 8; ++g) {
-                const uint32_t hi = b32[g + 1];
-                uint32_t x = __funnelshift_r(lo, hi, sh);
-                lo = hi;
-                const int vb = nb - 4 * g;
-                if (vb < 4) {
-                    const uint32_t keep = vb <= 0 ? 0u : (1u << (8 * vb)) - 1u;
-                    x = (x & keep) | (0x41414141u & ~keep);
-                }
-                v = (v << 8) | pack4(x);
-                plain &= plain4(x);
-            }
-            if (!plain) {  // N, lower case or other letters: byte by byte
-                const uint8_t* sb = buf + a;
-                bool hn = false;
-                v = 0;
-                for (int j = 0; j < nb; ++j) {
-                    const uint8_t c = sb[j];
-                    hn |= (c == 'N');
-                    v = (v << 2) | uint64_t(ascii_code(c));
-                }
-                v <<= 2 * (32 - nb);
-                if (hn) nflag[r] = 1;
-            }
-            packed[(t * PACK_READS + r) * W + w] = v;
+            const uint32_t have = nr * uint32_t(L);
+            for (uint32_t b = threadIdx.x; b < tile_bytes; b += blockDim.x) buf[b] = b < have ? src[b] : 'A';
         }
         __syncthreads();
-        if (threadIdx.x < nr) has_n[t * PACK_READS + threadIdx.x] = nflag[threadIdx.x];
+        // pass 1: 16 bytes -> 32 bits of codes, first base in the top bits
+        for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
+            const uint4 x = reinterpret_cast<const uint4*>(buf)[g];
+            uint32_t c = (pack4(x.x) << 24) | (pack4(x.y) << 16) | (pack4(x.z) << 8) | pack4(x.w);
+            if (!(acgt4(x.x) & acgt4(x.y) & acgt4(x.z) & acgt4(x.w))) {
+                // N, other letters: byte by byte
+                c = 0;
+                for (uint32_t j = 0; j < 16; ++j) {
+                    const uint8_t ch = buf[16 * g + j];
+                    c = (c << 2) | uint32_t(ascii_code(ch));
+                    if (ch == 'N') nf[(16 * g + j) / uint32_t(L)] = 1;
+                }
+            }
+            codes[g] = c;
+        }
         __syncthreads();
+        // pass 2: the 32 bases of word w0 of each read, from the code string
+        for (uint32_t r = r0; r < nr; r += 32) {
+            const uint32_t o = r * uint32_t(L) + 32u * w0;
+            const uint32_t k = o >> 4, sh = (o & 15u) * 2u;
+            uint64_t v = (uint64_t(codes[k]) << 32) | codes[k + 1];
+            if (sh) v = (v << sh) | (codes[k + 2] >> (32u - sh));
+            packed[(t * PACK_READS + r) * W + w0] = v & tail_mask;
+        }
+        for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+            has_n[t * PACK_READS + i] = nf[i];
+            nf[i] = 0;
+        }
     }
-    // drain a prefetch that was issued but not consumed (cannot happen: a
-    // prefetch is only issued for a tile this block will process)
 }
 
 __global__ void invert_flags_kernel(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, uint64_t n) {
@@ -187,18 +194,20 @@ void pack_reads(const uint8_t* seq, uint64_t n, int L, uint64_t* packed, uint8_t
                 cudaStream_t s) {
     if (n == 0) return;
     const int W = (L + 31) / 32;
-    const uint32_t tile_bytes = uint32_t(PACK_READS) * uint32_t(L);
     const bool aligned = (reinterpret_cast<uintptr_t>(seq) & 15u) == 0;
-    const size_t smem = 2 * ((tile_bytes + 64u + 127u) & ~127u);
+    const size_t smem = pack_smem_bytes(L);
     static bool attr_set = false;
     if (!attr_set) {
         CURC_CHECK(cudaFuncSetAttribute(pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        2 * (64 * 512 + 64 + 128)));
+                                        int(pack_smem_bytes(512))));
         attr_set = true;
     }
+    const int threads = 32 * W;
+    int per_sm = 0;
+    CURC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pack_kernel, threads, smem));
     const uint64_t tiles = div_up(n, PACK_READS);
-    const int grid = int(std::min<uint64_t>(tiles, uint64_t(SM_COUNT_B200) * 8));
-    pack_kernel<<<grid, PACK_THREADS, smem, s>>>(seq, n, L, W, tile_bytes, aligned, packed, has_n, err);
+    const int grid = int(std::min<uint64_t>(tiles, uint64_t(SM_COUNT_B200) * uint64_t(std::max(1, per_sm))));
+    pack_kernel<<<grid, threads, smem, s>>>(seq, n, L, W, aligned, packed, has_n, err);
     CURC_LAUNCH_CHECK();
 }
 

@@ -1,6 +1,8 @@
 // Device-wide primitives: arena, scan, stable compaction, stable radix sort.
 #include <algorithm>
 #include <atomic>
+#include <cstring>
+#include <stdexcept>
 
 #include "primitives.cuh"
 
@@ -69,6 +71,41 @@ void Arena::release(const Mark& m) {
     for (size_t i = m.chunk + 1; i < chunks_.size(); ++i) chunks_[i].used = 0;
     cur_ = m.chunk;
     if (cur_ < chunks_.size()) chunks_[cur_].used = m.used;
+}
+
+// ---------------------------------------------------------------- small reads
+
+namespace {
+constexpr size_t READ_SMALL_MAX = 4096;
+
+__global__ void read_small_kernel(const uint8_t* __restrict__ src, size_t bytes, uint8_t* dst) {
+    for (size_t i = threadIdx.x; i < bytes; i += blockDim.x) dst[i] = src[i];
+}
+
+// Mapped pinned buffer of this host thread (portable: valid on every device
+// through unified addressing), allocated on first use and kept until exit.
+uint8_t* thread_readback_buffer() {
+    thread_local struct Buf {
+        uint8_t* p = nullptr;
+        ~Buf() {
+            if (p) cudaFreeHost(p);
+        }
+    } b;
+    if (!b.p)
+        CURC_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&b.p), READ_SMALL_MAX,
+                                 cudaHostAllocMapped | cudaHostAllocPortable));
+    return b.p;
+}
+}  // namespace
+
+void read_small(void* host, const void* dev, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return;
+    if (bytes > READ_SMALL_MAX) throw std::runtime_error("read_small: more than 4 KiB");
+    uint8_t* buf = thread_readback_buffer();
+    read_small_kernel<<<1, 128, 0, s>>>(static_cast<const uint8_t*>(dev), bytes, buf);
+    CURC_LAUNCH_CHECK();
+    CURC_CHECK(cudaStreamSynchronize(s));
+    std::memcpy(host, buf, bytes);
 }
 
 // ---------------------------------------------------------------- pinned arena

@@ -124,12 +124,18 @@ void fill(T* p, T v, size_t n, cudaStream_t s);
 
 void iota(uint32_t* p, size_t n, cudaStream_t s);
 
+// Reads back `bytes` (at most 4 KiB) of device memory after the stream's
+// work so far, and synchronises the stream.  A one-block kernel stores them
+// into mapped pinned host memory (one buffer per host thread), so the read
+// never waits on a copy engine: another pipeline's multi-gigabyte input copy
+// on the same device cannot hold it back.
+void read_small(void* host, const void* dev, size_t bytes, cudaStream_t s);
+
 // Reads back one device value (synchronises the stream).
 template <class T>
 T read_scalar(const T* dev, cudaStream_t s) {
     T v;
-    CURC_CHECK(cudaMemcpyAsync(&v, dev, sizeof(T), cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaStreamSynchronize(s));
+    read_small(&v, dev, sizeof(T), s);
     return v;
 }
 

@@ -605,9 +605,8 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
     CURC_LAUNCH_CHECK();
     uint64_t total_removed = 0;
     uint32_t len_bytes = 0;
-    CURC_CHECK(cudaMemcpyAsync(&total_removed, removed + K, 8, cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaMemcpyAsync(&len_bytes, cnt + 3, 4, cudaMemcpyDeviceToHost, s));
-    CURC_CHECK(cudaStreamSynchronize(s));
+    read_small(&total_removed, removed + K, 8, s);
+    read_small(&len_bytes, cnt + 3, 4, s);
     uint64_t hi[4] = {K, uint64_t(K) * (std32 ? 4 : 8), 1 + uint64_t(len_bytes), dl - total_removed};
     r.map_off = moff;
     r.off_len = hi[1];
