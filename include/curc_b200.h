@@ -115,8 +115,10 @@ int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* 
  *
  * curc_batch_submit queues n x read_len ASCII reads (host memory that must
  * stay valid until the drain returns) and returns a ticket.  curc_batch_drain
- * runs every queued block; after each one it calls done(user, ticket) (one
- * call at a time, in completion order, from the thread that ran the block),
+ * runs every queued block (blocks of at least 2^28 bases first, double-buffered
+ * from the calling thread; the rest on concurrent pipelines); after each one it
+ * calls done(user, ticket) (one call at a time, in completion order, from the
+ * thread that ran the block),
  * during which curc_block_get on that thread returns that block's results.
  * A non-zero return from done stops the drain with CURC_ERR_STATE.
  * curc_batch_workers sets the number of pipelines (1..16, default 2). */
