@@ -83,13 +83,25 @@ __device__ __forceinline__ int cmp_keyed(const Acc& acc, uint64_t ka, uint32_t a
     return acc.cmp(a, aoff + Acc::KS, b, boff + Acc::KS, len - Acc::KS);
 }
 
-// keys of the list entries at offset off
+// Keys of the list entries at offset off.  With sym_count (2-bit reads
+// only), also how many entries have each base at off-1: the list is sorted
+// by read[off-1, L), so these counts give the base runs' bounds.  Each
+// thread counts in four 16-bit fields (a resident grid leaves it far fewer
+// than 65536 entries), then one atomic per block and base.
 template <class Acc>
 __global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, const uint32_t* __restrict__ m_dev, int off,
-                                 uint64_t* __restrict__ key) {
+                                 uint64_t* __restrict__ key, uint32_t* __restrict__ sym_count) {
     const uint32_t m = *m_dev;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-        key[i] = acc.key(ids[i], off);
+    uint64_t c = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t id = ids[i];
+        key[i] = acc.key(id, off);
+        if constexpr (Acc::ALPHA == 4)
+            if (sym_count) c += 1ull << (16 * acc.sym(id, off - 1));
+    }
+    if constexpr (Acc::ALPHA == 4)
+        if (sym_count)
+            for (int b = 0; b < 4; ++b) block_tally<uint32_t>(uint32_t(c >> (16 * b)) & 0xFFFFu, sym_count + b);
 }
 
 // bounds[c] = first index whose symbol at off-1 is >= c (the list is
@@ -152,15 +164,24 @@ __global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t
 // reads themselves only when the first key symbols are equal.
 constexpr int MP_ITEMS = 8;
 
+// bounds: the run bounds (ALPHA + 1 entries), or with `counts` the number of
+// entries per symbol, from which the bounds are summed.
 template <class Acc>
 __global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict__ in, const uint64_t* __restrict__ ink,
                                    uint32_t* __restrict__ out, uint64_t* __restrict__ outk,
-                                   const uint32_t* __restrict__ bounds, const uint32_t* __restrict__ m_dev,
+                                   const uint32_t* __restrict__ bounds, bool counts, const uint32_t* __restrict__ m_dev,
                                    int width) {
     const uint32_t m = *m_dev;
     uint32_t bd[Acc::ALPHA + 1];
+    if (counts) {
+        bd[0] = 0;
 #pragma unroll
-    for (int c = 0; c <= Acc::ALPHA; ++c) bd[c] = bounds[c];
+        for (int c = 0; c < Acc::ALPHA - 1; ++c) bd[c + 1] = bd[c] + bounds[c];
+        bd[Acc::ALPHA] = m;
+    } else {
+#pragma unroll
+        for (int c = 0; c <= Acc::ALPHA; ++c) bd[c] = bounds[c];
+    }
     const int len = acc.L - off;
     auto run_at = [&](int r) { return bd[r < Acc::ALPHA ? r : Acc::ALPHA]; };
     // entry x against entry y (positions in the input)
@@ -330,8 +351,10 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     const int gk = resident_grid(list_keys_kernel<Acc>, 256, cnt);
     const int gm = resident_grid(merge_level_kernel<Acc>, 256, div_up(cnt, MP_ITEMS));
     const int gg = resident_grid(merge_groups_kernel<Acc>, 128, cnt);
-    list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, pre, len, 0, pk);
+    list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, pre, len, 0, pk, nullptr);
     CURC_LAUNCH_CHECK();
+    // 2-bit reads: the base runs' bounds come from counts taken with the keys
+    constexpr bool by_count = Acc::ALPHA == 4;
     constexpr int CHECK_EVERY = 8;
     int par = 0;
     for (int off = 1; off < acc.L; ++off, par ^= 1) {
@@ -340,9 +363,13 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
         uint32_t* mp_out = len + 2 * (par ^ 1);
         uint32_t* ms_out = mp_out + 1;
         SubStage sp_merge("full_match.resort");
-        run_bounds_kernel<Acc><<<1, 256, 0, s>>>(acc, suf, ms_in, off, bounds);
-        CURC_LAUNCH_CHECK();
-        list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, suf, ms_in, off, sk);
+        if (by_count) {
+            CURC_CHECK(cudaMemsetAsync(bounds, 0, 4 * sizeof(uint32_t), s));
+        } else {
+            run_bounds_kernel<Acc><<<1, 256, 0, s>>>(acc, suf, ms_in, off, bounds);
+            CURC_LAUNCH_CHECK();
+        }
+        list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, suf, ms_in, off, sk, by_count ? bounds : nullptr);
         CURC_LAUNCH_CHECK();
         {
             // levels: runs merged in pairs, then pairs of pairs, ...; the last
@@ -355,7 +382,8 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
                 const bool last = l + 1 == levels;
                 uint32_t* dst = last ? suf2 : (l % 2 == 0 ? mtmp : suf);
                 uint64_t* dstk = last ? sk2 : (l % 2 == 0 ? mk2 : sk);
-                merge_level_kernel<Acc><<<gm, 256, 0, s>>>(acc, off, src, srck, dst, dstk, bounds, ms_in, 1 << l);
+                merge_level_kernel<Acc><<<gm, 256, 0, s>>>(acc, off, src, srck, dst, dstk, bounds, by_count, ms_in,
+                                                            1 << l);
                 CURC_LAUNCH_CHECK();
                 src = dst;
                 srck = dstk;
