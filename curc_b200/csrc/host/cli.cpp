@@ -2,6 +2,8 @@
 // Compression: `curc -c -i in.fastq[,in_2.fastq] -o name [--working_dir d]
 // [--block_ratio r] [--flzma2_level l] [--flzma2_thread_num t]
 // [--preserve_order]` writes <working_dir>/<name>.curc.
+// Decompression: `curc -d -i in.curc -o name [--working_dir d]` writes
+// <working_dir>/<name>.seq (or <name>_1.seq and <name>_2.seq), host only.
 #include <dlfcn.h>
 #include <limits.h>
 #include <stdlib.h>
@@ -39,7 +41,7 @@ int usage() {
     std::puts(
         "curc (B200 path)\n"
         "  -c, --compress            compress file\n"
-        "  -d, --decompress          decompress archive (use the reference decoder)\n"
+        "  -d, --decompress          decompress archive\n"
         "  -i, --input arg           input path (paired-end fastq paths are separated by commas)\n"
         "  -o, --output arg          output file name\n"
         "      --working_dir arg     working directory (default .)\n"
@@ -88,13 +90,35 @@ int main(int argc, char** argv) {
         std::puts("compression and decompression options conflict");
         return 0;
     }
-    if (decomp) {
-        std::puts("decompression is not part of the B200 path yet: use the reference `curc -d`");
-        return 2;
-    }
     struct stat st;
     if (stat(wd.c_str(), &st) != 0) {
         std::puts("invalid working dir");
+        return 0;
+    }
+    if (decomp) {
+        // src/main.cpp:139-152: one archive path ending in .curc
+        if (input.find(',') != std::string::npos) {
+            std::puts("invalid input path number");
+            return 0;
+        }
+        if (stat(input.c_str(), &st) != 0 || !has_ext(input, ".curc")) {
+            std::puts("please check the archive path (filename extension is .curc)");
+            return 0;
+        }
+        std::string tmp = wd + "/curc_tmp_XXXXXX";
+        if (!mkdtemp(&tmp[0])) {
+            std::puts("cannot create a working directory");
+            return 1;
+        }
+        uint64_t reads = 0;
+        const int rc = curc_decompress_file(input.c_str(), (wd + "/" + output).c_str(), (self_dir() + "/bsc").c_str(),
+                                            tmp.c_str(), 0, &reads);
+        rmdir(tmp.c_str());
+        if (rc != CURC_OK) {
+            std::fprintf(stderr, "curc: %s\n", curc_last_error(nullptr));
+            return 1;
+        }
+        std::printf("reads count : %llu \n", (unsigned long long)reads);
         return 0;
     }
     if (!(ratio > 0 && ratio <= 1)) {

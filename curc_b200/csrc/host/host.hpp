@@ -62,6 +62,21 @@ struct IngestResult {
 };
 IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double block_ratio, IngestSink& sink);
 
+// Product decoder: a `.curc` archive to <out_prefix>.seq (single-end) or
+// <out_prefix>_1.seq and _2.seq (paired-end), one read per line, in the
+// reference decoder's order (decompress.cu:760-1060).  Host only.
+struct DecodeParams {
+    std::string bsc_path;  // the bsc executable (strand stream)
+    std::string tmpdir;    // scratch files for bsc
+    int threads = 0;       // host threads (0: all)
+};
+struct DecodeResult {
+    uint64_t reads = 0;
+    int blocks = 0, read_len = 0;
+    bool paired_end = false, preserve_order = false;
+};
+DecodeResult decode_archive(const std::string& archive, const std::string& out_prefix, const DecodeParams& p);
+
 // Read length of the first record (preprocess.cpp:286-300).
 int first_read_length(const std::string& f1);
 

@@ -99,6 +99,19 @@ int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2, const cha
                         int preserve_order, int flzma2_level, int flzma2_threads, const char* bsc_path,
                         const char* tmpdir, uint64_t* reads_out, uint32_t* blocks_out);
 
+/* Whole-archive decompression, the drop-in for `curc -d` (src/decompress.cu:
+ * 760-1060, src/decompress.cpp): reads the .curc archive at archive_path and
+ * writes <out_prefix>.seq (single end) or <out_prefix>_1.seq and
+ * <out_prefix>_2.seq (paired end), one read per line, byte for byte what the
+ * reference decoder writes.  Host only: needs no context and no GPU.  The
+ * strand stream goes through the `bsc` executable at bsc_path, with scratch
+ * files in tmpdir; threads = host threads (0: all).  *reads_out (may be
+ * NULL) receives the read count.  Errors (CURC_ERR_IO for files,
+ * CURC_ERR_STATE for a malformed archive) are described by
+ * curc_last_error(NULL). */
+int curc_decompress_file(const char* archive_path, const char* out_prefix, const char* bsc_path, const char* tmpdir,
+                         int threads, uint64_t* reads_out);
+
 /* Host view of a named result of the last block run ("strand", "mis_cnt",
  * "mis_base", "read_off", "ref", ... and the stage intermediates
  * "sorted_ids", "next", "prev", "offset", "hq_seq", ...).  The pointer stays
