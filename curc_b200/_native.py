@@ -62,6 +62,8 @@ def lib() -> ctypes.CDLL:
         L.curc_compress_files.argtypes = [c_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
                                           c_int, c_int, c_int, ctypes.c_char_p, ctypes.c_char_p,
                                           ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
+        L.curc_decompress_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, c_int,
+                                           ctypes.POINTER(c_u64)]
         L.curc_kernel_launches.restype = ctypes.c_uint64
         _lib = L
     return _lib
@@ -73,6 +75,21 @@ def kernel_launches() -> int:
 
 class CurcError(RuntimeError):
     pass
+
+
+def decompress_file(archive: str, out_prefix: str, bsc: str | None = None, tmpdir: str = "/tmp",
+                    threads: int = 0) -> int:
+    """`curc -d`: a .curc archive to <out_prefix>.seq (single end) or
+    <out_prefix>_1.seq / _2.seq (paired end), byte for byte the reference
+    decoder's output.  Host only (no GPU).  Returns the read count."""
+    if bsc is None:
+        bsc = os.path.join(os.path.dirname(LIB_PATH), "_build", "bsc")
+    n = ctypes.c_uint64()
+    rc = lib().curc_decompress_file(archive.encode(), out_prefix.encode(), bsc.encode(), tmpdir.encode(), threads,
+                                    ctypes.byref(n))
+    if rc != 0:
+        raise CurcError(f"curc_decompress_file: {lib().curc_last_error(None).decode()} (code {rc})")
+    return n.value
 
 
 class Context:

@@ -172,3 +172,13 @@ def test_cli_decompress(tmp_path):
     # an output directory that cannot be written
     rc, _, err = decode(archive, tmp_path / "no" / "such" / "dir")
     assert rc == CURC_ERR_IO, err
+
+
+def test_python_wrapper(tmp_path):
+    from curc_b200 import CurcError, decompress_file
+    archive = os.path.join(GOLDEN, "se250_n8k.curc")
+    assert decompress_file(archive, str(tmp_path / "py"), tmpdir=str(tmp_path)) == 8000
+    assert decode(archive, tmp_path)[0] == CURC_OK
+    assert outputs(tmp_path, "py", False) == outputs(tmp_path, "mine", False)
+    with pytest.raises(CurcError):
+        decompress_file(str(tmp_path / "missing.curc"), str(tmp_path / "x"), tmpdir=str(tmp_path))
