@@ -148,13 +148,42 @@ def probe_bytes(st, L):
 PROBE_DRAM_BYTES_PER_PROBE = 5.662e9 / 20.207e6
 
 
+def rank_seed(rank):
+    """Seed of a rank's block: every rank compresses its own block of the same
+    generator (independent blocks, weak scaling)."""
+    return 1 + 1000 * rank
+
+
+def init_dist(world):
+    """One process per GPU; NCCL when the ranks have GPUs, gloo otherwise (the
+    CPU tests of this plumbing).  A short timeout ends a rank that waits for
+    one that is gone."""
+    if world <= 1:
+        return
+    import datetime
+    import torch
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+
+
+def reduce_max(values, world, device="cpu"):
+    """Each value's maximum over the ranks (the step time of a weak-scaling run
+    is the slowest rank's); the values unchanged on one rank."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def run_ours(a, rank, world):
     import torch
     from curc_b200 import Context, kernel_launches
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    w = workload(a.pairs, a.genome, seed=1 + 1000 * rank)
+    w = workload(a.pairs, a.genome, seed=rank_seed(rank))
     seqs = w.sequences()
     n, L = seqs.shape
     bases = n * L
@@ -238,10 +267,7 @@ def run_ours(a, rank, world):
                      [int(x) for x in ctx.get("stats", np.uint64)]))
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     step_s = dev_ms / 1000.0 / a.steps
-    if world > 1:
-        t = torch.tensor([step_s, e2e_s, e2e_plain_s], dtype=torch.float64, device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        step_s, e2e_s, e2e_plain_s = float(t[0]), float(t[1]), float(t[2])
+    step_s, e2e_s, e2e_plain_s = reduce_max([step_s, e2e_s, e2e_plain_s], world, f"cuda:{dev}")
     batched = None
     if not a.no_batched and rank == 0:
         batched = batched_vs_plain(ctx, a)
@@ -372,14 +398,17 @@ def run_reference(a):
     return {"bases": w.bases, "s": mean, "steps": len(times)}, None
 
 
+def finish_dist(world):
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    if world > 1:
-        import torch
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    init_dist(world)
     cfg = {"workload": f"paired-end 150 bp, {a.pairs} pairs ({2 * a.pairs * 150 / 1e9:.1f} Gbases) from a "
                        f"{a.genome / 1e6:.0f} Mbp genome (40% GC, 5% repeats at 1% divergence), insert N(400,50), "
                        "0.2% substitutions, 0.01% N, --preserve_order, block_ratio 1",
@@ -387,10 +416,12 @@ def main():
            "l2_flush": "inputs (3 GB ASCII per block) are larger than L2"}
     if a.impl == "reference":
         if rank != 0:
+            finish_dist(world)
             return
         ref, why = run_reference(a)
         if ref is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
+            finish_dist(world)
             return
         v = ref["bases"] / ref["s"] / 1e6
         out = {"metric": METRIC, "value": v, "unit": "Mbases/s", "n_gpus": 1, "steps": ref["steps"],
@@ -402,9 +433,11 @@ def main():
                                           f"{a.ref_sample_pairs} pairs of the same generator"},
                "e2e": {"value": v, "unit": "Mbases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
+        finish_dist(world)
         return
     r = run_ours(a, rank, world)
     if rank != 0:
+        finish_dist(world)
         return
     peak, peak_kind = hbm_peak()
     pack_ms = r["stage_ms"]["pack"]
@@ -455,12 +488,10 @@ def main():
         out["batched"] = r["batched"]
     if not a.no_learned and rank == 0:
         out["learned_coder"] = learned_eval(a)
-    if not a.no_cpu_baseline:
+    if not a.no_cpu_baseline and world == 1:
         out["cpu_baseline"] = cpu_baseline(a)
     print(json.dumps(out))
-    if world > 1:
-        import torch
-        torch.distributed.destroy_process_group()
+    finish_dist(world)
 
 
 if __name__ == "__main__":
