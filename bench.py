@@ -300,9 +300,15 @@ def cpu_baseline(a):
     t = time.perf_counter()
     OracleBlock(seqs, True, True, threads=threads)
     dt = time.perf_counter() - t
+    # the same on one core, for the scaling of the restatement with cores
+    t = time.perf_counter()
+    OracleBlock(seqs, True, True, threads=1)
+    dt1 = time.perf_counter() - t
     return {"value": seqs.size / dt / 1e6, "unit": "Mbases/s", "cores": threads, "kind": "port",
+            "value_1_core": seqs.size / dt1 / 1e6,
             "sample": f"{a.cpu_sample_pairs} pairs x 150 bp of the same generator ({seqs.size / 1e6:.0f} Mbases), "
-                      f"block streams without the entropy coders, {dt:.1f} s"}
+                      f"block streams without the entropy coders, {dt:.1f} s on {threads} threads, {dt1:.1f} s on "
+                      "one (OpenMP only in the mapping loop)"}
 
 
 # Record headers long enough for the reference's block-boundary heuristic
