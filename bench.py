@@ -278,6 +278,7 @@ def run_ours(a, rank, world):
             ws = workload(a.ref_sample_pairs, a.genome, seed=1)
             v_s, t_s, sz_s = cli_run(ctx, ws, td, "sample")
         cli = {"value": v_full, "unit": "Mbases/s", "s": t_full, "archive_bytes": sz_full,
+               "archive_bits_per_base": 8.0 * sz_full / w.bases,
                "sample_value": v_s, "sample": f"{a.ref_sample_pairs} pairs of the same generator (the reference "
                                                f"arm's sample), {t_s:.2f} s, archive {sz_s} bytes",
                "includes": "FASTQ parse and block split, device path, host stream coders, archive write "

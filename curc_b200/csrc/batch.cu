@@ -266,7 +266,11 @@ int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user) {
             work(*q.pool[0], 0);
             for (auto& t : th) t.join();
         }
-        if (err) std::rethrow_exception(err);
+        // no copy may still read the caller's reads once the drain returns
+        if (err) {
+            cudaStreamSynchronize(q.copy_stream);
+            std::rethrow_exception(err);
+        }
         return int(CURC_OK);
     });
 }
