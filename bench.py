@@ -274,11 +274,12 @@ def run_ours(a, rank, world):
     cli = None
     if not a.no_cli and rank == 0:
         with tempfile.TemporaryDirectory() as td:
-            v_full, t_full, sz_full = cli_run(ctx, w, td, "full")
+            v_full, t_full, sz_full, host_ms = cli_run(ctx, w, td, "full")
             ws = workload(a.ref_sample_pairs, a.genome, seed=1)
-            v_s, t_s, sz_s = cli_run(ctx, ws, td, "sample")
+            v_s, t_s, sz_s, _ = cli_run(ctx, ws, td, "sample")
         cli = {"value": v_full, "unit": "Mbases/s", "s": t_full, "archive_bytes": sz_full,
                "archive_bits_per_base": 8.0 * sz_full / w.bases,
+               "host_stage_ms": host_ms,
                "sample_value": v_s, "sample": f"{a.ref_sample_pairs} pairs of the same generator (the reference "
                                                f"arm's sample), {t_s:.2f} s, archive {sz_s} bytes",
                "includes": "FASTQ parse and block split, device path, host stream coders, archive write "
@@ -325,10 +326,18 @@ def cli_run(ctx, w, td, tag):
     ctx.compress_files(files, os.path.join(td, tag + ".curc"), 1.0, True, os.path.join(ROOT, "curc_b200", "_build", "bsc"),
                        td)
     dt = time.perf_counter() - t
+    host_ms = {}
+    for k in ["files.total", "files.ingest", "files.device", "files.snapshot", "files.until_last_block",
+              "files.coder_tail", "files.coders", "coder.id_pos", "coder.strand", "coder.ref", "coder.maps",
+              "coder.mis_cnt", "coder.mis_base", "coder.mis_off", "coder.read_off", "coder.pe_order"]:
+        try:
+            host_ms[k] = round(ctx.stage_ms(k), 3)
+        except Exception:
+            pass
     size = os.path.getsize(os.path.join(td, tag + ".curc"))
     for f in files + [os.path.join(td, tag + ".curc")]:
         os.remove(f)
-    return w.bases / dt / 1e6, dt, size
+    return w.bases / dt / 1e6, dt, size, host_ms
 
 
 def batched_vs_plain(ctx, a):

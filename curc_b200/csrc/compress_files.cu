@@ -8,7 +8,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <future>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -45,10 +47,23 @@ std::shared_ptr<Snapshot> snapshot(const Block& b) {
 // into one of two pinned staging buffers, copied asynchronously into the
 // block's device input while the next window is read and parsed; the block
 // then runs and its streams are coded on a host thread.
+// Host-stage seconds of one whole-file run, summed over its blocks (coder
+// threads add theirs concurrently).
+struct FileTimes {
+    std::mutex mu;
+    double ingest = 0, device = 0, snapshot = 0, coders = 0;
+    std::map<std::string, double> coder;
+    void add_coder(const char* what, double s) {
+        std::lock_guard<std::mutex> g(mu);
+        coder[what] += s;
+    }
+};
+
 class DeviceSink : public host::IngestSink {
 public:
-    DeviceSink(Block& blk, bool po, bool pe, const host::CoderParams& cp, bool verbose)
-        : blk_(blk), po_(po), pe_(pe), cp_(cp), verbose_(verbose) {
+    DeviceSink(Block& blk, bool po, bool pe, const host::CoderParams& cp, bool verbose, FileTimes& times)
+        : blk_(blk), po_(po), pe_(pe), cp_(cp), verbose_(verbose), times_(times) {
+        cp_.on_time = [t = &times_](const char* what, double s) { t->add_coder(what, s); };
         for (auto& e : ev_) CURC_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     ~DeviceSink() override {
@@ -96,10 +111,22 @@ public:
         const size_t bi = bodies.size();
         const bool verbose = verbose_;
         const host::CoderParams cp = cp_;
-        bodies.push_back(std::async(std::launch::async, [snap, cp, verbose, bi] {
+        FileTimes* times = &times_;
+        {
+            std::lock_guard<std::mutex> g(times_.mu);
+            times_.ingest += secs(t_begin_, ta);
+            times_.device += secs(ta, tb);
+            times_.snapshot += secs(tb, tc);
+        }
+        bodies.push_back(std::async(std::launch::async, [snap, cp, verbose, bi, times] {
             const auto e0 = clk::now();
             std::string body = host::encode_block(snap->view, cp);
-            if (verbose) std::fprintf(stderr, "curc: block %zu coders %.3f s\n", bi, secs(e0, clk::now()));
+            const double s = secs(e0, clk::now());
+            {
+                std::lock_guard<std::mutex> g(times->mu);
+                times->coders += s;
+            }
+            if (verbose) std::fprintf(stderr, "curc: block %zu coders %.3f s\n", bi, s);
             return body;
         }));
         if (verbose_)
@@ -119,6 +146,7 @@ private:
     bool po_, pe_;
     host::CoderParams cp_;
     bool verbose_;
+    FileTimes& times_;
     Stage stage_[2];
     cudaEvent_t ev_[2];
     int cur_ = 0, L_ = 0;
@@ -165,8 +193,10 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
         // CURC_VERBOSE=1 prints host-side stage times to stderr
         const bool verbose = std::getenv("CURC_VERBOSE") != nullptr;
         const auto t0 = std::chrono::steady_clock::now();
-        curc::DeviceSink sink(blk, preserve_order != 0, !s2.empty(), cp, verbose);
+        curc::FileTimes times;
+        curc::DeviceSink sink(blk, preserve_order != 0, !s2.empty(), cp, verbose, times);
         const auto res = curc::host::ingest_fastq(f1, s2, block_ratio, sink);
+        const auto t1 = std::chrono::steady_clock::now();
         const int L = res.read_len;
         auto& bodies = sink.bodies;
         blk.keep_intermediates = keep_inter;
@@ -179,9 +209,23 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
             std::fwrite(b.data(), 1, b.size(), out);
         }
         std::fclose(out);
-        if (verbose)
-            std::fprintf(stderr, "curc: total %.3f s\n",
-                         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+        const auto t2 = std::chrono::steady_clock::now();
+        auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return float(std::chrono::duration<double, std::milli>(b - a).count());
+        };
+        if (verbose) std::fprintf(stderr, "curc: total %.3f s\n", ms(t0, t2) / 1000.0);
+        // host-stage times of this call, readable with curc_block_stage_ms
+        blk.stage_ms["files.total"] = ms(t0, t2);
+        blk.stage_ms["files.until_last_block"] = ms(t0, t1);
+        blk.stage_ms["files.coder_tail"] = ms(t1, t2);
+        {
+            std::lock_guard<std::mutex> g(times.mu);
+            blk.stage_ms["files.ingest"] = float(times.ingest * 1000.0);
+            blk.stage_ms["files.device"] = float(times.device * 1000.0);
+            blk.stage_ms["files.snapshot"] = float(times.snapshot * 1000.0);
+            blk.stage_ms["files.coders"] = float(times.coders * 1000.0);
+            for (const auto& kv : times.coder) blk.stage_ms["coder." + kv.first] = float(kv.second * 1000.0);
+        }
         if (reads_out) *reads_out = res.reads;
         if (blocks_out) *blocks_out = uint32_t(res.blocks);
         return CURC_OK;

@@ -270,13 +270,13 @@ std::string pe_order(const uint32_t* order, size_t n, int level, int thr) {
 
 // CURC_VERBOSE=1: time of each coder on stderr.
 template <class F>
-std::string timed(const char* what, F&& f) {
+std::string timed(const CoderParams& cp, const char* what, F&& f) {
     static const bool verbose = std::getenv("CURC_VERBOSE") != nullptr;
-    if (!verbose) return f();
     const auto t0 = std::chrono::steady_clock::now();
     std::string r = f();
-    std::fprintf(stderr, "curc:   coder %-16s %.3f s, %zu bytes\n", what,
-                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), r.size());
+    const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (verbose) std::fprintf(stderr, "curc:   coder %-16s %.3f s, %zu bytes\n", what, s, r.size());
+    if (cp.on_time) cp.on_time(what, s);
     return r;
 }
 
@@ -298,7 +298,7 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
     // concurrent coders
     std::future<std::string> f_idpos, f_strand, f_ref, f_peorder;
     if (v.preserve_order) {
-        f_idpos = std::async(std::launch::async, [&] { return timed("id_pos", [&] {
+        f_idpos = std::async(std::launch::async, [&] { return timed(cp, "id_pos", [&] {
             const Buf& b = S("id_to_pos");
             const uint64_t* p = reinterpret_cast<const uint64_t*>(b.ptr);
             const size_t n = b.size / 8;
@@ -312,11 +312,11 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
             return join_std ? pe_id_to_pos<uint32_t>(p, n, lvl, thr) : pe_id_to_pos<uint64_t>(p, n, lvl, thr);
         }); });
     }
-    f_strand = std::async(std::launch::async, [&] { return timed("strand", [&] {
+    f_strand = std::async(std::launch::async, [&] { return timed(cp, "strand", [&] {
         const Buf& b = S("strand");
         return bsc_strand(cp.bsc_path, cp.tmpdir, b.ptr, b.size);
     }); });
-    f_ref = std::async(std::launch::async, [&] { return timed("ref", [&] {
+    f_ref = std::async(std::launch::async, [&] { return timed(cp, "ref", [&] {
         std::string joined_ref;
         joined_ref.reserve(S("ref").size + S("unmap_ref").size + S("unmap_n_ref").size);
         for (const char* nm : {"ref", "unmap_ref", "unmap_n_ref"})
@@ -336,19 +336,19 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
         return r;
     }); });
     if (!v.preserve_order && v.paired_end) {
-        f_peorder = std::async(std::launch::async, [&] {
+        f_peorder = std::async(std::launch::async, [&] { return timed(cp, "pe_order", [&] {
             const Buf& b = S("pe_order");
             return pe_order(reinterpret_cast<const uint32_t*>(b.ptr), b.size / 4, lvl, thr);
-        });
+        }); });
     }
     // mismatch offsets (CLR range coder) in parallel per class
     const int max_mm = L / 5;
     std::vector<std::future<std::string>> f_off;
     for (int m = 1; m <= max_mm; ++m) {
-        f_off.push_back(std::async(std::launch::async, [&, m] {
+        f_off.push_back(std::async(std::launch::async, [&, m] { return timed(cp, "mis_off", [&] {
             const Buf& b = S(("mis_off_" + std::to_string(m)).c_str());
             return offsets(L, reinterpret_cast<const uint16_t*>(b.ptr), b.size / 2, size_t(m));
-        }));
+        }); }));
     }
     // the PPMd / LZMA streams (serialised inside `container`)
     auto plain = [&](const char* nm, uint8_t coder, int param, double est) {
@@ -357,13 +357,13 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
     };
     std::string read_off, unmap_n_off, unmap_off;
     if (!v.preserve_order) {
-        read_off = plain("read_off", PPMD7_CODER, 3, 1);
-        unmap_n_off = plain("unmap_n_read_off", PPMD7_CODER, 3, 1);
-        unmap_off = plain("unmap_read_off", PPMD7_CODER, 3, 1);
+        read_off = timed(cp, "read_off", [&] { return plain("read_off", PPMD7_CODER, 3, 1); });
+        unmap_n_off = timed(cp, "read_off", [&] { return plain("unmap_n_read_off", PPMD7_CODER, 3, 1); });
+        unmap_off = timed(cp, "read_off", [&] { return plain("unmap_read_off", PPMD7_CODER, 3, 1); });
     }
     const double est = simpleUintCompressionEstimate(S("ref").size, ref_std ? 0xFFFFFFFFull : ~0ull);
     const int period = ref_std ? 2 : 3;
-    std::string maps = timed("maps", [&] {
+    std::string maps = timed(cp, "maps", [&] {
     std::string maps;
     for (auto pr : {std::make_pair("ref_off", "ref_len_map"), std::make_pair("unmap_ref_off", "unmap_ref_len"),
                     std::make_pair("unmap_n_ref_off", "unmap_n_ref_len")}) {
@@ -372,9 +372,9 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
     }
     return maps;
     });
-    const std::string mis_cnt = timed("mis_cnt", [&] { return plain("mis_cnt", PPMD7_CODER, 2, 1); });
+    const std::string mis_cnt = timed(cp, "mis_cnt", [&] { return plain("mis_cnt", PPMD7_CODER, 2, 1); });
     const std::string mis_base =
-        timed("mis_base", [&] { return plain("mis_base", PPMD7_CODER, 2, COMPRESSION_ESTIMATION_MIS_SYM); });
+        timed(cp, "mis_base", [&] { return plain("mis_base", PPMD7_CODER, 2, COMPRESSION_ESTIMATION_MIS_SYM); });
 
     std::string out = hdr;
     if (v.preserve_order) out += blob(f_idpos.get());

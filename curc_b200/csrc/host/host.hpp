@@ -29,6 +29,8 @@ struct CoderParams {
     int flzma2_threads = 16;  // --flzma2_thread_num
     std::string bsc_path;     // the bsc executable (strand stream)
     std::string tmpdir;       // scratch files for bsc
+    // called (from coder threads) with each coder's name and seconds
+    std::function<void(const char*, double)> on_time;
 };
 
 // Block body in the reference layout (compress.cu:1364-2146).
