@@ -181,7 +181,13 @@ uint64_t curc_kernel_launches(void);
 /* Milliseconds of device time of the last block run, by stage
  * (CUDA events on the context's stream): "pack", "sort_dedupe", "overlap",
  * "chain_filter", "full_match", "assembly", "mapping", "emit",
- * "unmapped_refs", "refmatch", and "total" (the whole run). */
+ * "unmapped_refs", "refmatch", and "total" (the whole run).  After
+ * curc_compress_files, also its host-stage wall times summed over blocks:
+ * "files.total", "files.ingest", "files.device", "files.snapshot",
+ * "files.coders" (coder threads), "files.until_last_block",
+ * "files.coder_tail" (coding left after the last block ran), and
+ * "coder.<stream>" per coder ("id_pos", "strand", "ref", "maps",
+ * "mis_cnt", "mis_base", "mis_off", "read_off", "pe_order"). */
 int curc_block_stage_ms(curc_ctx* ctx, const char* stage, float* ms);
 
 #ifdef __cplusplus
