@@ -19,6 +19,7 @@
 #include <stdexcept>
 #include <thread>
 
+#include "../../../include/curc_b200.h"
 #include "host.hpp"
 
 namespace curc {
@@ -294,3 +295,63 @@ IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double r
 
 }  // namespace host
 }  // namespace curc
+
+namespace curc {
+std::string& ctxless_error();
+
+namespace {
+// Ingest sink that hands each block's reads, in host memory, to a callback.
+class HostSink : public host::IngestSink {
+public:
+    HostSink(curc_fastq_block_fn fn, void* user) : fn_(fn), user_(user) {}
+    void begin_block(size_t max_bytes, int L) override {
+        L_ = L;
+        off_ = 0;
+        buf_.resize(std::max(buf_.size(), max_bytes));
+    }
+    char* window_buffer(size_t bytes) override {
+        if (off_ + bytes > buf_.size()) buf_.resize(off_ + bytes);
+        return buf_.data() + off_;
+    }
+    void window_done(uint64_t reads) override { off_ += size_t(reads) * size_t(L_); }
+    void end_block() override {
+        const uint64_t n = off_ / size_t(L_);
+        if (fn_(user_, index_++, buf_.data(), n, uint16_t(L_)) != 0)
+            throw std::logic_error("curc_fastq_blocks stopped by the callback");
+    }
+
+private:
+    curc_fastq_block_fn fn_;
+    void* user_;
+    std::vector<char> buf_;
+    size_t off_ = 0;
+    int L_ = 1;
+    uint32_t index_ = 0;
+};
+}  // namespace
+}  // namespace curc
+
+extern "C" int curc_fastq_blocks(const char* f1, const char* f2, double block_ratio, curc_fastq_block_fn block,
+                                 void* user, uint64_t* reads_out, uint32_t* blocks_out) {
+    if (!f1 || !block) {
+        curc::ctxless_error() = "curc_fastq_blocks: null path or callback";
+        return CURC_ERR_ARG;
+    }
+    if (!(block_ratio > 0 && block_ratio <= 1)) {
+        curc::ctxless_error() = "block ratio is a float number in the range (0,1]";
+        return CURC_ERR_ARG;
+    }
+    try {
+        curc::HostSink sink(block, user);
+        const auto r = curc::host::ingest_fastq(f1, f2 ? f2 : "", block_ratio, sink);
+        if (reads_out) *reads_out = r.reads;
+        if (blocks_out) *blocks_out = uint32_t(r.blocks);
+        return CURC_OK;
+    } catch (const std::logic_error& e) {
+        curc::ctxless_error() = e.what();
+        return CURC_ERR_STATE;
+    } catch (const std::exception& e) {
+        curc::ctxless_error() = e.what();
+        return CURC_ERR_IO;
+    }
+}

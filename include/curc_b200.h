@@ -99,6 +99,19 @@ int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2, const cha
                         int preserve_order, int flzma2_level, int flzma2_threads, const char* bsc_path,
                         const char* tmpdir, uint64_t* reads_out, uint32_t* blocks_out);
 
+/* FASTQ ingest alone, host only (the block split of process(),
+ * preprocess.cpp:66-254): reads f1 (and f2 for paired end, else NULL) in
+ * the reference's windows, cuts blocks where it does, and calls
+ * block(user, index, seqs, n, read_len) once per block with its n reads
+ * (n x read_len ASCII bytes in block order, mates interleaved; valid during
+ * the call), e.g. to queue them with curc_batch_submit after a copy.  A
+ * non-zero return from block stops with CURC_ERR_STATE; unreadable or
+ * malformed input gives CURC_ERR_IO.  *reads_out / *blocks_out (may be
+ * NULL) receive the totals. */
+typedef int (*curc_fastq_block_fn)(void* user, uint32_t index, const char* seqs, uint64_t n, uint16_t read_len);
+int curc_fastq_blocks(const char* f1, const char* f2, double block_ratio, curc_fastq_block_fn block, void* user,
+                      uint64_t* reads_out, uint32_t* blocks_out);
+
 /* Whole-archive decompression, the drop-in for `curc -d` (src/decompress.cu:
  * 760-1060, src/decompress.cpp): reads the .curc archive at archive_path and
  * writes <out_prefix>.seq (single end) or <out_prefix>_1.seq and

@@ -600,3 +600,38 @@ uint64_t oracle_decode_offsets(const char* buf, uint64_t n, int read_len, int m,
     return run(std::integral_constant<size_t, 512>{});
 }
 }
+
+extern "C" {
+
+// The block split of split_fastq (preprocess.cpp:66-254): block count,
+// read length, reads per block (counts, up to 255 entries) and all blocks'
+// reads concatenated (*seqs, freed with oracle_buf_free).  Returns 0, or -1
+// with the message in *seqs.
+int oracle_split_fastq(const char* f1, const char* f2, double ratio, uint32_t* nblocks, int* read_len,
+                       uint64_t* counts, char** seqs, uint64_t* seq_bytes) {
+    try {
+        int L = 0;
+        auto blocks = oracle::split_fastq(f1, f2 ? f2 : "", L, ratio);
+        size_t total = 0;
+        for (const auto& b : blocks) total += b.seqs.size();
+        char* out = static_cast<char*>(std::malloc(total ? total : 1));
+        size_t off = 0;
+        for (size_t i = 0; i < blocks.size(); ++i) {
+            counts[i] = blocks[i].count;
+            if (!blocks[i].seqs.empty()) std::memcpy(out + off, blocks[i].seqs.data(), blocks[i].seqs.size());
+            off += blocks[i].seqs.size();
+        }
+        *nblocks = uint32_t(blocks.size());
+        *read_len = L;
+        *seqs = out;
+        *seq_bytes = total;
+        return 0;
+    } catch (const std::exception& e) {
+        const std::string m = e.what();
+        char* out = static_cast<char*>(std::malloc(m.size() + 1));
+        std::memcpy(out, m.c_str(), m.size() + 1);
+        *seqs = out;
+        return -1;
+    }
+}
+}
