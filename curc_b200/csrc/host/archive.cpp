@@ -37,6 +37,7 @@
 #include <range_coder/clr.cdr>
 #include <range_coder/simple_model.h>
 
+#include "../../../include/curc_b200.h"
 #include "host.hpp"
 
 namespace curc {
@@ -420,3 +421,65 @@ std::string archive_header(bool po, bool pe, int read_len, int blocks) {
 
 }  // namespace host
 }  // namespace curc
+
+namespace curc {
+std::string& ctxless_error();
+}
+
+extern "C" {
+
+int curc_encode_block(uint32_t reads_count, uint16_t read_len, int preserve_order, int paired_end,
+                      const char* const* names, const void* const* ptrs, const uint64_t* sizes, uint32_t count,
+                      int flzma2_level, int flzma2_threads, const char* bsc_path, const char* tmpdir, char** out,
+                      uint64_t* out_bytes) {
+    if (!out || !out_bytes || !bsc_path || !tmpdir || (count && (!names || !ptrs || !sizes)) || read_len < 1 ||
+        read_len > 511) {
+        curc::ctxless_error() = "curc_encode_block: bad argument";
+        return CURC_ERR_ARG;
+    }
+    *out = nullptr;
+    *out_bytes = 0;
+    try {
+        curc::host::BlockView v;
+        v.reads_count = reads_count;
+        v.read_len = read_len;
+        v.preserve_order = preserve_order != 0;
+        v.paired_end = paired_end != 0;
+        for (uint32_t i = 0; i < count; ++i) {
+            if (!names[i] || (sizes[i] && !ptrs[i])) throw std::invalid_argument("curc_encode_block: null stream");
+            v.streams[names[i]] = curc::host::Buf{static_cast<const uint8_t*>(ptrs[i]), size_t(sizes[i])};
+        }
+        curc::host::CoderParams cp;
+        cp.flzma2_level = flzma2_level;
+        cp.flzma2_threads = flzma2_threads;
+        cp.bsc_path = bsc_path;
+        cp.tmpdir = tmpdir;
+        const std::string body = curc::host::encode_block(v, cp);
+        char* b = static_cast<char*>(std::malloc(body.size() ? body.size() : 1));
+        if (!b) throw std::bad_alloc();
+        std::memcpy(b, body.data(), body.size());
+        *out = b;
+        *out_bytes = body.size();
+        return CURC_OK;
+    } catch (const std::invalid_argument& e) {
+        curc::ctxless_error() = e.what();
+        return CURC_ERR_ARG;
+    } catch (const std::exception& e) {
+        curc::ctxless_error() = e.what();
+        return CURC_ERR_STATE;
+    }
+}
+
+void curc_buffer_free(char* p) { std::free(p); }
+
+int curc_archive_header(int preserve_order, int paired_end, uint16_t read_len, uint32_t blocks, char* out5) {
+    if (!out5 || blocks > 254 || read_len < 1 || read_len > 511) {
+        curc::ctxless_error() = "curc_archive_header: bad argument";
+        return CURC_ERR_ARG;
+    }
+    const std::string h = curc::host::archive_header(preserve_order != 0, paired_end != 0, read_len, int(blocks));
+    std::memcpy(out5, h.data(), 5);
+    return CURC_OK;
+}
+
+}  // extern "C"

@@ -99,6 +99,25 @@ int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2, const cha
                         int preserve_order, int flzma2_level, int flzma2_threads, const char* bsc_path,
                         const char* tmpdir, uint64_t* reads_out, uint32_t* blocks_out);
 
+/* One block's streams to its archive body in the reference's block layout
+ * (compress.cu:1364-2146), host only: the coders curc_compress_files uses,
+ * on streams named as curc_block_get names them ("decoder_table", "sizes",
+ * "strand", "ref", "unmap_ref", "unmap_n_ref", "id_to_pos" or "read_off",
+ * "unmap_read_off", "unmap_n_read_off", "pe_order", the six repeat maps,
+ * "mis_cnt", "mis_base", "mis_off_<m>"), e.g. those a curc_batch_drain
+ * callback reads.  count streams: names[i], ptrs[i], sizes[i] bytes.  The
+ * strand stream goes through the `bsc` executable at bsc_path (scratch files
+ * in tmpdir).  *out (free it with curc_buffer_free) receives the body,
+ * *out_bytes its size; a missing stream gives CURC_ERR_STATE. */
+int curc_encode_block(uint32_t reads_count, uint16_t read_len, int preserve_order, int paired_end,
+                      const char* const* names, const void* const* ptrs, const uint64_t* sizes, uint32_t count,
+                      int flzma2_level, int flzma2_threads, const char* bsc_path, const char* tmpdir, char** out,
+                      uint64_t* out_bytes);
+void curc_buffer_free(char* p);
+/* The 5-byte archive header (preprocess.cpp:261-266) into out5: an archive
+ * is this header followed by its block bodies in order (at most 254). */
+int curc_archive_header(int preserve_order, int paired_end, uint16_t read_len, uint32_t blocks, char* out5);
+
 /* FASTQ ingest alone, host only (the block split of process(),
  * preprocess.cpp:66-254): reads f1 (and f2 for paired end, else NULL) in
  * the reference's windows, cuts blocks where it does, and calls
