@@ -211,7 +211,9 @@ int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user) {
             if (rc != 0) throw std::runtime_error("batch drain stopped by the callback");
         };
         // large blocks first, from this thread: while one pipeline runs a
-        // block, the next block's reads are already queued on the other's stream
+        // block, the next block's reads already cross to the other pipeline's
+        // input slot on the copy stream (pageable input is first copied to
+        // pinned staging on this thread, which that overlap does not cover)
         if (!large.empty()) {
             const int P = std::min(W, 2);
             try {
