@@ -11,7 +11,10 @@
 // memory from the archive bytes (the reference writes each stream to a
 // scratch file and reads it back; only bsc, an executable, still goes
 // through files), and the reads are rebuilt by OpenMP over bounded output
-// chunks written in the reference decoder's order.
+// chunks written in the reference decoder's order.  The LZMA and PPMd
+// payloads go straight to the LZMA SDK's decoders and the var-len DNA
+// payload to a bounds-checked restatement, so a corrupt archive gives an
+// error instead of ending the process (the vendored wrappers exit()).
 #include <omp.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -33,6 +36,9 @@
 #define ABS std::abs
 #endif
 #include <fast-lzma2/fast-lzma2.h>
+#include <lzma/Alloc.h>
+#include <lzma/LzmaDec.h>
+#include <lzma/Ppmd7.h>
 #include <lzma/VarLenDNACoder/LzmaLib.h>
 #include <range_coder/clr.cdr>
 #include <range_coder/simple_model.h>
@@ -117,6 +123,96 @@ std::vector<T> as_array(const std::string& bytes) {
     return v;
 }
 
+// ---- coded payloads (the formats LzmaLib.cpp writes), decoded without the
+// wrappers' exit() paths
+
+struct MemByteIn {
+    IByteIn vt;
+    const Byte* cur;
+    const Byte* lim;
+    bool overrun;
+};
+Byte mem_read_byte(const IByteIn* p) {
+    MemByteIn* m = reinterpret_cast<MemByteIn*>(const_cast<IByteIn*>(p));
+    if (m->cur < m->lim) return *m->cur++;
+    m->overrun = true;
+    return 0;
+}
+
+// LZMA: 5 property bytes, then the raw LZMA stream.
+void lzma_payload(const uint8_t* src, size_t n, uint8_t* dst, size_t out) {
+    if (n < LZMA_PROPS_SIZE) throw std::runtime_error("corrupt LZMA stream");
+    SizeT dl = out, sl = n - LZMA_PROPS_SIZE;
+    ELzmaStatus st;
+    const SRes r = LzmaDecode(dst, &dl, src + LZMA_PROPS_SIZE, &sl, src, LZMA_PROPS_SIZE, LZMA_FINISH_ANY, &st,
+                              &g_Alloc);
+    if (r != SZ_OK || dl != out) throw std::runtime_error("corrupt LZMA stream");
+}
+
+// PPMd (variant H, 7z range coder): the model order, the model memory size
+// (u32), then the range-coded symbols; every coded byte must be consumed.
+void ppmd_payload(const uint8_t* src, size_t n, uint8_t* dst, size_t out) {
+    if (n < 5) throw std::runtime_error("corrupt PPMd stream");
+    const unsigned order = src[0];
+    uint32_t mem;
+    std::memcpy(&mem, src + 1, 4);
+    if (order < PPMD7_MIN_ORDER || order > PPMD7_MAX_ORDER || mem < PPMD7_MIN_MEM_SIZE || mem > PPMD7_MAX_MEM_SIZE)
+        throw std::runtime_error("corrupt PPMd stream properties");
+    CPpmd7 ppmd;
+    Ppmd7_Construct(&ppmd);
+    if (!Ppmd7_Alloc(&ppmd, mem, &g_Alloc)) throw std::bad_alloc();
+    Ppmd7_Init(&ppmd, order);
+    MemByteIn in{{mem_read_byte}, src + 5, src + n, false};
+    CPpmd7z_RangeDec rd;
+    Ppmd7z_RangeDec_CreateVTable(&rd);
+    rd.Stream = &in.vt;
+    bool ok = Ppmd7z_RangeDec_Init(&rd) != 0;
+    size_t i = 0;
+    if (ok) {
+        for (; i < out; ++i) {
+            const int sym = Ppmd7_DecodeSymbol(&ppmd, &rd.vt);
+            if (sym < 0 || in.overrun) break;
+            dst[i] = Byte(sym);
+        }
+    }
+    ok = ok && i == out && !in.overrun && in.cur == in.lim && Ppmd7z_RangeDec_IsFinishedOK(&rd);
+    Ppmd7_Free(&ppmd, &g_Alloc);
+    if (!ok) throw std::runtime_error("corrupt PPMd stream");
+}
+
+// PgRC's var-len DNA coding: a coder byte (static or dynamic book) and a book
+// id, the code book as text (up to 256 codes of one to four symbols, one per
+// line, the first a single symbol, ended by a zero byte), then one byte per
+// code, each standing for its code's symbols.
+void varlen_payload(const uint8_t* src, size_t n, uint8_t* dst, size_t out) {
+    using VL = PgSAHelpers::VarLenDNACoder;
+    if (n < 2 || (src[0] != VL::STATIC_CODES_CODER_PARAM && src[0] != VL::DYNAMIC_CODES_CODER_PARAM))
+        throw std::runtime_error("corrupt var-len DNA stream");
+    const uint8_t* book = src + 2;
+    const uint8_t* end = static_cast<const uint8_t*>(std::memchr(book, 0, n - 2));
+    if (!end) throw std::runtime_error("corrupt var-len DNA code book");
+    std::vector<std::string> codes;
+    const uint8_t* a = book;
+    for (;;) {
+        const uint8_t* b = static_cast<const uint8_t*>(std::memchr(a, '\n', size_t(end - a)));
+        const uint8_t* e = b ? b : end;
+        if (e - a > 4 || codes.size() == 256) throw std::runtime_error("corrupt var-len DNA code book");
+        codes.emplace_back(reinterpret_cast<const char*>(a), size_t(e - a));
+        if (!b) break;
+        a = b + 1;
+    }
+    if (codes[0].size() != 1) throw std::runtime_error("corrupt var-len DNA code book");
+    size_t o = 0;
+    for (const uint8_t* p = end + 1; p < src + n; ++p) {
+        if (*p >= codes.size()) continue;  // an unused code stands for nothing
+        const std::string& c = codes[*p];
+        if (c.size() > out - o) throw std::runtime_error("var-len DNA stream longer than stated");
+        std::memcpy(dst + o, c.data(), c.size());
+        o += c.size();
+    }
+    if (o != out) throw std::runtime_error("var-len DNA stream shorter than stated");
+}
+
 // A payload read front to back: size-prefixed blobs (u64 size, bytes) and
 // the LZMA SDK containers of LzmaLib.cpp (decoded size, coded size, coder,
 // coded bytes), which carry no size prefix of their own.  A container's
@@ -134,23 +230,15 @@ public:
     }
     template <class T>
     std::vector<T> values() {
-        const size_t end = container_end(off_, 0);
-        if (u64_at(off_) % sizeof(T)) throw std::runtime_error("coded stream size is not a whole number of values");
-        std::istringstream in(s_);
-        in.seekg(std::streamoff(off_));
-        std::vector<T> v;
-        readCompressed(in, v);
-        if (!in) throw std::runtime_error("truncated coded stream");
-        off_ = end;
+        const std::string b = text();
+        if (b.size() % sizeof(T)) throw std::runtime_error("coded stream size is not a whole number of values");
+        std::vector<T> v(b.size() / sizeof(T));
+        if (!v.empty()) std::memcpy(v.data(), b.data(), b.size());
         return v;
     }
     std::string text() {
         const size_t end = container_end(off_, 0);
-        std::istringstream in(s_);
-        in.seekg(std::streamoff(off_));
-        std::string v;
-        readCompressed(in, v);
-        if (!in) throw std::runtime_error("truncated coded stream");
+        std::string v = decode_at(off_);
         off_ = end;
         return v;
     }
@@ -184,6 +272,26 @@ private:
         if (coder != LZMA_CODER && coder != PPMD7_CODER) throw std::runtime_error("unsupported coder in a coded stream");
         need(at + 17, src);
         return at + 17 + size_t(src);
+    }
+    // the decoded bytes of the (checked) container at `at`
+    std::string decode_at(size_t at) const {
+        const uint64_t dest = u64_at(at);
+        std::string out(size_t(dest), '\0');
+        if (dest == 0) return out;
+        const uint64_t src = u64_at(at + 8);
+        const uint8_t coder = uint8_t(s_[at + 16]);
+        uint8_t* d = reinterpret_cast<uint8_t*>(&out[0]);
+        if (coder == COMPOUND_CODER_TYPE) {
+            const std::string inner = decode_at(at + 18);  // src bytes of var-len DNA coding
+            varlen_payload(reinterpret_cast<const uint8_t*>(inner.data()), inner.size(), d, out.size());
+            return out;
+        }
+        const uint8_t* p = reinterpret_cast<const uint8_t*>(s_.data()) + at + 17;
+        if (coder == LZMA_CODER)
+            lzma_payload(p, size_t(src), d, out.size());
+        else
+            ppmd_payload(p, size_t(src), d, out.size());
+        return out;
     }
     const std::string& s_;
     size_t off_ = 0;
@@ -506,7 +614,8 @@ Block decode_block(Reader& ar, bool po, bool pe, int L, const DecodeParams& dp, 
         const std::string packed = fl2_decode(s_ref, thr);
         std::string ref(size_t(b.ref_size + b.unmap_size + b.unmap_n_size), '\0');
         if (!ref.empty())
-            Uncompress(&ref[0], ref.size(), packed.data(), packed.size(), VARLEN_DNA_CODER);
+            varlen_payload(reinterpret_cast<const uint8_t*>(packed.data()), packed.size(),
+                           reinterpret_cast<uint8_t*>(&ref[0]), ref.size());
         return ref;
     });
     std::future<std::string> f_maps[6];

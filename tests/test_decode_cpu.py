@@ -182,3 +182,32 @@ def test_python_wrapper(tmp_path):
     assert outputs(tmp_path, "py", False) == outputs(tmp_path, "mine", False)
     with pytest.raises(CurcError):
         decompress_file(str(tmp_path / "missing.curc"), str(tmp_path / "x"), tmpdir=str(tmp_path))
+
+
+def test_corrupt_payloads_do_not_end_the_process(tmp_path):
+    from tests.archive import split_archive
+    data = bytearray(open(os.path.join(GOLDEN, "se75_n20k.curc"), "rb").read())
+    blk = split_archive(bytes(data))["blocks"][0]
+    # the mismatch-count container: decoded size, coded size, coder (PPMd), then the model order
+    c = blk["mismatch_count"]
+    at = bytes(data).find(c)
+    assert at > 0 and data[at + 16] == 3
+    bad = bytearray(data)
+    bad[at + 17] = 1  # model order below the minimum
+    p = tmp_path / "order.curc"
+    p.write_bytes(bytes(bad))
+    rc, _, err = decode(p, tmp_path)
+    assert rc == CURC_ERR_STATE and "PPMd" in err
+    # flipped bytes inside coded payloads: an error or some output, never an exit
+    rng = np.random.default_rng(5)
+    for name in ("mismatch_base", "ref_off_map", "mismatch_count"):
+        s = blk[name]
+        at = bytes(data).find(s)
+        for _ in range(3):
+            bad = bytearray(data)
+            k = at + 22 + int(rng.integers(0, max(1, len(s) - 22)))
+            bad[k] ^= 0x5A
+            p = tmp_path / f"flip_{name}.curc"
+            p.write_bytes(bytes(bad))
+            rc, _, err = decode(p, tmp_path)
+            assert rc in (CURC_OK, CURC_ERR_STATE), err
