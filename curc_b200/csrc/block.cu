@@ -230,6 +230,19 @@ int curc_ctx_create(int device, curc_ctx** out) {
     }
 }
 
+int curc_device_count(int* count) {
+    if (!count) return CURC_ERR_ARG;
+    *count = 0;
+    const cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *count = 0;
+        curc::ctxless_error() = cudaGetErrorString(e);
+        return CURC_ERR_CUDA;
+    }
+    return CURC_OK;
+}
+
 void curc_ctx_destroy(curc_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);

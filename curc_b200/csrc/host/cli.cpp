@@ -118,8 +118,7 @@ int main(int argc, char** argv) {
             std::fprintf(stderr, "curc: %s\n", curc_last_error(nullptr));
             return 1;
         }
-        std::printf("reads count : %llu \n", (unsigned long long)reads);
-        return 0;
+        return 0;  // the reference's decoder prints nothing either
     }
     if (!(ratio > 0 && ratio <= 1)) {
         std::puts("block ratio is a float number in the range (0,1]");
@@ -148,6 +147,12 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "GPU assert: %s\n", curc_last_error(nullptr));
         return 1;
     }
+    int devices = 0;
+    curc_device_count(&devices);
+    // the reference's progress lines (compress.cu:2183-2190, preprocess.cpp)
+    std::printf("gpu context init finish\n");
+    std::printf("GPU device count : %d\n", devices);
+    std::fflush(stdout);
     std::string tmp = wd + "/curc_tmp_XXXXXX";
     if (!mkdtemp(&tmp[0])) {
         std::puts("cannot create a working directory");
@@ -171,6 +176,12 @@ int main(int argc, char** argv) {
     stat(archive.c_str(), &ast);
     std::printf("reads count : %llu \n", (unsigned long long)reads);
     std::printf("block count : %u \n", blocks);
+    std::printf("waiting block compress ...\n");
+    std::vector<uint64_t> block_bytes(256, 0);
+    uint32_t nb = 0;
+    if (curc_archive_info(archive.c_str(), nullptr, nullptr, nullptr, &nb, block_bytes.data(), nullptr) == CURC_OK)
+        for (uint32_t b = 0; b < nb; ++b)
+            std::printf("block %u compress finish, compressed size : %llu\n", b, (unsigned long long)block_bytes[b]);
     std::printf("archive size : %lld bytes \n", (long long)ast.st_size);
     return 0;
 }

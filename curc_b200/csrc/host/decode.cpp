@@ -578,35 +578,64 @@ struct Block {
     std::vector<uint64_t> id_pos;    // preserved order: per read
 };
 
-Block decode_block(Reader& ar, bool po, bool pe, int L, const DecodeParams& dp, uint32_t index) {
-    Block b;
+// One block's fields and coded payloads, in archive order (the block layout
+// of compress.cu:1364-2146, read back at decompress.cu:763-814).
+struct BlockPayloads {
+    uint32_t reads = 0;
+    char table[16];
+    bool join32 = false, ref32 = false;
+    uint64_t ref_size = 0, unmap_size = 0, unmap_n_size = 0;
+    std::string idpos, strand, ref, roff, unoff, uoff, peorder, maps[6], cnt, base;
+    int max_mm = 0;
+    std::vector<std::string> off;  // index m = 1 .. max_mm
+};
+
+BlockPayloads read_block(Reader& ar, bool po, bool pe) {
+    BlockPayloads b;
     b.reads = ar.get<uint32_t>();
-    std::memset(b.table, 'N', sizeof(b.table));
-    for (char row : {'A', 'T', 'C', 'G'}) {
-        const std::string t = ar.bytes(4);
-        std::memcpy(b.table[int(row)], t.data(), 4);
-    }
+    const std::string t = ar.bytes(16);
+    std::memcpy(b.table, t.data(), 16);
     if (po) b.join32 = ar.get<uint8_t>() != 0;
     b.ref32 = ar.get<uint8_t>() != 0;
     b.ref_size = ar.get<uint64_t>();
     b.unmap_size = ar.get<uint64_t>();
     b.unmap_n_size = ar.get<uint64_t>();
-    std::string s_idpos, s_strand, s_ref, s_roff, s_unoff, s_uoff, s_peorder;
-    if (po) s_idpos = ar.blob();
-    s_strand = ar.blob();
-    s_ref = ar.blob();
+    if (po) b.idpos = ar.blob();
+    b.strand = ar.blob();
+    b.ref = ar.blob();
     if (!po) {
-        s_roff = ar.blob();
-        s_unoff = ar.blob();
-        s_uoff = ar.blob();
-        if (pe) s_peorder = ar.blob();
+        b.roff = ar.blob();
+        b.unoff = ar.blob();
+        b.uoff = ar.blob();
+        if (pe) b.peorder = ar.blob();
     }
-    std::string maps[6];
-    for (auto& m : maps) m = ar.blob();
-    const std::string s_cnt = ar.blob(), s_base = ar.blob();
-    const int max_mm = ar.get<uint8_t>();
-    std::vector<std::string> s_off(size_t(max_mm) + 1);
-    for (int m = 1; m <= max_mm; ++m) s_off[size_t(m)] = ar.blob();
+    for (auto& m : b.maps) m = ar.blob();
+    b.cnt = ar.blob();
+    b.base = ar.blob();
+    b.max_mm = ar.get<uint8_t>();
+    b.off.resize(size_t(b.max_mm) + 1);
+    for (int m = 1; m <= b.max_mm; ++m) b.off[size_t(m)] = ar.blob();
+    return b;
+}
+
+Block decode_block(Reader& ar, bool po, bool pe, int L, const DecodeParams& dp, uint32_t index) {
+    Block b;
+    BlockPayloads bp = read_block(ar, po, pe);
+    b.reads = bp.reads;
+    std::memset(b.table, 'N', sizeof(b.table));
+    const char rows[4] = {'A', 'T', 'C', 'G'};
+    for (int r = 0; r < 4; ++r) std::memcpy(b.table[int(rows[r])], bp.table + 4 * r, 4);
+    b.join32 = bp.join32;
+    b.ref32 = bp.ref32;
+    b.ref_size = bp.ref_size;
+    b.unmap_size = bp.unmap_size;
+    b.unmap_n_size = bp.unmap_n_size;
+    const std::string &s_idpos = bp.idpos, &s_strand = bp.strand, &s_ref = bp.ref, &s_roff = bp.roff,
+                      &s_unoff = bp.unoff, &s_uoff = bp.uoff, &s_peorder = bp.peorder, &s_cnt = bp.cnt,
+                      &s_base = bp.base;
+    const std::string* maps = bp.maps;
+    const int max_mm = bp.max_mm;
+    const std::vector<std::string>& s_off = bp.off;
 
     const int thr = dp.threads;
     auto f_strand = std::async(std::launch::async, [&] { return bsc_decode(dp.bsc_path, dp.tmpdir, s_strand, index); });
@@ -827,6 +856,24 @@ void write_block(const Block& b, bool po, bool pe, int L, std::ofstream& o1, std
 
 }  // namespace
 
+ArchiveInfo archive_info(const std::string& archive) {
+    const std::string data = read_whole(archive);
+    Reader ar(data);
+    ArchiveInfo info;
+    info.preserve_order = ar.get<uint8_t>() != 0;
+    info.paired_end = ar.get<uint8_t>() != 0;
+    info.read_len = ar.get<uint16_t>();
+    const int blocks = ar.get<uint8_t>();
+    for (int k = 0; k < blocks; ++k) {
+        const size_t before = ar.left();
+        const BlockPayloads bp = read_block(ar, info.preserve_order, info.paired_end);
+        info.block_reads.push_back(bp.reads);
+        info.block_bytes.push_back(before - ar.left());
+    }
+    if (ar.left() != 0) throw std::runtime_error("bytes after the last block");
+    return info;
+}
+
 DecodeResult decode_archive(const std::string& archive, const std::string& out_prefix, const DecodeParams& dp) {
     const std::string data = read_whole(archive);
     Reader ar(data);
@@ -885,6 +932,34 @@ extern "C" int curc_decompress_file(const char* archive_path, const char* out_pr
         p.threads = threads;
         const auto r = curc::host::decode_archive(archive_path, out_prefix, p);
         if (reads_out) *reads_out = r.reads;
+        return CURC_OK;
+    } catch (const std::ios_base::failure& e) {
+        curc::ctxless_error() = e.what();
+        return CURC_ERR_IO;
+    } catch (const std::exception& e) {
+        curc::ctxless_error() = e.what();
+        return CURC_ERR_STATE;
+    }
+}
+
+extern "C" int curc_archive_info(const char* archive_path, int* preserve_order, int* paired_end, uint16_t* read_len,
+                                 uint32_t* blocks, uint64_t* block_bytes, uint32_t* block_reads) {
+    if (!archive_path) {
+        curc::ctxless_error() = "curc_archive_info: null path";
+        return CURC_ERR_ARG;
+    }
+    try {
+        struct stat st;
+        if (stat(archive_path, &st) != 0) throw std::ios_base::failure(std::string("cannot open ") + archive_path);
+        const auto info = curc::host::archive_info(archive_path);
+        if (preserve_order) *preserve_order = info.preserve_order;
+        if (paired_end) *paired_end = info.paired_end;
+        if (read_len) *read_len = uint16_t(info.read_len);
+        if (blocks) *blocks = uint32_t(info.block_bytes.size());
+        for (size_t k = 0; k < info.block_bytes.size(); ++k) {
+            if (block_bytes) block_bytes[k] = info.block_bytes[k];
+            if (block_reads) block_reads[k] = info.block_reads[k];
+        }
         return CURC_OK;
     } catch (const std::ios_base::failure& e) {
         curc::ctxless_error() = e.what();

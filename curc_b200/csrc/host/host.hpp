@@ -78,6 +78,15 @@ struct DecodeResult {
     bool paired_end = false, preserve_order = false;
 };
 DecodeResult decode_archive(const std::string& archive, const std::string& out_prefix, const DecodeParams& p);
+// Layout of an archive without decoding it: flags, read length, and each
+// block's body size and read count.
+struct ArchiveInfo {
+    bool preserve_order = false, paired_end = false;
+    int read_len = 0;
+    std::vector<uint64_t> block_bytes;
+    std::vector<uint32_t> block_reads;
+};
+ArchiveInfo archive_info(const std::string& archive);
 
 // Read length of the first record (preprocess.cpp:286-300).
 int first_read_length(const std::string& f1);

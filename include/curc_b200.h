@@ -131,6 +131,17 @@ typedef int (*curc_fastq_block_fn)(void* user, uint32_t index, const char* seqs,
 int curc_fastq_blocks(const char* f1, const char* f2, double block_ratio, curc_fastq_block_fn block, void* user,
                       uint64_t* reads_out, uint32_t* blocks_out);
 
+/* Layout of a .curc archive without decoding it, host only: its flags,
+ * read length, block count, and per block its body size in bytes and its
+ * read count (block_bytes / block_reads hold up to 254 entries; any output
+ * pointer may be NULL). */
+int curc_archive_info(const char* archive_path, int* preserve_order, int* paired_end, uint16_t* read_len,
+                      uint32_t* blocks, uint64_t* block_bytes, uint32_t* block_reads);
+
+/* Number of CUDA devices (the reference CLI's "GPU device count" line,
+ * compress.cu:2183-2190). */
+int curc_device_count(int* count);
+
 /* Whole-archive decompression, the drop-in for `curc -d` (src/decompress.cu:
  * 760-1060, src/decompress.cpp): reads the .curc archive at archive_path and
  * writes <out_prefix>.seq (single end) or <out_prefix>_1.seq and
