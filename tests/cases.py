@@ -29,6 +29,9 @@ CASES = {
     "se75_20k": lambda: se(12, 20_000, 75, 150_000, err=0.003),
     "se150_hiN": lambda: se(13, 10_000, 150, 100_000, err=0.004, n_rate=0.002),
     "se250_8k": lambda: se(14, 8_000, 250, 300_000, err=0.002),
+    # long reads: 10 and 16 words per read
+    "se300_4k": lambda: se(19, 4_000, 300, 200_000, err=0.002),
+    "se511_2k": lambda: se(20, 2_000, 511, 200_000, err=0.002),
     "pe150_po": lambda: pe(15, 8_000, 150, 400_000, True),
     "pe150": lambda: pe(16, 8_000, 150, 400_000, False),
     "dups": lambda: duplicates(),
