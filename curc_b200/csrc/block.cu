@@ -49,9 +49,16 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     } timer_scope(&T);
     cudaStream_t s = stream;
     const int W = p.W;
-    cudaEvent_t ev0, ev1;
-    CURC_CHECK(cudaEventCreate(&ev0));
-    CURC_CHECK(cudaEventCreate(&ev1));
+    struct RunEvents {  // released on every exit from the run
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~RunEvents() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } run_ev;
+    CURC_CHECK(cudaEventCreate(&run_ev.a));
+    CURC_CHECK(cudaEventCreate(&run_ev.b));
+    cudaEvent_t ev0 = run_ev.a, ev1 = run_ev.b;
     CURC_CHECK(cudaEventRecord(ev0, s));
     uint32_t* counts = arena.alloc<uint32_t>(16);
     uint32_t* err = arena.alloc<uint32_t>(1);
@@ -172,8 +179,6 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     float total = 0;
     CURC_CHECK(cudaEventElapsedTime(&total, ev0, ev1));
     stage_ms["total"] = total;
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
 }
 
 }  // namespace curc

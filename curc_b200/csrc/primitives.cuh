@@ -73,6 +73,13 @@ struct StageTimer {
         open.pop_back();
     }
     void collect(std::map<std::string, float>& out);
+    // spans not collected (a run that threw) release their events here
+    ~StageTimer() {
+        for (auto& e : ev) {
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+    }
 };
 
 // The timer of the block run in progress on this thread (or null).
