@@ -1,11 +1,12 @@
 // FASTQ ingest with the reference's block split (preprocess.cpp:66-254).
 //
-// The windows and block boundaries are the reference's; inside a window the
-// work is spread over host threads: the window is read with parallel preads,
-// its newlines are counted per chunk, and every chunk then copies the
-// sequence lines (line 1 of each 4-line record) it starts to their slots in
-// the caller's buffer (mates interleaved).
+// The windows and block boundaries are the reference's; the files are mapped
+// (as the reference maps them) and each window is parsed in place, its work
+// spread over host threads: its newlines are counted per chunk, and every
+// chunk then copies the sequence lines (line 1 of each 4-line record) it
+// starts to their slots in the caller's buffer (mates interleaved).
 #include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
@@ -127,8 +128,20 @@ struct File {
         size = uint64_t(st.st_size);
     }
     ~File() {
+        if (map_ && map_ != MAP_FAILED) ::munmap(map_, size_t(size));
         if (fd >= 0) ::close(fd);
     }
+    // the whole file, mapped read-only (the windows are parsed in place, with
+    // no copy out of the page cache)
+    const char* map() {
+        if (!map_) {
+            map_ = size ? ::mmap(nullptr, size_t(size), PROT_READ, MAP_PRIVATE, fd, 0) : nullptr;
+            if (map_ == MAP_FAILED) throw std::runtime_error("cannot map the input file");
+            if (map_) ::madvise(map_, size_t(size), MADV_SEQUENTIAL);
+        }
+        return static_cast<const char*>(map_);
+    }
+    void* map_ = nullptr;
     void read_range(uint64_t off, size_t n, char* dst) const {
         size_t got = 0;
         while (got < n) {
@@ -137,27 +150,17 @@ struct File {
             got += size_t(k);
         }
     }
-    // n bytes at off into buf (plus a terminating zero), in parallel pieces
-    void read_at(uint64_t off, size_t n, std::vector<char>& buf, Team& team) const {
-        buf.resize(n + 1);
-        const int T = team.size();
-        const size_t piece = (n + T - 1) / T;
-        team.run(T, [&](int t) {
-            const size_t a = std::min(n, size_t(t) * piece), b = std::min(n, a + piece);
-            if (b > a) read_range(off + a, b - a, buf.data() + a);
-        });
-        buf[n] = '\0';
-    }
 };
 
 // Record-boundary heuristic of preprocess.cpp:114-137: scanning back from the
 // window end, the cut is the first line start '@' whose bytes repeat, at the
 // same columns, more than 5 consecutive bytes of the window's first line
 // (the run counter carries over between candidates, as in the reference).
-size_t cut_window(const std::vector<char>& b, size_t end) {
+size_t cut_window(const char* b, size_t end) {
     if (b[0] != '@') throw std::runtime_error("io_buffer doesn't start with @");
     size_t fl = 0;
-    while (b[fl] != '\n') ++fl;
+    while (fl < end && b[fl] != '\n') ++fl;
+    if (fl == end) throw std::runtime_error("no record boundary found in a 50 MB window");
     size_t ne = end - fl;
     int eq = 0;
     while (ne > 0) {
@@ -178,7 +181,7 @@ size_t cut_window(const std::vector<char>& b, size_t end) {
 // Sequence lines of the records in b[0, end) (which starts at a record and
 // ends after a newline) to dst + record * stride; returns the record count.
 // Every sequence line must hold L bases (preprocess.cpp:147-160).
-uint64_t parse_window(const std::vector<char>& b, size_t end, int L, char* dst, size_t stride, Team& team) {
+uint64_t parse_window(const char* b, size_t end, int L, char* dst, size_t stride, Team& team) {
     if (end == 0) return 0;
     if (b[end - 1] != '\n') throw std::runtime_error("truncated FASTQ record");
     const int T = std::max(1, std::min(team.size() * 4, int(end / 65536) + 1));
@@ -186,7 +189,7 @@ uint64_t parse_window(const std::vector<char>& b, size_t end, int L, char* dst, 
     std::vector<uint64_t> nl(T + 1, 0);
     team.run(T, [&](int t) {
         const size_t a = std::min(end, size_t(t) * piece), e = std::min(end, a + piece);
-        nl[t + 1] = uint64_t(std::count(b.data() + a, b.data() + e, '\n'));
+        nl[t + 1] = uint64_t(std::count(b + a, b + e, '\n'));
     });
     for (int t = 0; t < T; ++t) nl[t + 1] += nl[t];
     const uint64_t lines = nl[T];
@@ -198,17 +201,17 @@ uint64_t parse_window(const std::vector<char>& b, size_t end, int L, char* dst, 
         uint64_t li = nl[t];
         size_t p = a;
         if (a > 0 && b[a - 1] != '\n') {
-            const char* q = static_cast<const char*>(std::memchr(b.data() + a, '\n', e - a));
+            const char* q = static_cast<const char*>(std::memchr(b + a, '\n', e - a));
             if (!q) return;
-            p = size_t(q - b.data()) + 1;
+            p = size_t(q - b) + 1;
             ++li;
         }
         while (p < e && p < end) {
-            const char* q = static_cast<const char*>(std::memchr(b.data() + p, '\n', end - p));
-            const size_t le = size_t(q - b.data());
+            const char* q = static_cast<const char*>(std::memchr(b + p, '\n', end - p));
+            const size_t le = size_t(q - b);
             if ((li & 3) == 1) {
                 if (le - p != size_t(L)) throw std::runtime_error("read length isn't fix");
-                std::memcpy(dst + (li >> 2) * stride, b.data() + p, size_t(L));
+                std::memcpy(dst + (li >> 2) * stride, b + p, size_t(L));
             }
             ++li;
             p = le + 1;
@@ -250,7 +253,8 @@ IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double r
     const int mates = pe ? 2 : 1;
     Team team(int(std::max(1u, std::min(32u, std::thread::hardware_concurrency()))));
     uint64_t total = 0, last_total = 0;
-    std::vector<char> wa, wb;
+    const char* A = a.map();
+    const char* B = pe ? b->map() : nullptr;
     bool open = false;
     auto begin_block = [&] {
         // sequence bytes of the block are at most its FASTQ bytes
@@ -261,8 +265,8 @@ IngestResult ingest_fastq(const std::string& f1, const std::string& f2, double r
     while (total < fq) {
         if (!open) begin_block();
         size_t end = size_t(std::min(win, fq - total));
-        a.read_at(total, end, wa, team);
-        if (pe) b->read_at(total, end, wb, team);
+        const char* wa = A + total;
+        const char* wb = pe ? B + total : nullptr;
         total += end;
         if (total < fq) {
             const size_t ne = cut_window(wa, end);
@@ -307,23 +311,32 @@ public:
     void begin_block(size_t max_bytes, int L) override {
         L_ = L;
         off_ = 0;
-        buf_.resize(std::max(buf_.size(), max_bytes));
+        reserve(max_bytes);
     }
     char* window_buffer(size_t bytes) override {
-        if (off_ + bytes > buf_.size()) buf_.resize(off_ + bytes);
-        return buf_.data() + off_;
+        reserve(off_ + bytes);
+        return buf_.get() + off_;
     }
     void window_done(uint64_t reads) override { off_ += size_t(reads) * size_t(L_); }
     void end_block() override {
         const uint64_t n = off_ / size_t(L_);
-        if (fn_(user_, index_++, buf_.data(), n, uint16_t(L_)) != 0)
+        if (fn_(user_, index_++, buf_.get(), n, uint16_t(L_)) != 0)
             throw std::logic_error("curc_fastq_blocks stopped by the callback");
     }
 
 private:
+    // grows keeping the bytes already written (no zero fill of new space)
+    void reserve(size_t bytes) {
+        if (bytes <= cap_) return;
+        std::unique_ptr<char[]> nb(new char[bytes]);
+        if (off_) std::memcpy(nb.get(), buf_.get(), off_);
+        buf_ = std::move(nb);
+        cap_ = bytes;
+    }
     curc_fastq_block_fn fn_;
     void* user_;
-    std::vector<char> buf_;
+    std::unique_ptr<char[]> buf_;
+    size_t cap_ = 0;
     size_t off_ = 0;
     int L_ = 1;
     uint32_t index_ = 0;
