@@ -49,7 +49,9 @@ int usage() {
         "      --flzma2_level arg    fast-lzma2 compression level [1...10] (default 10)\n"
         "      --flzma2_thread_num   fast-lzma2 thread number (default 16)\n"
         "      --preserve_order      preserve order information\n"
-        "      --device arg          CUDA device (default 0)\n");
+        "      --device arg          CUDA device (default 0)\n"
+        "  -v, --version             print version\n"
+        "  -h, --help                print usage\n");
     return 0;
 }
 
@@ -78,6 +80,10 @@ int main(int argc, char** argv) {
             else if (a == "--preserve_order") po = true;
             else if (a == "--device") device = std::stoi(val());
             else if (a == "-h" || a == "--help") return usage();
+            else if (a == "-v" || a == "--version") {
+                std::puts("v1.0.0");  // the archive format version (CURC 1.0.0)
+                return 0;
+            }
             else if (a == "--decode_buffer_size") val();
             else throw std::runtime_error("unknown option " + a);
         } catch (const std::exception& e) {
@@ -136,9 +142,10 @@ int main(int argc, char** argv) {
         std::puts("invalid input path number");
         return 0;
     }
-    for (const auto& f : files) {
-        if (stat(f.c_str(), &st) != 0 || !has_ext(f, ".fastq", ".fq")) {
-            std::puts("please check the fastq path (filename extension is .fastq or .fq)");
+    for (size_t k = 0; k < files.size(); ++k) {
+        if (stat(files[k].c_str(), &st) != 0 || !has_ext(files[k], ".fastq", ".fq")) {
+            std::printf("please check the %s fastq path (filename extension is .fastq or .fq)\n",
+                        k == 0 ? "first" : "second");
             return 0;
         }
     }
