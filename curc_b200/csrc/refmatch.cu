@@ -175,9 +175,13 @@ __device__ Hit extend_full(const RmIndex& ix, const uint64_t* dest, uint64_t dl,
 // One thread per probe; the four probes of a segment sit in four adjacent
 // lanes and the segment takes its first accepting probe (the reference's
 // segment stops at its first hit, compress.cu:746-807).  cand[seg] = (dest, source) position.
+// Probes at index dic or later (the tail of the last segment) take no hit:
+// their 36-mer runs past the destination end, and in the reference any hit
+// there ends past it too, so its length arithmetic (compress.cu:910-913)
+// wraps and its compaction (compress.cu:960-963) moves out of bounds.
 __global__ void __launch_bounds__(256) probe_segments_kernel(RmIndex ix, const uint64_t* __restrict__ dest, uint64_t dl,
-                                                             uint64_t dpad, uint64_t segs, bool dest_is_ref,
-                                                             uint8_t* __restrict__ flag,
+                                                             uint64_t dpad, uint64_t segs, uint64_t dic,
+                                                             bool dest_is_ref, uint8_t* __restrict__ flag,
                                                              ulonglong2* __restrict__ cand) {
     const uint64_t P = segs * 4;
     const uint32_t lane = threadIdx.x & 31u;
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(256) probe_segments_kernel(RmIndex ix, const u
     // lanes of a warp share i - lane, so the warp stays converged for the ballot
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i - lane < P; i += stride) {
         uint64_t sp = 0;
-        const bool hit = i < P && probe_candidate(ix, dest, dl, dpad, i * RM_DEST_STEP, dest_is_ref, &sp);
+        const bool hit = i < dic && probe_candidate(ix, dest, dl, dpad, i * RM_DEST_STEP, dest_is_ref, &sp);
         const uint32_t g = (__ballot_sync(0xFFFFFFFFu, hit) >> (lane & ~3u)) & 0xFu;
         if (i < P) {
             if ((lane & 3u) == 0) flag[i >> 2] = g != 0;
@@ -513,7 +517,7 @@ void refmatch_one(const RmIndex& ix, const uint8_t* dest, uint64_t dl, bool has_
         const uint64_t dpad = (words - 1) * 32;
         ulonglong2* cand = a.alloc<ulonglong2>(nslots);
         probe_segments_kernel<<<resident_grid(probe_segments_kernel, 256, nslots * 4), 256, 0, s>>>(
-            ix, packed, dl, dpad, nslots, dest_is_ref, flag, cand);
+            ix, packed, dl, dpad, nslots, dic, dest_is_ref, flag, cand);
         CURC_LAUNCH_CHECK();
         extend_runs_kernel<<<grid_for(nslots, 256), 256, 0, s>>>(ix, packed, dl, dpad, nslots, flag, cand, hits);
     } else {

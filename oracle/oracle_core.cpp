@@ -684,9 +684,13 @@ void refmatch_apply(const RefMatcherIndex& ix, std::string& dest, bool dest_has_
         return false;
     };
     if (!dest_has_n) {
+        // segments of 4 probes; the probes of the last segment at index dic
+        // or later take no hit (their 36-mer runs past the end, and a hit
+        // there would end past it, which the reference's compaction cannot
+        // handle: compress.cu:910-913, 960-963)
         const uint64_t segs = (dic + 3) / 4;
         for (uint64_t i = 0; i < segs; ++i)
-            for (uint64_t s = 0; s < 4; ++s)
+            for (uint64_t s = 0; s < 4 && i * 4 + s < dic; ++s)
                 if (probe((i * 4 + s) * RM_DEST_STEP)) break;
     } else {
         for (uint64_t i = 0; i < dic; ++i) probe(i * RM_DEST_STEP);

@@ -29,6 +29,11 @@ CASES = {
     "se75_20k": lambda: se(12, 20_000, 75, 150_000, err=0.003),
     "se150_hiN": lambda: se(13, 10_000, 150, 100_000, err=0.004, n_rate=0.002),
     "se250_8k": lambda: se(14, 8_000, 250, 300_000, err=0.002),
+    # a RefMatcher probe in the tail of the last 4-probe segment of the
+    # unmapped pseudogenome matches into the zero padding: it must take no hit
+    "pe133_po_tail": lambda: (lambda w: (w.sequences(), True, True))(
+        synth.paired_repeats(seed=551869, pairs=1585, read_len=133, genome_len=63594, err=0.001, n_rate=0.003,
+                             preserve_order=True)),
     # long reads: 10 and 16 words per read
     "se300_4k": lambda: se(19, 4_000, 300, 200_000, err=0.002),
     "se511_2k": lambda: se(20, 2_000, 511, 200_000, err=0.002),

@@ -106,6 +106,10 @@ ORACLE_CASES = {
                                                    n_rate=0.002, preserve_order=True),
     "pe75": lambda: synth.paired_repeats(seed=46, pairs=6_000, read_len=75, genome_len=200_000,
                                          preserve_order=False),
+    # a RefMatcher probe past the last full 36-mer of a pseudogenome, where the
+    # reference's length arithmetic breaks: found by a random sweep
+    "pe133_po_tail": lambda: synth.paired_repeats(seed=551869, pairs=1585, read_len=133, genome_len=63594,
+                                                  err=0.001, n_rate=0.003, preserve_order=True),
 }
 
 
