@@ -32,16 +32,11 @@
 #include <string>
 #include <vector>
 
-#ifndef ABS
-#define ABS std::abs
-#endif
 #include <fast-lzma2/fast-lzma2.h>
 #include <lzma/Alloc.h>
 #include <lzma/LzmaDec.h>
 #include <lzma/Ppmd7.h>
 #include <lzma/VarLenDNACoder/LzmaLib.h>
-#include <range_coder/clr.cdr>
-#include <range_coder/simple_model.h>
 
 #include "../../../include/curc_b200.h"
 #include "host.hpp"
@@ -318,44 +313,120 @@ std::string bsc_decode(const std::string& bsc, const std::string& dir, const std
     return s;
 }
 
+// The range decoder and adaptive frequency model of the mismatch-offset
+// streams: the CLR range coder (32-bit range and code, 64-bit low, 2^24
+// renormalisation threshold, eight start bytes of which the last four form the
+// code) and a model of NSYM symbols kept roughly sorted by frequency (step 8,
+// halved above 2^16 - 32, one neighbour swap every 16 symbols), as the
+// encoder's vendored copies define them (range_coder/clr.cdr,
+// range_coder/simple_model.h).  Restated here with two guards the originals
+// lack, so a corrupt stream is an error and not an out-of-bounds read or a
+// division by zero: the decoded frequency must lie below the model's total,
+// and the range must stay at least the total.  Bytes past the stream read as
+// zero.
+class OffRangeDecoder {
+public:
+    OffRangeDecoder(const uint8_t* p, size_t n) : p_(p), end_(p + n) {
+        for (int i = 0; i < 8; ++i) code_ = (code_ << 8) | next();
+    }
+    uint32_t get_freq(uint32_t tot) {
+        range_ /= tot;
+        if (range_ == 0) throw std::runtime_error("corrupt mismatch offset stream");
+        return code_ / range_;
+    }
+    void decode(uint32_t cum, uint32_t freq) {
+        const uint32_t t = cum * range_;
+        low_ += t;
+        code_ -= t;
+        range_ *= freq;
+        while (range_ < (1u << 24)) {
+            if (uint8_t((low_ ^ (low_ + range_)) >> 56)) range_ = (uint32_t(low_) | ((1u << 24) - 1)) - uint32_t(low_);
+            code_ = (code_ << 8) | next();
+            range_ <<= 8;
+            low_ <<= 8;
+        }
+    }
+
+private:
+    uint32_t next() { return p_ < end_ ? *p_++ : 0u; }
+    const uint8_t* p_;
+    const uint8_t* end_;
+    uint64_t low_ = 0;
+    uint32_t range_ = 0xFFFFFFFFu, code_ = 0;
+};
+
+template <int NSYM>
+class OffModel {
+public:
+    OffModel() {
+        for (int i = 0; i < NSYM; ++i) {
+            sym_[i] = uint16_t(i);
+            freq_[i] = 1;
+        }
+    }
+    uint16_t decode(OffRangeDecoder& rc) {
+        const uint32_t f = rc.get_freq(tot_);
+        if (f >= tot_) throw std::runtime_error("corrupt mismatch offset stream");
+        uint32_t acc = 0;
+        int i = 0;
+        while (acc + freq_[i] <= f) acc += freq_[i++];  // ends below NSYM since f < tot_
+        rc.decode(acc, freq_[i]);
+        freq_[i] = uint16_t(freq_[i] + STEP);
+        tot_ += STEP;
+        if (tot_ > MAXF) {
+            tot_ = 0;
+            for (int k = 0; k < NSYM; ++k) {
+                freq_[k] = uint16_t(freq_[k] - (freq_[k] >> 1));
+                tot_ += freq_[k];
+            }
+        }
+        const uint16_t out = sym_[i];
+        if (((++bub_ & 15u) == 0) && i > 0 && freq_[i] > freq_[i - 1]) {
+            std::swap(freq_[i], freq_[i - 1]);
+            std::swap(sym_[i], sym_[i - 1]);
+        }
+        return out;
+    }
+
+private:
+    static constexpr uint32_t STEP = 8, MAXF = (1u << 16) - 32;
+    uint16_t sym_[NSYM], freq_[NSYM];
+    uint32_t tot_ = NSYM, bub_ = 0;
+};
+
 // Mismatch offsets of the records with m mismatches, from their range-coded
 // stream: the inverse of the encoder's flag / first / gap coding
 // (decompress.cu:357-416): `m` offsets for each of `records` records.
 template <size_t MaxL>
 std::vector<uint16_t> offsets_decode(const std::string& coded, size_t m, size_t records, int L) {
-    std::vector<char> buf(coded.begin(), coded.end());
-    buf.resize(buf.size() + 64, 0);  // the decoder may look a few bytes ahead
-    RangeCoder rc{};
-    rc.input(buf.data());
-    rc.StartDecode();
-    SIMPLE_MODEL<2> flag;
-    SIMPLE_MODEL<MaxL / 2 + 1> first;
-    SIMPLE_MODEL<MaxL> value;
+    OffRangeDecoder rc(reinterpret_cast<const uint8_t*>(coded.data()), coded.size());
+    OffModel<2> flag;
+    OffModel<int(MaxL / 2 + 1)> first;
+    OffModel<int(MaxL)> value;
     std::vector<uint16_t> out(records * m);
     for (size_t r = 0; r < records; ++r) {
         uint16_t* t = out.data() + r * m;
-        const bool from_end = flag.decodeSymbol(&rc) != 0;
+        const bool from_end = flag.decode(rc) != 0;
         if (!from_end) {
             // first offset, then gaps forward
-            t[0] = first.decodeSymbol(&rc);
+            t[0] = first.decode(rc);
             if (m == 2) {
-                t[1] = uint16_t(value.decodeSymbol(&rc) + t[0] + 1);
+                t[1] = uint16_t(value.decode(rc) + t[0] + 1);
             } else if (m > 2) {
-                const uint32_t min_gap = value.decodeSymbol(&rc) + 1u;
-                for (size_t k = 1; k < m; ++k) t[k] = uint16_t(value.decodeSymbol(&rc) + t[k - 1] + min_gap);
+                const uint32_t min_gap = value.decode(rc) + 1u;
+                for (size_t k = 1; k < m; ++k) t[k] = uint16_t(value.decode(rc) + t[k - 1] + min_gap);
             }
         } else {
             // last offset from the read's end, then gaps backward
-            t[m - 1] = uint16_t(L - 1 - first.decodeSymbol(&rc));
+            t[m - 1] = uint16_t(L - 1 - first.decode(rc));
             if (m == 2) {
-                t[0] = uint16_t(t[1] - value.decodeSymbol(&rc) - 1);
+                t[0] = uint16_t(t[1] - value.decode(rc) - 1);
             } else if (m > 2) {
-                const uint32_t min_gap = value.decodeSymbol(&rc) + 1u;
-                for (size_t k = m - 1; k > 0; --k) t[k - 1] = uint16_t(t[k] - value.decodeSymbol(&rc) - min_gap);
+                const uint32_t min_gap = value.decode(rc) + 1u;
+                for (size_t k = m - 1; k > 0; --k) t[k - 1] = uint16_t(t[k] - value.decode(rc) - min_gap);
             }
         }
     }
-    rc.FinishDecode();
     return out;
 }
 

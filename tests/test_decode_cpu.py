@@ -250,3 +250,22 @@ def test_device_count_without_gpu():
         assert rc == CURC_OK and n.value >= 1
     else:
         assert rc in (CURC_OK, -2) and n.value == 0
+
+
+def test_random_corruptions_are_errors_or_output(tmp_path):
+    # seeded multi-byte corruptions and truncations of every golden archive: each
+    # decode returns an error code or writes reads, and this process survives
+    rng = np.random.default_rng(11)
+    for name in sorted(f for f in os.listdir(GOLDEN) if f.endswith(".curc")):
+        data = open(os.path.join(GOLDEN, name), "rb").read()
+        for t in range(6):
+            bad = bytearray(data)
+            if t % 3 == 2:
+                bad = bad[:int(rng.integers(1, len(bad)))]
+            else:
+                for k in rng.integers(0, len(bad), size=int(rng.integers(1, 12))):
+                    bad[int(k)] = int(rng.integers(0, 256))
+            p = tmp_path / f"bad_{name}_{t}.curc"
+            p.write_bytes(bytes(bad))
+            rc, _, err = decode(p, tmp_path)
+            assert rc in (CURC_OK, CURC_ERR_STATE), (name, t, err)
