@@ -269,3 +269,33 @@ def test_random_corruptions_are_errors_or_output(tmp_path):
             p.write_bytes(bytes(bad))
             rc, _, err = decode(p, tmp_path)
             assert rc in (CURC_OK, CURC_ERR_STATE), (name, t, err)
+
+
+def _random_case(rnd):
+    L = rnd.choice([rnd.randint(20, 40), rnd.randint(41, 160), rnd.randint(161, 511)])
+    pe, po = rnd.random() < 0.5, rnd.random() < 0.5
+    n = rnd.randint(50, 2000)
+    kw = dict(err=rnd.choice([0.0, 0.001, 0.01]), n_rate=rnd.choice([0.0, 0.0001, 0.003, 0.02]))
+    seed = rnd.randint(0, 10**6)
+    if pe:
+        return synth.paired_repeats(seed=seed, pairs=n, read_len=L, genome_len=rnd.randint(3 * L + 20_000, 100_000),
+                                    preserve_order=po, **kw)
+    w = synth.small_single(seed=seed, n_reads=n, read_len=L, genome_len=rnd.randint(2 * L + 1000, 100_000), **kw)
+    w.preserve_order = po
+    return w
+
+
+@pytest.mark.parametrize("sweep_seed", range(12))
+def test_random_small_archives(sweep_seed, tmp_path):
+    # random read lengths (20-511), ends, order, error and N rates: the oracle's
+    # archive must decode, with the product decoder and the reference's, to the
+    # input reads (this sweep found the RefMatcher tail rule)
+    import random
+    w = _random_case(random.Random(1000 + sweep_seed))
+    files = w.write(str(tmp_path / "in"))
+    pe = w.mate2 is not None
+    rc = oracle_lib().oracle_compress_files(files[0].encode(), files[1].encode() if pe else None,
+                                            str(tmp_path).encode(), b"oracle", 1.0, int(w.preserve_order),
+                                            os.path.join(REF_DIR, "bsc").encode(), 8)
+    assert rc == 0
+    check(tmp_path / "oracle.curc", w, tmp_path)
