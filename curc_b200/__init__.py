@@ -4,8 +4,8 @@ The compute path is libcurc_b200.so (CUDA kernels behind the C-ABI in
 include/curc_b200.h); this package is a thin host-side binding used by the
 tests and the benchmark.
 """
-from ._native import (Context, CurcError, LIB_PATH, Learner, decompress_file, kernel_launches,  # noqa: F401
-                      learn_param_count, lib, plain_mismatch_bytes)
+from ._native import (Context, CurcError, LIB_PATH, Learner, archive_info, decompress_file,  # noqa: F401
+                      fastq_blocks, kernel_launches, learn_param_count, lib, plain_mismatch_bytes)
 
 RECORD_DTYPE = None
 

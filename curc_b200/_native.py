@@ -64,6 +64,11 @@ def lib() -> ctypes.CDLL:
                                           ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
         L.curc_decompress_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, c_int,
                                            ctypes.POINTER(c_u64)]
+        L.curc_archive_info.argtypes = [ctypes.c_char_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                        ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint32),
+                                        ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
+        L.curc_fastq_blocks.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double, FASTQ_BLOCK, c_p,
+                                        ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
         L.curc_kernel_launches.restype = ctypes.c_uint64
         _lib = L
     return _lib
@@ -75,6 +80,41 @@ def kernel_launches() -> int:
 
 class CurcError(RuntimeError):
     pass
+
+
+FASTQ_BLOCK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64,
+                               ctypes.c_uint16)
+
+
+def archive_info(archive: str) -> dict:
+    """Layout of a .curc archive without decoding it: flags, read length,
+    and per block its body size and read count."""
+    po, pe, L, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint16(), ctypes.c_uint32()
+    sizes, reads = (ctypes.c_uint64 * 256)(), (ctypes.c_uint32 * 256)()
+    rc = lib().curc_archive_info(archive.encode(), ctypes.byref(po), ctypes.byref(pe), ctypes.byref(L),
+                                 ctypes.byref(nb), sizes, reads)
+    if rc != 0:
+        raise CurcError(f"curc_archive_info: {lib().curc_last_error(None).decode()} (code {rc})")
+    return {"preserve_order": bool(po.value), "paired_end": bool(pe.value), "read_len": L.value,
+            "block_bytes": [int(sizes[i]) for i in range(nb.value)],
+            "block_reads": [int(reads[i]) for i in range(nb.value)]}
+
+
+def fastq_blocks(f1: str, f2: str | None = None, block_ratio: float = 1.0) -> list:
+    """The reference's block split of FASTQ file(s), host only: a list of
+    (n, L) uint8 arrays of ASCII reads in block order (mates interleaved)."""
+    out = []
+
+    def cb(_user, _index, seqs, n, L):
+        out.append(np.frombuffer(ctypes.string_at(seqs, n * L), dtype=np.uint8).reshape(n, L).copy() if n
+                   else np.zeros((0, L), dtype=np.uint8))
+        return 0
+
+    fn = FASTQ_BLOCK(cb)
+    rc = lib().curc_fastq_blocks(f1.encode(), f2.encode() if f2 else None, block_ratio, fn, None, None, None)
+    if rc != 0:
+        raise CurcError(f"curc_fastq_blocks: {lib().curc_last_error(None).decode()} (code {rc})")
+    return out
 
 
 def decompress_file(archive: str, out_prefix: str, bsc: str | None = None, tmpdir: str = "/tmp",

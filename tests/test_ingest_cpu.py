@@ -118,3 +118,15 @@ def test_bad_inputs(tmp_path):
     assert rc == CURC_ERR_IO and "length" in err
     rc, _, _, _, err = product_blocks([str(tmp_path / "missing.fastq")], 1.0)
     assert rc == CURC_ERR_IO
+
+
+def test_python_wrappers(tmp_path):
+    from curc_b200 import archive_info, fastq_blocks
+    w, ratio = CASES["pe_blocks"]()
+    files = w.write(str(tmp_path / "p"), name=b"synthetic_read_")
+    blocks = fastq_blocks(files[0], files[1], ratio)
+    assert len(blocks) >= 2
+    assert np.array_equal(np.concatenate(blocks), w.sequences())
+    info = archive_info(os.path.join(ROOT, "tests", "golden", "pe150_po_p8k.curc"))
+    assert info["paired_end"] and info["preserve_order"] and info["read_len"] == 150
+    assert info["block_reads"] == [16000]
