@@ -108,3 +108,19 @@ def test_missing_stream(tmp_path):
     streams = {k: ora.get(k) for k in stream_names(L, False, False)}
     rc, err = encode(n, L, False, False, streams, tmp_path, drop="mis_base")
     assert rc == CURC_ERR_STATE and "mis_base" in err
+
+
+@pytest.mark.parametrize("sweep_seed", range(8))
+def test_random_block_bodies_match_oracle(sweep_seed, tmp_path):
+    # random read lengths (20-511), ends, order, error and N rates
+    import random
+    from tests.test_decode_cpu import _random_case
+    w = _random_case(random.Random(2000 + sweep_seed))
+    seqs = w.sequences()
+    n, L = seqs.shape
+    po, pe = w.preserve_order, w.mate2 is not None
+    ora = OracleBlock(seqs, po, pe)
+    streams = {k: ora.get(k) for k in stream_names(L, po, pe)}
+    rc, body = encode(n, L, po, pe, streams, tmp_path)
+    assert rc == CURC_OK, body
+    assert body == ora.encode(str(tmp_path))
