@@ -205,11 +205,14 @@ class Context:
         return t.value
 
     def batch_workers(self, workers: int):
+        """Number of block pipelines of the drain (1..16, default 2)."""
         self._check(lib().curc_batch_workers(self._h, workers), "curc_batch_workers")
 
     def batch_drain(self, on_block=None):
-        """Run the queued blocks; on_block(ticket) is called after each, while
-        get() returns that block's results."""
+        """Run the queued blocks (those of at least 2^28 bases first, one at a
+        time with the next one's reads already crossing to the device; the
+        rest on concurrent pipelines); on_block(ticket) is called after each,
+        in completion order, while get() returns that block's results."""
         err = []
 
         def cb(_user, ticket):
