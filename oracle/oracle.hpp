@@ -61,9 +61,31 @@ void pack_reads(const char* seq, size_t n, int L, uint64_t* packed, uint8_t* has
 void sort_dedupe(const uint64_t* db, int W, std::vector<uint32_t>& ids,
                  uint32_t* next, uint32_t* prev, uint16_t* offset);
 
+// a4 contested runs.  In one overlap pass, suffixes whose [off, L) equals
+// the same run of prefixes compete for the run's free prefixes.  In the
+// reference each suffix is a thread and a prefix goes to whichever thread's
+// atomicCAS (compress.cu:1518) lands first, so the outcome depends on
+// scheduling; canonically the suffixes take them in list order.
+struct ContestPick {      // in overlap pass `pass`, `suffix` goes before the rest
+    int pass;
+    uint32_t suffix;
+};
+struct ContestMember {    // one suffix of a run that two or more suffixes shared
+    uint32_t pass;
+    uint32_t run;         // index of the run's first prefix in the bucketed prefix list
+    uint32_t suffix;
+    uint32_t prefix;      // the prefix it took in this pass, or INVALID
+};
+struct OverlapControl {
+    std::vector<ContestPick> picks;        // empty: canonical order
+    std::vector<ContestMember>* log = nullptr;
+};
+
 // a3+a4: k-mer index over prefix reads and the max_off-1 overlap passes.
+// `ctl` (test use only) replays another serialisation of the contested runs
+// and records every contested run.
 void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_t>& sorted_ids,
-                  uint32_t* next, uint32_t* prev, uint16_t* offset);
+                  uint32_t* next, uint32_t* prev, uint16_t* offset, const OverlapControl* ctl = nullptr);
 
 // a5: chain filter; returns (ref ids, unmatched ids), both in sorted order.
 void chain_filter(size_t reads_count, const std::vector<uint32_t>& sorted_ids,
@@ -119,6 +141,7 @@ struct BlockInput {
     std::vector<uint32_t> reads_id;  // non-N ids ascending
     std::vector<char> nreads;        // ASCII of N reads, N_reads_id order
     std::vector<uint32_t> n_ids;     // ids of reads containing N
+    std::vector<ContestPick> contest_picks;  // a4 serialisation (empty: canonical)
 };
 
 struct BlockStreams {
@@ -141,6 +164,7 @@ struct BlockStreams {
     Pseudogenome hq;
     MapResult map;
     std::vector<Record> records;             // emission order
+    std::vector<ContestMember> contests;     // a4 contested runs
 };
 
 void compress_block(const Params& p, const BlockInput& in, BlockStreams& out, int threads = 1);

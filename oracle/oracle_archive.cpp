@@ -414,14 +414,19 @@ void view(const V& v, const void** ptr, uint64_t* bytes) {
 extern "C" {
 
 // Runs the oracle on one block.  `seqs` holds n reads of length L (ASCII),
-// in block id order (paired end: mates interleaved).
-void* oracle_block_new(const char* seqs, uint64_t n, int L, int po, int pe, int threads) {
+// in block id order (paired end: mates interleaved).  `picks` (npicks pairs
+// of overlap pass and suffix read id, may be null) replays another
+// serialisation of the contested overlap runs: in that pass the suffix is
+// visited before the others.
+void* oracle_block_new_picks(const char* seqs, uint64_t n, int L, int po, int pe, int threads, const uint32_t* picks,
+                             uint64_t npicks) {
     auto* h = new Handle;
     h->p = oracle::Params::derive(L, po != 0, pe != 0);
     oracle::RawBlock rb;
     rb.seqs.assign(seqs, seqs + n * L);
     rb.count = n;
     oracle::BlockInput in = oracle::make_block_input(h->p, rb, h->db);
+    for (uint64_t i = 0; i < npicks; ++i) in.contest_picks.push_back({int(picks[2 * i]), picks[2 * i + 1]});
     h->has_n.assign(n, 0);
     for (uint32_t id : in.n_ids) h->has_n[id] = 1;
     oracle::compress_block(h->p, in, h->s, threads);
@@ -438,6 +443,10 @@ void* oracle_block_new(const char* seqs, uint64_t n, int L, int po, int pe, int 
     flat(h->s.hq.records, h->hq_rec);
     flat(h->s.records, h->all_rec);
     return h;
+}
+
+void* oracle_block_new(const char* seqs, uint64_t n, int L, int po, int pe, int threads) {
+    return oracle_block_new_picks(seqs, n, L, po, pe, threads, nullptr, 0);
 }
 
 int oracle_block_get(void* hv, const char* name, const void** ptr, uint64_t* bytes) {
@@ -458,6 +467,7 @@ int oracle_block_get(void* hv, const char* name, const void** ptr, uint64_t* byt
     else if (n == "map_mm") view(s.map.mm, ptr, bytes);
     else if (n == "map_strand") view(s.map.strand, ptr, bytes);
     else if (n == "map_pos") view(s.map.pos, ptr, bytes);
+    else if (n == "contests") view(s.contests, ptr, bytes);  // u32 (pass, run, suffix, prefix) per member
     else if (n == "ref") view(s.ref, ptr, bytes);
     else if (n == "unmap_ref") view(s.unmap_ref, ptr, bytes);
     else if (n == "unmap_n_ref") view(s.unmap_n_ref, ptr, bytes);

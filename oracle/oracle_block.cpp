@@ -59,7 +59,10 @@ void compress_block(const Params& p, const BlockInput& in, BlockStreams& out, in
     out.sorted_ids = in.reads_id;
     sort_dedupe(in.db, W, out.sorted_ids, out.next.data(), out.prev.data(), out.offset.data());
     // a3 + a4
-    overlap_link(p, in.db, out.sorted_ids, out.next.data(), out.prev.data(), out.offset.data());
+    OverlapControl ctl;
+    ctl.picks = in.contest_picks;
+    ctl.log = &out.contests;
+    overlap_link(p, in.db, out.sorted_ids, out.next.data(), out.prev.data(), out.offset.data(), &ctl);
     // a5
     chain_filter(n, out.sorted_ids, out.next.data(), out.prev.data(), out.offset.data(), out.ref_ids,
                  out.unmatch_ids);

@@ -160,7 +160,7 @@ static int cmp_shifted(const uint64_t* a, uint64_t aoff, const uint64_t* b, uint
 }
 
 void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_t>& sorted,
-                  uint32_t* next, uint32_t* prev, uint16_t* offset) {
+                  uint32_t* next, uint32_t* prev, uint16_t* offset, const OverlapControl* ctl) {
     const int W = p.unit, L = p.read_len, k = p.kmer_size, kip = p.kmer_index_pos;
     // compress.cu:1427-1438: prefix set (no duplicate predecessor) and suffix set
     std::vector<uint32_t> pre, suf;
@@ -183,9 +183,19 @@ void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_
     // compress.cu:1473-1532, one suffix at a time in list order
     for (int off = 1; off < p.max_off; ++off) {
         const int cl = L - off;
-        std::vector<uint32_t> rem;
-        rem.reserve(suf.size());
-        for (uint32_t s : suf) {
+        // visiting order: this pass's picks that are still unlinked suffixes
+        // (in the order given), then the rest in list order
+        std::vector<uint32_t> order;
+        if (ctl)
+            for (const ContestPick& c : ctl->picks)
+                if (c.pass == off && std::find(order.begin(), order.end(), c.suffix) == order.end() &&
+                    std::find(suf.begin(), suf.end(), c.suffix) != suf.end())
+                    order.push_back(c.suffix);
+        const size_t npick = order.size();
+        for (uint32_t s : suf)
+            if (std::find(order.begin(), order.begin() + npick, s) == order.begin() + npick) order.push_back(s);
+        std::vector<std::pair<uint32_t, uint32_t>> runs;  // (run, suffix) of suffixes with a matching prefix
+        for (uint32_t s : order) {
             const uint64_t* sr = db + size_t(s) * W;
             uint32_t h = uint32_t(murmur64(word_at(sr, kip + off, k)) & mask);
             auto rng = std::equal_range(vk.begin(), vk.end(), h);
@@ -201,6 +211,8 @@ void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_
                     cnt = step;
                 }
             }
+            if (ctl && ctl->log && lo < hi && cmp_shifted(db + size_t(va[lo]) * W, 0, sr, off, cl) == 0)
+                runs.push_back({uint32_t(lo), s});
             for (size_t q = lo; q < hi; ++q) {
                 uint32_t pr = va[q];
                 if (pr == s || prev[pr] != INVALID) continue;
@@ -211,8 +223,23 @@ void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_
                 }
                 break;
             }
-            if (next[s] == INVALID) rem.push_back(s);
         }
+        if (ctl && ctl->log) {
+            std::stable_sort(runs.begin(), runs.end(),
+                             [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (size_t i = 0; i < runs.size();) {
+                size_t j = i;
+                while (j < runs.size() && runs[j].first == runs[i].first) ++j;
+                if (j - i > 1)
+                    for (size_t k = i; k < j; ++k)
+                        ctl->log->push_back({uint32_t(off), runs[k].first, runs[k].second, next[runs[k].second]});
+                i = j;
+            }
+        }
+        std::vector<uint32_t> rem;
+        rem.reserve(suf.size());
+        for (uint32_t s : suf)
+            if (next[s] == INVALID) rem.push_back(s);
         suf.swap(rem);
     }
 }

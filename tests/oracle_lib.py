@@ -21,6 +21,9 @@ def lib():
         L.oracle_block_new.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int]
         L.oracle_block_new.restype = ctypes.c_void_p
+        L.oracle_block_new_picks.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64]
+        L.oracle_block_new_picks.restype = ctypes.c_void_p
         L.oracle_block_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p),
                                        ctypes.POINTER(ctypes.c_uint64)]
         L.oracle_block_encode.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
@@ -35,11 +38,23 @@ def lib():
 
 
 class OracleBlock:
-    def __init__(self, seqs: np.ndarray, preserve_order=False, paired_end=False, threads=8):
+    """One block through the oracle.  `picks`, a list of (overlap pass,
+    suffix read id), replays another serialisation of the contested overlap
+    runs: in that pass the suffix is visited before the others (the order a
+    GPU run of the reference may take; the default is list order)."""
+
+    def __init__(self, seqs: np.ndarray, preserve_order=False, paired_end=False, threads=8, picks=()):
         seqs = np.ascontiguousarray(seqs, dtype=np.uint8)
         n, L = seqs.shape
         self.L = L
-        self._h = lib().oracle_block_new(seqs.ctypes.data, n, L, int(preserve_order), int(paired_end), threads)
+        pk = np.ascontiguousarray(np.array(list(picks), dtype=np.uint32).reshape(-1, 2))
+        self._h = lib().oracle_block_new_picks(seqs.ctypes.data, n, L, int(preserve_order), int(paired_end), threads,
+                                               pk.ctypes.data, len(pk))
+
+    def contests(self):
+        """Members of contested overlap runs: rows of (pass, run, suffix,
+        prefix taken in that pass or 0xFFFFFFFF), in visiting order per run."""
+        return self.get("contests", np.uint32).reshape(-1, 4)
 
     def get(self, name, dtype=np.uint8):
         p, nb = ctypes.c_void_p(), ctypes.c_uint64()

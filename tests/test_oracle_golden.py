@@ -4,9 +4,21 @@ tests/golden/*.curc are archives written by the unmodified reference
 `curc -c` on a B200 (tests/golden/make_golden.py, which records in
 golden_meta.json whether three runs of the reference agreed).  The oracle
 compresses the same seeded inputs here; every archive must decode with the
-reference's own `curc -d` to the input reads, and where the reference was
-deterministic the oracle's archive must equal the reference's byte for byte
-(or, for the listed cases, stream for stream except the noted ones)."""
+reference's own `curc -d` to the input reads.
+
+Byte equality.  The reference links overlapping reads with a race: in each
+overlap pass the suffix reads that share a run of equal prefixes claim them
+with atomicCAS (compress.cu:1518), so which suffix gets a prefix depends on
+thread scheduling.  The oracle takes them in list order.  For every golden
+archive, tests/golden/contested_links.json (made by
+tests/golden/find_contested_links.py) lists the few contested runs that the
+reference's run resolved the other way; replaying those picks, the oracle
+writes the reference's archive byte for byte.  Each pick is checked to be a
+genuine contest: at that pass the picked suffix and the one it displaces
+share a run, and in list order the displaced one links while the picked one
+does not.  One archive (8k pairs, order not preserved), on which the
+reference differed on every run and its own decoder crashes, is pinned as
+far as the race that decides it allows (see its note in the fixture)."""
 import json
 import os
 import subprocess
@@ -20,7 +32,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 import make_golden  # noqa: E402
 from tests.archive import split_archive  # noqa: E402
-from tests.oracle_lib import REF_DIR, lib  # noqa: E402
+from tests.oracle_lib import REF_DIR, OracleBlock, decode_ref, lib, read_compressed  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 META = json.load(open(os.path.join(GOLDEN, "golden_meta.json")))
@@ -71,13 +83,107 @@ def test_oracle_roundtrip_through_reference_decoder(name):
                 assert np.array_equal(np.sort(gp), np.sort(ep))
 
 
-@pytest.mark.parametrize("name", [n for n in sorted(META) if META[n]["deterministic"]])
-def test_oracle_matches_deterministic_reference(name):
-    ref = open(os.path.join(GOLDEN, name + ".curc"), "rb").read()
+CONTESTED = json.load(open(os.path.join(GOLDEN, "contested_links.json")))
+INVALID = 0xFFFFFFFF
+
+
+def _oracle(name, picks=()):
+    w = make_golden.CASES[name]()
+    o = OracleBlock(w.sequences(), w.preserve_order, w.mate2 is not None, picks=[tuple(p) for p in picks])
     with tempfile.TemporaryDirectory() as td:
-        _, mine = oracle_archive(name, td)
-    a, b = split_archive(mine)["blocks"][0], split_archive(ref)["blocks"][0]
-    differing = sorted(k for k in b if a[k] != b[k])
-    if name == "pe150_po_p8k":
-        pytest.xfail(f"known divergence from the reference's contested-link resolution: {differing}")
-    assert mine == ref, differing
+        body = o.encode(td)
+    hdr = bytes([int(w.preserve_order), int(w.mate2 is not None), w.read_len & 255, w.read_len >> 8, 1])
+    return w, o, hdr + body
+
+
+def _check_picks_are_contests(name, o):
+    rows = o.contests()
+    for p, s in CONTESTED[name]["picks"]:
+        mine = rows[(rows[:, 0] == p) & (rows[:, 2] == s)]
+        assert len(mine) == 1, f"{name}: suffix {s} is in no contested run of pass {p}"
+        run = rows[(rows[:, 0] == p) & (rows[:, 1] == mine[0, 1])]
+        assert mine[0, 3] == INVALID, f"{name}: suffix {s} already links in list order at pass {p}"
+        assert (run[:, 3] != INVALID).any(), f"{name}: nobody wins the run of suffix {s} at pass {p}"
+
+
+@pytest.mark.parametrize("name", sorted(n for n in CONTESTED if not CONTESTED[n]["still_differ"]))
+def test_oracle_writes_reference_archive_given_its_contested_links(name):
+    ref = open(os.path.join(GOLDEN, name + ".curc"), "rb").read()
+    _, canon, mine = _oracle(name)
+    _check_picks_are_contests(name, canon)
+    if not CONTESTED[name]["picks"]:
+        assert mine == ref
+        return
+    # list order alone gives another valid run of the reference ...
+    assert mine != ref
+    # ... and the reference's own resolution of the listed runs gives its archive
+    _, _, replayed = _oracle(name, CONTESTED[name]["picks"])
+    a, b = split_archive(replayed)["blocks"][0], split_archive(ref)["blocks"][0]
+    assert replayed == ref, sorted(k for k in b if a[k] != b[k])
+
+
+def _leb(b, i):
+    v = sh = 0
+    while True:
+        x = b[i]
+        i += 1
+        v |= (x & 0x7F) << sh
+        sh += 7
+        if x < 0x80:
+            return v, i
+
+
+def _recover(coded, offs, lens, std):
+    """The decoder's repeat restoration for the main pseudogenome
+    (decompress.cu:418-444 with srcIsDest)."""
+    comp = bytes.maketrans(b"ACGTN", b"TGCAN")
+    out = bytearray()
+    tml, li = _leb(lens, 0)
+    oi = pos = 0
+    while (mark := coded.find(b"%", pos)) >= 0:
+        out += coded[pos:mark]
+        pos = mark + 1
+        src = int.from_bytes(offs[oi:oi + (4 if std else 8)], "little")
+        oi += 4 if std else 8
+        ml, li = _leb(lens, li)
+        out += bytes(out[src:src + ml + tml]).translate(comp)[::-1]
+    return bytes(out + coded[pos:])
+
+
+def test_unstable_reference_archive_is_pinned_up_to_its_mapping_tie():
+    name = "pe150_p8k"
+    spec = CONTESTED[name]
+    ref = split_archive(open(os.path.join(GOLDEN, name + ".curc"), "rb").read())["blocks"][0]
+    _, canon, _ = _oracle(name)
+    _check_picks_are_contests(name, canon)
+    w, o, mine = _oracle(name, spec["picks"])
+    b = split_archive(mine)["blocks"][0]
+    # unmapped and N pseudogenomes, their repeat maps and read offsets: identical
+    for k in ("unmap_ref_off_map", "unmap_ref_len_map", "unmap_n_ref_off_map", "unmap_n_ref_len_map",
+              "unmap_read_off", "unmap_n_read_off"):
+        assert b[k] == ref[k], k
+    assert b["sizes"][1:] == ref["sizes"][1:]
+    with tempfile.TemporaryDirectory() as td:
+        rj = decode_ref(ref["ref"], sum(ref["sizes"]), td)
+    assert rj[ref["sizes"][0]:] == decode_ref_tail(b)
+    # the main pseudogenome before repeat removal: identical
+    hq = _recover(rj[:ref["sizes"][0]], read_compressed(ref["ref_off_map"]), read_compressed(ref["ref_len_map"]),
+                  ref["ref_std"] != 0)
+    assert hq == o.get("hq_seq").tobytes()
+    # the first mapped record that differs: one read, two positions with equal mismatches
+    t = spec["tie"]
+    read = w.sequences()[t["read"]]
+    g = np.frombuffer(hq, np.uint8)
+    L = w.read_len
+    for p in (t["reference_pos"], t["oracle_pos"]):
+        assert int((g[p:p + L] != read).sum()) == t["mismatches"]
+    ref_pos = np.cumsum(np.frombuffer(read_compressed(ref["read_off"]), np.uint16).astype(np.int64))
+    my_pos = np.cumsum(np.frombuffer(read_compressed(b["read_off"]), np.uint16).astype(np.int64))
+    first = int(np.nonzero(ref_pos[:len(my_pos)] != my_pos[:len(ref_pos)])[0][0])
+    assert ref_pos[first] == t["reference_pos"]
+    assert t["oracle_pos"] in set(my_pos.tolist())
+
+
+def decode_ref_tail(block):
+    with tempfile.TemporaryDirectory() as td:
+        return decode_ref(block["ref"], sum(block["sizes"]), td)[block["sizes"][0]:]
