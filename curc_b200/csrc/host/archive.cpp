@@ -11,9 +11,11 @@
 // unmodified: fast-lzma2 (pseudogenome, positions), the LZMA SDK with PPMd7
 // and PgRC's VarLenDNACoder, the CLR range coder (mismatch offsets), and the
 // `bsc` executable built from libbsc (strand stream, run as a subprocess
-// exactly as util.cuh:527-535 does).  Independent streams are coded
-// concurrently; calls into the LZMA/PPMd container are serialised because
-// that library writes to a shared log stream.
+// exactly as util.cuh:527-535 does).  Independent streams, and the
+// sub-streams of the position and pair-order coders, are coded concurrently:
+// the LZMA / PPMd7 container of LzmaLib.cpp is restated here over the LZMA
+// SDK's encoders (the library's own entry point also writes to a shared log
+// stream, which concurrent callers would race on).
 #include <sys/stat.h>
 #include <unistd.h>
 
@@ -33,6 +35,9 @@
 #define ABS std::abs
 #endif
 #include <fast-lzma2/fast-lzma2.h>
+#include <lzma/Alloc.h>
+#include <lzma/LzmaEnc.h>
+#include <lzma/Ppmd7.h>
 #include <lzma/VarLenDNACoder/LzmaLib.h>
 #include <range_coder/clr.cdr>
 #include <range_coder/simple_model.h>
@@ -45,14 +50,105 @@ namespace host {
 
 namespace {
 
-std::mutex g_lzmalib_mu;
+// PPMd7 coded bytes as LzmaLib.cpp:229-264 writes them at level 3
+// (PGRC_CODER_LEVEL_MAX): 5 property bytes (model order, u32 memory size),
+// then the range coder's output.  The memory size is 192 MiB shrunk to the
+// smallest power of two 2^16..2^31 that is at least 16 times the input
+// (LzmaLib.cpp:118-159).
+struct ByteSink {
+    IByteOut vt;
+    std::string* out;
+    static void put(const IByteOut* p, Byte b) {
+        reinterpret_cast<const ByteSink*>(p)->out->push_back(char(b));
+    }
+};
 
+std::string ppmd7_coded(const uint8_t* src, size_t n, int order) {
+    uint32_t mem = 192u << 20;
+    if (mem / 16 > n)
+        for (unsigned i = 16; i <= 31; ++i) {
+            const uint32_t m = 1u << i;
+            if (n <= m / 16) {
+                if (mem > m) mem = m;
+                break;
+            }
+        }
+    CPpmd7 ppmd;
+    Ppmd7_Construct(&ppmd);
+    if (!Ppmd7_Alloc(&ppmd, mem, &g_Alloc)) throw std::runtime_error("PPMd7: out of memory");
+    Ppmd7_Init(&ppmd, unsigned(order));
+    std::string out(5, '\0');
+    out[0] = char(order);
+    std::memcpy(&out[1], &mem, 4);
+    out.reserve(5 + n / 2 + 64);
+    ByteSink sink{{&ByteSink::put}, &out};
+    CPpmd7z_RangeEnc rc;
+    Ppmd7z_RangeEnc_Init(&rc);
+    rc.Stream = &sink.vt;
+    for (size_t i = 0; i < n; ++i) Ppmd7_EncodeSymbol(&ppmd, &rc, src[i]);
+    Ppmd7z_RangeEnc_FlushData(&rc);
+    Ppmd7_Free(&ppmd, &g_Alloc);
+    return out;
+}
+
+// LZMA coded bytes as LzmaLib.cpp:88-117 and :162-181 write them at level 3:
+// level 9, dictionary 1.5 GiB (reduced to the input by the encoder), lc 3,
+// lp = pb = the data period code, 273 fast bytes, 2 threads; 5 property
+// bytes, then the stream.
+std::string lzma_coded(const uint8_t* src, size_t n, int period, size_t bound) {
+    CLzmaEncProps props;
+    LzmaEncProps_Init(&props);
+    props.level = 9;
+    props.dictSize = 3u << 29;
+    props.lc = 3;
+    props.lp = period;
+    props.pb = period;
+    props.fb = 273;
+    props.numThreads = 2;
+    props.reduceSize = n;
+    std::string out(bound, '\0');
+    SizeT props_size = LZMA_PROPS_SIZE, len = bound - LZMA_PROPS_SIZE;
+    const SRes r = LzmaEncode(reinterpret_cast<Byte*>(&out[LZMA_PROPS_SIZE]), &len, src, n, &props,
+                              reinterpret_cast<Byte*>(&out[0]), &props_size, 0, nullptr, &g_Alloc, &g_Alloc);
+    if (r != SZ_OK) throw std::runtime_error("LZMA: encoding failed (code " + std::to_string(r) + ")");
+    out.resize(LZMA_PROPS_SIZE + len);
+    return out;
+}
+
+// The LzmaLib container (writeCompressed, LzmaLib.cpp:539-552) at level 3:
+// u64 input length; unless it is zero, u64 coded length, u8 coder type and
+// the coded bytes.  The library sizes its output buffer from the caller's
+// ratio estimate and fails (exits) when the coded bytes do not fit; the
+// same bound makes that an error here.
 std::string container(const void* src, size_t n, uint8_t coder, int param, double est) {
-    // LzmaLib.cpp:539-552 container at level 3
-    std::lock_guard<std::mutex> g(g_lzmalib_mu);
-    std::ostringstream o;
-    writeCompressed(o, static_cast<const char*>(src), n, coder, 3, param, est);
-    return o.str();
+    std::string o(8, '\0');
+    const uint64_t n64 = n;
+    std::memcpy(&o[0], &n64, 8);
+    if (n == 0) return o;
+    const size_t bound = size_t(double(LZMA_PROPS_SIZE) + double(n + n / 3) * est + 128);
+    const uint8_t* p = static_cast<const uint8_t*>(src);
+    std::string coded;
+    if (coder == PPMD7_CODER) {
+        coded = ppmd7_coded(p, n, param);
+        if (coded.size() > bound) throw std::runtime_error("PPMd7: coded stream above the container's bound");
+    } else if (coder == LZMA_CODER) {
+        coded = lzma_coded(p, n, param, bound);
+    } else {
+        throw std::runtime_error("unsupported container coder");
+    }
+    const uint64_t c64 = coded.size();
+    o.append(reinterpret_cast<const char*>(&c64), 8);
+    o.push_back(char(coder));
+    return o + coded;
+}
+
+// Containers coded on concurrent threads, returned in order.
+std::string containers(std::initializer_list<std::function<std::string()>> parts) {
+    std::vector<std::future<std::string>> f;
+    for (const auto& p : parts) f.push_back(std::async(std::launch::async, p));
+    std::string o;
+    for (auto& x : f) o += x.get();
+    return o;
 }
 
 // fast-lzma2 stream with the feeding pattern of the reference's file helper
@@ -205,13 +301,17 @@ std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr
     }
     auto fb = std::async(std::launch::async, [&] { return fl2(base.data(), base.size() * sizeof(T), level, thr); });
     auto fn = std::async(std::launch::async, [&] { return fl2(notbase.data(), notbase.size() * sizeof(T), level, thr); });
+    const double bm = COMPRESSION_ESTIMATION_UINT8_BITMAP;
+    std::string mid = containers({
+        [&] { return container(off_flag.data(), off_flag.size(), PPMD7_CODER, 3, bm); },
+        [&] { return container(off_first.data(), off_first.size(), PPMD7_CODER, 3, bm); },
+        [&] { return container(off_val.data(), off_val.size() * 2, PPMD7_CODER, 3, 1); },
+        [&] { return container(d_flag.data(), d_flag.size(), PPMD7_CODER, 3, bm); },
+        [&] { return container(d_first.data(), d_first.size(), PPMD7_CODER, 3, bm); },
+        [&] { return container(d_val.data(), d_val.size() * 2, PPMD7_CODER, 3, 1); },
+    });
     std::string o = blob(fb.get());
-    o += container(off_flag.data(), off_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
-    o += container(off_first.data(), off_first.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
-    o += container(off_val.data(), off_val.size() * 2, PPMD7_CODER, 3, 1);
-    o += container(d_flag.data(), d_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
-    o += container(d_first.data(), d_first.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
-    o += container(d_val.data(), d_val.size() * 2, PPMD7_CODER, 3, 1);
+    o += mid;
     o += blob(fn.get());
     return o;
 }
@@ -256,12 +356,14 @@ std::string pe_order(const uint32_t* order, size_t n, int level, int thr) {
     }
     auto fd = std::async(std::launch::async, [&] { return fl2(d8_val.data(), d8_val.size(), level, thr); });
     auto fo = std::async(std::launch::async, [&] { return fl2(offs.data(), offs.size() * 4, level, thr); });
-    std::string out;
-    out += container(off8_flag.data(), off8_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
-    out += container(off8_val.data(), off8_val.size(), PPMD7_CODER, 2, 1);
-    out += container(d8_flag.data(), d8_flag.size(), PPMD7_CODER, 3, COMPRESSION_ESTIMATION_UINT8_BITMAP);
-    out += container(off_pair.data(), off_pair.size(), PPMD7_CODER, 2, COMPRESSION_ESTIMATION_UINT8_BITMAP);
-    out += container(non_off_pair.data(), non_off_pair.size(), PPMD7_CODER, 2, COMPRESSION_ESTIMATION_UINT8_BITMAP);
+    const double bm = COMPRESSION_ESTIMATION_UINT8_BITMAP;
+    std::string out = containers({
+        [&] { return container(off8_flag.data(), off8_flag.size(), PPMD7_CODER, 3, bm); },
+        [&] { return container(off8_val.data(), off8_val.size(), PPMD7_CODER, 2, 1); },
+        [&] { return container(d8_flag.data(), d8_flag.size(), PPMD7_CODER, 3, bm); },
+        [&] { return container(off_pair.data(), off_pair.size(), PPMD7_CODER, 2, bm); },
+        [&] { return container(non_off_pair.data(), non_off_pair.size(), PPMD7_CODER, 2, bm); },
+    });
     out += blob(fd.get());
     out += blob(fo.get());
     return out;
@@ -322,15 +424,17 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
         joined_ref.reserve(S("ref").size + S("unmap_ref").size + S("unmap_n_ref").size);
         for (const char* nm : {"ref", "unmap_ref", "unmap_n_ref"})
             joined_ref.append(reinterpret_cast<const char*>(S(nm).ptr), S(nm).size);
+        // compress.cu:2099-2102: the VarLenDNA coder (called directly; it
+        // keeps no shared state), then fast-lzma2
         size_t clen = 0;
-        char* enc;
-        {
-            std::lock_guard<std::mutex> g(g_lzmalib_mu);
-            enc = Compress(clen, joined_ref.data(), joined_ref.size(), VARLEN_DNA_CODER, 3,
-                           PgSAHelpers::VarLenDNACoder::getCoderParam(
-                               PgSAHelpers::VarLenDNACoder::STATIC_CODES_CODER_PARAM,
-                               PgSAHelpers::VarLenDNACoder::AG_EXTENDED_CODES_ID),
-                           1);
+        unsigned char* enc = nullptr;
+        const int rc = PgSAHelpers::VarLenDNACoder::Compress(
+            enc, clen, reinterpret_cast<const unsigned char*>(joined_ref.data()), joined_ref.size(),
+            PgSAHelpers::VarLenDNACoder::getCoderParam(PgSAHelpers::VarLenDNACoder::STATIC_CODES_CODER_PARAM,
+                                                       PgSAHelpers::VarLenDNACoder::AG_EXTENDED_CODES_ID));
+        if (rc != SZ_OK) {
+            delete[] enc;
+            throw std::runtime_error("VarLenDNA coder failed");
         }
         std::string r = fl2(enc, clen, lvl, thr);
         delete[] enc;
@@ -351,45 +455,45 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
             return offsets(L, reinterpret_cast<const uint16_t*>(b.ptr), b.size / 2, size_t(m));
         }); }));
     }
-    // the PPMd / LZMA streams (serialised inside `container`)
-    auto plain = [&](const char* nm, uint8_t coder, int param, double est) {
-        const Buf& b = S(nm);
-        return container(b.ptr, b.size, coder, param, est);
+    // the PPMd7 / LZMA container streams, each on its own thread
+    auto plain = [&](const char* what, const char* nm, uint8_t coder, int param, double est) {
+        return std::async(std::launch::async, [&, what, nm, coder, param, est] {
+            return timed(cp, what, [&] {
+                const Buf& b = S(nm);
+                return container(b.ptr, b.size, coder, param, est);
+            });
+        });
     };
-    std::string read_off, unmap_n_off, unmap_off;
+    std::future<std::string> read_off, unmap_n_off, unmap_off;
     if (!v.preserve_order) {
-        read_off = timed(cp, "read_off", [&] { return plain("read_off", PPMD7_CODER, 3, 1); });
-        unmap_n_off = timed(cp, "read_off", [&] { return plain("unmap_n_read_off", PPMD7_CODER, 3, 1); });
-        unmap_off = timed(cp, "read_off", [&] { return plain("unmap_read_off", PPMD7_CODER, 3, 1); });
+        read_off = plain("read_off", "read_off", PPMD7_CODER, 3, 1);
+        unmap_n_off = plain("read_off", "unmap_n_read_off", PPMD7_CODER, 3, 1);
+        unmap_off = plain("read_off", "unmap_read_off", PPMD7_CODER, 3, 1);
     }
     const double est = simpleUintCompressionEstimate(S("ref").size, ref_std ? 0xFFFFFFFFull : ~0ull);
     const int period = ref_std ? 2 : 3;
-    std::string maps = timed(cp, "maps", [&] {
-    std::string maps;
+    std::vector<std::future<std::string>> maps;
     for (auto pr : {std::make_pair("ref_off", "ref_len_map"), std::make_pair("unmap_ref_off", "unmap_ref_len"),
                     std::make_pair("unmap_n_ref_off", "unmap_n_ref_len")}) {
-        maps += blob(plain(pr.first, LZMA_CODER, period, est));
-        maps += blob(plain(pr.second, LZMA_CODER, 0, 1));
+        maps.push_back(plain("maps", pr.first, LZMA_CODER, period, est));
+        maps.push_back(plain("maps", pr.second, LZMA_CODER, 0, 1));
     }
-    return maps;
-    });
-    const std::string mis_cnt = timed(cp, "mis_cnt", [&] { return plain("mis_cnt", PPMD7_CODER, 2, 1); });
-    const std::string mis_base =
-        timed(cp, "mis_base", [&] { return plain("mis_base", PPMD7_CODER, 2, COMPRESSION_ESTIMATION_MIS_SYM); });
+    auto mis_cnt = plain("mis_cnt", "mis_cnt", PPMD7_CODER, 2, 1);
+    auto mis_base = plain("mis_base", "mis_base", PPMD7_CODER, 2, COMPRESSION_ESTIMATION_MIS_SYM);
 
     std::string out = hdr;
     if (v.preserve_order) out += blob(f_idpos.get());
     out += blob(f_strand.get());
     out += blob(f_ref.get());
     if (!v.preserve_order) {
-        out += blob(read_off);
-        out += blob(unmap_n_off);
-        out += blob(unmap_off);
+        out += blob(read_off.get());
+        out += blob(unmap_n_off.get());
+        out += blob(unmap_off.get());
         if (v.paired_end) out += blob(f_peorder.get());
     }
-    out += maps;
-    out += blob(mis_cnt);
-    out += blob(mis_base);
+    for (auto& m : maps) out += blob(m.get());
+    out += blob(mis_cnt.get());
+    out += blob(mis_base.get());
     const uint8_t mm = uint8_t(max_mm);
     out.append(reinterpret_cast<const char*>(&mm), 1);
     for (auto& f : f_off) out += blob(f.get());

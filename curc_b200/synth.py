@@ -232,19 +232,32 @@ def position_ramp(read_len: int, lo: float, hi: float) -> np.ndarray:
     return np.linspace(lo, hi, read_len)
 
 
-def batched_blocks(seed: int = 2, count: int = 64, scale: float = 1.0):
-    """Independent single-end blocks from different random genomes (2-20 Mbp),
-    read counts log-uniform in [50k, 5M] x ``scale``, read lengths from
-    {75, 100, 150, 250}, error rates uniform in [0.1%, 0.5%]."""
+def batched_specs(seed: int = 2, count: int = 64, scale: float = 1.0):
+    """(genome length, read count, read length, error rate) of each block of
+    :func:`batched_blocks`, without generating any reads."""
     rng = np.random.default_rng(seed)
     out = []
-    for b in range(count):
+    for _ in range(count):
         glen = int(rng.integers(2_000_000, 20_000_001) * scale) + 10_000
         n = max(1000, int(np.exp(rng.uniform(np.log(50_000), np.log(5_000_000))) * scale))
         L = int(rng.choice([75, 100, 150, 250]))
         e = float(rng.uniform(0.001, 0.005))
-        brng = np.random.default_rng([seed, b])
-        g = random_genome(brng, glen)
-        r = sample_single(brng, g, n, L, e, 0.0001)
-        out.append(Workload(f"batch{b}_se{L}_n{n}", L, r, None, False))
+        out.append((glen, n, L, e))
     return out
+
+
+def batched_block(seed: int, b: int, spec) -> Workload:
+    """Block ``b`` of :func:`batched_blocks` from its spec (each block has
+    its own generator, so one block can be drawn alone)."""
+    glen, n, L, e = spec
+    brng = np.random.default_rng([seed, b])
+    g = random_genome(brng, glen)
+    r = sample_single(brng, g, n, L, e, 0.0001)
+    return Workload(f"batch{b}_se{L}_n{n}", L, r, None, False)
+
+
+def batched_blocks(seed: int = 2, count: int = 64, scale: float = 1.0):
+    """Independent single-end blocks from different random genomes (2-20 Mbp),
+    read counts log-uniform in [50k, 5M] x ``scale``, read lengths from
+    {75, 100, 150, 250}, error rates uniform in [0.1%, 0.5%]."""
+    return [batched_block(seed, b, sp) for b, sp in enumerate(batched_specs(seed, count, scale))]
