@@ -8,10 +8,15 @@ substitutions, 0.01% N, --preserve_order, block_ratio 1 (one block).
 
 One step = one block through the whole device path (pack ... repeat removal),
 streams returned to the host.  `value` is Mbases/s with the ASCII reads
-already in HBM; `e2e` is the same through the C-ABI from pinned host memory
-(H2D of the reads and D2H of every stream inside the timed region).
+already in HBM (CUDA events).  `e2e` is the whole `curc -c` a user runs: the
+product binary, one process per step, from the FASTQ files to the closed
+archive (parse, copies to and from the device, device path, stream coders,
+archive write) -- the same work the reference arm times for the reference's
+own `curc -c`.  `e2e_same_sample` runs both binaries on identical files (the
+first pairs of the workload's own FASTQ files) for a like-for-like ratio.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --impl reference --ref-full   # the reference on the whole workload, once
 
 Under torchrun every rank compresses its own block (independent blocks, no
 collective: weak scaling); the time is the max over ranks.
@@ -46,7 +51,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=10_000_000)
     ap.add_argument("--genome", type=int, default=50_000_000)
     ap.add_argument("--cpu-sample-pairs", type=int, default=100_000)
-    ap.add_argument("--ref-sample-pairs", type=int, default=1_000_000)
+    ap.add_argument("--ref-sample-pairs", type=int, default=1_000_000,
+                    help="pairs per step of the reference arm (the first pairs of the workload's FASTQ files)")
+    ap.add_argument("--ref-full", action="store_true",
+                    help="reference arm: time one run on the whole workload instead of the sampled steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cli", action="store_true", help="skip the whole-file `curc -c` measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain measurement")
@@ -139,6 +147,38 @@ def probe_bytes(st, L):
     row = 32 * -(-8 * ((L + 31) // 32) // 32)
     return (32 * st["overlap_probes"] + 32 * st["overlap_searched"] + (32 + row) * st["overlap_compares"]
             + 32 * st["overlap_hits"])
+
+
+# Algorithmic bytes of the first-word read sort (sub-stage sort_dedupe.radix):
+# per non-N read one 32-byte sector for its first packed word, then 8 LSD
+# passes of 8-bit digits that each read and write a 12-byte (key, id) pair.
+# The lower bound of any sort (each read's words read once, ids in and out)
+# is 8W + 8 per read.
+def sort_bytes(m, L):
+    return m * (32 + 8 * 2 * 12)
+
+
+def sort_lower_bound_bytes(m, L):
+    return m * (8 * ((L + 31) // 32) + 8)
+
+
+# Algorithmic bytes of the overlap resolve kernel (its launches over all
+# passes): per hit its 16-byte record, its run slot (32), the prefix id and
+# the prefix's predecessor (32 each) and one prefix row (32 * ceil(8W/32));
+# per link 10 bytes of next/prev/offset and the bucket's free word (32).
+def resolve_bytes(st, L):
+    row = 32 * -(-8 * ((L + 31) // 32) // 32)
+    return st["overlap_hits"] * (16 + 32 + 64 + row) + st["overlap_links"] * (10 + 32)
+
+
+# Algorithmic bytes of the mapping kernels (forward and reverse complement):
+# per read searched its packed row (8W); per k-mer probe the bucket range,
+# one 32-byte sector; per candidate its pos_array slot (32) and the
+# pseudogenome window, 32 * (ceil((2L + 62) / 256) + 1).
+def map_bytes(st, L, strand):
+    win = 32 * (-(-(2 * L + 62) // 256) + 1)
+    return (st[f"map_reads_{strand}"] * 8 * ((L + 31) // 32) + st[f"map_probes_{strand}"] * 32
+            + st[f"map_candidates_{strand}"] * (32 + win))
 
 
 # DRAM bytes per listed suffix of the probe kernel, from ncu
@@ -263,7 +303,8 @@ def run_ours(a, rank, world):
     stats = dict(zip(["reads", "non_n", "n_reads", "pseudogenome_reads", "unmatched", "mapped", "unmapped",
                       "unmapped_n", "overlap_passes", "contested", "records", "mismatches",
                       "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits",
-                      "overlap_searched", "overlap_compares"],
+                      "overlap_searched", "overlap_compares", "overlap_links", "map_reads_fwd", "map_probes_fwd",
+                      "map_candidates_fwd", "map_reads_rc", "map_probes_rc", "map_candidates_rc"],
                      [int(x) for x in ctx.get("stats", np.uint64)]))
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     step_s = dev_ms / 1000.0 / a.steps
@@ -272,18 +313,8 @@ def run_ours(a, rank, world):
     if not a.no_batched and rank == 0:
         batched = batched_vs_plain(ctx, a)
     cli = None
-    if not a.no_cli and rank == 0:
-        with tempfile.TemporaryDirectory() as td:
-            v_full, t_full, sz_full, host_ms = cli_run(ctx, w, td, "full")
-            ws = workload(a.ref_sample_pairs, a.genome, seed=1)
-            v_s, t_s, sz_s, _ = cli_run(ctx, ws, td, "sample")
-        cli = {"value": v_full, "unit": "Mbases/s", "s": t_full, "archive_bytes": sz_full,
-               "archive_bits_per_base": 8.0 * sz_full / w.bases,
-               "host_stage_ms": host_ms,
-               "sample_value": v_s, "sample": f"{a.ref_sample_pairs} pairs of the same generator (the reference "
-                                               f"arm's sample), {t_s:.2f} s, archive {sz_s} bytes",
-               "includes": "FASTQ parse and block split, device path, host stream coders, archive write "
-                           "(in-process call; files in page cache)"}
+    if not a.no_cli and world == 1:
+        cli = cli_measure(ctx, w, a, dev)
     res = dict(bases=bases, n=n, L=L, step_s=step_s, e2e_s=e2e_s, wall=wall, launches=launches, stats=stats,
                stage_ms={k: v / a.steps for k, v in stage_tot.items()},
                substage_ms={k: round(v / a.steps, 3) for k, v in sub_tot.items()}, clocks=clocks.summary(),
@@ -316,28 +347,104 @@ def cpu_baseline(a):
 # Record headers long enough for the reference's block-boundary heuristic
 # (it matches more than 5 bytes of the first header at a line start).
 FASTQ_NAME = b"synthetic_read_"
+CURC_EXE = os.path.join(ROOT, "curc_b200", "_build", "curc")
+BSC_EXE = os.path.join(ROOT, "curc_b200", "_build", "bsc")
+HOST_STAGES = ["files.total", "files.ingest", "files.device", "files.snapshot", "files.until_last_block",
+               "files.coder_tail", "files.coders", "coder.id_pos", "coder.strand", "coder.ref", "coder.maps",
+               "coder.mis_cnt", "coder.mis_base", "coder.mis_off", "coder.read_off", "coder.pe_order"]
 
 
-def cli_run(ctx, w, td, tag):
-    """`curc -c` of a workload through the library (FASTQ files on disk to a
-    .curc archive), timed from the call to the archive's close."""
-    files = w.write(os.path.join(td, tag), name=FASTQ_NAME)
-    t = time.perf_counter()
-    ctx.compress_files(files, os.path.join(td, tag + ".curc"), 1.0, True, os.path.join(ROOT, "curc_b200", "_build", "bsc"),
-                       td)
-    dt = time.perf_counter() - t
-    host_ms = {}
-    for k in ["files.total", "files.ingest", "files.device", "files.snapshot", "files.until_last_block",
-              "files.coder_tail", "files.coders", "coder.id_pos", "coder.strand", "coder.ref", "coder.maps",
-              "coder.mis_cnt", "coder.mis_base", "coder.mis_off", "coder.read_off", "coder.pe_order"]:
-        try:
-            host_ms[k] = round(ctx.stage_ms(k), 3)
-        except Exception:
-            pass
-    size = os.path.getsize(os.path.join(td, tag + ".curc"))
-    for f in files + [os.path.join(td, tag + ".curc")]:
-        os.remove(f)
-    return w.bases / dt / 1e6, dt, size, host_ms
+def sample_of(w, pairs):
+    """The first `pairs` pairs of a workload: its FASTQ files are the first
+    records of the workload's own files, byte for byte."""
+    from curc_b200 import synth
+    return synth.Workload(w.name + f"_first{pairs}", w.read_len, w.mate1[:pairs],
+                          None if w.mate2 is None else w.mate2[:pairs], w.preserve_order)
+
+
+def timed_runs(cmd, cwd, steps, warmup, env=None, archive=None, timeout=900):
+    """Runs `cmd` warmup + steps times; per timed run its wall time and the
+    arrival time of each stdout line (line-buffered)."""
+    runs = []
+    for i in range(warmup + steps):
+        t = time.perf_counter()
+        p = subprocess.Popen(["stdbuf", "-oL"] + cmd, cwd=cwd, env=env, stdout=subprocess.PIPE,
+                             stderr=subprocess.PIPE, text=True)
+        lines = []
+        for line in p.stdout:
+            lines.append((time.perf_counter() - t, line.rstrip("\n")))
+        err = p.stderr.read()
+        rc = p.wait(timeout=timeout)
+        dt = time.perf_counter() - t
+        if rc != 0:
+            raise RuntimeError(f"{cmd[0]} exited {rc}: {lines[-3:]} {err[-300:]}")
+        if archive and os.path.exists(archive):
+            size = os.path.getsize(archive)
+            os.remove(archive)
+        else:
+            size = None
+        if i >= warmup:
+            runs.append({"s": dt, "lines": lines, "archive_bytes": size})
+    return runs
+
+
+def line_stages(runs):
+    """Mean time between the progress lines `curc -c` prints (the reference's
+    preprocess.cpp:69-279 and the same lines from the product's CLI): CUDA
+    context set-up, FASTQ parse and block split (with the packing), block
+    compression (device path and stream coders), archive write, exit."""
+    marks = [("init", "gpu context init finish"), ("parse_split", "waiting block compress"),
+             ("block_compress", "compress finish"), ("archive_write", "archive size")]
+    out = {}
+    for name, key in marks:
+        ts = [next((t for t, l in r["lines"] if key in l), None) for r in runs]
+        if all(x is not None for x in ts):
+            out[name] = sum(ts) / len(ts)
+    prev, res = 0.0, {}
+    for name, _ in marks:
+        if name in out:
+            res[name + "_s"] = round(out[name] - prev, 4)
+            prev = out[name]
+    res["exit_s"] = round(sum(r["s"] for r in runs) / len(runs) - prev, 4)
+    return res
+
+
+def curc_runs(files, td, steps, warmup, dev, tag):
+    archive = os.path.join(td, tag + ".curc")
+    cmd = [CURC_EXE, "-c", "-i", ",".join(files), "-o", tag, "--working_dir", td, "--preserve_order",
+           "--device", str(dev)]
+    return timed_runs(cmd, td, steps, warmup, archive=archive)
+
+
+def cli_measure(ctx, w, a, dev):
+    """`curc -c` of the workload: the product binary, one process per step
+    (the headline e2e), on the whole workload and on the reference arm's
+    sample; plus one in-process whole-file call for the host-stage split."""
+    with tempfile.TemporaryDirectory() as td:
+        files = w.write(os.path.join(td, "full"), name=FASTQ_NAME)
+        t = time.perf_counter()
+        ctx.compress_files(files, os.path.join(td, "inproc.curc"), 1.0, True, BSC_EXE, td)
+        t_in = time.perf_counter() - t
+        os.remove(os.path.join(td, "inproc.curc"))
+        host_ms = {}
+        for k in HOST_STAGES:
+            try:
+                host_ms[k] = round(ctx.stage_ms(k), 3)
+            except Exception:
+                pass
+        full = curc_runs(files, td, a.steps, a.warmup, dev, "full")
+        for f in files:
+            os.remove(f)
+        ws = sample_of(w, a.ref_sample_pairs)
+        sfiles = ws.write(os.path.join(td, "sample"), name=FASTQ_NAME)
+        sample = curc_runs(sfiles, td, a.steps, a.warmup, dev, "sample")
+    mean = sum(r["s"] for r in full) / len(full)
+    smean = sum(r["s"] for r in sample) / len(sample)
+    return {"s": mean, "value": w.bases / mean / 1e6, "archive_bytes": full[0]["archive_bytes"],
+            "archive_bits_per_base": 8.0 * full[0]["archive_bytes"] / w.bases,
+            "line_stages": line_stages(full), "in_process_s": t_in, "host_stage_ms": host_ms,
+            "sample": {"value": ws.bases / smean / 1e6, "s": smean, "pairs": a.ref_sample_pairs,
+                       "archive_bytes": sample[0]["archive_bytes"], "line_stages": line_stages(sample)}}
 
 
 def batched_vs_plain(ctx, a):
@@ -388,30 +495,34 @@ def learned_eval(a):
 
 
 def run_reference(a):
-    """The reference `curc -c` (built from its sources, oracle/_ref) end to
-    end on a bounded sample of the workload, on this box."""
+    """The reference `curc -c` (built from its sources, oracle/_ref), one
+    process per step, on the first pairs of the workload's own FASTQ files
+    (or on the whole workload once with --ref-full), on this box."""
     ref_dir = os.path.join(ROOT, "oracle", "_ref")
     exe = os.path.join(ref_dir, "curc_shared")
     if not os.path.exists(exe):
         return None, "reference build missing (oracle/_ref/curc_shared)"
-    w = workload(a.ref_sample_pairs, a.genome, seed=1)
-    times = []
+    w = workload(a.pairs, a.genome, seed=1)
+    ws = w if a.ref_full else sample_of(w, a.ref_sample_pairs)
+    steps, warmup = (1, 0) if a.ref_full else (a.steps, a.warmup)
     with tempfile.TemporaryDirectory() as td:
-        files = w.write(os.path.join(td, "in"), name=FASTQ_NAME)
-        env = dict(os.environ, LD_PRELOAD=os.path.join(ref_dir, "libzero_alloc.so"))
-        for i in range(a.warmup + a.steps):
-            t = time.perf_counter()
-            r = subprocess.run([exe, "-c", "-i", ",".join(files), "-o", f"out{i}", "--working_dir", td,
-                                "--preserve_order"], cwd=ref_dir, env=env, capture_output=True, text=True,
-                               timeout=300)
-            dt = time.perf_counter() - t
-            if r.returncode != 0:
-                return None, f"reference exited {r.returncode}: {r.stdout[-200:]} {r.stderr[-200:]}"
-            os.remove(os.path.join(td, f"out{i}.curc"))
-            if i >= a.warmup:
-                times.append(dt)
-    mean = sum(times) / len(times)
-    return {"bases": w.bases, "s": mean, "steps": len(times)}, None
+        files = ws.write(os.path.join(td, "in"), name=FASTQ_NAME)
+        del w
+        shim_log = os.path.join(td, "shim.log")
+        env = dict(os.environ, LD_PRELOAD=os.path.join(ref_dir, "libzero_alloc.so"), CURC_SHIM_LOG=shim_log)
+        cmd = [exe, "-c", "-i", ",".join(files), "-o", "out", "--working_dir", td, "--preserve_order"]
+        try:
+            runs = timed_runs(cmd, ref_dir, steps, warmup, env=env, archive=os.path.join(td, "out.curc"),
+                              timeout=3600)
+        except RuntimeError as e:
+            return None, str(e)[:300]
+        fills = [tuple(float(x) for x in l.split()) for l in open(shim_log)] if os.path.exists(shim_log) else []
+    fills = fills[warmup:]
+    mean = sum(r["s"] for r in runs) / len(runs)
+    return {"bases": ws.bases, "pairs": ws.mate1.shape[0], "s": mean, "steps": len(runs),
+            "archive_bytes": runs[0]["archive_bytes"], "line_stages": line_stages(runs),
+            "zero_fill": {"allocations": fills[0][0] if fills else None,
+                          "s": sum(f[1] for f in fills) / len(fills) if fills else None}}, None
 
 
 def finish_dist(world):
@@ -440,14 +551,21 @@ def main():
             finish_dist(world)
             return
         v = ref["bases"] / ref["s"] / 1e6
+        what = ("the whole workload, once" if a.ref_full else
+                f"the first {ref['pairs']} pairs of the workload's FASTQ files ({ref['bases'] / 1e6:.0f} Mbases) "
+                "per step")
         out = {"metric": METRIC, "value": v, "unit": "Mbases/s", "n_gpus": 1, "steps": ref["steps"],
-               "warmup": a.warmup, "ms_per_step": ref["s"] * 1000, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
-               "config": dict(cfg, sample=f"{a.ref_sample_pairs} pairs per step"),
+               "warmup": 0 if a.ref_full else a.warmup, "ms_per_step": ref["s"] * 1000, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
+               "config": cfg,
                "cpu_baseline": {"value": v, "unit": "Mbases/s", "cores": os.cpu_count(), "kind": "reference",
-                                "sample": f"reference curc -c end to end (GPU stages + host coders) on "
-                                          f"{a.ref_sample_pairs} pairs of the same generator"},
-               "e2e": {"value": v, "unit": "Mbases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                                "sample": f"reference curc -c end to end, one process per step (CUDA set-up, "
+                                          f"FASTQ parse, GPU stages, host coders, archive write) on {what}"},
+               "e2e": {"value": v, "unit": "Mbases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+               "line_stages": ref["line_stages"], "archive_bytes": ref["archive_bytes"],
+               "zero_fill": dict(ref["zero_fill"], note="LD_PRELOAD shim that zero-fills each cudaMalloc "
+                                                        "(cudaMemset + cudaDeviceSynchronize): mean seconds per "
+                                                        "run, included in the time above")}
         print(json.dumps(out))
         finish_dist(world)
         return
@@ -463,6 +581,17 @@ def main():
     probe_ms = r["substage_ms"].get("overlap.probe", 0.0)
     passes = max(1, st["overlap_passes"])
     probe_ach = probe_bytes(st, r["L"]) / (probe_ms / 1000.0) / 1e9 if probe_ms > 0 else None
+    def roof(kernel, nbytes, ms, launches, extra=None):
+        ach = nbytes / (ms / 1000.0) / 1e9 if ms > 0 else None
+        d = {"kernel": kernel, "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+             "frac": ach / peak if ach else None, "traffic": None,
+             "algorithmic_bytes_per_launch": nbytes / max(1, launches), "launches": launches,
+             "ms_per_launch": ms / max(1, launches)}
+        d.update(extra or {})
+        return d
+
+    sub = r["substage_ms"]
+    m_reads = st["non_n"]
     out = {
         "metric": METRIC,
         "value": r["bases"] * world / r["step_s"] / 1e6,
@@ -477,10 +606,19 @@ def main():
         "dtype": "u8",
         "data": "synthetic",
         "config": cfg,
-        "e2e": {"value": r["bases"] * world / r["e2e_s"] / 1e6, "unit": "Mbases/s",
-                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
-                "api": "curc_batch_submit/curc_batch_drain, one block per step from pinned host memory",
-                "one_call_per_step": r["bases"] * world / r["e2e_plain_s"] / 1e6},
+        "e2e": ({"value": r["cli"]["value"], "unit": "Mbases/s", "h2d_bytes_per_step": r["h2d"],
+                 "d2h_bytes_per_step": r["d2h"],
+                 "api": "the product's curc -c binary, one process per step, FASTQ files (page cache) to the "
+                        "closed archive: parse, H2D, device path, D2H, stream coders, archive write",
+                 "s_per_step": r["cli"]["s"]} if r["cli"] else
+                {"value": r["bases"] * world / r["e2e_s"] / 1e6, "unit": "Mbases/s",
+                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                 "api": "curc_batch_submit/curc_batch_drain, one block per step from pinned host memory "
+                        "(no stream coders)"}),
+        "e2e_batched_device_path": {"value": r["bases"] * world / r["e2e_s"] / 1e6, "unit": "Mbases/s",
+                                    "api": "curc_batch_submit/curc_batch_drain from pinned host memory, streams "
+                                           "back to the host, no stream coders",
+                                    "one_call_per_step": r["bases"] * world / r["e2e_plain_s"] / 1e6},
         "roofline": {"kernel": "probe_kernel (overlap passes, stage a4; the largest share of the launch list)",
                      "bound": "hbm", "achieved": probe_ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": probe_ach / peak if probe_ach else None,
@@ -491,6 +629,16 @@ def main():
         "roofline_pack": {"kernel": "pack_kernel (stage a1)", "bound": "hbm", "achieved": achieved, "peak": peak,
                           "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                           "traffic": None},
+        "roofline_sort": roof("first-word LSD radix sort of the reads (sub-stage sort_dedupe.radix, stage a2)",
+                              sort_bytes(m_reads, r["L"]), sub.get("sort_dedupe.radix", 0.0), 1,
+                              {"frac_of_lower_bound": (sort_lower_bound_bytes(m_reads, r["L"]) /
+                                                       (sub["sort_dedupe.radix"] / 1000.0) / 1e9 / peak)
+                               if sub.get("sort_dedupe.radix") else None}),
+        "roofline_resolve": roof("resolve_kernel (overlap passes, stage a4)", resolve_bytes(st, r["L"]),
+                                 sub.get("overlap.resolve", 0.0), passes),
+        "roofline_map": roof("map_kernel forward + reverse complement (stage a9)",
+                             map_bytes(st, r["L"], "fwd") + map_bytes(st, r["L"], "rc"),
+                             sub.get("mapping.map_fwd", 0.0) + sub.get("mapping.map_rc", 0.0), 2),
         "stage_ms": r["stage_ms"],
         "substage_ms": r["substage_ms"],
         "block_stats": r["stats"],
@@ -499,7 +647,9 @@ def main():
         "gpu_launches": r["launches"],
     }
     if r["cli"]:
-        out["cli_e2e"] = r["cli"]
+        out["cli"] = r["cli"]
+        out["e2e_same_sample"] = dict(r["cli"]["sample"], unit="Mbases/s",
+                                      note="the product's curc -c on the same files as the reference arm's steps")
     if r["batched"]:
         out["batched"] = r["batched"]
     if not a.no_learned and rank == 0:

@@ -23,7 +23,7 @@ def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C curc_b200` "
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C curc_b200 REF=<reference source root>` "
                                "(or __graft_entry__.build())")
         L = ctypes.CDLL(LIB_PATH)
         c_p, c_u64, c_int = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int

@@ -164,6 +164,8 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     mo.mm = arena.alloc<uint8_t>(U + NN + 1);
     mo.strand = arena.alloc<uint8_t>(U + NN + 1);
     mo.pos = arena.alloc<uint64_t>(U + NN + 1);
+    mo.tally = arena.alloc<unsigned long long>(6);
+    CURC_CHECK(cudaMemsetAsync(mo.tally, 0, 6 * sizeof(unsigned long long), s));
     map_reads(p, hq.packed, hq.len, udb, U, nreads, NN, mo, arena, s);
     T.end();
     if (keep_intermediates) {

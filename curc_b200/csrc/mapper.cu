@@ -97,15 +97,15 @@ __device__ __forceinline__ int ascii_mismatches(const uint64_t* __restrict__ ref
 // chunk in which a count <= target appears.  A candidate's count is exact
 // below the read's starting count (the bound of the early exit), which is
 // all the comparison needs.
+// One read per warp; returns (in every lane) the probes listed and the
+// candidates compared for the algorithmic-byte counters.
 template <bool RC>
-__global__ void __launch_bounds__(128) map_kernel(MapIndex ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
-                                                  const uint64_t* __restrict__ udb, uint32_t U,
-                                                  const uint8_t* __restrict__ ndb, uint32_t NN, int L, int W, int k,
-                                                  int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
-                                                  uint64_t* __restrict__ pos) {
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31u;
-    if (i >= U + NN) return;  // whole warp
+__device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
+                                         const uint64_t* __restrict__ udb, uint32_t U,
+                                         const uint8_t* __restrict__ ndb, int L, int W, int k, int step,
+                                         uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
+                                         uint64_t* __restrict__ pos, uint32_t i, uint32_t lane, uint32_t& listed,
+                                         uint32_t& compared) {
     const int init = mm[i];
     if (init <= BlockParams::target_mm) return;
     const bool isn = i >= U;
@@ -141,7 +141,9 @@ __global__ void __launch_bounds__(128) map_kernel(MapIndex ix, const uint64_t* _
             if (lane >= uint32_t(d)) incl += v;
         }
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        listed += uint32_t(min(32, probes - p0));
         for (uint32_t cs = 0; cs < total; cs += 32) {
+            compared += min(32u, total - cs);
             const uint32_t ci = cs + lane;
             int c = 0x7FFF;
             uint64_t mp = 0;
@@ -190,6 +192,25 @@ __global__ void __launch_bounds__(128) map_kernel(MapIndex ix, const uint64_t* _
         mm[i] = uint8_t(best);
         strand[i] = RC ? 1 : 0;
         pos[i] = best_pos;
+    }
+}
+
+template <bool RC>
+__global__ void __launch_bounds__(128) map_kernel(MapIndex ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
+                                                  const uint64_t* __restrict__ udb, uint32_t U,
+                                                  const uint8_t* __restrict__ ndb, uint32_t NN, int L, int W, int k,
+                                                  int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
+                                                  uint64_t* __restrict__ pos, unsigned long long* __restrict__ tally) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t listed = 0, compared = 0;
+    const bool searched = i < U + NN && mm[i] > BlockParams::target_mm;
+    if (i < U + NN)  // whole warp
+        map_read<RC>(ix, ref, ref_len, udb, U, ndb, L, W, k, step, mm, strand, pos, i, lane, listed, compared);
+    if (tally) {  // lane 0 carries its warp's counts
+        block_tally<unsigned long long>(lane == 0 && searched ? 1u : 0u, &tally[0]);
+        block_tally<unsigned long long>(lane == 0 ? listed : 0u, &tally[1]);
+        block_tally<unsigned long long>(lane == 0 ? compared : 0u, &tally[2]);
     }
 }
 
@@ -245,12 +266,13 @@ void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, cons
             SubStage sp_map(rc ? "mapping.map_rc" : "mapping.map_fwd");
             MapIndex ix{hs - 1, kr, pos, parts[q].start};
             const int g = grid_for(uint64_t(total) * 32, 128);
+            unsigned long long* t = out.tally ? out.tally + 3 * rc : nullptr;
             if (rc)
                 map_kernel<true><<<g, 128, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
-                                                   out.strand, out.pos);
+                                                   out.strand, out.pos, t);
             else
                 map_kernel<false><<<g, 128, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
-                                                    out.strand, out.pos);
+                                                    out.strand, out.pos, t);
             CURC_LAUNCH_CHECK();
             a.release(mk);
         }

@@ -24,7 +24,10 @@
 // Host code cannot use the array's name as a device address.  The first
 // call on a device, with that device current, looks the address up with
 // cudaGetSymbolAddress and caches it; that first call therefore also loads
-// the module, and should come before any stream capture.
+// the module, and should come before any stream capture.  The cached
+// address belongs to the device's primary context: after cudaDeviceReset
+// (or any teardown of that context) it is stale, so a process that resets a
+// device must not call this entry point on it again.
 #include <mutex>
 #include <string>
 

@@ -14,6 +14,9 @@
 // block has 32*W threads, so both passes keep every thread busy; packed
 // words of a tile are contiguous in HBM, so stores coalesce.  Bytes per
 // read: L in, 8*W + 1 out.
+#include <mutex>
+#include <stdexcept>
+
 #include "stages.cuh"
 
 namespace curc {
@@ -21,6 +24,7 @@ namespace curc {
 namespace {
 constexpr int PACK_READS = 64;
 constexpr uint32_t WAIT_LIMIT = 1u << 26;
+constexpr int MAX_DEVICES = 64;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -111,7 +115,8 @@ __global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ s
     uint64_t t = blockIdx.x;
     if (use_tma && threadIdx.x == 0 && t < tiles && full(t)) issue(t, 0);
     uint32_t pending = (use_tma && t < tiles && full(t)) ? 1u : 0u;  // bit s: a copy into stage s is in flight
-    for (uint32_t it = 0; t < tiles; t += gridDim.x, ++it) {
+    uint32_t it = 0;
+    for (; t < tiles; t += gridDim.x, ++it) {
         const int stage = it & 1;
         const uint64_t nt = t + gridDim.x;
         if (use_tma && nt < tiles && full(nt)) {
@@ -128,13 +133,31 @@ __global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ s
         const uint32_t nr = rem < uint64_t(PACK_READS) ? uint32_t(rem) : uint32_t(PACK_READS);
         if (pending >> stage & 1u) {
             uint32_t spins = 0;
+            bool late = false;
             while (!mbar_try_wait(&bar[stage], (it >> 1) & 1)) {
-                if (++spins > WAIT_LIMIT) {  // never expected: report and stop cleanly
-                    if (threadIdx.x == 0) atomicExch(err, 1u);
+                if (++spins > WAIT_LIMIT) {  // never expected
+                    late = true;
                     break;
                 }
             }
             pending &= ~(1u << stage);
+            if (__syncthreads_or(late)) {
+                // report, write nothing of this tile, and leave only once the
+                // other stage's copy (if one is in flight) has also landed or
+                // had the same bounded wait, so that, as far as waiting can
+                // tell, no bulk copy still targets this block's shared memory
+                if (threadIdx.x == 0) {
+                    atomicExch(err, 1u);
+                    const int other = stage ^ 1;
+                    if (pending >> other & 1u) {
+                        const uint32_t par = ((it + 1) >> 1) & 1;
+                        for (uint32_t w = 0; w < WAIT_LIMIT && !mbar_try_wait(&bar[other], par); ++w) {
+                        }
+                    }
+                }
+                __syncthreads();
+                return;
+            }
         } else {
             // the last, partial tile: plain loads, the rest of the tile 'A'
             const uint8_t* src = seq + t * uint64_t(PACK_READS) * L;
@@ -196,11 +219,20 @@ void pack_reads(const uint8_t* seq, uint64_t n, int L, uint64_t* packed, uint8_t
     const int W = (L + 31) / 32;
     const bool aligned = (reinterpret_cast<uintptr_t>(seq) & 15u) == 0;
     const size_t smem = pack_smem_bytes(L);
-    static bool attr_set = false;
-    if (!attr_set) {
-        CURC_CHECK(cudaFuncSetAttribute(pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(pack_smem_bytes(512))));
-        attr_set = true;
+    // the dynamic shared-memory limit is a per-device attribute: raise it
+    // once on every device this process packs on
+    static std::mutex mu;
+    static bool attr_set[MAX_DEVICES] = {};
+    int dev = 0;
+    CURC_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAX_DEVICES) throw std::runtime_error("device ordinal out of range");
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (!attr_set[dev]) {
+            CURC_CHECK(cudaFuncSetAttribute(pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(pack_smem_bytes(512))));
+            attr_set[dev] = true;
+        }
     }
     const int threads = 32 * W;
     int per_sm = 0;

@@ -91,6 +91,9 @@ struct MapOut {
     uint8_t* mm = nullptr;       // per read (U then N)
     uint8_t* strand = nullptr;
     uint64_t* pos = nullptr;
+    // optional counters, forward then reverse complement: reads searched,
+    // k-mer probes listed, candidate windows compared
+    unsigned long long* tally = nullptr;
 };
 void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, const uint64_t* udb, uint32_t U,
                const uint8_t* ndb, uint32_t NN, MapOut& out, Arena& a, cudaStream_t s);

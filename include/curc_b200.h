@@ -58,8 +58,9 @@ int curc_pack_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t r
  * limits a call to 2^27 reads; larger calls return CURC_ERR_ARG.  Calls share
  * that array, so calls that overlap on the GPU race; stream-ordered calls do
  * not.  The first call on a device sets up the array's address and should
- * come before any stream capture.  No context: errors are read with
- * curc_last_error(NULL). */
+ * come before any stream capture; that address is kept for the process and
+ * is not valid after cudaDeviceReset on the device.  No context: errors are
+ * read with curc_last_error(NULL). */
 int curc_pack_split_noalloc(int device, const char* seqs_dev, uint64_t n, uint16_t read_len, uint64_t* packed_dev,
                             uint8_t* has_n_dev, uint32_t* reads_id_dev, uint32_t* n_reads_id_dev,
                             uint32_t* counts_dev, void* stream);

@@ -3,14 +3,16 @@
 # binaries are the checker (archive round trips through `curc -d`, golden
 # archives from `curc -c` on a GPU machine) and the reference arm of bench.py.
 #
-#   make -f oracle/ref.mk REF=/root/reference
+#   make -f oracle/ref.mk REF=<root of the reference source tree>
 #
 # The reference's own CMake build is not used.  Deviations from it, all
 # needed to build with gcc 13 / nvcc 12.9 and none changing behaviour:
 #   * -include cstdint (Param.hpp uses uint8_t without including it);
 #   * fast-lzma2 compiled from its C sources (the shipped .so is not used);
 #   * no -march=native (the binary must run on other x86-64 hosts).
-REF ?= /root/reference
+ifndef REF
+$(error REF must name the root of the reference source tree)
+endif
 OUT ?= oracle/_ref
 NVCC ?= nvcc
 CXX := g++
@@ -91,7 +93,7 @@ $(OUT)/curc_shared: $(CURC_OBJ) $(LZMA_OBJ) $(OUT)/libfast-lzma2.a
 	$(NVCC) $(ARCH) -cudart shared -o $@ $(CURC_OBJ) $(LZMA_OBJ) $(OUT)/libfast-lzma2.a -lgomp -lstdc++fs -lpthread
 
 $(OUT)/libzero_alloc.so: oracle/ref_zero_alloc.c
-	$(CC) -O2 -shared -fPIC -o $@ $< -L$(CUDA_HOME)/lib64 -lcudart -ldl
+	$(CC) -O2 -shared -fPIC -o $@ $< -L$(CUDA_HOME)/lib64 -lcudart -ldl -lpthread
 
 CUDA_HOME ?= /usr/local/cuda
 .PHONY: golden

@@ -16,7 +16,7 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(ORACLE_SO):
-            raise RuntimeError(f"{ORACLE_SO} missing: run `make -f oracle/ref.mk && make -C oracle`")
+            raise RuntimeError(f"{ORACLE_SO} missing: run `make -f oracle/ref.mk REF=<reference source root> && make -C oracle REF=<reference source root>`")
         L = ctypes.CDLL(ORACLE_SO)
         L.oracle_block_new.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int]
