@@ -59,7 +59,12 @@ def parse():
     ap.add_argument("--no-cli", action="store_true", help="skip the whole-file `curc -c` measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-coder evaluation")
-    ap.add_argument("--learned-pairs", type=int, default=200_000)
+    ap.add_argument("--learned-pairs", type=int, default=1_000_000, help="pairs per training seed")
+    ap.add_argument("--learned-eval-pairs", type=int, default=10_000_000, help="pairs per evaluation seed")
+    ap.add_argument("--workload", default="pe150", choices=["pe150", "large"],
+                    help="large: the single-end 250 bp case (40M reads, 200 Mbp genome), device throughput, "
+                         "whole-file round trip and learned-coder bytes, one JSON line")
+    ap.add_argument("--large-reads", type=int, default=40_000_000)
     ap.add_argument("--batched-blocks", type=int, default=16)
     ap.add_argument("--batched-scale", type=float, default=0.1)
     return ap.parse_args()
@@ -477,20 +482,31 @@ def batched_vs_plain(ctx, a):
 
 
 def learned_eval(a):
-    """Bits/base of the mismatch streams, learned vs plain coders, on the
-    position-dependent-error workload: 8 training seeds, 2 disjoint
-    evaluation seeds (paired-end 150 bp, error rising 0.1% -> 1.0% along the
-    read, transitions 2:1), every learned stream decoded back and checked."""
+    """Bits/base of the mismatch streams, learned vs plain coders and vs
+    fast-lzma2 level 10 and libbsc on the same streams, on the
+    position-dependent-error workload at the benchmark block's shape
+    (paired-end 150 bp, error rising 0.1% -> 1.0% along the read, transitions
+    2:1): trained on 8 seeds (blocks of the same coverage), evaluated on 2
+    disjoint seeds of 10M pairs from 50 Mbp genomes, every learned stream
+    decoded back and checked."""
     from curc_b200.learned import train_and_evaluate
     t = time.perf_counter()
-    r = train_and_evaluate(train_seeds=list(range(301, 309)), eval_seeds=[401, 402], pairs=a.learned_pairs,
-                           genome_len=4_000_000, epochs=2, batch=4096)
-    return {"workload": f"paired-end 150 bp, {a.learned_pairs} pairs per seed from 4 Mbp genomes, substitutions "
-                        "0.1% -> 1.0% along the read, Ti:Tv 2:1; 8 training seeds, 2 evaluation seeds",
+    with tempfile.TemporaryDirectory() as td:
+        r = train_and_evaluate(train_seeds=list(range(301, 309)), eval_seeds=[401, 402], pairs=a.learned_pairs,
+                               genome_len=a.learned_pairs * 5, epochs=2, batch=4096,
+                               eval_pairs=a.learned_eval_pairs, eval_genome_len=a.genome,
+                               general=(BSC_EXE, td))
+    return {"workload": f"paired-end 150 bp, substitutions 0.1% -> 1.0% along the read, Ti:Tv 2:1; training: 8 seeds "
+                        f"of {a.learned_pairs} pairs from {a.learned_pairs * 5 / 1e6:.0f} Mbp genomes; evaluation: "
+                        f"2 seeds of {a.learned_eval_pairs} pairs from {a.genome / 1e6:.0f} Mbp genomes",
             "plain_bits_per_base": r["plain_bits_per_base"], "learned_bits_per_base": r["learned_bits_per_base"],
+            "fl2_level10_bits_per_base": r.get("fl2_level10_bits_per_base"),
+            "libbsc_bits_per_base": r.get("libbsc_bits_per_base"),
             "plain_bytes": {"counts": r["plain"][0], "bases": r["plain"][1], "offsets": r["plain"][2]},
-            "learned_bytes": {"counts (plain)": r["plain"][0], "gaps and bases": r["learned"]},
-            "gaps_and_bases_vs_plain": r["gaps_and_bases_ratio"], "lossless": r["lossless"],
+            "learned_bytes": {"counts (plain)": r["plain"][0], "gaps and bases": r["learned"],
+                              "model (stored once per learned block)": r["model_bytes"]},
+            "gaps_and_bases_vs_plain": r["gaps_and_bases_ratio"],
+            "mismatch_streams_vs_plain": r["mismatch_streams_ratio"], "lossless": r["lossless"],
             "train_anchors": r["train_anchors"], "final_loss": r["loss"], "s": time.perf_counter() - t}
 
 
@@ -525,6 +541,106 @@ def run_reference(a):
                           "s": sum(f[1] for f in fills) / len(fills) if fills else None}}, None
 
 
+def run_large(a):
+    """The single-end 250 bp case: 40M reads (10 Gbases) from a 200 Mbp genome
+    (45% GC, 8% repeats of 0.5-10 kbp at 0.5-2% divergence), substitutions
+    0.1% -> 1.5% along the read, N 0.02%, preserved order, one block.  Device
+    throughput (reads in HBM), the whole-file `curc -c` in learned mode (a
+    model trained on a disjoint small seed of the same generator; per block
+    the smaller of plain and learned coding), and the round trip of that
+    archive through the product decoder, read for read."""
+    import torch
+    from curc_b200 import Context, Learner, decompress_file, synth
+    t0 = time.perf_counter()
+    w = synth.large_combined(seed=4, n_reads=a.large_reads)
+    gen_s = time.perf_counter() - t0
+    seqs = w.mate1
+    n, L = seqs.shape
+    peak, peak_kind = hbm_peak()
+    out = {"workload": f"single-end {L} bp, {n} reads ({n * L / 1e9:.1f} Gbases) from a 200 Mbp genome (45% GC, 8% "
+                       "repeats of 0.5-10 kbp at 0.5-2% divergence), substitutions 0.1% -> 1.5% along the read, "
+                       "N 0.02%, --preserve_order, block_ratio 1", "generate_s": gen_s}
+    with Context(0) as ctx, Learner(0) as lrn:
+        # a model from a disjoint seed of the same generator (1M reads)
+        ws = synth.large_combined(seed=40, n_reads=1_000_000, genome_len=5_000_000)
+        ctx.block_run(ws.mate1, True, False)
+        lrn.add_block(ctx)
+        lrn.train(epochs=2, batch=4096)
+        model = lrn.model()
+        del ws
+        ctx.keep_intermediates(False)
+        d = torch.from_numpy(seqs.reshape(-1)).cuda()
+        for _ in range(a.warmup):
+            ctx.block_run_device(d.data_ptr(), n, L, True, False)
+        ms = []
+        with ClockSampler(0) as clocks:
+            clocks.wait_first()
+            for _ in range(a.steps):
+                ctx.block_run_device(d.data_ptr(), n, L, True, False)
+                ms.append(ctx.stage_ms("total"))
+        stage = {k: ctx.stage_ms(k) for k in ["pack", "sort_dedupe", "overlap", "chain_filter", "full_match",
+                                              "assembly", "mapping", "emit", "unmapped_refs", "refmatch"]}
+        pack_ms = stage["pack"]
+        del d
+        torch.cuda.empty_cache()
+        step = sum(ms) / len(ms)
+        out.update({"value": n * L / (step / 1000.0) / 1e6, "unit": "Mbases/s", "ms_per_step": step,
+                    "steps": a.steps, "stage_ms": stage, "clocks": clocks.summary(),
+                    "roofline_pack": {"achieved": pack_bytes(n, L) / (pack_ms / 1000.0) / 1e9, "peak": peak,
+                                      "peak_kind": peak_kind, "unit": "GB/s",
+                                      "frac": pack_bytes(n, L) / (pack_ms / 1000.0) / 1e9 / peak}})
+        try:
+            out.update(_large_files(ctx, w, seqs, model))
+        except Exception as e:  # e.g. no room for the 21 GB FASTQ file
+            out["e2e_learned_mode"] = {"error": str(e)[:300]}
+    return out
+
+
+def _large_files(ctx, w, seqs, model):
+    """Whole-file `curc -c` of the large workload in learned mode, then the
+    product decoder, compared read for read."""
+    from curc_b200 import decompress_file
+    n, L = seqs.shape
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        files = w.write(os.path.join(td, "large"), name=FASTQ_NAME)
+        arc = os.path.join(td, "large.curc")
+        ctx.set_mismatch_model(model)
+        t = time.perf_counter()
+        ctx.compress_files(files, arc, 1.0, True, BSC_EXE, td)
+        e2e_s = time.perf_counter() - t
+        out["e2e_learned_mode"] = {"value": n * L / e2e_s / 1e6, "unit": "Mbases/s", "s": e2e_s,
+                                   "archive_bytes": os.path.getsize(arc),
+                                   "archive_bits_per_base": 8.0 * os.path.getsize(arc) / (n * L),
+                                   "mismatch_plain_kb": ctx.stage_ms("files.mismatch_plain_kb"),
+                                   "mismatch_learned_kb": ctx.stage_ms("files.mismatch_learned_kb"),
+                                   "learned_blocks": ctx.stage_ms("files.learned_blocks"),
+                                   "host_stage_ms": {k: round(ctx.stage_ms(k), 1) for k in HOST_STAGES
+                                                     if _has_stage(ctx, k)}}
+        ctx.set_mismatch_model(None)
+        for f in files:
+            os.remove(f)
+        t = time.perf_counter()
+        got = decompress_file(arc, os.path.join(td, "dec"), BSC_EXE, td)
+        dec_s = time.perf_counter() - t
+        ok = got == n
+        if ok:
+            rows = np.memmap(os.path.join(td, "dec.seq"), dtype=np.uint8, mode="r").reshape(n, L + 1)
+            for c0 in range(0, n, 1_000_000):
+                ok &= bool(np.array_equal(rows[c0:c0 + 1_000_000, :L], seqs[c0:c0 + 1_000_000]))
+            del rows
+        out["roundtrip"] = {"lossless": ok, "decode_s": dec_s, "reads": got}
+    return out
+
+
+def _has_stage(ctx, k):
+    try:
+        ctx.stage_ms(k)
+        return True
+    except Exception:
+        return False
+
+
 def finish_dist(world):
     if world > 1:
         import torch
@@ -541,6 +657,10 @@ def main():
                        "0.2% substitutions, 0.01% N, --preserve_order, block_ratio 1",
            "global_batch": a.pairs * 2 * world, "read_len": 150, "parallelism": f"independent blocks x{world}",
            "l2_flush": "inputs (3 GB ASCII per block) are larger than L2"}
+    if a.workload == "large":
+        print(json.dumps(run_large(a)))
+        finish_dist(world)
+        return
     if a.impl == "reference":
         if rank != 0:
             finish_dist(world)

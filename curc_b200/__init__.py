@@ -5,7 +5,8 @@ include/curc_b200.h); this package is a thin host-side binding used by the
 tests and the benchmark.
 """
 from ._native import (Context, CurcError, LIB_PATH, Learner, archive_info, decompress_file,  # noqa: F401
-                      fastq_blocks, kernel_launches, learn_param_count, lib, plain_mismatch_bytes)
+                      fastq_blocks, general_mismatch_bytes, kernel_launches, learn_param_count, lib,
+                      plain_mismatch_bytes)
 
 RECORD_DTYPE = None
 

@@ -38,6 +38,11 @@ def lib() -> ctypes.CDLL:
         L.curc_block_get.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(c_p), ctypes.POINTER(c_u64)]
         L.curc_block_stage_ms.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
         L.curc_ctx_keep_intermediates.argtypes = [c_p, c_int]
+        L.curc_ctx_set_mismatch_model.argtypes = [c_p, c_p, c_u64]
+        L.curc_ctx_set_tuning.argtypes = [c_p, c_p]
+        L.curc_ctx_get_tuning.argtypes = [c_p, c_p]
+        L.curc_autotune.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_int, c_int, ctypes.c_char_p,
+                                    ctypes.POINTER(c_int)]
         L.curc_kernel_launches.argtypes = []
         L.curc_batch_submit.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_int, c_int,
                                         ctypes.POINTER(ctypes.c_uint32)]
@@ -55,10 +60,12 @@ def lib() -> ctypes.CDLL:
         L.curc_learn_set_model.argtypes = [c_p, c_p, c_u64]
         L.curc_learn_encode.argtypes = [c_p, c_p, ctypes.POINTER(c_p), ctypes.POINTER(c_u64)]
         L.curc_learn_decode_check.argtypes = [c_p, c_p, c_p, c_u64, ctypes.POINTER(c_int)]
+        L.curc_learn_infer_check.argtypes = [c_p, c_p, ctypes.POINTER(c_u64), ctypes.POINTER(c_u64)]
         L.curc_learn_param_count.argtypes = []
         L.curc_learn_param_count.restype = c_u64
         L.curc_learn_grad.argtypes = [c_p, c_p, c_p, c_p, c_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), c_p]
         L.curc_plain_mismatch_bytes.argtypes = [c_p, c_p]
+        L.curc_mismatch_general_bytes.argtypes = [c_p, ctypes.c_char_p, ctypes.c_char_p, c_p]
         L.curc_compress_files.argtypes = [c_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
                                           c_int, c_int, c_int, ctypes.c_char_p, ctypes.c_char_p,
                                           ctypes.POINTER(c_u64), ctypes.POINTER(ctypes.c_uint32)]
@@ -242,6 +249,35 @@ class Context:
                     "curc_compress_files")
         return reads.value, blocks.value
 
+    TUNING_KNOBS = ("table_factor", "bitmap_bits", "check_every", "map_threads")
+
+    def tuning(self) -> dict:
+        k = (ctypes.c_int32 * 4)()
+        self._check(lib().curc_ctx_get_tuning(self._h, k), "curc_ctx_get_tuning")
+        return dict(zip(self.TUNING_KNOBS, list(k)))
+
+    def set_tuning(self, **knobs):
+        cur = self.tuning()
+        cur.update(knobs)
+        k = (ctypes.c_int32 * 4)(*[cur[n] for n in self.TUNING_KNOBS])
+        self._check(lib().curc_ctx_set_tuning(self._h, k), "curc_ctx_set_tuning")
+
+    def autotune(self, ptr: int, n: int, L: int, preserve_order=False, paired_end=False, cache: str | None = None):
+        """Autotunes on a block already in device memory; returns (tuning,
+        whether it came from the cache)."""
+        fc = ctypes.c_int(0)
+        self._check(lib().curc_autotune(self._h, ctypes.c_void_p(ptr), n, L, int(preserve_order), int(paired_end),
+                                        cache.encode() if cache else None, ctypes.byref(fc)), "curc_autotune")
+        return self.tuning(), bool(fc.value)
+
+    def set_mismatch_model(self, model: bytes | None):
+        """Learned mode of compress_files (model bytes from Learner.model()),
+        or plain mode with None."""
+        if model:
+            self._check(lib().curc_ctx_set_mismatch_model(self._h, model, len(model)), "curc_ctx_set_mismatch_model")
+        else:
+            self._check(lib().curc_ctx_set_mismatch_model(self._h, None, 0), "curc_ctx_set_mismatch_model")
+
     def pack_device(self, seqs_ptr: int, n: int, L: int, packed_ptr: int, has_n_ptr: int, stream: int = 0):
         self._check(lib().curc_pack_device(self._h, ctypes.c_void_p(seqs_ptr), n, L, ctypes.c_void_p(packed_ptr),
                                            ctypes.c_void_p(has_n_ptr), ctypes.c_void_p(stream)), "curc_pack_device")
@@ -298,6 +334,14 @@ class Learner:
                     "curc_learn_encode")
         return ctypes.string_at(p.value, n.value)
 
+    def infer_check(self, ctx: "Context"):
+        """(anchors, anchors whose tensor-core frequencies differ from the
+        host model's) over the context's last block."""
+        n, bad = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib().curc_learn_infer_check(self._h, ctx.handle, ctypes.byref(n), ctypes.byref(bad)),
+                    "curc_learn_infer_check")
+        return n.value, bad.value
+
     def decode_check(self, ctx: "Context", stream: bytes) -> bool:
         ok = ctypes.c_int()
         self._check(lib().curc_learn_decode_check(self._h, ctx.handle, stream, len(stream), ctypes.byref(ok)),
@@ -328,3 +372,13 @@ def plain_mismatch_bytes(ctx: "Context"):
     if rc != 0:
         raise CurcError(f"curc_plain_mismatch_bytes: {lib().curc_last_error(ctx.handle).decode()}")
     return tuple(int(v) for v in out)
+
+
+def general_mismatch_bytes(ctx: "Context", bsc: str, tmpdir: str = "/tmp"):
+    """(fast-lzma2 level 10, libbsc) bytes of the last block's mismatch
+    streams (counts, bases, offsets, each coded on its own)."""
+    out = (ctypes.c_uint64 * 2)()
+    rc = lib().curc_mismatch_general_bytes(ctx.handle, bsc.encode(), tmpdir.encode(), out)
+    if rc != 0:
+        raise CurcError(f"curc_mismatch_general_bytes: {lib().curc_last_error(ctx.handle).decode()}")
+    return int(out[0]), int(out[1])

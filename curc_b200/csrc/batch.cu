@@ -188,7 +188,10 @@ int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user) {
             }
             q.pool.push_back(std::move(w));
         }
-        for (auto& w : q.pool) w->blk->keep_intermediates = ctx->block->keep_intermediates;
+        for (auto& w : q.pool) {
+            w->blk->keep_intermediates = ctx->block->keep_intermediates;
+            w->blk->tune = ctx->block->tune;
+        }
         // every pipeline sized for the largest queued block up front: growing a
         // slot later would allocate (and synchronise) in the middle of the drain
         size_t most = 0;

@@ -38,6 +38,7 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     if (n_reads > 0xFFFFFFFFull) throw std::runtime_error("more than 2^32-1 reads in one block");
     if (L < 1 || (L + 31) / 32 > 16) throw std::runtime_error("read length must be in [1, 512]");
     p = BlockParams::derive(L, po, pe);
+    p.tune = tune;
     n = uint32_t(n_reads);
     host.clear();
     stage_ms.clear();

@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 
+#include "learned_model.hpp"
 #include "stages.cuh"
 
 namespace curc {
@@ -21,6 +22,7 @@ struct Block {
     cudaStream_t stream = nullptr;
     Arena arena;
     bool keep_intermediates = true;
+    Tuning tune;  // launch and table choices for the next runs (no effect on results)
 
     BlockParams p;
     uint32_t n = 0, m = 0, NN = 0, n_ref = 0, U = 0;
@@ -122,6 +124,11 @@ struct BatchQueue {
 // drain callback runs (null otherwise).
 Block*& batch_current();
 
+namespace learned {
+// The learned mismatch stream of a block's last run (learned.cu).
+std::string encode_stream(const Model& model, Block& b);
+}  // namespace learned
+
 }  // namespace curc
 
 // The C-ABI context (include/curc_b200.h): one device, one block pipeline.
@@ -129,5 +136,7 @@ struct curc_ctx {
     int device = 0;
     std::unique_ptr<curc::Block> block;
     std::unique_ptr<curc::BatchQueue> batch;
+    // set: whole-file compression also tries the learned mismatch coder
+    std::unique_ptr<curc::learned::Model> mismatch_model;
     std::string err;
 };

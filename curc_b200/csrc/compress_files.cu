@@ -5,6 +5,7 @@
 #include <unistd.h>
 
 #include <chrono>
+#include <cstring>
 #include <cstdio>
 #include <cstdlib>
 #include <future>
@@ -52,6 +53,7 @@ std::shared_ptr<Snapshot> snapshot(const Block& b) {
 struct FileTimes {
     std::mutex mu;
     double ingest = 0, device = 0, snapshot = 0, coders = 0;
+    uint64_t mis_plain = 0, mis_learned = 0, learned_blocks = 0;  // learned mode: mismatch bytes per coding
     std::map<std::string, double> coder;
     void add_coder(const char* what, double s) {
         std::lock_guard<std::mutex> g(mu);
@@ -61,9 +63,16 @@ struct FileTimes {
 
 class DeviceSink : public host::IngestSink {
 public:
-    DeviceSink(Block& blk, bool po, bool pe, const host::CoderParams& cp, bool verbose, FileTimes& times)
-        : blk_(blk), po_(po), pe_(pe), cp_(cp), verbose_(verbose), times_(times) {
+    DeviceSink(Block& blk, bool po, bool pe, const host::CoderParams& cp, bool verbose, FileTimes& times,
+               const learned::Model* model)
+        : blk_(blk), po_(po), pe_(pe), cp_(cp), verbose_(verbose), times_(times), model_(model) {
         cp_.on_time = [t = &times_](const char* what, double s) { t->add_coder(what, s); };
+        cp_.on_learned = [t = &times_](uint64_t plain, uint64_t learned) {
+            std::lock_guard<std::mutex> g(t->mu);
+            t->mis_plain += plain;
+            t->mis_learned += learned;
+            t->learned_blocks += learned < plain;
+        };
         for (auto& e : ev_) CURC_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     ~DeviceSink() override {
@@ -107,6 +116,15 @@ public:
         blk_.run(dev_, reads_, L_, po_, pe_);
         const auto tb = clk::now();
         auto snap = snapshot(blk_);
+        if (model_) {
+            // learned mode: the block's learned mismatch stream, from the
+            // block's device state before the next block reuses it; the
+            // writer keeps it when it is smaller than the plain coding
+            const auto l0 = clk::now();
+            snap->view.learned_stream = learned::encode_stream(*model_, blk_);
+            snap->view.learned_model.assign(reinterpret_cast<const char*>(model_), sizeof(learned::Model));
+            times_.add_coder("learned", secs(l0, clk::now()));
+        }
         const auto tc = clk::now();
         const size_t bi = bodies.size();
         const bool verbose = verbose_;
@@ -147,6 +165,7 @@ private:
     host::CoderParams cp_;
     bool verbose_;
     FileTimes& times_;
+    const learned::Model* model_;
     Stage stage_[2];
     cudaEvent_t ev_[2];
     int cur_ = 0, L_ = 0;
@@ -169,6 +188,23 @@ const Buf& BlockView::get(const char* name) const {
 }
 }  // namespace host
 }  // namespace curc
+
+extern "C" int curc_ctx_set_mismatch_model(curc_ctx* ctx, const void* model, uint64_t bytes) {
+    if (!ctx) return CURC_ERR_ARG;
+    if (!model || !bytes) {
+        ctx->mismatch_model.reset();
+        return CURC_OK;
+    }
+    if (bytes != sizeof(curc::learned::Model)) {
+        ctx->err = "mismatch model: " + std::to_string(bytes) + " bytes, expected " +
+                   std::to_string(sizeof(curc::learned::Model));
+        return CURC_ERR_ARG;
+    }
+    auto m = std::make_unique<curc::learned::Model>();
+    std::memcpy(m.get(), model, sizeof(curc::learned::Model));
+    ctx->mismatch_model = std::move(m);
+    return CURC_OK;
+}
 
 extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2, const char* archive_path,
                                    double block_ratio, int preserve_order, int flzma2_level, int flzma2_threads,
@@ -194,7 +230,7 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
         const bool verbose = std::getenv("CURC_VERBOSE") != nullptr;
         const auto t0 = std::chrono::steady_clock::now();
         curc::FileTimes times;
-        curc::DeviceSink sink(blk, preserve_order != 0, !s2.empty(), cp, verbose, times);
+        curc::DeviceSink sink(blk, preserve_order != 0, !s2.empty(), cp, verbose, times, ctx->mismatch_model.get());
         const auto res = curc::host::ingest_fastq(f1, s2, block_ratio, sink);
         const auto t1 = std::chrono::steady_clock::now();
         const int L = res.read_len;
@@ -225,6 +261,13 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
             blk.stage_ms["files.snapshot"] = float(times.snapshot * 1000.0);
             blk.stage_ms["files.coders"] = float(times.coders * 1000.0);
             for (const auto& kv : times.coder) blk.stage_ms["coder." + kv.first] = float(kv.second * 1000.0);
+            if (ctx->mismatch_model) {
+                // learned mode: mismatch-stream kilobytes of each coding and
+                // the blocks that kept the learned one
+                blk.stage_ms["files.mismatch_plain_kb"] = float(double(times.mis_plain) / 1000.0);
+                blk.stage_ms["files.mismatch_learned_kb"] = float(double(times.mis_learned) / 1000.0);
+                blk.stage_ms["files.learned_blocks"] = float(times.learned_blocks);
+            }
         }
         if (reads_out) *reads_out = res.reads;
         if (blocks_out) *blocks_out = uint32_t(res.blocks);

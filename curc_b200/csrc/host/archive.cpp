@@ -244,6 +244,8 @@ void write_file(const std::string& p, const void* d, size_t n) {
     std::fclose(f);
 }
 
+// libbsc through its executable (util.cuh:527-535 runs it so for the strand
+// stream): `bsc e in out -pm0 -e2`.
 std::string bsc_strand(const std::string& bsc, const std::string& dir, const void* d, size_t n) {
     static std::atomic<uint64_t> seq{0};
     const std::string tag = std::to_string(getpid()) + "_" + std::to_string(seq.fetch_add(1));
@@ -493,10 +495,32 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
     }
     for (auto& m : maps) out += blob(m.get());
     out += blob(mis_cnt.get());
-    out += blob(mis_base.get());
     const uint8_t mm = uint8_t(max_mm);
-    out.append(reinterpret_cast<const char*>(&mm), 1);
-    for (auto& f : f_off) out += blob(f.get());
+    std::string tail = blob(mis_base.get());
+    tail.append(reinterpret_cast<const char*>(&mm), 1);
+    for (auto& f : f_off) tail += blob(f.get());
+    if (!v.learned_stream.empty()) {
+        // learned mode: the mismatch-base container holds, under the coder
+        // byte LEARNED_CODER, the model and the learned stream of bases and
+        // offsets together; the offset streams are then empty.  Kept only
+        // where it is smaller than the plain coding of the same streams.
+        std::string c(17, '\0');
+        const uint64_t src = S("mis_base").size;
+        const uint64_t clen = 4 + v.learned_model.size() + v.learned_stream.size();
+        std::memcpy(&c[0], &src, 8);
+        std::memcpy(&c[8], &clen, 8);
+        c[16] = char(LEARNED_CODER);
+        const uint32_t msize = uint32_t(v.learned_model.size());
+        c.append(reinterpret_cast<const char*>(&msize), 4);
+        c += v.learned_model;
+        c += v.learned_stream;
+        std::string lt = blob(c);
+        lt.append(reinterpret_cast<const char*>(&mm), 1);
+        lt.append(size_t(max_mm) * 8, '\0');
+        if (cp.on_learned) cp.on_learned(tail.size(), lt.size());
+        if (lt.size() < tail.size()) tail.swap(lt);
+    }
+    out += tail;
     return out;
 }
 
@@ -511,6 +535,26 @@ void plain_mismatch_bytes(const BlockView& v, uint64_t out[3]) {
         o += offsets(L, reinterpret_cast<const uint16_t*>(b.ptr), b.size / 2, size_t(m)).size();
     }
     out[2] = o;
+}
+
+void general_mismatch_bytes(const BlockView& v, const CoderParams& cp, uint64_t out[2]) {
+    // the three raw mismatch streams: counts, recoded bases, and the offset
+    // values of every count class one after another
+    const int L = v.read_len;
+    std::string offs;
+    for (int m = 1; m <= L / 5; ++m) {
+        const Buf& b = v.get(("mis_off_" + std::to_string(m)).c_str());
+        offs.append(reinterpret_cast<const char*>(b.ptr), b.size);
+    }
+    const Buf& c = v.get("mis_cnt");
+    const Buf& b = v.get("mis_base");
+    const std::pair<const void*, size_t> streams[3] = {{c.ptr, c.size}, {b.ptr, b.size}, {offs.data(), offs.size()}};
+    out[0] = out[1] = 0;
+    for (const auto& st : streams) {
+        if (!st.second) continue;
+        out[0] += fl2(st.first, st.second, cp.flzma2_level, cp.flzma2_threads).size();
+        out[1] += bsc_strand(cp.bsc_path, cp.tmpdir, st.first, st.second).size();
+    }
 }
 
 std::string archive_header(bool po, bool pe, int read_len, int blocks) {

@@ -50,6 +50,9 @@ int usage() {
         "      --flzma2_thread_num   fast-lzma2 thread number (default 16)\n"
         "      --preserve_order      preserve order information\n"
         "      --device arg          CUDA device (default 0)\n"
+        "      --coder arg           mismatch coder: plain (the reference's streams, default) or learned\n"
+        "                            (per block, the learned coder where it is smaller; needs --model)\n"
+        "      --model arg           learned mismatch model file (from the training API)\n"
         "  -v, --version             print version\n"
         "  -h, --help                print usage\n");
     return 0;
@@ -62,6 +65,7 @@ int main(int argc, char** argv) {
     std::string input, output, wd = ".";
     double ratio = 1.0;
     int level = 10, threads = 16, device = 0;
+    std::string coder = "plain", model_path;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto val = [&]() -> std::string {
@@ -79,6 +83,8 @@ int main(int argc, char** argv) {
             else if (a == "--flzma2_thread_num") threads = std::stoi(val());
             else if (a == "--preserve_order") po = true;
             else if (a == "--device") device = std::stoi(val());
+            else if (a == "--coder") coder = val();
+            else if (a == "--model") model_path = val();
             else if (a == "-h" || a == "--help") return usage();
             else if (a == "-v" || a == "--version") {
                 std::puts("v1.0.0");  // the archive format version (CURC 1.0.0)
@@ -149,10 +155,30 @@ int main(int argc, char** argv) {
             return 0;
         }
     }
+    std::string model;
+    if (coder == "learned") {
+        FILE* mf = model_path.empty() ? nullptr : std::fopen(model_path.c_str(), "rb");
+        if (!mf) {
+            std::puts("--coder learned needs a readable --model file");
+            return 0;
+        }
+        char buf[1 << 16];
+        size_t k;
+        while ((k = std::fread(buf, 1, sizeof(buf), mf)) > 0) model.append(buf, k);
+        std::fclose(mf);
+    } else if (coder != "plain") {
+        std::puts("--coder is plain or learned");
+        return 0;
+    }
     curc_ctx* ctx = nullptr;
     if (curc_ctx_create(device, &ctx) != CURC_OK) {
         std::fprintf(stderr, "GPU assert: %s\n", curc_last_error(nullptr));
         return 1;
+    }
+    if (!model.empty() && curc_ctx_set_mismatch_model(ctx, model.data(), model.size()) != CURC_OK) {
+        std::printf("%s\n", curc_last_error(ctx));
+        curc_ctx_destroy(ctx);
+        return 0;
     }
     int devices = 0;
     curc_device_count(&devices);

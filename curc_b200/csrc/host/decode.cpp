@@ -40,6 +40,7 @@
 
 #include "../../../include/curc_b200.h"
 #include "host.hpp"
+#include "../learned_model.hpp"
 
 namespace curc {
 namespace host {
@@ -689,6 +690,57 @@ BlockPayloads read_block(Reader& ar, bool po, bool pe) {
     return b;
 }
 
+// Mismatch offsets and symbols of a learned block: the container (u64 base
+// count, u64 payload length, u8 LEARNED_CODER) holds u32 model size, the
+// model and the stream; records are the main-pseudogenome reads in record
+// order (read id order with preserved order), with their positions and
+// strands already decoded.  Bases become the symbols the plain stream
+// would hold: their rank in the block's decoder table row.
+void learned_mismatches(Block& b, const std::string& payload, bool po, int L) {
+    if (payload.size() < 21) throw std::runtime_error("learned container too short");
+    uint64_t nbase, clen;
+    uint32_t msize;
+    std::memcpy(&nbase, payload.data(), 8);
+    std::memcpy(&clen, payload.data() + 8, 8);
+    std::memcpy(&msize, payload.data() + 17, 4);
+    if (clen != payload.size() - 17 || msize != sizeof(learned::Model) || clen < 4ull + msize)
+        throw std::runtime_error("learned container is malformed");
+    learned::Model M;
+    std::memcpy(&M, payload.data() + 21, sizeof(M));
+    const uint8_t* stream = reinterpret_cast<const uint8_t*>(payload.data()) + 21 + msize;
+    const size_t sbytes = size_t(clen - 4 - msize);
+    const size_t R = b.mis_cnt.size();
+    if (b.mis_first[R] != nbase) throw std::runtime_error("learned container: base count disagrees with the counts");
+    std::vector<uint64_t> pos;
+    pos.reserve(R);
+    if (po) {
+        for (uint64_t p : b.id_pos)
+            if (p < b.hq.size()) pos.push_back(p);
+    } else {
+        if (b.hq_n != R) throw std::runtime_error("record streams disagree");
+        pos.assign(b.pos.begin(), b.pos.begin() + R);
+    }
+    if (pos.size() != R || b.strand.size() != R) throw std::runtime_error("record streams disagree");
+    std::vector<uint8_t> strand(R);
+    for (size_t r = 0; r < R; ++r) strand[r] = b.strand[r] == '1';
+    b.mis_off.assign(nbase, 0);
+    std::string bases(nbase, '\0');
+    const std::string why =
+        learned::decode_stream(M, stream, sbytes, reinterpret_cast<const uint8_t*>(b.hq.data()), b.hq.size(), L, R,
+                               pos.data(), strand.data(), b.mis_cnt.data(), b.mis_off.data(), &bases[0]);
+    if (!why.empty()) throw std::runtime_error(why);
+    b.mis_base.assign(nbase, '\0');
+    for (size_t r = 0; r < R; ++r)
+        for (uint64_t k = b.mis_first[r]; k < b.mis_first[r + 1]; ++k) {
+            const char gb = b.hq[pos[r] + b.mis_off[k]];
+            int sym = -1;
+            for (int j = 0; j < 4; ++j)
+                if (b.table[uint8_t(gb) & 127][j] == bases[k]) sym = j;
+            if (sym < 0) throw std::runtime_error("learned stream: base outside the decoder table");
+            b.mis_base[k] = char(sym);
+        }
+}
+
 Block decode_block(Reader& ar, bool po, bool pe, int L, const DecodeParams& dp, uint32_t index) {
     Block b;
     BlockPayloads bp = read_block(ar, po, pe);
@@ -721,7 +773,11 @@ Block decode_block(Reader& ar, bool po, bool pe, int L, const DecodeParams& dp, 
     std::future<std::string> f_maps[6];
     for (int k = 0; k < 6; ++k)
         f_maps[k] = std::async(std::launch::async, [&, k] { return Cursor(maps[k]).text(); });
-    auto f_base = std::async(std::launch::async, [&] { return Cursor(s_base).text(); });
+    // a block whose mismatch bases and offsets the learned coder wrote: the
+    // base container carries LEARNED_CODER, the model and the stream, and
+    // is decoded below once positions and pseudogenome are known
+    const bool learned = s_base.size() >= 17 && uint8_t(s_base[16]) == LEARNED_CODER;
+    auto f_base = std::async(std::launch::async, [&] { return learned ? std::string() : Cursor(s_base).text(); });
     auto f_mis = std::async(std::launch::async, [&] {
         b.mis_cnt = Cursor(s_cnt).values<uint8_t>();
         const size_t R = b.mis_cnt.size();
@@ -735,6 +791,7 @@ Block decode_block(Reader& ar, bool po, bool pe, int L, const DecodeParams& dp, 
             ++per[b.mis_cnt[r]];
         }
         b.mis_first[R] = acc;
+        if (learned) return;  // offsets come from the learned stream
         // every class decodes on its own; then records take their offsets in order
         std::vector<std::future<std::vector<uint16_t>>> f(size_t(max_mm) + 1);
         for (int m = 1; m <= max_mm; ++m)
@@ -831,6 +888,7 @@ Block decode_block(Reader& ar, bool po, bool pe, int L, const DecodeParams& dp, 
     b.hq = recover_ref(hq_coded, nullptr, mapv[0], mapv[1], b.ref32);
     b.lq = recover_ref(lq_coded, &b.hq, mapv[2], mapv[3], b.ref32);
     b.nq = recover_ref(nq_coded, &b.hq, mapv[4], mapv[5], b.ref32);
+    if (learned) learned_mismatches(b, s_base, po, L);
     if (b.strand.size() != b.mis_cnt.size() || b.mis_base.size() != b.mis_off.size())
         throw std::runtime_error("record streams disagree");
     return b;

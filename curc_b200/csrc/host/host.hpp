@@ -22,7 +22,15 @@ struct BlockView {
     bool preserve_order = false, paired_end = false;
     std::map<std::string, Buf> streams;
     const Buf& get(const char* name) const;
+    // learned mismatch coding (learned mode only): the serialised model and
+    // the block's learned stream; empty in plain mode
+    std::string learned_model, learned_stream;
 };
+
+// Coder byte of the mismatch-base container when the block's mismatch bases
+// and offsets are coded by the learned coder (the container's other coder
+// bytes are LzmaLib.h's LZMA_CODER 1, PPMD7_CODER 3, VARLEN_DNA_CODER 11).
+constexpr uint8_t LEARNED_CODER = 100;
 
 struct CoderParams {
     int flzma2_level = 10;    // --flzma2_level
@@ -31,6 +39,9 @@ struct CoderParams {
     std::string tmpdir;       // scratch files for bsc
     // called (from coder threads) with each coder's name and seconds
     std::function<void(const char*, double)> on_time;
+    // learned mode: called with the bytes of the plain and of the learned
+    // coding of a block's mismatch bases and offsets
+    std::function<void(uint64_t, uint64_t)> on_learned;
 };
 
 // Block body in the reference layout (compress.cu:1364-2146).
@@ -38,6 +49,10 @@ std::string encode_block(const BlockView& v, const CoderParams& cp);
 // Coded sizes of a block's mismatch streams with the plain coders (the
 // same calls as encode_block): counts, bases, offsets.
 void plain_mismatch_bytes(const BlockView& v, uint64_t out[3]);
+// Sizes of the same raw mismatch streams (counts, bases, offsets) under the
+// general-purpose coders of the block's other streams: fast-lzma2 at the
+// configured level and libbsc (for comparison with the learned coder).
+void general_mismatch_bytes(const BlockView& v, const CoderParams& cp, uint64_t out[2]);
 // Archive header (preprocess.cpp:261-266).
 std::string archive_header(bool po, bool pe, int read_len, int blocks);
 

@@ -10,8 +10,9 @@
 // bias/ReLU, softmax cross-entropy over the two output groups, column sums);
 // the trained network is quantised to int8 weights, int32 accumulation and
 // fixed-point requantisation (learned_model.hpp), and inference on the GPU
-// uses dp4a over the packed int8 rows, which gives exactly the integers of
-// the host reference, so the host decoder derives the same frequencies.
+// runs the two dense layers on the tensor cores (tcgen05.mma kind::i8, s32
+// accumulators in TMEM), which gives exactly the integers of the host
+// reference, so the host decoder derives the same frequencies.
 // The range-coded stream is split into chunks of records coded
 // independently, so coding and the losslessness check run in parallel.
 #include <omp.h>
@@ -21,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <random>
 
 #include "../../include/curc_b200.h"
@@ -45,7 +47,6 @@ struct __align__(16) Anchor {
 static_assert(sizeof(Anchor) == 32, "anchor layout");
 
 constexpr int NPARAM = HID * IN + HID + HID * HID + HID + OUT * HID + OUT;
-constexpr int CHUNK_RECORDS = 16384;
 
 // Mismatch positions and bases of record r in pseudogenome order (as the
 // emission kernel derives them).
@@ -250,60 +251,280 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 }
 
 // ---------------------------------------------------------------- inference
+//
+// The int8 network on the 5th-generation tensor cores.  One CTA of 128
+// threads takes 128 anchors at a time (one per thread and TMEM lane):
+//   layer 1 (one-hot inputs): the sum of the anchor's weight columns, by the
+//     thread itself, requantised to int8 and stored as the A operand;
+//   layer 2: tcgen05.mma kind::i8, D[128 x 128] s32 in TMEM = A[128 x 128]
+//     x W2^T, four K=32 steps issued by one thread; the thread of each
+//     anchor reads its row back (tcgen05.ld), adds the bias, requantises and
+//     stores it as the next A operand;
+//   layer 3: the same with N = 32 (the 20 output rows of W3, zero padded);
+//     each thread turns its 20 logits into frequencies.
+// Integer accumulation is exact in any order, so the frequencies equal the
+// host model's (learned_model.hpp) bit for bit.  Operands live in shared
+// memory in the no-swizzle K-major core-matrix layout: 8 rows x 16 bytes per
+// 128-byte core matrix, the K chunks of a row group 128 bytes apart (leading
+// byte offset) and row groups 1024 bytes apart (stride byte offset).  Waits
+// on the MMA barrier are bounded: a wait that gives up sets the error word,
+// and the CTA frees its TMEM and leaves.
 
-// int8 network per anchor, the integers of model_freqs: the sparse first
-// layer as column sums, the dense layers as dp4a over packed int8 rows.
-__global__ void __launch_bounds__(128) infer_kernel(const Model* __restrict__ gm, const Anchor* __restrict__ a,
-                                                    uint32_t n, uint16_t* __restrict__ freq) {
-    __shared__ Model M;
+constexpr int TC_ROWS = 128;                 // anchors per tile (MMA M)
+constexpr int TC_N3 = 32;                    // padded output rows of layer 3
+constexpr int W1T_STRIDE = HID + 4;          // bytes per input row of W1^T (bank spread)
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
+constexpr uint32_t TC_TMEM_COLS = 128;
+
+// Device copy of a model in the kernel's shared-memory layout.
+struct TcModel {
+    int8_t w1t[IN * W1T_STRIDE];             // W1 transposed: row = input feature
+    int8_t w2[HID * HID];                    // B operand of layer 2, core-matrix layout
+    int8_t w3[TC_N3 * HID];                  // B operand of layer 3, core-matrix layout
+    int32_t b1[HID], b2[HID], b3[OUT];
+    int32_t m1, sh1, m2, sh2, zmul, pad[3];
+    uint32_t lut[LUTN];
+};
+
+// Byte offset of element (row r, k) of a K-major operand of 128 K bytes.
+__host__ __device__ constexpr uint32_t core_off(int r, int k) {
+    return uint32_t((r >> 3) * 1024 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15));
+}
+
+TcModel tc_model(const Model& M) {
+    TcModel t{};
+    for (int i = 0; i < IN; ++i)
+        for (int h = 0; h < HID; ++h) t.w1t[i * W1T_STRIDE + h] = M.w1[h][i];
+    for (int h = 0; h < HID; ++h)
+        for (int k = 0; k < HID; ++k) t.w2[core_off(h, k)] = M.w2[h][k];
+    for (int o = 0; o < TC_N3; ++o)
+        for (int k = 0; k < HID; ++k) t.w3[core_off(o, k)] = o < OUT ? M.w3[o][k] : int8_t(0);
+    std::memcpy(t.b1, M.b1, sizeof(t.b1));
+    std::memcpy(t.b2, M.b2, sizeof(t.b2));
+    std::memcpy(t.b3, M.b3, sizeof(t.b3));
+    t.m1 = M.m1;
+    t.sh1 = M.sh1;
+    t.m2 = M.m2;
+    t.sh2 = M.sh2;
+    t.zmul = M.zmul;
+    std::memcpy(t.lut, M.lut, sizeof(t.lut));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t s_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor, no swizzle, K-major (version 1 for sm_100).
+__device__ __forceinline__ uint64_t smem_desc(const void* base) {
+    const uint64_t a = (s_addr(base) >> 4) & 0x3FFFu;
+    const uint64_t lbo = 128u >> 4, sbo = 1024u >> 4;
+    return a | (lbo << 16) | (sbo << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::i8: s32 accumulator, signed A and B, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(TC_ROWS >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool tc_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(s_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, int32_t* v) {
+    uint32_t* r = reinterpret_cast<uint32_t*>(v);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Bounded wait on the MMA barrier by every thread; false when it gave up.
+__device__ __forceinline__ bool tc_wait_all(uint64_t* bar, uint32_t parity) {
+    bool late = false;
+    for (uint32_t w = 0; !tc_try_wait(bar, parity); ++w)
+        if (w > TC_WAIT_LIMIT) {
+            late = true;
+            break;
+        }
+    return !__syncthreads_or(late);
+}
+
+constexpr size_t TC_SMEM = sizeof(TcModel) + TC_ROWS * HID + 1024;
+
+__global__ void __launch_bounds__(TC_ROWS) infer_tc_kernel(const TcModel* __restrict__ gm,
+                                                            const Anchor* __restrict__ a, uint32_t n,
+                                                            uint16_t* __restrict__ freq, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    // 1024-aligned operand tile, then the model
+    uint8_t* base = tc_smem + ((1024u - (s_addr(tc_smem) & 1023u)) & 1023u);
+    int8_t* A = reinterpret_cast<int8_t*>(base);
+    TcModel& M = *reinterpret_cast<TcModel*>(base + TC_ROWS * HID);
     {
-        const int words = sizeof(Model) / 4;
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(gm);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&M);
+        const int words = sizeof(TcModel) / 16;
+        const uint4* src = reinterpret_cast<const uint4*>(gm);
+        uint4* dst = reinterpret_cast<uint4*>(&M);
         for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
     }
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_addr(&tmem_slot)),
+                     "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
     __syncthreads();
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const Anchor an = a[k];
-    int32_t a1p[HID / 4];  // layer-1 activations packed 4 per word (0..127)
-    for (int h4 = 0; h4 < HID / 4; ++h4) {
-        uint32_t w = 0;
-        for (int q = 0; q < 4; ++q) {
-            const int h = 4 * h4 + q;
-            int32_t acc = M.b1[h];
-            for (int t = 0; t < an.nidx; ++t) acc += M.w1[h][an.idx[t]];
-            w |= uint32_t(requant(acc, M.m1, M.sh1)) << (8 * q);
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t lane_addr = tmem + (uint32_t(warp * 32) << 16);
+    const uint32_t id2 = idesc_i8(HID), id3 = idesc_i8(TC_N3);
+    uint32_t phase = 0;
+    const uint32_t tiles = (n + TC_ROWS - 1) / TC_ROWS;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint32_t k = t * TC_ROWS + uint32_t(tid);
+        const bool live = k < n;
+        Anchor an{};
+        if (live) an = a[k];
+        // layer 1: sum of the active weight columns, 32 hidden units at a time
+        for (int h0 = 0; h0 < HID; h0 += 32) {
+            int32_t acc[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc[j] = M.b1[h0 + j];
+            for (int f = 0; f < (live ? int(an.nidx) : 0); ++f) {
+                const int8_t* col = M.w1t + int(an.idx[f]) * W1T_STRIDE + h0;
+#pragma unroll
+                for (int j = 0; j < 32; j += 4) {
+                    const char4 w = *reinterpret_cast<const char4*>(col + j);
+                    acc[j] += w.x;
+                    acc[j + 1] += w.y;
+                    acc[j + 2] += w.z;
+                    acc[j + 3] += w.w;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 32; j += 16) {
+                uint32_t v[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uint32_t w = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) w |= uint32_t(requant(acc[j + 4 * q + b], M.m1, M.sh1)) << (8 * b);
+                    v[q] = w;
+                }
+                *reinterpret_cast<uint4*>(A + core_off(tid, h0 + j)) = make_uint4(v[0], v[1], v[2], v[3]);
+            }
         }
-        a1p[h4] = int32_t(w);
-    }
-    int32_t a2p[HID / 4];
-    for (int h4 = 0; h4 < HID / 4; ++h4) {
-        uint32_t w = 0;
-        for (int q = 0; q < 4; ++q) {
-            const int h = 4 * h4 + q;
-            const int32_t* row = reinterpret_cast<const int32_t*>(M.w2[h]);
-            int32_t acc = M.b2[h];
-#pragma unroll 8
-            for (int t = 0; t < HID / 4; ++t) acc = __dp4a(row[t], a1p[t], acc);
-            w |= uint32_t(requant(acc, M.m2, M.sh2)) << (8 * q);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        // layer 2 on the tensor cores
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int s = 0; s < HID / 32; ++s)
+                tc_mma(tmem, smem_desc(A + s * 256), smem_desc(M.w2 + s * 256), id2, s > 0);
+            tc_commit(&bar);
         }
-        a2p[h4] = int32_t(w);
+        if (!tc_wait_all(&bar, phase)) {
+            if (tid == 0) atomicExch(err, 1u);
+            break;
+        }
+        phase ^= 1;
+        tc_fence_after();
+        // read back, bias, requantise: the A operand of layer 3
+        for (int h0 = 0; h0 < HID; h0 += 32) {
+            int32_t d[32];
+            tc_ld32(lane_addr + uint32_t(h0), d);
+#pragma unroll
+            for (int j = 0; j < 32; j += 16) {
+                uint32_t v[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uint32_t w = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int h = j + 4 * q + b;
+                        w |= uint32_t(requant(d[h] + M.b2[h0 + h], M.m2, M.sh2)) << (8 * b);
+                    }
+                    v[q] = w;
+                }
+                *reinterpret_cast<uint4*>(A + core_off(tid, h0 + j)) = make_uint4(v[0], v[1], v[2], v[3]);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        // layer 3 on the tensor cores (columns 0..31 again: layer 2's values are read)
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int s = 0; s < HID / 32; ++s)
+                tc_mma(tmem, smem_desc(A + s * 256), smem_desc(M.w3 + s * 256), id3, s > 0);
+            tc_commit(&bar);
+        }
+        if (!tc_wait_all(&bar, phase)) {
+            if (tid == 0) atomicExch(err, 1u);
+            break;
+        }
+        phase ^= 1;
+        tc_fence_after();
+        int32_t z[32];
+        tc_ld32(lane_addr, z);
+        if (live) {
+            int32_t zz[OUT];
+#pragma unroll
+            for (int o = 0; o < OUT; ++o) zz[o] = z[o] + M.b3[o];
+            uint32_t fb[NB], fg[NG];
+            logits_to_freq_lut(M.lut, M.zmul, zz, NB, NB, fb);
+            logits_to_freq_lut(M.lut, M.zmul, zz + NB, gap_bin(an.gmax) + 1, NG, fg);
+            uint16_t* f = freq + size_t(k) * OUT;
+            for (int j = 0; j < NB; ++j) f[j] = uint16_t(fb[j]);
+            for (int j = 0; j < NG; ++j) f[NB + j] = uint16_t(fg[j]);
+        }
+        tc_fence_before();
+        __syncthreads();  // every lane read before the next tile's MMA overwrites TMEM
     }
-    int32_t z[OUT];
-    for (int o = 0; o < OUT; ++o) {
-        const int32_t* row = reinterpret_cast<const int32_t*>(M.w3[o]);
-        int32_t acc = M.b3[o];
-#pragma unroll 8
-        for (int t = 0; t < HID / 4; ++t) acc = __dp4a(row[t], a2p[t], acc);
-        z[o] = acc;
-    }
-    uint32_t fb[NB], fg[NG];
-    logits_to_freq(M, z, NB, NB, fb);
-    logits_to_freq(M, z + NB, gap_bin(an.gmax) + 1, NG, fg);
-    uint16_t* f = freq + size_t(k) * OUT;
-    for (int j = 0; j < NB; ++j) f[j] = uint16_t(fb[j]);
-    for (int j = 0; j < NG; ++j) f[NB + j] = uint16_t(fg[j]);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
 }
 
 // ---------------------------------------------------------------- host side
@@ -394,25 +615,8 @@ struct curc_learn {
     Trainer t;
 };
 
-namespace {
-
-template <class F>
-int guarded_learn(curc_learn* L, F&& f) {
-    try {
-        CURC_CHECK(cudaSetDevice(L->t.device));
-        f();
-        return CURC_OK;
-    } catch (const CudaError& e) {
-        L->t.err = e.what();
-        return CURC_ERR_CUDA;
-    } catch (const std::invalid_argument& e) {
-        L->t.err = e.what();
-        return CURC_ERR_ARG;
-    } catch (const std::exception& e) {
-        L->t.err = e.what();
-        return CURC_ERR_STATE;
-    }
-}
+namespace curc {
+namespace learned {
 
 // Anchors of a context's last block (device memory of `a`).
 Anchor* block_anchors(Block& b, Arena& a, uint32_t* count_out) {
@@ -436,6 +640,129 @@ Anchor* block_anchors(Block& b, Arena& a, uint32_t* count_out) {
     if (read_scalar(tot + 1, b.stream)) throw std::runtime_error("learned: mismatch recount disagrees");
     *count_out = na;
     return out;
+}
+
+// Frequencies of n anchors (device) from a quantised model, on the tensor
+// cores.
+void infer(const Model& model, const Anchor* a, uint32_t n, uint16_t* fq, Arena& ar, cudaStream_t s) {
+    if (!n) return;
+    static std::mutex mu;
+    static bool attr[64] = {};
+    int dev = 0;
+    CURC_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal out of range");
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (!attr[dev]) {
+            CURC_CHECK(cudaFuncSetAttribute(infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(TC_SMEM)));
+            attr[dev] = true;
+        }
+    }
+    const TcModel hm = tc_model(model);
+    TcModel* dm = ar.alloc<TcModel>(1);
+    uint32_t* err = ar.alloc<uint32_t>(1);
+    CURC_CHECK(cudaMemcpyAsync(dm, &hm, sizeof(TcModel), cudaMemcpyHostToDevice, s));
+    CURC_CHECK(cudaMemsetAsync(err, 0, 4, s));
+    const uint32_t tiles = (n + TC_ROWS - 1) / TC_ROWS;
+    const int grid = int(std::min<uint32_t>(tiles, uint32_t(SM_COUNT_B200) * 3));
+    infer_tc_kernel<<<grid, TC_ROWS, TC_SMEM, s>>>(dm, a, n, fq, err);
+    CURC_LAUNCH_CHECK();
+    if (read_scalar(err, s)) throw std::runtime_error("learned: tensor-core wait timed out");
+}
+
+// The learned stream of a block (its anchors listed and the network run on
+// the GPU, the range coding on the host, chunks of records in parallel).
+std::string encode_stream(const Model& model, Block& b) {
+    auto mk = b.arena.mark();
+    uint32_t na = 0;
+    Anchor* a = block_anchors(b, b.arena, &na);
+    uint16_t* fq = b.arena.alloc<uint16_t>(size_t(na ? na : 1) * OUT);
+    infer(model, a, na, fq, b.arena, b.stream);
+    std::vector<Anchor> ha(na);
+    std::vector<uint16_t> hf(size_t(na) * OUT);
+    if (na) {
+        CURC_CHECK(cudaMemcpyAsync(ha.data(), a, size_t(na) * sizeof(Anchor), cudaMemcpyDeviceToHost, b.stream));
+        CURC_CHECK(cudaMemcpyAsync(hf.data(), fq, hf.size() * 2, cudaMemcpyDeviceToHost, b.stream));
+    }
+    CURC_CHECK(cudaStreamSynchronize(b.stream));
+    b.arena.release(mk);
+    // chunk boundaries: anchors of CHUNK_RECORDS records with mismatches
+    std::vector<size_t> cut{0};
+    uint32_t recs = 0;
+    for (size_t k = 0; k < na; ++k)
+        if (ha[k].tbase < 0 && k > 0 && ++recs % CHUNK_RECORDS == 0) cut.push_back(k);
+    cut.push_back(na);
+    const int nc = int(cut.size()) - 1;
+    std::vector<std::string> chunks(nc);
+    double bits[3] = {0, 0, 0};  // bases, gap bins, offsets inside bins
+#pragma omp parallel for schedule(dynamic)
+    for (int c = 0; c < nc; ++c) {
+        RangeEncoder enc;
+        BinModels bins;
+        double cb[3] = {0, 0, 0};
+        for (size_t k = cut[c]; k < cut[c + 1]; ++k) {
+            const Anchor& x = ha[k];
+            const uint16_t* f = &hf[k * OUT];
+            if (x.tbase >= 0) {
+                uint32_t cum = 0;
+                for (int j = 0; j < x.tbase; ++j) cum += f[j];
+                enc.encode(cum, f[x.tbase], TOTAL);
+                cb[0] -= std::log2(double(f[x.tbase]) / TOTAL);
+            }
+            if (x.tgap >= 0) {
+                uint32_t cum = 0;
+                for (int j = 0; j < x.tgap; ++j) cum += f[NB + j];
+                enc.encode(cum, f[NB + x.tgap], TOTAL);
+                cb[1] -= std::log2(double(f[NB + x.tgap]) / TOTAL);
+                const int lo = gap_bin_lo(x.tgap);
+                const int hi = std::min(gap_bin_lo(x.tgap + 1), int(x.gmax) + 1);
+                uint32_t oc, of, ot;
+                bins.lookup(x.tgap, x.gap - lo, hi - lo, oc, of, ot);
+                enc.encode(oc, of, ot);
+                cb[2] -= std::log2(double(of) / ot);
+                bins.update(x.tgap, x.gap - lo);
+            }
+        }
+        chunks[c] = enc.finish();
+#pragma omp critical
+        for (int q = 0; q < 3; ++q) bits[q] += cb[q];
+    }
+    if (std::getenv("CURC_VERBOSE"))
+        std::fprintf(stderr, "curc: learned bytes: bases %.0f, gap bins %.0f, offsets in bins %.0f (%u anchors)\n",
+                     bits[0] / 8, bits[1] / 8, bits[2] / 8, na);
+    std::string s;
+    const uint32_t ncu = uint32_t(nc);
+    s.append(reinterpret_cast<const char*>(&ncu), 4);
+    for (auto& c : chunks) {
+        const uint32_t len = uint32_t(c.size());
+        s.append(reinterpret_cast<const char*>(&len), 4);
+    }
+    for (auto& c : chunks) s += c;
+    return s;
+}
+
+}  // namespace learned
+}  // namespace curc
+
+namespace {
+
+template <class F>
+int guarded_learn(curc_learn* L, F&& f) {
+    try {
+        CURC_CHECK(cudaSetDevice(L->t.device));
+        f();
+        return CURC_OK;
+    } catch (const CudaError& e) {
+        L->t.err = e.what();
+        return CURC_ERR_CUDA;
+    } catch (const std::invalid_argument& e) {
+        L->t.err = e.what();
+        return CURC_ERR_ARG;
+    } catch (const std::exception& e) {
+        L->t.err = e.what();
+        return CURC_ERR_STATE;
+    }
 }
 
 // Quantises the float parameters (host copy) into the integer model, with
@@ -680,17 +1007,28 @@ int curc_learn_encode(curc_learn* L, curc_ctx* ctx, const void** out, uint64_t* 
     return guarded_learn(L, [&] {
         Trainer& T = L->t;
         if (!T.quantised) throw std::runtime_error("learned: no quantised model");
+        const std::string s = encode_stream(T.model, *ctx->block);
+        T.stream.assign(s.begin(), s.end());
+        *out = T.stream.data();
+        *bytes = T.stream.size();
+    });
+}
+
+// Runs the tensor-core inference over the context's last block and
+// recomputes every anchor's frequencies with the host model
+// (learned_model.hpp, the decoder's integers): *anchors receives the
+// number of anchors and *mismatched how many differ in any frequency.
+int curc_learn_infer_check(curc_learn* L, curc_ctx* ctx, uint64_t* anchors, uint64_t* mismatched) {
+    if (!L || !ctx || !anchors || !mismatched) return CURC_ERR_ARG;
+    return guarded_learn(L, [&] {
+        Trainer& T = L->t;
+        if (!T.quantised) throw std::runtime_error("learned: no quantised model");
         Block& b = *ctx->block;
         auto mk = b.arena.mark();
         uint32_t na = 0;
         Anchor* a = block_anchors(b, b.arena, &na);
-        Model* dm = b.arena.alloc<Model>(1);
-        CURC_CHECK(cudaMemcpyAsync(dm, &T.model, sizeof(Model), cudaMemcpyHostToDevice, b.stream));
         uint16_t* fq = b.arena.alloc<uint16_t>(size_t(na ? na : 1) * OUT);
-        if (na) {
-            infer_kernel<<<grid_for(na, 128), 128, 0, b.stream>>>(dm, a, na, fq);
-            CURC_LAUNCH_CHECK();
-        }
+        infer(T.model, a, na, fq, b.arena, b.stream);
         std::vector<Anchor> ha(na);
         std::vector<uint16_t> hf(size_t(na) * OUT);
         if (na) {
@@ -699,61 +1037,21 @@ int curc_learn_encode(curc_learn* L, curc_ctx* ctx, const void** out, uint64_t* 
         }
         CURC_CHECK(cudaStreamSynchronize(b.stream));
         b.arena.release(mk);
-        // chunk boundaries: anchors of CHUNK_RECORDS records with mismatches
-        std::vector<size_t> cut{0};
-        uint32_t recs = 0;
-        for (size_t k = 0; k < na; ++k)
-            if (ha[k].tbase < 0 && k > 0 && ++recs % CHUNK_RECORDS == 0) cut.push_back(k);
-        cut.push_back(na);
-        const int nc = int(cut.size()) - 1;
-        std::vector<std::string> chunks(nc);
-        double bits[3] = {0, 0, 0};  // bases, gap bins, offsets inside bins
-#pragma omp parallel for schedule(dynamic)
-        for (int c = 0; c < nc; ++c) {
-            RangeEncoder enc;
-            BinModels bins;
-            double cb[3] = {0, 0, 0};
-            for (size_t k = cut[c]; k < cut[c + 1]; ++k) {
-                const Anchor& x = ha[k];
-                const uint16_t* f = &hf[k * OUT];
-                if (x.tbase >= 0) {
-                    uint32_t cum = 0;
-                    for (int j = 0; j < x.tbase; ++j) cum += f[j];
-                    enc.encode(cum, f[x.tbase], TOTAL);
-                    cb[0] -= std::log2(double(f[x.tbase]) / TOTAL);
-                }
-                if (x.tgap >= 0) {
-                    uint32_t cum = 0;
-                    for (int j = 0; j < x.tgap; ++j) cum += f[NB + j];
-                    enc.encode(cum, f[NB + x.tgap], TOTAL);
-                    cb[1] -= std::log2(double(f[NB + x.tgap]) / TOTAL);
-                    const int lo = gap_bin_lo(x.tgap);
-                    const int hi = std::min(gap_bin_lo(x.tgap + 1), int(x.gmax) + 1);
-                    uint32_t oc, of, ot;
-                    bins.lookup(x.tgap, x.gap - lo, hi - lo, oc, of, ot);
-                    enc.encode(oc, of, ot);
-                    cb[2] -= std::log2(double(of) / ot);
-                    bins.update(x.tgap, x.gap - lo);
-                }
-            }
-            chunks[c] = enc.finish();
-#pragma omp critical
-            for (int q = 0; q < 3; ++q) bits[q] += cb[q];
+        uint64_t bad = 0;
+#pragma omp parallel for reduction(+ : bad)
+        for (int64_t k = 0; k < int64_t(na); ++k) {
+            int idx[24];
+            for (int t = 0; t < ha[k].nidx; ++t) idx[t] = ha[k].idx[t];
+            uint32_t fb[NB], fg[NG];
+            model_freqs(T.model, idx, ha[k].nidx, ha[k].gmax, fb, fg);
+            const uint16_t* f = &hf[size_t(k) * OUT];
+            bool same = true;
+            for (int j = 0; j < NB; ++j) same &= f[j] == fb[j];
+            for (int j = 0; j < NG; ++j) same &= f[NB + j] == fg[j];
+            bad += same ? 0 : 1;
         }
-        if (std::getenv("CURC_VERBOSE"))
-            std::fprintf(stderr, "curc: learned bytes: bases %.0f, gap bins %.0f, offsets in bins %.0f (%u anchors)\n",
-                         bits[0] / 8, bits[1] / 8, bits[2] / 8, na);
-        std::string s;
-        const uint32_t ncu = uint32_t(nc);
-        s.append(reinterpret_cast<const char*>(&ncu), 4);
-        for (auto& c : chunks) {
-            const uint32_t len = uint32_t(c.size());
-            s.append(reinterpret_cast<const char*>(&len), 4);
-        }
-        for (auto& c : chunks) s += c;
-        T.stream.assign(s.begin(), s.end());
-        *out = T.stream.data();
-        *bytes = T.stream.size();
+        *anchors = na;
+        *mismatched = bad;
     });
 }
 
@@ -781,75 +1079,32 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
         }
         if (b.hq.len) CURC_CHECK(cudaMemcpy(ref.data(), b.hq.seq, b.hq.len, cudaMemcpyDeviceToHost));
         const int Lr = b.p.L;
-        // records with mismatches, in order, and their first anchor index
-        std::vector<uint32_t> rlist, first;
-        for (size_t k = 0; k < na; ++k)
-            if (ha[k].tbase < 0) {
-                rlist.push_back(ha[k].rec);
-                first.push_back(uint32_t(k));
-            }
-        const uint8_t* p = static_cast<const uint8_t*>(data);
-        if (bytes < 4) throw std::runtime_error("learned: short stream");
-        uint32_t nc;
-        std::memcpy(&nc, p, 4);
-        const uint32_t expect = uint32_t((rlist.size() + CHUNK_RECORDS - 1) / CHUNK_RECORDS);
-        if (nc != expect && !(nc == 1 && rlist.empty())) throw std::runtime_error("learned: chunk count mismatch");
-        std::vector<uint64_t> coff(nc + 1);
-        coff[0] = 4 + 4ull * nc;
-        for (uint32_t c = 0; c < nc; ++c) {
-            uint32_t len;
-            std::memcpy(&len, p + 4 + 4 * c, 4);
-            coff[c + 1] = coff[c] + len;
+        std::vector<uint64_t> pos(Tn), first(Tn);
+        std::vector<uint8_t> strand(Tn);
+        uint64_t total = 0;
+        for (uint32_t r = 0; r < Tn; ++r) {
+            pos[r] = rec[r].pos;
+            strand[r] = rec[r].strand;
+            first[r] = total;
+            total += mis[r];
         }
-        if (coff[nc] != bytes) throw std::runtime_error("learned: stream length mismatch");
-        int bad = 0;
-#pragma omp parallel for schedule(dynamic) reduction(+ : bad)
-        for (int c = 0; c < int(nc); ++c) {
-            RangeDecoder dec(p + coff[c], size_t(coff[c + 1] - coff[c]));
-            BinModels bins;
-            const size_t r0 = size_t(c) * CHUNK_RECORDS, r1 = std::min(rlist.size(), r0 + CHUNK_RECORDS);
-            for (size_t ri = r0; ri < r1; ++ri) {
-                const DevRecord& r = rec[rlist[ri]];
-                const int m = mis[rlist[ri]];
-                int q = -1;
-                char prev = 0;  // read base decoded at the previous anchor
-                for (int j = 0; j <= m; ++j) {
-                    int idx[20];
-                    const int gmx = j < m ? Lr - 1 - q - (m - j) : 0;
-                    const int n =
-                        anchor_features(ref.data(), ref.size(), r.pos, q, Lr, r.strand, prev, m - j, gmx, idx);
-                    uint32_t fb[NB], fg[NG];
-                    model_freqs(T.model, idx, n, gmx, fb, fg);
-                    const Anchor& truth = ha[first[ri] + j];
-                    if (j > 0) {
-                        const uint32_t v = dec.peek(TOTAL);
-                        uint32_t cum = 0;
-                        int o = 0;
-                        while (cum + fb[o] <= v) cum += fb[o++];
-                        dec.consume(cum, fb[o]);
-                        if (o != truth.tbase) ++bad;
-                        prev = outcome_base(char(ref[r.pos + q]), o);
-                    }
-                    if (j < m) {
-                        uint32_t v = dec.peek(TOTAL), cum = 0;
-                        int gb = 0;
-                        while (cum + fg[gb] <= v) cum += fg[gb++];
-                        dec.consume(cum, fg[gb]);
-                        const int lo = gap_bin_lo(gb), hi = std::min(gap_bin_lo(gb + 1), gmx + 1);
-                        const int w = std::max(1, hi - lo);
-                        uint32_t oc, of;
-                        const uint32_t ov = dec.peek(bins.total(gb, w));
-                        const int o = bins.find(gb, w, ov, oc, of);
-                        dec.consume(oc, of);
-                        bins.update(gb, o);
-                        const int g = lo + o;
-                        if (g != truth.gap) ++bad;
-                        q = q + 1 + g;
-                    }
-                }
+        // what the block holds: offsets and bases from its anchors
+        std::vector<uint16_t> toff(total), off(total);
+        std::vector<char> tbase(total), base(total);
+        for (size_t k = 0; k < na; ++k) {
+            if (ha[k].tbase >= 0) continue;  // a record's start anchor
+            const uint32_t r = ha[k].rec;
+            int q = -1;
+            for (int j = 0; j < mis[r]; ++j) {
+                q += 1 + ha[k + j].gap;
+                toff[first[r] + j] = uint16_t(q);
+                tbase[first[r] + j] = outcome_base(char(ref[pos[r] + uint64_t(q)]), ha[k + j + 1].tbase);
             }
         }
-        *ok = bad == 0 ? 1 : 0;
+        const std::string why = decode_stream(T.model, static_cast<const uint8_t*>(data), bytes, ref.data(),
+                                              ref.size(), Lr, Tn, pos.data(), strand.data(), mis.data(), off.data(),
+                                              base.data());
+        *ok = why.empty() && off == toff && base == tbase ? 1 : 0;
     });
 }
 
@@ -864,6 +1119,25 @@ int curc_plain_mismatch_bytes(curc_ctx* ctx, uint64_t* out) {
         v.paired_end = b.p.paired_end;
         for (const auto& kv : b.host) v.streams[kv.first] = host::Buf{kv.second.ptr, kv.second.size};
         host::plain_mismatch_bytes(v, out);
+        return CURC_OK;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return CURC_ERR_STATE;
+    }
+}
+
+int curc_mismatch_general_bytes(curc_ctx* ctx, const char* bsc_path, const char* tmpdir, uint64_t* out) {
+    if (!ctx || !bsc_path || !tmpdir || !out) return CURC_ERR_ARG;
+    try {
+        const Block& b = *ctx->block;
+        host::BlockView v;
+        v.reads_count = b.n;
+        v.read_len = b.p.L;
+        for (const auto& kv : b.host) v.streams[kv.first] = host::Buf{kv.second.ptr, kv.second.size};
+        host::CoderParams cp;
+        cp.bsc_path = bsc_path;
+        cp.tmpdir = tmpdir;
+        host::general_mismatch_bytes(v, cp, out);
         return CURC_OK;
     } catch (const std::exception& e) {
         ctx->err = e.what();

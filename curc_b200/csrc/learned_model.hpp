@@ -16,6 +16,7 @@
 // frequencies.
 #pragma once
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -136,8 +137,9 @@ LM_HD int32_t requant(int32_t acc, int32_t m, int32_t sh) {
 }
 
 // Frequencies (total TOTAL) of the first `k` outcomes from their logits,
-// each >= 1; outcomes k .. n-1 cannot occur and get 0.
-LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, int n, uint32_t* f) {
+// each >= 1; outcomes k .. n-1 cannot occur and get 0.  `lut` and `zmul`
+// are the model's exponential table and logit scale.
+LM_HD void logits_to_freq_lut(const uint32_t* lut, int32_t zmul, const int32_t* z, int k, int n, uint32_t* f) {
     for (int j = k; j < n; ++j) f[j] = 0;
     int32_t mx = z[0];
     int am = 0;
@@ -150,9 +152,9 @@ LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, int n, uint32
     uint32_t e[NG];
     for (int j = 0; j < k; ++j) {
         const int64_t d = int64_t(mx) - z[j];
-        int64_t i = (d * M.zmul) >> 16;
+        int64_t i = (d * zmul) >> 16;
         if (i > LUTN - 1) i = LUTN - 1;
-        e[j] = M.lut[i];
+        e[j] = lut[i];
         tot += e[j];
     }
     uint32_t sum = 0;
@@ -161,6 +163,10 @@ LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, int n, uint32
         sum += f[j];
     }
     f[am] += TOTAL - sum;
+}
+
+LM_HD void logits_to_freq(const Model& M, const int32_t* z, int k, int n, uint32_t* f) {
+    logits_to_freq_lut(M.lut, M.zmul, z, k, n, f);
 }
 
 // The network at one anchor: base and gap frequencies (gap bins beyond the
@@ -305,6 +311,107 @@ private:
     size_t n_, i_ = 0;
     uint32_t code_ = 0, range_ = 0xFFFFFFFFu, r_ = 1;
 };
+
+// ------------------------------------------------------------ stream decoder
+// Records with mismatches are coded in chunks of this many records, each
+// chunk an independent range-coded stream (so chunks code and decode in
+// parallel).  Stream layout: u32 chunk count, u32 byte length per chunk,
+// then the chunks.
+constexpr size_t CHUNK_RECORDS = 16384;
+
+// Decodes a learned stream.  Records come in emission order with their
+// position on the main pseudogenome `ref` (ASCII, length rl), strand and
+// mismatch count; the mismatches of record r are written from index first[r]
+// = (counts of the records before it) on: their offsets along the read in
+// pseudogenome order, and the read bases.  Returns an error message, empty
+// when the stream decoded completely and consistently.
+inline std::string decode_stream(const Model& M, const uint8_t* p, size_t bytes, const uint8_t* ref, uint64_t rl,
+                                 int L, size_t records, const uint64_t* pos, const uint8_t* strand,
+                                 const uint8_t* cnt, uint16_t* off, char* base) {
+    std::vector<uint32_t> rlist;
+    std::vector<uint64_t> first;
+    uint64_t acc = 0;
+    for (size_t r = 0; r < records; ++r) {
+        if (cnt[r]) {
+            if (pos[r] > rl || uint64_t(L) > rl - pos[r]) return "a record lies outside the pseudogenome";
+            rlist.push_back(uint32_t(r));
+            first.push_back(acc);
+        }
+        acc += cnt[r];
+    }
+    if (bytes < 4) return "short learned stream";
+    uint32_t nc;
+    std::memcpy(&nc, p, 4);
+    const uint64_t expect = (rlist.size() + CHUNK_RECORDS - 1) / CHUNK_RECORDS;
+    if (nc != expect && !(nc == 1 && rlist.empty())) return "learned stream: chunk count disagrees with the records";
+    if (bytes < 4 + 4ull * nc) return "short learned stream";
+    std::vector<uint64_t> coff(size_t(nc) + 1);
+    coff[0] = 4 + 4ull * nc;
+    for (uint32_t c = 0; c < nc; ++c) {
+        uint32_t len;
+        std::memcpy(&len, p + 4 + 4 * size_t(c), 4);
+        coff[c + 1] = coff[c] + len;
+    }
+    if (coff[nc] != bytes) return "learned stream: length disagrees with its chunks";
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : bad)
+    for (int c = 0; c < int(nc); ++c) {
+        RangeDecoder dec(p + coff[c], size_t(coff[c + 1] - coff[c]));
+        BinModels bins;
+        const size_t r0 = size_t(c) * CHUNK_RECORDS, r1 = std::min(rlist.size(), r0 + CHUNK_RECORDS);
+        for (size_t ri = r0; ri < r1 && !bad; ++ri) {
+            const size_t r = rlist[ri];
+            const int m = cnt[r];
+            int q = -1;
+            char prev = 0;
+            for (int j = 0; j <= m; ++j) {
+                int idx[24];
+                const int gmx = j < m ? L - 1 - q - (m - j) : 0;
+                if (j < m && gmx < 0) {
+                    ++bad;
+                    break;
+                }
+                const int n = anchor_features(ref, rl, pos[r], q, L, strand[r], prev, m - j, gmx, idx);
+                uint32_t fb[NB], fg[NG];
+                model_freqs(M, idx, n, gmx, fb, fg);
+                if (j > 0) {
+                    const uint32_t v = dec.peek(TOTAL);
+                    uint32_t cum = 0;
+                    int o = 0;
+                    while (o < NB - 1 && cum + fb[o] <= v) cum += fb[o++];
+                    dec.consume(cum, fb[o]);
+                    prev = outcome_base(char(ref[pos[r] + uint64_t(q)]), o);
+                    base[first[ri] + uint64_t(j - 1)] = prev;
+                }
+                if (j < m) {
+                    uint32_t v = dec.peek(TOTAL), cum = 0;
+                    int gb = 0;
+                    while (gb < NG - 1 && cum + fg[gb] <= v) cum += fg[gb++];
+                    if (!fg[gb]) {
+                        ++bad;
+                        break;
+                    }
+                    dec.consume(cum, fg[gb]);
+                    const int lo = gap_bin_lo(gb), hi = std::min(gap_bin_lo(gb + 1), gmx + 1);
+                    const int w = hi - lo > 1 ? hi - lo : 1;
+                    uint32_t oc, of;
+                    const uint32_t ov = dec.peek(bins.total(gb, w));
+                    const int o = bins.find(gb, w, ov, oc, of);
+                    dec.consume(oc, of);
+                    bins.update(gb, o);
+                    const int g = lo + o;
+                    q = q + 1 + g;
+                    if (q > L - 1) {
+                        ++bad;
+                        break;
+                    }
+                    off[first[ri] + uint64_t(j)] = uint16_t(q);
+                }
+            }
+        }
+    }
+    return bad ? "learned stream does not decode consistently" : "";
+}
 
 }  // namespace learned
 }  // namespace curc

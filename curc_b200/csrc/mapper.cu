@@ -196,7 +196,7 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
 }
 
 template <bool RC>
-__global__ void __launch_bounds__(128) map_kernel(MapIndex ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
+__global__ void __launch_bounds__(256) map_kernel(MapIndex ix, const uint64_t* __restrict__ ref, uint64_t ref_len,
                                                   const uint64_t* __restrict__ udb, uint32_t U,
                                                   const uint8_t* __restrict__ ndb, uint32_t NN, int L, int W, int k,
                                                   int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
@@ -265,14 +265,15 @@ void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, cons
             sp_index.stop();
             SubStage sp_map(rc ? "mapping.map_rc" : "mapping.map_fwd");
             MapIndex ix{hs - 1, kr, pos, parts[q].start};
-            const int g = grid_for(uint64_t(total) * 32, 128);
+            const int mt = p.tune.map_threads;
+            const int g = grid_for(uint64_t(total) * 32, mt);
             unsigned long long* t = out.tally ? out.tally + 3 * rc : nullptr;
             if (rc)
-                map_kernel<true><<<g, 128, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
-                                                   out.strand, out.pos, t);
+                map_kernel<true><<<g, mt, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
+                                                  out.strand, out.pos, t);
             else
-                map_kernel<false><<<g, 128, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
-                                                    out.strand, out.pos, t);
+                map_kernel<false><<<g, mt, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
+                                                   out.strand, out.pos, t);
             CURC_LAUNCH_CHECK();
             a.release(mk);
         }

@@ -408,11 +408,11 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     // rejected by the comparison.  The reference sizes it to the prefix count
     // (get_hash_size); four times that keeps most probes of unlinkable
     // suffixes at one empty bucket instead of a binary search.
-    const uint32_t hs = hash_size_for(uint64_t(mp) * 4);
+    const uint32_t hs = hash_size_for(uint64_t(mp) * uint64_t(p.tune.table_factor));
     // presence bitmap, 16 bits per prefix (2^20..2^32 bits): a test that stays
     // in L2 rejects most suffixes without touching the bucket table
     int bbits = 20;
-    while (bbits < 32 && (1ull << bbits) < uint64_t(mp) * 16) ++bbits;
+    while (bbits < 32 && (1ull << bbits) < uint64_t(mp) * uint64_t(p.tune.bitmap_bits)) ++bbits;
     const uint64_t bwords = (1ull << bbits) / 32;
     uint32_t* present = a.alloc<uint32_t>(bwords);
     CURC_CHECK(cudaMemsetAsync(present, 0, bwords * 4, s));
@@ -486,7 +486,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     Compactor cp(ms, a, s);
     const int gp = resident_grid(probe_kernel, 512, ms ? ms : 1);
     const int gr = resident_grid(resolve_kernel, 512, ms ? ms : 1);
-    constexpr int CHECK_EVERY = 8;
+    const int CHECK_EVERY = p.tune.check_every;
     uint32_t passes = 0, active = ms;
     uint64_t links_seen = 0, active_sum = 0;
     const uint32_t ms0 = ms;

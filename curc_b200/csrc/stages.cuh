@@ -12,9 +12,20 @@ namespace curc {
 
 std::string& ctxless_error();
 
+// Launch and table choices that change no result (the autotuner's knobs):
+// the overlap index's bucket table size as a multiple of the prefix count
+// (the reference's get_hash_size is factor 1; equal strings share a bucket
+// whatever the size), bits of the prefix presence bitmap per prefix, how
+// many overlap passes run between host reads of the link count, and the
+// threads per block of the mapping kernel (one warp per read).
+struct Tuning {
+    int table_factor = 4, bitmap_bits = 16, check_every = 8, map_threads = 128;
+};
+
 struct BlockParams {
     int L = 0, W = 0, max_off = 0, k = 0, kip = 0, max_mm = 0;
     bool preserve_order = false, paired_end = false;
+    Tuning tune;
     static BlockParams derive(int L, bool po, bool pe) {  // preprocess.cpp:295-313
         BlockParams p;
         p.L = L;

@@ -226,6 +226,19 @@ def paired_repeats(seed: int = 1, pairs: int = 10_000_000, read_len: int = 150,
     return Workload(f"pe{read_len}_p{pairs}_g{genome_len}_s{seed}", read_len, m1, m2, preserve_order)
 
 
+def large_combined(seed: int = 4, n_reads: int = 40_000_000, read_len: int = 250,
+                   genome_len: int = 200_000_000) -> Workload:
+    """Single end, 45% GC genome with 8% covered by 0.5-10 kbp repeat copies at
+    0.5-2% divergence, substitutions rising from 0.1% at base 1 to 1.5% at the
+    last base, N at 0.02%, preserved order: the 40M x 250 bp case at its
+    default sizes."""
+    rng = np.random.default_rng(seed)
+    g = random_genome(rng, genome_len, gc=0.45, repeat_frac=0.08, repeat_len=(500, 10_000),
+                      repeat_div=(0.005, 0.02))
+    r = sample_single(rng, g, n_reads, read_len, position_ramp(read_len, 0.001, 0.015), 0.0002)
+    return Workload(f"se{read_len}_n{n_reads}_g{genome_len}_s{seed}", read_len, r, None, True)
+
+
 def position_ramp(read_len: int, lo: float, hi: float) -> np.ndarray:
     """Per-position error rate rising linearly from ``lo`` at base 1 to ``hi``
     at the last base."""

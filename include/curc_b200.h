@@ -86,6 +86,34 @@ int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint1
  * streams are always returned.  No reference counterpart. */
 int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep);
 
+/* Autotuner (no counterpart in the reference).  Knobs, in this order: the
+ * overlap index's bucket table size as a multiple of the prefix count
+ * {1, 2, 4, 8}, presence-bitmap bits per prefix {8, 16, 32}, overlap passes
+ * between host reads of the link count {2, 4, 8, 16}, threads per block of
+ * the mapping kernel {64, 128, 256}.  None changes any result: every stream
+ * is the same under every setting; only the time does.  curc_autotune runs
+ * the given block (device memory) under the candidates one knob at a time,
+ * keeps the fastest, and sets it on the context; with cache_path, choices
+ * are read from and saved to that file per (read length, read count rounded
+ * down to a power of two), and *from_cache tells whether the file had one.
+ * The k-mer length and the other derived parameters are part of the format
+ * and are not tuned. */
+int curc_ctx_set_tuning(curc_ctx* ctx, const int32_t* knobs);
+int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs);
+int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
+                  int paired_end, const char* cache_path, int* from_cache);
+
+/* Learned mode of whole-file compression (no counterpart in the reference;
+ * the plain coders are the reference's, src/compress.cu:1923-2146).  With a
+ * model set (the bytes curc_learn_model returns), curc_compress_files also
+ * codes each block's mismatch bases and offsets with the learned coder and
+ * keeps, per block, the smaller of the two codings; a learned block marks
+ * its mismatch-base container with the coder byte 100 (the reference's
+ * decoder cannot read such blocks, the product decoder can).  NULL or 0
+ * bytes restores plain mode, whose archives are the reference's byte for
+ * byte.  CURC_ERR_ARG when the size is not a model's. */
+int curc_ctx_set_mismatch_model(curc_ctx* ctx, const void* model, uint64_t bytes);
+
 /* Whole-file compression, the drop-in for `curc -c` (src/main.cpp:53-161,
  * src/preprocess.cpp:66-283 and the coders of src/compress.cu:1923-2146):
  * reads f1 (and f2 for paired end, else NULL) with the reference's block
@@ -207,6 +235,10 @@ int curc_learn_model(curc_learn* l, const void** ptr, uint64_t* bytes);
 int curc_learn_set_model(curc_learn* l, const void* ptr, uint64_t bytes);
 int curc_learn_encode(curc_learn* l, curc_ctx* ctx, const void** out, uint64_t* bytes);
 int curc_learn_decode_check(curc_learn* l, curc_ctx* ctx, const void* data, uint64_t bytes, int* ok);
+/* Test support: runs the tensor-core inference over the context's last
+ * block and recomputes each anchor's frequencies with the host integer
+ * model; *mismatched counts anchors whose frequencies differ. */
+int curc_learn_infer_check(curc_learn* l, curc_ctx* ctx, uint64_t* anchors, uint64_t* mismatched);
 /* Test support: loss and gradients of one FP32 forward/backward pass over n
  * dense inputs (n x 128) with base / gap targets (-1: none), for the parameter
  * vector `params` (curc_learn_param_count floats: W1 128x128, b1, W2 128x128,
@@ -217,6 +249,11 @@ int curc_learn_grad(curc_learn* l, const float* params, const float* x, const in
 /* Coded sizes, with the reference's plain coders, of the context's last
  * block's mismatch streams: out[0] counts, out[1] bases, out[2] offsets. */
 int curc_plain_mismatch_bytes(curc_ctx* ctx, uint64_t* out);
+/* Bytes of the same mismatch streams of the context's last block (counts,
+ * bases, offsets; each coded on its own) under fast-lzma2 level 10 (out[0])
+ * and libbsc through the bsc executable (out[1]), for comparison with the
+ * learned coder.  No counterpart in the reference. */
+int curc_mismatch_general_bytes(curc_ctx* ctx, const char* bsc_path, const char* tmpdir, uint64_t* out);
 
 /* Number of kernels the library has launched in this process (no
  * reference counterpart; used to report launches per benchmark step). */

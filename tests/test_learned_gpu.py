@@ -67,6 +67,21 @@ def test_gradients_match_float64():
     np.testing.assert_allclose(g, ref_g, rtol=1e-3, atol=1e-5)
 
 
+def test_tensor_core_inference_equals_host_model():
+    # the int8 network on tcgen05 (kind::i8, s32 accumulators in TMEM) must
+    # give every anchor exactly the frequencies of the host decoder's model
+    from curc_b200 import Context, Learner, synth
+    w = synth.paired_repeats(seed=77, pairs=40_000, genome_len=400_000, preserve_order=False,
+                             ti_tv=2.0, err=synth.position_ramp(150, 0.001, 0.01))
+    with Context(0) as ctx, Learner(0) as lrn:
+        ctx.block_run(w.sequences(), False, True)
+        lrn.add_block(ctx)
+        lrn.train(epochs=1, batch=2048)
+        n, bad = lrn.infer_check(ctx)
+    assert n > 1000
+    assert bad == 0, f"{bad} of {n} anchors differ from the host model"
+
+
 def test_learned_coder_is_lossless_and_smaller():
     from curc_b200.learned import train_and_evaluate
     r = train_and_evaluate(train_seeds=[101, 102, 103, 104], eval_seeds=[201], pairs=60_000, genome_len=600_000,
