@@ -773,7 +773,10 @@ def main():
     if r["batched"]:
         out["batched"] = r["batched"]
     if not a.no_learned and rank == 0:
-        out["learned_coder"] = learned_eval(a)
+        try:
+            out["learned_coder"] = learned_eval(a)
+        except Exception as e:  # reported, the rest of the line stands
+            out["learned_coder"] = {"error": str(e)[:300]}
     if not a.no_cpu_baseline and world == 1:
         out["cpu_baseline"] = cpu_baseline(a)
     print(json.dumps(out))
