@@ -146,12 +146,13 @@ def pack_bytes(n, L):
 # Algorithmic bytes of the overlap probe kernel (its launches over all
 # passes), with one 32-byte sector per random access: per listed suffix its
 # k-mer (32); per bucket searched the bucket range (32); per prefix
-# comparison the prefix id (32) and row (32 * ceil(8W/32)); per hit the run
-# slot (32).  Counts come from the kernel's own counters.
+# comparison the prefix entry, id and first word (32); per prefix row read
+# (only when the first 32 bases agree) the row (32 * ceil(8W/32)); per hit
+# the run slot (32).  Counts come from the kernel's own counters.
 def probe_bytes(st, L):
     row = 32 * -(-8 * ((L + 31) // 32) // 32)
-    return (32 * st["overlap_probes"] + 32 * st["overlap_searched"] + (32 + row) * st["overlap_compares"]
-            + 32 * st["overlap_hits"])
+    return (32 * st["overlap_probes"] + 32 * st["overlap_searched"] + 32 * st["overlap_compares"]
+            + row * st.get("overlap_rows", 0) + 32 * st["overlap_hits"])
 
 
 # Algorithmic bytes of the first-word read sort (sub-stage sort_dedupe.radix):
@@ -250,7 +251,7 @@ def run_ours(a, rank, world):
         dev_step()
     stage_names = ["pack", "sort_dedupe", "overlap", "chain_filter", "full_match", "assembly", "mapping", "emit",
                    "unmapped_refs", "refmatch"]
-    sub_names = ["sort_dedupe.radix", "overlap.index", "overlap.index_sort", "overlap.index_mask",
+    sub_names = ["pack.kernel", "sort_dedupe.first_word", "sort_dedupe.radix", "overlap.index", "overlap.index_sort", "overlap.index_mask",
                  "overlap.probe_resolve", "overlap.filter", "overlap.probe", "overlap.resolve", "overlap.compact",
                  "full_match.resort", "full_match.groups", "full_match.compact", "assembly.ranking", "assembly.walk", "assembly.jump",
                  "assembly.order_place", "mapping.index_fwd", "mapping.map_fwd", "mapping.index_rc", "mapping.map_rc",
@@ -309,7 +310,7 @@ def run_ours(a, rank, world):
                       "unmapped_n", "overlap_passes", "contested", "records", "mismatches",
                       "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits",
                       "overlap_searched", "overlap_compares", "overlap_links", "map_reads_fwd", "map_probes_fwd",
-                      "map_candidates_fwd", "map_reads_rc", "map_probes_rc", "map_candidates_rc"],
+                      "map_candidates_fwd", "map_reads_rc", "map_probes_rc", "map_candidates_rc", "overlap_rows"],
                      [int(x) for x in ctx.get("stats", np.uint64)]))
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     step_s = dev_ms / 1000.0 / a.steps
@@ -694,7 +695,7 @@ def main():
         finish_dist(world)
         return
     peak, peak_kind = hbm_peak()
-    pack_ms = r["stage_ms"]["pack"]
+    pack_ms = r["substage_ms"].get("pack.kernel") or r["stage_ms"]["pack"]
     dominant = max(r["stage_ms"], key=r["stage_ms"].get)
     achieved = pack_bytes(r["n"], r["L"]) / (pack_ms / 1000.0) / 1e9 if pack_ms > 0 else None
     st = r["stats"]
@@ -746,14 +747,17 @@ def main():
                      "algorithmic_bytes_per_launch": probe_bytes(st, r["L"]) / passes, "launches": passes,
                      "ms_per_launch": probe_ms / passes,
                      "traffic_source": "ncu dram bytes per probe on the 2M-pair case, times this launch's probes"},
-        "roofline_pack": {"kernel": "pack_kernel (stage a1)", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "roofline_pack": {"kernel": "pack_kernel (stage a1, sub-stage pack.kernel)", "bound": "hbm",
+                          "achieved": achieved, "peak": peak,
                           "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                           "traffic": None},
-        "roofline_sort": roof("first-word LSD radix sort of the reads (sub-stage sort_dedupe.radix, stage a2)",
-                              sort_bytes(m_reads, r["L"]), sub.get("sort_dedupe.radix", 0.0), 1,
+        "roofline_sort": roof("first-word LSD radix sort of the reads (gather + 8 passes, sub-stage "
+                              "sort_dedupe.first_word, stage a2)",
+                              sort_bytes(m_reads, r["L"]), sub.get("sort_dedupe.first_word", 0.0), 1,
                               {"frac_of_lower_bound": (sort_lower_bound_bytes(m_reads, r["L"]) /
-                                                       (sub["sort_dedupe.radix"] / 1000.0) / 1e9 / peak)
-                               if sub.get("sort_dedupe.radix") else None}),
+                                                       (sub["sort_dedupe.first_word"] / 1000.0) / 1e9 / peak)
+                               if sub.get("sort_dedupe.first_word") else None,
+                               "whole_sort_ms": sub.get("sort_dedupe.radix")}),
         "roofline_resolve": roof("resolve_kernel (overlap passes, stage a4)", resolve_bytes(st, r["L"]),
                                  sub.get("overlap.resolve", 0.0), passes),
         "roofline_map": roof("map_kernel forward + reverse complement (stage a9)",

@@ -69,7 +69,10 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     T.begin("pack");
     db = arena.alloc<uint64_t>(size_t(n) * W + 1);
     uint8_t* has_n = arena.alloc<uint8_t>(n ? n : 1);
-    pack_reads(d_seq, n, L, db, has_n, err, s);
+    {
+        SubStage sp("pack.kernel");  // the packing kernel alone (the stage also splits and reads counts back)
+        pack_reads(d_seq, n, L, db, has_n, err, s);
+    }
     reads_id = arena.alloc<uint32_t>(n ? n : 1);
     n_ids = arena.alloc<uint32_t>(n ? n : 1);
     split_n_reads(has_n, n, reads_id, n_ids, counts, arena, s);

@@ -39,7 +39,7 @@ struct __align__(16) Anchor {
     uint8_t nidx;
     int8_t tbase;   // base outcome at this anchor's mismatch (-1: start anchor)
     int8_t tgap;    // gap bin to the next mismatch (-1: none)
-    uint8_t pad0;
+    uint8_t strand; // the record's strand
     uint16_t gap;   // gap to the next mismatch
     uint16_t gmax;  // largest valid gap from this anchor
     uint32_t rec;   // record index
@@ -136,7 +136,7 @@ __global__ void anchors_kernel(const DevRecord* __restrict__ rec, const uint8_t*
         }
         // the next mismatch leaves room for the m - j - 1 after it
         x.gmax = uint16_t(gmx);
-        x.pad0 = 0;
+        x.strand = r.strand;
         x.rec = i;
         a[j] = x;
     }
@@ -260,8 +260,8 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 //     x W2^T, four K=32 steps issued by one thread; the thread of each
 //     anchor reads its row back (tcgen05.ld), adds the bias, requantises and
 //     stores it as the next A operand;
-//   layer 3: the same with N = 32 (the 20 output rows of W3, zero padded);
-//     each thread turns its 20 logits into frequencies.
+//   layer 3: the same with N = 32 (the OUT = 28 output rows of W3, zero
+//     padded); each thread turns its logits into frequencies.
 // Integer accumulation is exact in any order, so the frequencies equal the
 // host model's (learned_model.hpp) bit for bit.  Operands live in shared
 // memory in the no-swizzle K-major core-matrix layout: 8 rows x 16 bytes per
@@ -272,6 +272,7 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 
 constexpr int TC_ROWS = 128;                 // anchors per tile (MMA M)
 constexpr int TC_N3 = 32;                    // padded output rows of layer 3
+static_assert(OUT <= TC_N3, "layer 3 outputs exceed the padded MMA width");
 constexpr int W1T_STRIDE = HID + 4;          // bytes per input row of W1^T (bank spread)
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
 constexpr uint32_t TC_TMEM_COLS = 128;
@@ -674,6 +675,7 @@ void infer(const Model& model, const Anchor* a, uint32_t n, uint16_t* fq, Arena&
 // The learned stream of a block (its anchors listed and the network run on
 // the GPU, the range coding on the host, chunks of records in parallel).
 std::string encode_stream(const Model& model, Block& b) {
+    const int L = b.p.L;
     auto mk = b.arena.mark();
     uint32_t na = 0;
     Anchor* a = block_anchors(b, b.arena, &na);
@@ -701,9 +703,11 @@ std::string encode_stream(const Model& model, Block& b) {
         RangeEncoder enc;
         BinModels bins;
         double cb[3] = {0, 0, 0};
+        int q = -1;  // the anchor's offset along the read, in pseudogenome order
         for (size_t k = cut[c]; k < cut[c + 1]; ++k) {
             const Anchor& x = ha[k];
             const uint16_t* f = &hf[k * OUT];
+            if (x.tbase < 0) q = -1;  // a record's start anchor
             if (x.tbase >= 0) {
                 uint32_t cum = 0;
                 for (int j = 0; j < x.tbase; ++j) cum += f[j];
@@ -717,11 +721,13 @@ std::string encode_stream(const Model& model, Block& b) {
                 cb[1] -= std::log2(double(f[NB + x.tgap]) / TOTAL);
                 const int lo = gap_bin_lo(x.tgap);
                 const int hi = std::min(gap_bin_lo(x.tgap + 1), int(x.gmax) + 1);
+                const int bc = bin_context(q, L, x.strand);
                 uint32_t oc, of, ot;
-                bins.lookup(x.tgap, x.gap - lo, hi - lo, oc, of, ot);
+                bins.lookup(bc, x.tgap, x.gap - lo, hi - lo, oc, of, ot);
                 enc.encode(oc, of, ot);
                 cb[2] -= std::log2(double(of) / ot);
-                bins.update(x.tgap, x.gap - lo);
+                bins.update(bc, x.tgap, x.gap - lo);
+                q += 1 + x.gap;
             }
         }
         chunks[c] = enc.finish();

@@ -34,15 +34,17 @@ namespace learned {
 constexpr int IN = 128;      // input features (one-hots, zero padded)
 constexpr int HID = 128;     // hidden units per layer
 constexpr int NB = 4;        // base outcomes: the three other bases, then N
-constexpr int NG = 16;       // gap bins
+constexpr int NG = 24;       // gap bins
 constexpr int OUT = NB + NG;
 constexpr int CTX = 16;      // pseudogenome bases around an anchor
 constexpr int LUTN = 256;    // exponential table entries
 constexpr uint32_t TOTAL = 4096;  // frequency total (12 bits)
 
-// Gap bins: [lo, lo + width) with widths 1,1,1,1,2,2,4,4,8,8,16,16,32,32,64,320.
+// Gap bins: [lo, lo + width) with widths 1 x4, 2 x4, 4 x4, 8 x4, 16 x4, 32 x2,
+// 64 and 260 (gaps of reads up to 512 bases).
 LM_HD int gap_bin_lo(int b) {
-    constexpr int lo[NG + 1] = {0, 1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 512};
+    constexpr int lo[NG + 1] = {0,  1,  2,  3,  4,  6,   8,   10,  12,  16,  20,  24, 28,
+                                36, 44, 52, 60, 76, 92, 108, 124, 156, 188, 252, 512};
     return lo[b];
 }
 LM_HD int gap_bin(int g) {
@@ -193,56 +195,65 @@ LM_HD void model_freqs(const Model& M, const int* idx, int nidx, int gmax, uint3
     logits_to_freq(M, z + NB, gap_bin(gmax < 0 ? 0 : gmax) + 1, NG, fg);
 }
 
+// Context of the adaptive in-bin models: the read's strand and where the
+// anchor lies along the read (8 buckets in pseudogenome order), since the
+// error rate, and with it the spread of a gap inside its bin, depends on
+// the sequencing cycle.
+constexpr int BIN_CTX = 16;
+LM_HD int bin_context(int q, int L, int strand) { return (strand ? 8 : 0) + ((q + 1) * 8) / (L + 1); }
+
 // Adaptive frequencies of the offset inside each gap bin (the network gives
-// the bin): reset at the start of each independently coded chunk, updated
-// after every coded gap in the same way by the encoder and the decoder.
+// the bin), one set per bin context: reset at the start of each
+// independently coded chunk, updated after every coded gap in the same way
+// by the encoder and the decoder.
 class BinModels {
 public:
     static constexpr uint32_t INC = 24, LIMIT = 1u << 15;
     BinModels() {
-        for (int b = 0; b < NG; ++b) {
-            f_[b].assign(size_t(gap_bin_lo(b + 1) - gap_bin_lo(b)), 1);
-            tot_[b] = uint32_t(f_[b].size());
-        }
+        for (int c = 0; c < BIN_CTX; ++c)
+            for (int b = 0; b < NG; ++b) {
+                f_[c][b].assign(size_t(gap_bin_lo(b + 1) - gap_bin_lo(b)), 1);
+                tot_[c][b] = uint32_t(f_[c][b].size());
+            }
     }
     // cumulative count, count and total of offset o among the first w offsets
-    void lookup(int b, int o, int w, uint32_t& cum, uint32_t& freq, uint32_t& total) const {
+    void lookup(int c, int b, int o, int w, uint32_t& cum, uint32_t& freq, uint32_t& total) const {
         cum = 0;
         total = 0;
         for (int j = 0; j < w; ++j) {
-            if (j < o) cum += f_[b][j];
-            total += f_[b][j];
+            if (j < o) cum += f_[c][b][j];
+            total += f_[c][b][j];
         }
-        freq = f_[b][o];
+        freq = f_[c][b][o];
     }
     // offset whose cumulative range holds v, among the first w offsets
-    int find(int b, int w, uint32_t v, uint32_t& cum, uint32_t& freq) const {
+    int find(int c, int b, int w, uint32_t v, uint32_t& cum, uint32_t& freq) const {
         cum = 0;
         int o = 0;
-        while (o + 1 < w && cum + f_[b][o] <= v) cum += f_[b][o++];
-        freq = f_[b][o];
+        while (o + 1 < w && cum + f_[c][b][o] <= v) cum += f_[c][b][o++];
+        freq = f_[c][b][o];
         return o;
     }
-    uint32_t total(int b, int w) const {
+    uint32_t total(int c, int b, int w) const {
         uint32_t t = 0;
-        for (int j = 0; j < w; ++j) t += f_[b][j];
+        for (int j = 0; j < w; ++j) t += f_[c][b][j];
         return t;
     }
-    void update(int b, int o) {
-        f_[b][o] += INC;
-        tot_[b] += INC;
-        if (tot_[b] > LIMIT) {
-            tot_[b] = 0;
-            for (auto& x : f_[b]) {
+    void update(int c, int b, int o) {
+        f_[c][b][o] += INC;
+        tot_[c][b] += INC;
+        if (tot_[c][b] > LIMIT) {
+            tot_[c][b] = 0;
+            for (auto& x : f_[c][b]) {
                 x = (x + 1) / 2;
-                tot_[b] += x;
+                tot_[c][b] += x;
             }
         }
     }
 
 private:
-    std::vector<uint32_t> f_[NG];
-    uint32_t tot_[NG];
+    std::vector<uint32_t> f_[BIN_CTX][NG];
+    uint32_t tot_[BIN_CTX][NG];
 };
 
 // ------------------------------------------------------------ range coder
@@ -394,11 +405,12 @@ inline std::string decode_stream(const Model& M, const uint8_t* p, size_t bytes,
                     dec.consume(cum, fg[gb]);
                     const int lo = gap_bin_lo(gb), hi = std::min(gap_bin_lo(gb + 1), gmx + 1);
                     const int w = hi - lo > 1 ? hi - lo : 1;
+                    const int bc = bin_context(q, L, strand[r]);
                     uint32_t oc, of;
-                    const uint32_t ov = dec.peek(bins.total(gb, w));
-                    const int o = bins.find(gb, w, ov, oc, of);
+                    const uint32_t ov = dec.peek(bins.total(bc, gb, w));
+                    const int o = bins.find(bc, gb, w, ov, oc, of);
                     dec.consume(oc, of);
-                    bins.update(gb, o);
+                    bins.update(bc, gb, o);
                     const int g = lo + o;
                     q = q + 1 + g;
                     if (q > L - 1) {

@@ -115,6 +115,7 @@ struct OverlapCtx {
     const uint32_t* present;  // bitmap of prefix k-mer hashes (high 32 bits)
     uint32_t bmask;
     const uint32_t* va;  // prefix ids sorted by (bucket, read)
+    const uint64_t* vw0; // first packed word of each prefix, in va order
     const uint32_t* kr;  // bucket ranges
     uint32_t* free_cnt;  // per bucket: prefixes without a predecessor
     uint32_t* bfree;     // per bucket: free_cnt != 0 (one bit, stays in L2)
@@ -191,13 +192,28 @@ struct ProbeListMove {
     __device__ void operator()(uint32_t j, uint32_t d) const { plist[d] = j; }
 };
 
+// Three-way compare of prefix entry `it` ([0, cl)) with the suffix's
+// [off, off + cl): the first 32 bases from the prefix's first word, stored
+// beside its id, so most comparisons need no row of the prefix; only when
+// they agree and more bases follow is the row read (counted in `rows`).
+__device__ __forceinline__ int cmp_prefix(const OverlapCtx& c, uint32_t it, const uint64_t* sr, int off, int cl,
+                                          uint32_t& rows) {
+    const int nb = cl < 32 ? cl : 32;
+    const uint64_t x = c.vw0[it] >> (64 - 2 * nb);
+    const uint64_t y = word_at(sr, off, nb);
+    if (x != y) return x < y ? -1 : 1;
+    if (cl <= 32) return 0;
+    ++rows;
+    return cmp_span(c.db + uint64_t(c.va[it]) * c.W, 32, sr, off + 32, cl - 32);
+}
+
 // compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
 // bound of suffix[off, L) among the bucket's prefix[0, L-off).  Returns
 // whether an equal prefix exists; then the hit (list index, run start,
 // bucket end, bucket) is set and the suffix joins the run's claimers.
 __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* __restrict__ sufw, uint32_t j, int off,
                                           RunSlot* __restrict__ run, uint32_t* __restrict__ gnext, uint4& hitrec,
-                                          uint32_t& searched, uint32_t& compares) {
+                                          uint32_t& searched, uint32_t& compares, uint32_t& rows) {
     const int cl = c.L - off;
     const uint64_t* sr = sufw + uint64_t(j) * c.W;
     const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
@@ -212,7 +228,7 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
     while (count > 0) {
         ++compares;
         const uint32_t step = count / 2, it = lo + step;
-        if (cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl) < 0) {
+        if (cmp_prefix(c, it, sr, off, cl, rows) < 0) {
             lo = it + 1;
             count -= step + 1;
         } else {
@@ -221,7 +237,7 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
     }
     if (lo >= e) return false;
     ++compares;
-    if (cmp_span(c.db + uint64_t(c.va[lo]) * c.W, 0, sr, off, cl) != 0) return false;
+    if (cmp_prefix(c, lo, sr, off, cl, rows) != 0) return false;
     // run membership: count, lowest list index, and a list of members
     atomicAdd(&run[lo].claim, 1u);
     atomicMin(&run[lo].lead, j);
@@ -233,7 +249,8 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
 // Probes every listed suffix and lists the hits (hlist, *hcount; their
 // order is immaterial to the resolution).  tally[0] counts probes,
 // tally[1] hits, tally[4] probes that searched a bucket, tally[5] prefix
-// comparisons (for the algorithmic bytes of the pass).
+// comparisons, tally[6] prefix rows read (for the algorithmic bytes of
+// the pass).
 __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
                                                     const uint32_t* __restrict__ plist,
                                                     const uint32_t* __restrict__ pcount, int off,
@@ -242,7 +259,7 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
                                                     unsigned long long* __restrict__ tally) {
     __shared__ uint4 s_hits[512];
     __shared__ uint32_t s_n, s_base;
-    uint32_t probes = 0, hits = 0, searched = 0, compares = 0;
+    uint32_t probes = 0, hits = 0, searched = 0, compares = 0, rows = 0;
     const uint32_t np = *pcount;
     for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < np; b0 += gridDim.x * blockDim.x) {
         const uint32_t q = b0 + threadIdx.x;
@@ -250,7 +267,7 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
         uint4 rec;
         if (q < np) {
             ++probes;
-            hit = probe_one(c, sufw, plist[q], off, run, gnext, rec, searched, compares);
+            hit = probe_one(c, sufw, plist[q], off, run, gnext, rec, searched, compares, rows);
             hits += hit;
         }
         if (threadIdx.x == 0) s_n = 0;
@@ -266,6 +283,7 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
     block_tally<unsigned long long>(hits, &tally[1]);
     block_tally<unsigned long long>(searched, &tally[4]);
     block_tally<unsigned long long>(compares, &tally[5]);
+    block_tally<unsigned long long>(rows, &tally[6]);
 }
 
 // A suffix alone on its run links directly.  A run claimed by several
@@ -417,7 +435,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     uint32_t* present = a.alloc<uint32_t>(bwords);
     CURC_CHECK(cudaMemsetAsync(present, 0, bwords * 4, s));
     OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, present, uint32_t((1ull << bbits) - 1), pre, nullptr, nullptr,
-                 nullptr, next, prev, offset};
+                 nullptr, nullptr, next, prev, offset};
     uint32_t* keys = a.alloc<uint32_t>(mp ? mp : 1);
     SubStage sp_sort("overlap.index_sort");
     if (mp) {
@@ -426,6 +444,9 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         CURC_LAUNCH_CHECK();
         radix_sort_pairs<uint32_t, uint32_t>(keys, pre, mp, 0, log2_exact(hs), a, s);
     }
+    uint64_t* vw0 = a.alloc<uint64_t>(mp ? mp : 1);
+    if (mp) gather_words(db, pre, mp, p.W, 0, vw0, s);
+    c.vw0 = vw0;
     uint32_t* kr = a.alloc<uint32_t>(size_t(hs) + 2);
     CURC_CHECK(cudaMemsetAsync(kr, 0, (size_t(hs) + 2) * sizeof(uint32_t), s));
     if (mp) {
@@ -469,8 +490,8 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     }
     sp_mask.stop();
     // probes, probes that met a prefix, links, contested members
-    unsigned long long* tally = a.alloc<unsigned long long>(6);
-    CURC_CHECK(cudaMemsetAsync(tally, 0, 48, s));
+    unsigned long long* tally = a.alloc<unsigned long long>(7);
+    CURC_CHECK(cudaMemsetAsync(tally, 0, 56, s));
     sp_index.stop();
 
     // List of size ms, of which `active` are unlinked; compacted once half
@@ -547,8 +568,8 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     }
     cp.check();
     if (st) {
-        unsigned long long t[6];
-        read_small(t, tally, 48, s);
+        unsigned long long t[7];
+        read_small(t, tally, 56, s);
         st->passes = passes;
         st->links = uint32_t(t[2]);
         st->contested = uint32_t(t[3]);
@@ -558,6 +579,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         st->hits = t[1];
         st->searched = t[4];
         st->compares = t[5];
+        st->rows = t[6];
     }
     a.release(mk);
 }

@@ -5,8 +5,9 @@
 //
 // B200 design: a persistent grid walks tiles of 64 reads.  Each tile is
 // 64*L contiguous bytes, moved into shared memory by a 1D TMA bulk copy
-// (cp.async.bulk + mbarrier) one tile ahead of the compute, so HBM reads
-// are full-line and overlap the packing.  The block then works in two
+// (cp.async.bulk + mbarrier) two tiles ahead of the compute (three stages),
+// so HBM reads are full-line, enough bytes are in flight per SM, and the
+// copies overlap the packing.  The block then works in two
 // conflict-free passes: every thread turns 16-byte groups of the tile into
 // 32 bits of codes (one 16-byte shared-memory load each), giving the tile's
 // bases as one contiguous 2-bit string, and then every thread cuts one
@@ -23,6 +24,7 @@ namespace curc {
 
 namespace {
 constexpr int PACK_READS = 64;
+constexpr int PACK_STAGES = 3;  // tiles in flight per block: PACK_STAGES - 1 copies ahead of the compute
 constexpr uint32_t WAIT_LIMIT = 1u << 26;
 constexpr int MAX_DEVICES = 64;
 
@@ -81,18 +83,20 @@ __device__ __forceinline__ bool acgt4(uint32_t x) {
 // its codes (4*L words of 16 bases, and 4 zero words after them).
 __host__ __device__ inline uint32_t pack_tile_stride(int L) { return (uint32_t(PACK_READS) * L + 127u) & ~127u; }
 __host__ __device__ inline uint32_t pack_code_words(int L) { return 4u * uint32_t(L) + 4u; }
-inline size_t pack_smem_bytes(int L) { return 2 * (size_t(pack_tile_stride(L)) + 4 * size_t(pack_code_words(L))); }
+inline size_t pack_smem_bytes(int L) {
+    return PACK_STAGES * (size_t(pack_tile_stride(L)) + 4 * size_t(pack_code_words(L)));
+}
 
 __global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ seq, uint64_t n, int L, int W,
                                                    bool use_tma, uint64_t* __restrict__ packed,
                                                    uint8_t* __restrict__ has_n, uint32_t* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bar[2];
-    __shared__ uint8_t nflag[2][PACK_READS];
+    __shared__ __align__(8) uint64_t bar[PACK_STAGES];
+    __shared__ uint8_t nflag[PACK_STAGES][PACK_READS];
     const uint32_t tile_bytes = uint32_t(PACK_READS) * uint32_t(L);
     const uint32_t groups = tile_bytes / 16;  // 4*L
     const uint32_t stride = pack_tile_stride(L);
-    uint32_t* codes_base = reinterpret_cast<uint32_t*>(smem + 2 * stride);
+    uint32_t* codes_base = reinterpret_cast<uint32_t*>(smem + PACK_STAGES * stride);
     const uint32_t cw = pack_code_words(L);
     const uint64_t tiles = div_up(n, PACK_READS);
     auto full = [&](uint64_t t) { return (t + 1) * PACK_READS <= n; };
@@ -101,30 +105,37 @@ __global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ s
         bulk_g2s(smem + stage * stride, seq + t * uint64_t(PACK_READS) * L, tile_bytes, &bar[stage]);
     };
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int st = 0; st < PACK_STAGES; ++st) mbar_init(&bar[st], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (uint32_t i = threadIdx.x; i < 2 * PACK_READS; i += blockDim.x) nflag[i / PACK_READS][i % PACK_READS] = 0;
-    if (threadIdx.x < 8) codes_base[(threadIdx.x / 4) * cw + groups + threadIdx.x % 4] = 0;
+    for (uint32_t i = threadIdx.x; i < PACK_STAGES * PACK_READS; i += blockDim.x)
+        nflag[i / PACK_READS][i % PACK_READS] = 0;
+    if (threadIdx.x < 4 * PACK_STAGES) codes_base[(threadIdx.x / 4) * cw + groups + threadIdx.x % 4] = 0;
     __syncthreads();
     // this thread's output column: word w0 of reads r0, r0 + 32, ...
     const uint32_t r0 = threadIdx.x / uint32_t(W), w0 = threadIdx.x - r0 * uint32_t(W);
     const int nb = min(32, L - int(w0) * 32);
     const uint64_t tail_mask = nb < 32 ? ~0ull << (64 - 2 * nb) : ~0ull;
     uint64_t t = blockIdx.x;
-    if (use_tma && threadIdx.x == 0 && t < tiles && full(t)) issue(t, 0);
-    uint32_t pending = (use_tma && t < tiles && full(t)) ? 1u : 0u;  // bit s: a copy into stage s is in flight
+    uint32_t pending = 0;  // bit s: a copy into stage s is in flight
+    for (int j = 0; j + 1 < PACK_STAGES; ++j) {
+        const uint64_t tj = t + uint64_t(j) * gridDim.x;
+        if (use_tma && tj < tiles && full(tj)) {
+            if (threadIdx.x == 0) issue(tj, j);
+            pending |= 1u << j;
+        }
+    }
     uint32_t it = 0;
     for (; t < tiles; t += gridDim.x, ++it) {
-        const int stage = it & 1;
-        const uint64_t nt = t + gridDim.x;
+        const int stage = int(it % PACK_STAGES);
+        const int ahead = int((it + PACK_STAGES - 1) % PACK_STAGES);  // the stage iteration it-1 used
+        const uint64_t nt = t + uint64_t(PACK_STAGES - 1) * gridDim.x;
         if (use_tma && nt < tiles && full(nt)) {
             if (threadIdx.x == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue(nt, stage ^ 1);
+                issue(nt, ahead);
             }
-            pending |= 1u << (stage ^ 1);
+            pending |= 1u << ahead;
         }
         uint8_t* buf = smem + stage * stride;
         uint32_t* codes = codes_base + stage * cw;
@@ -134,7 +145,7 @@ __global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ s
         if (pending >> stage & 1u) {
             uint32_t spins = 0;
             bool late = false;
-            while (!mbar_try_wait(&bar[stage], (it >> 1) & 1)) {
+            while (!mbar_try_wait(&bar[stage], (it / PACK_STAGES) & 1)) {
                 if (++spins > WAIT_LIMIT) {  // never expected
                     late = true;
                     break;
@@ -148,10 +159,12 @@ __global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ s
                 // tell, no bulk copy still targets this block's shared memory
                 if (threadIdx.x == 0) {
                     atomicExch(err, 1u);
-                    const int other = stage ^ 1;
-                    if (pending >> other & 1u) {
-                        const uint32_t par = ((it + 1) >> 1) & 1;
-                        for (uint32_t w = 0; w < WAIT_LIMIT && !mbar_try_wait(&bar[other], par); ++w) {
+                    for (int d = 1; d < PACK_STAGES; ++d) {
+                        const int other = int((it + d) % PACK_STAGES);  // holds the copy for iteration it + d
+                        if (pending >> other & 1u) {
+                            const uint32_t par = ((it + d) / PACK_STAGES) & 1;
+                            for (uint32_t w = 0; w < WAIT_LIMIT && !mbar_try_wait(&bar[other], par); ++w) {
+                            }
                         }
                     }
                 }

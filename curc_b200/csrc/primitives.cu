@@ -4,6 +4,8 @@
 #include <cstring>
 #include <stdexcept>
 
+#include <mutex>
+
 #include "primitives.cuh"
 
 namespace curc {
@@ -384,20 +386,54 @@ __global__ void __launch_bounds__(RS_THREADS) rs_hist_kernel(const K* __restrict
 
 // Stable scatter: items are ranked in index order.  Within a round of 256
 // items, a warp ranks equal digits with match_any; warps are ordered by a
-// per-round prefix over per-warp counts; rounds accumulate per digit.
+// per-round prefix over per-warp counts; rounds accumulate per digit.  The
+// tile is first reordered by digit in shared memory (its digit counts come
+// from the scanned histogram: the difference of consecutive offsets), then
+// written out in that order, so that items of one digit leave as one
+// contiguous run and the stores coalesce.
 template <class K, class V>
 __global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const K* __restrict__ kin, const V* __restrict__ vin,
                                                                 K* __restrict__ kout, V* __restrict__ vout, size_t n,
                                                                 int shift, uint32_t mask,
                                                                 const uint32_t* __restrict__ offsets, uint32_t tiles) {
+    extern __shared__ __align__(16) uint8_t rs_smem[];
+    K* sk = reinterpret_cast<K*>(rs_smem);
+    V* sv = reinterpret_cast<V*>(rs_smem + sizeof(K) * RS_TILE);
     __shared__ uint32_t gbase[256];
+    __shared__ uint32_t tstart[256];
     __shared__ uint32_t run[256];
     __shared__ uint32_t wcnt[RS_WARPS][256];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    gbase[tid] = offsets[size_t(tid) * tiles + blockIdx.x];
+    {
+        // this tile's count of digit tid, from the exclusive scan over
+        // (digit, tile): the next flattened entry minus this one
+        const size_t fi = size_t(tid) * tiles + blockIdx.x;
+        const uint32_t g = offsets[fi];
+        const uint32_t nx = fi + 1 < size_t(256) * tiles ? offsets[fi + 1] : uint32_t(n);
+        gbase[tid] = g;
+        tstart[tid] = nx - g;
+    }
     run[tid] = 0;
+    __syncthreads();
+    // exclusive scan of the tile's digit counts (256 entries, one per thread)
+    {
+        uint32_t v = tstart[tid];
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wcnt[0][warp] = x;
+        __syncthreads();
+        uint32_t wbase = 0;
+        for (int w = 0; w < warp; ++w) wbase += wcnt[0][w];
+        __syncthreads();
+        tstart[tid] = wbase + x - v;
+    }
     const uint32_t lt_mask = (1u << lane) - 1u;
     const size_t base = size_t(blockIdx.x) * RS_TILE;
+    const uint32_t items = uint32_t(min(size_t(RS_TILE), n - base));
     for (int r = 0; r < RS_ROUNDS; ++r) {
         const size_t idx = base + size_t(r) * RS_THREADS + tid;
         if (base + size_t(r) * RS_THREADS >= n) break;  // uniform across the block
@@ -426,12 +462,42 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const K* __restr
         }
         __syncthreads();
         if (valid) {
-            const uint32_t pos = gbase[d] + run[d] + wcnt[warp][d] + rank;
-            kout[pos] = k;
-            if (vout) vout[pos] = v;
+            const uint32_t lp = tstart[d] + run[d] + wcnt[warp][d] + rank;
+            sk[lp] = k;
+            if (vin) sv[lp] = v;
         }
         __syncthreads();
         run[tid] += acc;
+    }
+    __syncthreads();
+    // the tile in digit order: runs of one digit go to consecutive places
+    for (uint32_t p = tid; p < items; p += RS_THREADS) {
+        const K k = sk[p];
+        const uint32_t d = digit_of(k, shift, mask);
+        const uint32_t gpos = gbase[d] + (p - tstart[d]);
+        kout[gpos] = k;
+        if (vout) vout[gpos] = sv[p];
+    }
+}
+
+template <class K, class V>
+constexpr size_t rs_smem_bytes() {
+    return (sizeof(K) + sizeof(V)) * size_t(RS_TILE);
+}
+
+// The scatter kernel's dynamic shared-memory limit, raised once per device.
+template <class K, class V>
+void rs_prepare() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    CURC_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal out of range");
+    std::lock_guard<std::mutex> g(mu);
+    if (!done[dev]) {
+        CURC_CHECK(cudaFuncSetAttribute(rs_scatter_kernel<K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(rs_smem_bytes<K, V>())));
+        done[dev] = true;
     }
 }
 }  // namespace
@@ -447,6 +513,7 @@ void radix_sort_pairs(K* keys, V* vals, size_t n, int begin_bit, int end_bit, Ar
     uint32_t* hist = a.alloc<uint32_t>(size_t(256) * tiles);
     K* kc = keys;
     V* vc = vals;
+    rs_prepare<K, V>();
     for (int shift = begin_bit; shift < end_bit; shift += 8) {
         const int bits = std::min(8, end_bit - shift);
         const uint32_t mask = (1u << bits) - 1u;
@@ -455,7 +522,8 @@ void radix_sort_pairs(K* keys, V* vals, size_t n, int begin_bit, int end_bit, Ar
         exclusive_scan<uint32_t>(hist, hist, size_t(256) * tiles, nullptr, a, s);
         K* ko = (kc == keys) ? kalt : keys;
         V* vo = vals ? ((vc == vals) ? valt : vals) : nullptr;
-        rs_scatter_kernel<K, V><<<tiles, RS_THREADS, 0, s>>>(kc, vc, ko, vo, n, shift, mask, hist, tiles);
+        rs_scatter_kernel<K, V><<<tiles, RS_THREADS, rs_smem_bytes<K, V>(), s>>>(kc, vc, ko, vo, n, shift, mask,
+                                                                                 hist, tiles);
         CURC_LAUNCH_CHECK();
         kc = ko;
         vc = vo;
@@ -620,9 +688,13 @@ void sort_ids_by_reads(const uint64_t* db, int W, int L, uint32_t* ids, size_t n
     if (n <= 1) return;
     auto mk = a.mark();
     uint64_t* k0 = a.alloc<uint64_t>(n);
-    gather_words(db, ids, n, W, 0, k0, s);
-    const int lo0 = W == 1 ? 64 - 2 * L : 0;
-    radix_sort_pairs<uint64_t, uint32_t>(k0, ids, n, lo0, 64, a, s);
+    {
+        // the first-word sort alone (the tie runs below read counts back to the host)
+        SubStage sp("sort_dedupe.first_word");
+        gather_words(db, ids, n, W, 0, k0, s);
+        const int lo0 = W == 1 ? 64 - 2 * L : 0;
+        radix_sort_pairs<uint64_t, uint32_t>(k0, ids, n, lo0, 64, a, s);
+    }
     if (W > 1) {
         uint8_t* tie = a.alloc<uint8_t>(n);
         tie_flags_kernel<<<grid_for(n, 256), 256, 0, s>>>(k0, n, tie);

@@ -684,15 +684,16 @@ void Block::refmatch_all() {
     // unmatched, mapped, unmapped (non-N, N), overlap passes, contested
     // suffixes, records, mismatches; overlap suffixes, and summed over the
     // passes: unlinked suffixes, suffixes probed, probes that met a prefix,
-    // probes that searched a bucket, prefix comparisons; overlap links; and
-    // for the mapping, forward then reverse complement: reads searched, k-mer
-    // probes listed, candidate windows compared
+    // probes that searched a bucket, prefix comparisons; overlap links; for
+    // the mapping, forward then reverse complement: reads searched, k-mer
+    // probes listed, candidate windows compared; prefix rows the probes read
     unsigned long long mt[6] = {0, 0, 0, 0, 0, 0};
     if (mo.tally) read_small(mt, mo.tally, sizeof(mt), s);
-    const uint64_t stats[25] = {n,          m,           NN,         n_ref,         U,           n_map,
+    const uint64_t stats[26] = {n,          m,           NN,         n_ref,         U,           n_map,
                                 n_ug,       n_un,        ostats.passes, ostats.contested, n_records, n_mis,
                                 ostats.suffixes, ostats.active_sum, ostats.probes, ostats.hits, ostats.searched,
-                                ostats.compares, ostats.links, mt[0], mt[1], mt[2], mt[3], mt[4], mt[5]};
+                                ostats.compares, ostats.links, mt[0], mt[1], mt[2], mt[3], mt[4], mt[5],
+                                ostats.rows};
     put("stats", std::vector<uint8_t>(reinterpret_cast<const uint8_t*>(stats),
                                       reinterpret_cast<const uint8_t*>(stats) + sizeof(stats)));
 }

@@ -62,7 +62,7 @@ void dedupe_links(const uint64_t* db, int W, const uint32_t* sorted, uint32_t m,
                   uint16_t* offset, cudaStream_t s);
 struct OverlapStats {
     uint32_t passes = 0, links = 0, contested = 0, suffixes = 0;
-    uint64_t active_sum = 0, probes = 0, hits = 0, searched = 0, compares = 0;  // summed over passes
+    uint64_t active_sum = 0, probes = 0, hits = 0, searched = 0, compares = 0, rows = 0;  // summed over passes
 };
 void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sorted, uint32_t m, uint32_t* next,
                   uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s, OverlapStats* st = nullptr);

@@ -8,10 +8,18 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-IN, HID, OUT, NB = 128, 128, 20, 4
+IN, HID, NB = 128, 128, 4
+
+
+def _out():
+    # output logits (base outcomes + gap bins), from the library's parameter count
+    from curc_b200 import learn_param_count
+    return (learn_param_count() - (HID * IN + HID + HID * HID + HID)) // (HID + 1)
+
 
 
 def _unpack(p):
+    OUT = _out()
     o = 0
     out = []
     for shape in [(HID, IN), (HID,), (HID, HID), (HID,), (OUT, HID), (OUT,)]:
@@ -22,6 +30,7 @@ def _unpack(p):
 
 
 def _numpy_loss_grads(p, x, tb, tg):
+    OUT = _out()
     W1, b1, W2, b2, W3, b3 = _unpack(p.astype(np.float64))
     B = x.shape[0]
     h1 = np.maximum(x @ W1.T + b1, 0)
@@ -59,7 +68,7 @@ def test_gradients_match_float64():
     B = 48
     x = (rng.random((B, IN)) < 0.15).astype(np.float32)
     tb = rng.integers(-1, NB, B).astype(np.int8)
-    tg = rng.integers(-1, OUT - NB, B).astype(np.int8)
+    tg = rng.integers(-1, _out() - NB, B).astype(np.int8)
     with Learner(0) as lrn:
         loss, g = lrn.grad(p, x, tb, tg)
     ref_loss, ref_g = _numpy_loss_grads(p, x, tb, tg)
