@@ -1,5 +1,9 @@
 """The learned coder's host parts, no GPU: the range coder round trip
-(compiled from tests/helpers/rc_roundtrip.cpp against learned_model.hpp)."""
+(tests/helpers/rc_roundtrip.cpp) and the learned stream written from its
+coding rules with the host integer model and read back by the decoder the
+product uses for learned archive blocks, on random models, pseudogenomes
+and records at 75, 150 and 250 bp, corrupt streams included
+(tests/helpers/learned_roundtrip.cpp), both against learned_model.hpp."""
 import os
 import subprocess
 
@@ -13,3 +17,12 @@ def test_range_coder_round_trip(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "round trips ok" in r.stdout
+
+
+def test_learned_stream_round_trip(tmp_path):
+    exe = str(tmp_path / "lrt")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-fopenmp", "-I", os.path.join(ROOT, "curc_b200", "csrc"), "-o", exe,
+                    os.path.join(ROOT, "tests", "helpers", "learned_roundtrip.cpp")], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "learned round trips ok" in r.stdout
