@@ -61,9 +61,11 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-coder evaluation")
     ap.add_argument("--learned-pairs", type=int, default=1_000_000, help="pairs per training seed")
     ap.add_argument("--learned-eval-pairs", type=int, default=10_000_000, help="pairs per evaluation seed")
-    ap.add_argument("--workload", default="pe150", choices=["pe150", "large"],
+    ap.add_argument("--workload", default="pe150", choices=["pe150", "large", "batched"],
                     help="large: the single-end 250 bp case (40M reads, 200 Mbp genome), device throughput, "
-                         "whole-file round trip and learned-coder bytes, one JSON line")
+                         "whole-file round trip and learned-coder bytes; batched: the 64 mixed blocks at full "
+                         "scale, one block at a time against the batched drain, default against autotuned "
+                         "launch choices, streams compared; each prints one JSON line")
     ap.add_argument("--large-reads", type=int, default=40_000_000)
     ap.add_argument("--batched-blocks", type=int, default=16)
     ap.add_argument("--batched-scale", type=float, default=0.1)
@@ -634,6 +636,82 @@ def _large_files(ctx, w, seqs, model):
     return out
 
 
+def run_batched(a):
+    """The batched workload at full scale: 64 independent single-end blocks
+    from 64 seeded random genomes (2-20 Mbp), read counts log-uniform in
+    50k-5M, read lengths from {75, 100, 150, 250}, errors 0.1-0.5%.  Times
+    (host reads to host streams, no coders) one curc_block_run per block,
+    then the batched drain (concurrent block pipelines, large blocks
+    double-buffered), then the drain again with each block's launch choices
+    autotuned for its (read length, read-count bucket) on one block of that
+    bucket.  Every block's streams must be the same in all three runs."""
+    import hashlib
+    from curc_b200 import Context, synth
+    from tests.oracle_lib import stream_dtype, stream_names
+    t0 = time.perf_counter()
+    specs = synth.batched_specs(2, 64, 1.0)
+    blocks = [np.ascontiguousarray(synth.batched_block(2, b, sp).mate1) for b, sp in enumerate(specs)]
+    gen_s = time.perf_counter() - t0
+    bases = int(sum(b.size for b in blocks))
+
+    def digest(ctx, L):
+        h = hashlib.sha256()
+        for nm in stream_names(L):
+            h.update(ctx.get(nm, stream_dtype(nm)).tobytes())
+        return h.hexdigest()
+
+    out = {"workload": "64 single-end blocks from 64 seeded random genomes (2-20 Mbp), read counts log-uniform in "
+                       "50k-5M, read lengths from {75, 100, 150, 250}, errors 0.1-0.5%",
+           "blocks": len(blocks), "reads": int(sum(b.shape[0] for b in blocks)), "bases": bases,
+           "generate_s": gen_s, "unit": "Mbases/s",
+           "includes": "host reads to host streams (H2D, device path, D2H), no stream coders"}
+    with tempfile.TemporaryDirectory() as td, Context(0) as ctx:
+        ctx.keep_intermediates(False)
+        ctx.block_run(blocks[0])  # warm
+        plain = []
+        t = time.perf_counter()
+        for b in blocks:
+            ctx.block_run(b)
+            plain.append(digest(ctx, b.shape[1]))
+        # the digests are taken inside the timed loop here too, as in the drains
+        out["one_block_at_a_time"] = bases / (time.perf_counter() - t) / 1e6
+
+        # batched drain: digests per ticket
+        tickets = []
+        for b in blocks:
+            tickets.append(ctx.batch_submit(b))
+        dig = {}
+        t = time.perf_counter()
+        ctx.batch_workers(4)
+        ctx.batch_drain(lambda tk: dig.__setitem__(tk, digest(ctx, blocks[tickets.index(tk)].shape[1])))
+        out["batched"] = bases / (time.perf_counter() - t) / 1e6
+        out["batched_streams_equal"] = all(dig[tk] == plain[i] for i, tk in enumerate(tickets))
+        # autotune one block per (read length, read-count bucket), then drain with per-block choices
+        import torch
+        cache = os.path.join(td, "tune.txt")
+        seen = {}
+        t = time.perf_counter()
+        for i, b in enumerate(blocks):
+            key = (b.shape[1], int(np.floor(np.log2(b.shape[0]))))
+            if key in seen:
+                continue
+            d = torch.from_numpy(b.reshape(-1)).cuda()
+            seen[key] = ctx.autotune(d.data_ptr(), b.shape[0], b.shape[1], False, False, cache)[0]
+            del d
+        out["autotune_s"] = time.perf_counter() - t
+        out["tuned_buckets"] = {f"L{k[0]}_2^{k[1]}": v for k, v in seen.items()}
+        ctx.set_tuning(table_factor=4, bitmap_bits=16, check_every=8, map_threads=128)
+        ctx.use_tuning_cache(cache)
+        tickets = [ctx.batch_submit(b) for b in blocks]
+        dig = {}
+        t = time.perf_counter()
+        ctx.batch_drain(lambda tk: dig.__setitem__(tk, digest(ctx, blocks[tickets.index(tk)].shape[1])))
+        out["batched_autotuned"] = bases / (time.perf_counter() - t) / 1e6
+        out["autotuned_streams_equal"] = all(dig[tk] == plain[i] for i, tk in enumerate(tickets))
+        ctx.use_tuning_cache(None)
+    return out
+
+
 def _has_stage(ctx, k):
     try:
         ctx.stage_ms(k)
@@ -658,8 +736,8 @@ def main():
                        "0.2% substitutions, 0.01% N, --preserve_order, block_ratio 1",
            "global_batch": a.pairs * 2 * world, "read_len": 150, "parallelism": f"independent blocks x{world}",
            "l2_flush": "inputs (3 GB ASCII per block) are larger than L2"}
-    if a.workload == "large":
-        print(json.dumps(run_large(a)))
+    if a.workload in ("large", "batched"):
+        print(json.dumps(run_large(a) if a.workload == "large" else run_batched(a)))
         finish_dist(world)
         return
     if a.impl == "reference":

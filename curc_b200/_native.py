@@ -41,6 +41,7 @@ def lib() -> ctypes.CDLL:
         L.curc_ctx_set_mismatch_model.argtypes = [c_p, c_p, c_u64]
         L.curc_ctx_set_tuning.argtypes = [c_p, c_p]
         L.curc_ctx_get_tuning.argtypes = [c_p, c_p]
+        L.curc_ctx_use_tuning_cache.argtypes = [c_p, ctypes.c_char_p]
         L.curc_autotune.argtypes = [c_p, c_p, c_u64, ctypes.c_uint16, c_int, c_int, ctypes.c_char_p,
                                     ctypes.POINTER(c_int)]
         L.curc_kernel_launches.argtypes = []
@@ -269,6 +270,11 @@ class Context:
         self._check(lib().curc_autotune(self._h, ctypes.c_void_p(ptr), n, L, int(preserve_order), int(paired_end),
                                         cache.encode() if cache else None, ctypes.byref(fc)), "curc_autotune")
         return self.tuning(), bool(fc.value)
+
+    def use_tuning_cache(self, path: str | None):
+        """Per-block tuning from an autotune cache file (None: stop)."""
+        self._check(lib().curc_ctx_use_tuning_cache(self._h, path.encode() if path else None),
+                    "curc_ctx_use_tuning_cache")
 
     def set_mismatch_model(self, model: bytes | None):
         """Learned mode of compress_files (model bytes from Learner.model()),

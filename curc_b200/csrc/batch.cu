@@ -191,6 +191,7 @@ int curc_batch_drain(curc_ctx* ctx, curc_block_done_fn done, void* user) {
         for (auto& w : q.pool) {
             w->blk->keep_intermediates = ctx->block->keep_intermediates;
             w->blk->tune = ctx->block->tune;
+            w->blk->tune_cache = ctx->block->tune_cache;
         }
         // every pipeline sized for the largest queued block up front: growing a
         // slot later would allocate (and synchronise) in the middle of the drain

@@ -39,6 +39,10 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
     if (L < 1 || (L + 31) / 32 > 16) throw std::runtime_error("read length must be in [1, 512]");
     p = BlockParams::derive(L, po, pe);
     p.tune = tune;
+    if (tune_cache) {
+        auto it = tune_cache->find(tune_key(L, n_reads));
+        if (it != tune_cache->end()) p.tune = it->second;
+    }
     n = uint32_t(n_reads);
     host.clear();
     stage_ms.clear();

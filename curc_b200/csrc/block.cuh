@@ -23,6 +23,9 @@ struct Block {
     Arena arena;
     bool keep_intermediates = true;
     Tuning tune;  // launch and table choices for the next runs (no effect on results)
+    // when set: per-block choices by (read length, read-count bucket); blocks
+    // whose bucket is missing use `tune`
+    std::shared_ptr<const std::map<TuneKey, Tuning>> tune_cache;
 
     BlockParams p;
     uint32_t n = 0, m = 0, NN = 0, n_ref = 0, U = 0;

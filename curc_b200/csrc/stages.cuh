@@ -22,6 +22,18 @@ struct Tuning {
     int table_factor = 4, bitmap_bits = 16, check_every = 8, map_threads = 128;
 };
 
+// Autotuner cache key of a block: read length and read count rounded down
+// to a power of two.
+struct TuneKey {
+    int L, log2n;
+    bool operator<(const TuneKey& o) const { return L != o.L ? L < o.L : log2n < o.log2n; }
+};
+inline TuneKey tune_key(int L, uint64_t n) {
+    int b = 0;
+    while (b < 63 && (uint64_t(1) << (b + 1)) <= n) ++b;
+    return TuneKey{L, b};
+}
+
 struct BlockParams {
     int L = 0, W = 0, max_off = 0, k = 0, kip = 0, max_mm = 0;
     bool preserve_order = false, paired_end = false;

@@ -29,16 +29,7 @@
 namespace curc {
 namespace {
 
-struct Key {
-    int L, b;
-    bool operator<(const Key& o) const { return L != o.L ? L < o.L : b < o.b; }
-};
-
-int bucket_of(uint64_t n) {
-    int b = 0;
-    while (b < 63 && (uint64_t(1) << (b + 1)) <= n) ++b;
-    return b;
-}
+using Key = TuneKey;
 
 std::map<Key, Tuning> load_cache(const std::string& path) {
     std::map<Key, Tuning> m;
@@ -48,7 +39,7 @@ std::map<Key, Tuning> load_cache(const std::string& path) {
         std::istringstream ls(line);
         Key k;
         Tuning t;
-        if (ls >> k.L >> k.b >> t.table_factor >> t.bitmap_bits >> t.check_every >> t.map_threads) m[k] = t;
+        if (ls >> k.L >> k.log2n >> t.table_factor >> t.bitmap_bits >> t.check_every >> t.map_threads) m[k] = t;
     }
     return m;
 }
@@ -58,7 +49,7 @@ void save_cache(const std::string& path, const std::map<Key, Tuning>& m) {
     {
         std::ofstream out(tmp, std::ios::trunc);
         for (const auto& kv : m)
-            out << kv.first.L << ' ' << kv.first.b << ' ' << kv.second.table_factor << ' ' << kv.second.bitmap_bits
+            out << kv.first.L << ' ' << kv.first.log2n << ' ' << kv.second.table_factor << ' ' << kv.second.bitmap_bits
                 << ' ' << kv.second.check_every << ' ' << kv.second.map_threads << '\n';
         if (!out) throw std::runtime_error("autotune: cannot write " + tmp);
     }
@@ -103,13 +94,31 @@ int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs) {
     return CURC_OK;
 }
 
+int curc_ctx_use_tuning_cache(curc_ctx* ctx, const char* cache_path) {
+    if (!ctx) return CURC_ERR_ARG;
+    try {
+        if (!cache_path || !*cache_path) {
+            ctx->block->tune_cache.reset();
+            return CURC_OK;
+        }
+        auto m = std::make_shared<std::map<curc::Key, Tuning>>();
+        for (const auto& kv : curc::load_cache(cache_path))
+            if (curc::valid(kv.second)) (*m)[kv.first] = kv.second;
+        ctx->block->tune_cache = m;
+        return CURC_OK;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return CURC_ERR_IO;
+    }
+}
+
 int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
                   int paired_end, const char* cache_path, int* from_cache) {
     if (!ctx || !seqs_dev || !n) return CURC_ERR_ARG;
     try {
         CURC_CHECK(cudaSetDevice(ctx->device));
         curc::Block& blk = *ctx->block;
-        const curc::Key key{int(read_len), curc::bucket_of(n)};
+        const curc::Key key = curc::tune_key(int(read_len), n);
         std::map<curc::Key, Tuning> cache;
         if (cache_path && *cache_path) cache = curc::load_cache(cache_path);
         auto hit = cache.find(key);

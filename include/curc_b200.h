@@ -102,6 +102,11 @@ int curc_ctx_set_tuning(curc_ctx* ctx, const int32_t* knobs);
 int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs);
 int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
                   int paired_end, const char* cache_path, int* from_cache);
+/* Loads a cache file written by curc_autotune: every later block run of the
+ * context (batched blocks included) uses the choice of its own (read
+ * length, read-count bucket), or the context's setting when the bucket has
+ * none.  NULL or "" stops using it. */
+int curc_ctx_use_tuning_cache(curc_ctx* ctx, const char* cache_path);
 
 /* Learned mode of whole-file compression (no counterpart in the reference;
  * the plain coders are the reference's, src/compress.cu:1923-2146).  With a
