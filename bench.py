@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--pairs", type=int, default=10_000_000)
     ap.add_argument("--genome", type=int, default=50_000_000)
     ap.add_argument("--cpu-sample-pairs", type=int, default=100_000)
-    ap.add_argument("--ref-sample-pairs", type=int, default=1_000_000,
+    ap.add_argument("--ref-sample-pairs", type=int, default=3_000_000,
                     help="pairs per step of the reference arm (the first pairs of the workload's FASTQ files)")
     ap.add_argument("--ref-full", action="store_true",
                     help="reference arm: time one run on the whole workload instead of the sampled steps")
@@ -535,8 +535,10 @@ def run_reference(a):
                               timeout=3600)
         except RuntimeError as e:
             return None, str(e)[:300]
+        # one line per process that loaded the shim: the reference's own runs
+        # (their allocations filled), and the bsc processes it starts (none)
         fills = [tuple(float(x) for x in l.split()) for l in open(shim_log)] if os.path.exists(shim_log) else []
-    fills = fills[warmup:]
+    fills = [f for f in fills if f[0] > 0][warmup:]
     mean = sum(r["s"] for r in runs) / len(runs)
     return {"bases": ws.bases, "pairs": ws.mate1.shape[0], "s": mean, "steps": len(runs),
             "archive_bytes": runs[0]["archive_bytes"], "line_stages": line_stages(runs),
