@@ -204,7 +204,6 @@ int main(int argc, char** argv) {
         curc_ctx_destroy(ctx);
         return 1;
     }
-    curc_ctx_destroy(ctx);
     struct stat ast;
     stat(archive.c_str(), &ast);
     std::printf("reads count : %llu \n", (unsigned long long)reads);
@@ -216,5 +215,10 @@ int main(int argc, char** argv) {
         for (uint32_t b = 0; b < nb; ++b)
             std::printf("block %u compress finish, compressed size : %llu\n", b, (unsigned long long)block_bytes[b]);
     std::printf("archive size : %lld bytes \n", (long long)ast.st_size);
-    return 0;
+    // the archive is closed: leave without tearing the CUDA context and its
+    // device memory down one allocation at a time (the driver releases them
+    // with the process)
+    std::fflush(stdout);
+    std::fflush(stderr);
+    _exit(0);
 }
