@@ -148,9 +148,9 @@ def pack_bytes(n, L):
 # Algorithmic bytes of the overlap probe kernel (its launches over all
 # passes), with one 32-byte sector per random access: per listed suffix its
 # k-mer (32); per bucket searched the bucket range (32); per prefix
-# comparison the prefix entry, id and first word (32); per prefix row read
-# (only when the first 32 bases agree) the row (32 * ceil(8W/32)); per hit
-# the run slot (32).  Counts come from the kernel's own counters.
+# comparison the prefix entry (32) and the prefix's row (32 * ceil(8W/32),
+# counted as rows read); per hit the run slot (32).  Counts come from the
+# kernel's own counters.
 def probe_bytes(st, L):
     row = 32 * -(-8 * ((L + 31) // 32) // 32)
     return (32 * st["overlap_probes"] + 32 * st["overlap_searched"] + 32 * st["overlap_compares"]

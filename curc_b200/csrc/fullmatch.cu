@@ -330,8 +330,10 @@ struct MoveIdKey {
 template <class Acc>
 void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt, uint32_t* next, uint32_t* prev,
                      uint16_t* offset, Arena& a, cudaStream_t s) {
-    // one read cannot follow itself: with fewer than two ends nothing links
-    if (cnt < 2) return;
+    // nothing to link without ends; a single prefix and a single suffix can
+    // still link when they are different reads (the head and the tail of one
+    // chain, which then closes into a cycle, as the reference's merge does)
+    if (cnt == 0) return;
     auto mk = a.mark();
     uint32_t* suf2 = a.alloc<uint32_t>(cnt);
     uint32_t* tmp = a.alloc<uint32_t>(cnt);

@@ -260,7 +260,7 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 //     x W2^T, four K=32 steps issued by one thread; the thread of each
 //     anchor reads its row back (tcgen05.ld), adds the bias, requantises and
 //     stores it as the next A operand;
-//   layer 3: the same with N = 32 (the OUT = 28 output rows of W3, zero
+//   layer 3: the same with N = 32 (the OUT = 20 output rows of W3, zero
 //     padded); each thread turns its logits into frequencies.
 // Integer accumulation is exact in any order, so the frequencies equal the
 // host model's (learned_model.hpp) bit for bit.  Operands live in shared

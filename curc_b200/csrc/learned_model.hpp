@@ -34,17 +34,16 @@ namespace learned {
 constexpr int IN = 128;      // input features (one-hots, zero padded)
 constexpr int HID = 128;     // hidden units per layer
 constexpr int NB = 4;        // base outcomes: the three other bases, then N
-constexpr int NG = 24;       // gap bins
+constexpr int NG = 16;       // gap bins
 constexpr int OUT = NB + NG;
 constexpr int CTX = 16;      // pseudogenome bases around an anchor
 constexpr int LUTN = 256;    // exponential table entries
 constexpr uint32_t TOTAL = 4096;  // frequency total (12 bits)
 
-// Gap bins: [lo, lo + width) with widths 1 x4, 2 x4, 4 x4, 8 x4, 16 x4, 32 x2,
-// 64 and 260 (gaps of reads up to 512 bases).
+// Gap bins: [lo, lo + width) with widths 1,1,1,1,2,2,4,4,8,8,16,16,32,32,64,320
+// (gaps of reads up to 512 bases).
 LM_HD int gap_bin_lo(int b) {
-    constexpr int lo[NG + 1] = {0,  1,  2,  3,  4,  6,   8,   10,  12,  16,  20,  24, 28,
-                                36, 44, 52, 60, 76, 92, 108, 124, 156, 188, 252, 512};
+    constexpr int lo[NG + 1] = {0, 1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 512};
     return lo[b];
 }
 LM_HD int gap_bin(int g) {
@@ -195,12 +194,11 @@ LM_HD void model_freqs(const Model& M, const int* idx, int nidx, int gmax, uint3
     logits_to_freq(M, z + NB, gap_bin(gmax < 0 ? 0 : gmax) + 1, NG, fg);
 }
 
-// Context of the adaptive in-bin models: the read's strand and where the
-// anchor lies along the read (8 buckets in pseudogenome order), since the
-// error rate, and with it the spread of a gap inside its bin, depends on
-// the sequencing cycle.
-constexpr int BIN_CTX = 16;
-LM_HD int bin_context(int q, int L, int strand) { return (strand ? 8 : 0) + ((q + 1) * 8) / (L + 1); }
+// Context of the adaptive in-bin models.  One context: splitting them by
+// strand and read position (16 contexts) spread the 16384-record chunks too
+// thin and coded 1% larger on the ramped-error workload.
+constexpr int BIN_CTX = 1;
+LM_HD int bin_context(int, int, int) { return 0; }
 
 // Adaptive frequencies of the offset inside each gap bin (the network gives
 // the bin), one set per bin context: reset at the start of each

@@ -115,7 +115,6 @@ struct OverlapCtx {
     const uint32_t* present;  // bitmap of prefix k-mer hashes (high 32 bits)
     uint32_t bmask;
     const uint32_t* va;  // prefix ids sorted by (bucket, read)
-    const uint64_t* vw0; // first packed word of each prefix, in va order
     const uint32_t* kr;  // bucket ranges
     uint32_t* free_cnt;  // per bucket: prefixes without a predecessor
     uint32_t* bfree;     // per bucket: free_cnt != 0 (one bit, stays in L2)
@@ -193,18 +192,14 @@ struct ProbeListMove {
 };
 
 // Three-way compare of prefix entry `it` ([0, cl)) with the suffix's
-// [off, off + cl): the first 32 bases from the prefix's first word, stored
-// beside its id, so most comparisons need no row of the prefix; only when
-// they agree and more bases follow is the row read (counted in `rows`).
+// [off, off + cl); every comparison reads the prefix's row (counted in
+// `rows`).  Prefixes of one bucket share the indexed k-mer and, for true
+// overlaps, their first bases too, so a stored first word decided only a
+// quarter of the comparisons and cost more than it saved.
 __device__ __forceinline__ int cmp_prefix(const OverlapCtx& c, uint32_t it, const uint64_t* sr, int off, int cl,
                                           uint32_t& rows) {
-    const int nb = cl < 32 ? cl : 32;
-    const uint64_t x = c.vw0[it] >> (64 - 2 * nb);
-    const uint64_t y = word_at(sr, off, nb);
-    if (x != y) return x < y ? -1 : 1;
-    if (cl <= 32) return 0;
     ++rows;
-    return cmp_span(c.db + uint64_t(c.va[it]) * c.W, 32, sr, off + 32, cl - 32);
+    return cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl);
 }
 
 // compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
@@ -435,7 +430,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     uint32_t* present = a.alloc<uint32_t>(bwords);
     CURC_CHECK(cudaMemsetAsync(present, 0, bwords * 4, s));
     OverlapCtx c{db, p.W, p.L, p.k, p.kip, hs - 1, present, uint32_t((1ull << bbits) - 1), pre, nullptr, nullptr,
-                 nullptr, nullptr, next, prev, offset};
+                 nullptr, next, prev, offset};
     uint32_t* keys = a.alloc<uint32_t>(mp ? mp : 1);
     SubStage sp_sort("overlap.index_sort");
     if (mp) {
@@ -444,9 +439,6 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
         CURC_LAUNCH_CHECK();
         radix_sort_pairs<uint32_t, uint32_t>(keys, pre, mp, 0, log2_exact(hs), a, s);
     }
-    uint64_t* vw0 = a.alloc<uint64_t>(mp ? mp : 1);
-    if (mp) gather_words(db, pre, mp, p.W, 0, vw0, s);
-    c.vw0 = vw0;
     uint32_t* kr = a.alloc<uint32_t>(size_t(hs) + 2);
     CURC_CHECK(cudaMemsetAsync(kr, 0, (size_t(hs) + 2) * sizeof(uint32_t), s));
     if (mp) {
