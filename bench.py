@@ -66,6 +66,8 @@ def parse():
                          "whole-file round trip and learned-coder bytes; batched: the 64 mixed blocks at full "
                          "scale, one block at a time against the batched drain, default against autotuned "
                          "launch choices, streams compared; each prints one JSON line")
+    ap.add_argument("--loop-graph", type=int, default=1, choices=[0, 1],
+                    help="full-match passes replayed from a CUDA graph (1) or queued launch by launch (0)")
     ap.add_argument("--large-reads", type=int, default=40_000_000)
     ap.add_argument("--batched-blocks", type=int, default=16)
     ap.add_argument("--batched-scale", type=float, default=0.1)
@@ -241,6 +243,7 @@ def run_ours(a, rank, world):
     dseq = host.to(f"cuda:{dev}")
     ctx = Context(dev)
     ctx.keep_intermediates(False)
+    ctx.set_tuning(loop_graph=a.loop_graph)
 
     def dev_step():
         ctx.block_run_device(dseq.data_ptr(), n, L, True, True)
@@ -255,7 +258,7 @@ def run_ours(a, rank, world):
                    "unmapped_refs", "refmatch"]
     sub_names = ["pack.kernel", "sort_dedupe.first_word", "sort_dedupe.radix", "overlap.index", "overlap.index_sort", "overlap.index_mask",
                  "overlap.probe_resolve", "overlap.filter", "overlap.probe", "overlap.resolve", "overlap.compact",
-                 "full_match.resort", "full_match.groups", "full_match.compact", "assembly.ranking", "assembly.walk", "assembly.jump",
+                 "full_match.resort", "full_match.groups", "full_match.compact", "full_match.graph", "assembly.ranking", "assembly.walk", "assembly.jump",
                  "assembly.order_place", "mapping.index_fwd", "mapping.map_fwd", "mapping.index_rc", "mapping.map_rc",
                  "refmatch.index", "refmatch.probe_unmapped", "refmatch.probe_self", "refmatch.sort_unique",
                  "refmatch.accept"]

@@ -250,17 +250,17 @@ class Context:
                     "curc_compress_files")
         return reads.value, blocks.value
 
-    TUNING_KNOBS = ("table_factor", "bitmap_bits", "check_every", "map_threads")
+    TUNING_KNOBS = ("table_factor", "bitmap_bits", "check_every", "map_threads", "loop_graph")
 
     def tuning(self) -> dict:
-        k = (ctypes.c_int32 * 4)()
+        k = (ctypes.c_int32 * len(self.TUNING_KNOBS))()
         self._check(lib().curc_ctx_get_tuning(self._h, k), "curc_ctx_get_tuning")
         return dict(zip(self.TUNING_KNOBS, list(k)))
 
     def set_tuning(self, **knobs):
         cur = self.tuning()
         cur.update(knobs)
-        k = (ctypes.c_int32 * 4)(*[cur[n] for n in self.TUNING_KNOBS])
+        k = (ctypes.c_int32 * len(self.TUNING_KNOBS))(*[cur[n] for n in self.TUNING_KNOBS])
         self._check(lib().curc_ctx_set_tuning(self._h, k), "curc_ctx_set_tuning")
 
     def autotune(self, ptr: int, n: int, L: int, preserve_order=False, paired_end=False, cache: str | None = None):

@@ -37,6 +37,8 @@ struct CudaError : std::runtime_error {
 // Every kernel launch of the library goes through this check, which also
 // counts it (curc_kernel_launches).
 void count_launch();
+// Adds the launches a graph made on the device (its kernels times its replays).
+void count_launches(uint64_t n);
 #define CURC_LAUNCH_CHECK()             \
     do {                                \
         ::curc::count_launch();         \

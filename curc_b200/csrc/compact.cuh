@@ -36,9 +36,11 @@ template <class Keep, class Move>
 __global__ void __launch_bounds__(CP_THREADS) compact_kernel(const uint32_t* __restrict__ n_dev,
                                                              uint32_t* __restrict__ n_out, Keep keep, Move move,
                                                              unsigned long long* tiles, uint32_t* counter,
-                                                             uint32_t base, uint32_t epoch, uint32_t* err) {
+                                                             uint32_t base, uint32_t epoch_arg, uint32_t* err,
+                                                             const uint32_t* __restrict__ epoch_dev) {
     __shared__ uint32_t s_tile, s_excl, s_warp[CP_THREADS / 32];
     const uint32_t n = *n_dev;
+    const uint32_t epoch = epoch_dev ? *epoch_dev : epoch_arg;
     if (threadIdx.x == 0) {
         s_tile = atomicAdd(counter, 1u) - base;
         if (blockIdx.x == 0 && uint64_t(n) > uint64_t(gridDim.x) * CP_TILE) atomicExch(err, 2u);
@@ -127,27 +129,47 @@ __global__ void __launch_bounds__(CP_THREADS) compact_kernel(const uint32_t* __r
         if ((kept >> r) & 1u) move(uint32_t(first + r), d++);
 }
 
-// Owns the tile states of a sequence of compactions on one stream.
+// Before a replayable compaction: a fresh epoch and tile counter.
+static __global__ void cp_begin_kernel(uint32_t* counter, uint32_t* epoch) {
+    *counter = 0;
+    *epoch = *epoch + 1;
+}
+
+// Owns the tile states of a sequence of compactions on one stream.  A
+// Compactor is used either through run() (epoch and tile base kept on the
+// host, one launch per compaction) or through run_replayable() (kept on the
+// device and advanced by a one-thread kernel, so the launches can be
+// captured once and replayed from a graph), not both.
 class Compactor {
 public:
     Compactor(uint32_t max_items, Arena& a, cudaStream_t s) : s_(s) {
         max_tiles_ = uint32_t(div_up(uint64_t(max_items ? max_items : 1), uint64_t(CP_TILE)));
         tiles_ = a.alloc<unsigned long long>(max_tiles_);
-        counter_ = a.alloc<uint32_t>(2);
+        counter_ = a.alloc<uint32_t>(3);
         err_ = counter_ + 1;
+        epoch_dev_ = counter_ + 2;
         CURC_CHECK(cudaMemsetAsync(tiles_, 0, size_t(max_tiles_) * 8, s));
-        CURC_CHECK(cudaMemsetAsync(counter_, 0, 8, s));
+        CURC_CHECK(cudaMemsetAsync(counter_, 0, 12, s));
     }
     // Compacts the first *n_dev (<= max_items) items; *n_out = number kept.
     template <class Keep, class Move>
     void run(const uint32_t* n_dev, uint32_t n_max, uint32_t* n_out, Keep keep, Move move) {
-        const uint32_t grid = uint32_t(div_up(uint64_t(n_max ? n_max : 1), uint64_t(CP_TILE)));
-        if (grid > max_tiles_) throw std::runtime_error("Compactor: more items than it was sized for");
+        const uint32_t grid = grid_for_items(n_max);
         ++epoch_;
         compact_kernel<Keep, Move><<<grid, CP_THREADS, 0, s_>>>(n_dev, n_out, keep, move, tiles_, counter_, base_,
-                                                                  epoch_, err_);
+                                                                  epoch_, err_, nullptr);
         CURC_LAUNCH_CHECK();
         base_ += grid;
+    }
+    // The same, replayable: two launches that refer to no host state.
+    template <class Keep, class Move>
+    void run_replayable(const uint32_t* n_dev, uint32_t n_max, uint32_t* n_out, Keep keep, Move move) {
+        const uint32_t grid = grid_for_items(n_max);
+        cp_begin_kernel<<<1, 1, 0, s_>>>(counter_, epoch_dev_);
+        CURC_LAUNCH_CHECK();
+        compact_kernel<Keep, Move><<<grid, CP_THREADS, 0, s_>>>(n_dev, n_out, keep, move, tiles_, counter_, 0, 0,
+                                                                  err_, epoch_dev_);
+        CURC_LAUNCH_CHECK();
     }
     // Fails if any wait ran out (reads one value back).
     void check() {
@@ -155,11 +177,17 @@ public:
     }
 
 private:
+    uint32_t grid_for_items(uint32_t n_max) const {
+        const uint32_t grid = uint32_t(div_up(uint64_t(n_max ? n_max : 1), uint64_t(CP_TILE)));
+        if (grid > max_tiles_) throw std::runtime_error("Compactor: more items than it was sized for");
+        return grid;
+    }
     cudaStream_t s_;
     uint32_t max_tiles_ = 0, base_ = 0, epoch_ = 0;
     unsigned long long* tiles_ = nullptr;
     uint32_t* counter_ = nullptr;
     uint32_t* err_ = nullptr;
+    uint32_t* epoch_dev_ = nullptr;
 };
 
 }  // namespace curc

@@ -83,15 +83,24 @@ __device__ __forceinline__ int cmp_keyed(const Acc& acc, uint64_t ka, uint32_t a
     return acc.cmp(a, aoff + Acc::KS, b, boff + Acc::KS, len - Acc::KS);
 }
 
+// The pass's offset: a kernel argument when the host queues the passes,
+// read from device memory when the passes replay from a graph.
+struct FmOff {
+    int v;
+    const int* p;
+    __device__ __forceinline__ int get() const { return p ? *p : v; }
+};
+
 // Keys of the list entries at offset off.  With sym_count (2-bit reads
 // only), also how many entries have each base at off-1: the list is sorted
 // by read[off-1, L), so these counts give the base runs' bounds.  Each
 // thread counts in four 16-bit fields (a resident grid leaves it far fewer
 // than 65536 entries), then one atomic per block and base.
 template <class Acc>
-__global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, const uint32_t* __restrict__ m_dev, int off,
-                                 uint64_t* __restrict__ key, uint32_t* __restrict__ sym_count) {
+__global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, const uint32_t* __restrict__ m_dev,
+                                 FmOff fo, uint64_t* __restrict__ key, uint32_t* __restrict__ sym_count) {
     const uint32_t m = *m_dev;
+    const int off = fo.get();
     uint64_t c = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const uint32_t id = ids[i];
@@ -111,8 +120,9 @@ __global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, cons
 // independent loads replace a chain of ~log2(m) dependent ones.
 template <class Acc>
 __global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf,
-                                                         const uint32_t* __restrict__ m_dev, int off,
+                                                         const uint32_t* __restrict__ m_dev, FmOff fo,
                                                          uint32_t* __restrict__ bounds) {
+    const int off = fo.get();
     constexpr int NB = Acc::ALPHA - 1;  // boundaries to find: symbols 1 .. ALPHA-1 (at most 4)
     constexpr uint32_t S = 64;          // samples per boundary and round
     __shared__ uint32_t lo_s[4], hi_s[4];
@@ -167,11 +177,12 @@ constexpr int MP_ITEMS = 8;
 // bounds: the run bounds (ALPHA + 1 entries), or with `counts` the number of
 // entries per symbol, from which the bounds are summed.
 template <class Acc>
-__global__ void merge_level_kernel(Acc acc, int off, const uint32_t* __restrict__ in, const uint64_t* __restrict__ ink,
+__global__ void merge_level_kernel(Acc acc, FmOff fo, const uint32_t* __restrict__ in, const uint64_t* __restrict__ ink,
                                    uint32_t* __restrict__ out, uint64_t* __restrict__ outk,
                                    const uint32_t* __restrict__ bounds, bool counts, const uint32_t* __restrict__ m_dev,
                                    int width) {
     const uint32_t m = *m_dev;
+    const int off = fo.get();
     uint32_t bd[Acc::ALPHA + 1];
     if (counts) {
         bd[0] = 0;
@@ -293,10 +304,11 @@ __device__ __forceinline__ void group_one(const Acc& acc, uint32_t* pre, uint64_
 template <class Acc>
 __global__ void merge_groups_kernel(Acc acc, uint32_t* pre, uint64_t* pk, const uint32_t* __restrict__ mp_dev,
                                     const uint32_t* __restrict__ suf, const uint64_t* __restrict__ sk,
-                                    const uint32_t* __restrict__ ms_dev, int off, uint32_t* next, uint32_t* prev,
+                                    const uint32_t* __restrict__ ms_dev, FmOff fo, uint32_t* next, uint32_t* prev,
                                     uint16_t* offset) {
     const uint32_t mp = *mp_dev, ms = *ms_dev;
     if (mp == 0) return;
+    const int off = fo.get();
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < ms; j += gridDim.x * blockDim.x)
         group_one(acc, pre, pk, mp, suf, sk, ms, off, j, next, prev, offset);
 }
@@ -323,17 +335,45 @@ struct MoveIdKey {
     }
 };
 
-// The passes are queued without a host round trip: list lengths stay on
-// the device (two slots per list, read by one pass and written by its
-// compaction), kernels walk them with resident grids, and the host looks at
-// the lengths only every few passes to stop early once a list is empty.
+__global__ void fm_zero4_kernel(uint32_t* p) { p[threadIdx.x] = 0; }
+
+// Graph form of the pass loop.  After the first pass of a replayed pair the
+// offset advances; past the last offset the second pass's list lengths are
+// zeroed, so its launches find no work.
+__global__ void fm_step_kernel(int* offp, uint32_t* next_len, int L) {
+    const int o = ++*offp;
+    if (o >= L) {
+        next_len[0] = 0;
+        next_len[1] = 0;
+    }
+}
+
+// After the second pass: the device loop goes on while offsets remain and
+// both lists hold entries.  The offset grows by two per iteration, so the
+// loop ends after at most L / 2 iterations whatever the lists hold; the
+// iteration count is capped at L as well, independently of the offset.
+__global__ void fm_cond_kernel(cudaGraphConditionalHandle h, int* offp, const uint32_t* len, int L,
+                               uint32_t* iters) {
+    const int o = ++*offp;
+    const uint32_t it = ++*iters;
+    cudaGraphSetConditional(h, (o < L && it < uint32_t(L) && len[0] != 0 && len[1] != 0) ? 1u : 0u);
+}
+
+// The passes run without a host round trip: list lengths stay on the
+// device (two slots per list, read by one pass and written by its
+// compaction) and kernels walk them with resident grids.  Two ways to queue
+// them, with the same results: one launch per kernel from the host, which
+// looks at the lengths every few passes to stop early (and times the
+// sub-stages); or (tune.loop_graph) a graph whose conditional `while` node
+// replays a pair of passes, the offset and the stop test on the device, so
+// one graph launch runs the whole loop.
 template <class Acc>
 void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt, uint32_t* next, uint32_t* prev,
-                     uint16_t* offset, Arena& a, cudaStream_t s) {
+                     uint16_t* offset, bool use_graph, Arena& a, cudaStream_t s) {
     // nothing to link without ends; a single prefix and a single suffix can
     // still link when they are different reads (the head and the tail of one
     // chain, which then closes into a cycle, as the reference's merge does)
-    if (cnt == 0) return;
+    if (cnt == 0 || acc.L < 2) return;
     auto mk = a.mark();
     uint32_t* suf2 = a.alloc<uint32_t>(cnt);
     uint32_t* tmp = a.alloc<uint32_t>(cnt);
@@ -347,31 +387,37 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     uint64_t* mk2 = a.alloc<uint64_t>(cnt);
     uint32_t* bounds = a.alloc<uint32_t>(8);
     uint32_t* len = a.alloc<uint32_t>(4);  // mp, ms for even passes, then for odd passes
+    int* offp = a.alloc<int>(2);           // graph form: [0] the pass's offset, [1] iterations
     const uint32_t init[4] = {cnt, cnt, 0, 0};
     CURC_CHECK(cudaMemcpyAsync(len, init, sizeof(init), cudaMemcpyHostToDevice, s));
     Compactor cp(cnt, a, s);
     const int gk = resident_grid(list_keys_kernel<Acc>, 256, cnt);
     const int gm = resident_grid(merge_level_kernel<Acc>, 256, div_up(cnt, MP_ITEMS));
     const int gg = resident_grid(merge_groups_kernel<Acc>, 128, cnt);
-    list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, pre, len, 0, pk, nullptr);
+    list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, pre, len, FmOff{0, nullptr}, pk, nullptr);
     CURC_LAUNCH_CHECK();
     // 2-bit reads: the base runs' bounds come from counts taken with the keys
     constexpr bool by_count = Acc::ALPHA == 4;
-    constexpr int CHECK_EVERY = 8;
-    int par = 0;
-    for (int off = 1; off < acc.L; ++off, par ^= 1) {
+
+    // One pass over the lists in slots `par`, at offset fo.
+    auto pass = [&](FmOff fo, int par, bool graph) {
         uint32_t* mp_in = len + 2 * par;
         uint32_t* ms_in = mp_in + 1;
         uint32_t* mp_out = len + 2 * (par ^ 1);
         uint32_t* ms_out = mp_out + 1;
-        SubStage sp_merge("full_match.resort");
+        SubStage sp_merge("full_match.resort", !graph);
         if (by_count) {
-            CURC_CHECK(cudaMemsetAsync(bounds, 0, 4 * sizeof(uint32_t), s));
+            if (graph) {  // a kernel node rather than a memset node in the loop body
+                fm_zero4_kernel<<<1, 4, 0, s>>>(bounds);
+                CURC_LAUNCH_CHECK();
+            } else {
+                CURC_CHECK(cudaMemsetAsync(bounds, 0, 4 * sizeof(uint32_t), s));
+            }
         } else {
-            run_bounds_kernel<Acc><<<1, 256, 0, s>>>(acc, suf, ms_in, off, bounds);
+            run_bounds_kernel<Acc><<<1, 256, 0, s>>>(acc, suf, ms_in, fo, bounds);
             CURC_LAUNCH_CHECK();
         }
-        list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, suf, ms_in, off, sk, by_count ? bounds : nullptr);
+        list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, suf, ms_in, fo, sk, by_count ? bounds : nullptr);
         CURC_LAUNCH_CHECK();
         {
             // levels: runs merged in pairs, then pairs of pairs, ...; the last
@@ -384,7 +430,7 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
                 const bool last = l + 1 == levels;
                 uint32_t* dst = last ? suf2 : (l % 2 == 0 ? mtmp : suf);
                 uint64_t* dstk = last ? sk2 : (l % 2 == 0 ? mk2 : sk);
-                merge_level_kernel<Acc><<<gm, 256, 0, s>>>(acc, off, src, srck, dst, dstk, bounds, by_count, ms_in,
+                merge_level_kernel<Acc><<<gm, 256, 0, s>>>(acc, fo, src, srck, dst, dstk, bounds, by_count, ms_in,
                                                             1 << l);
                 CURC_LAUNCH_CHECK();
                 src = dst;
@@ -392,23 +438,88 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
             }
         }
         sp_merge.stop();
-        SubStage sp_groups("full_match.groups");
-        merge_groups_kernel<Acc><<<gg, 128, 0, s>>>(acc, pre, pk, mp_in, suf2, sk2, ms_in, off, next, prev, offset);
+        SubStage sp_groups("full_match.groups", !graph);
+        merge_groups_kernel<Acc><<<gg, 128, 0, s>>>(acc, pre, pk, mp_in, suf2, sk2, ms_in, fo, next, prev, offset);
         CURC_LAUNCH_CHECK();
         sp_groups.stop();
-        SubStage sp_comp("full_match.compact");
-        cp.run(mp_in, cnt, mp_out, FreeLink{pre, prev}, MoveIdKey{pre, pk, tmp, tk});
+        SubStage sp_comp("full_match.compact", !graph);
+        if (graph) {
+            cp.run_replayable(mp_in, cnt, mp_out, FreeLink{pre, prev}, MoveIdKey{pre, pk, tmp, tk});
+            cp.run_replayable(ms_in, cnt, ms_out, FreeLink{suf2, next}, MoveId{suf2, suf});
+        } else {
+            cp.run(mp_in, cnt, mp_out, FreeLink{pre, prev}, MoveIdKey{pre, pk, tmp, tk});
+            cp.run(ms_in, cnt, ms_out, FreeLink{suf2, next}, MoveId{suf2, suf});
+        }
         std::swap(pre, tmp);
         std::swap(pk, tk);
-        cp.run(ms_in, cnt, ms_out, FreeLink{suf2, next}, MoveId{suf2, suf});
         sp_comp.stop();
-        if (off % CHECK_EVERY == 0) {
-            uint32_t h[2];
-            read_small(h, mp_out, 8, s);
-            if (h[0] == 0 || h[1] == 0) break;
+    };
+
+    if (!use_graph) {
+        constexpr int CHECK_EVERY = 8;
+        int par = 0;
+        for (int off = 1; off < acc.L; ++off, par ^= 1) {
+            pass(FmOff{off, nullptr}, par, false);
+            if (off % CHECK_EVERY == 0) {
+                uint32_t h[2];
+                read_small(h, len + 2 * (par ^ 1), 8, s);
+                if (h[0] == 0 || h[1] == 0) break;
+            }
         }
+        cp.check();
+    } else {
+        SubStage sp_loop("full_match.graph");
+        const int init_off[2] = {1, 0};
+        CURC_CHECK(cudaMemcpyAsync(offp, init_off, sizeof(init_off), cudaMemcpyHostToDevice, s));
+        cudaGraph_t g = nullptr, body = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        uint64_t body_launches = 0;
+        try {
+            CURC_CHECK(cudaGraphCreate(&g, 0));
+            cudaGraphConditionalHandle h;
+            CURC_CHECK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams np = {};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            cudaGraphNode_t node;
+            CURC_CHECK(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+            body = np.conditional.phGraph_out[0];
+            CURC_CHECK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            try {
+                pass(FmOff{0, offp}, 0, true);
+                fm_step_kernel<<<1, 1, 0, s>>>(offp, len + 2, acc.L);
+                CURC_LAUNCH_CHECK();
+                pass(FmOff{0, offp}, 1, true);
+                fm_cond_kernel<<<1, 1, 0, s>>>(h, offp, len, acc.L, reinterpret_cast<uint32_t*>(offp + 1));
+                CURC_LAUNCH_CHECK();
+            } catch (...) {
+                cudaGraph_t dummy = nullptr;
+                cudaStreamEndCapture(s, &dummy);
+                if (dummy && dummy != body) cudaGraphDestroy(dummy);
+                throw;
+            }
+            CURC_CHECK(cudaStreamEndCapture(s, &body));
+            size_t nodes = 0;  // every node of the body is a kernel
+            CURC_CHECK(cudaGraphGetNodes(body, nullptr, &nodes));
+            body_launches = nodes;
+            CURC_CHECK(cudaGraphInstantiate(&ge, g, 0));
+            CURC_CHECK(cudaGraphLaunch(ge, s));
+        } catch (...) {
+            if (ge) cudaGraphExecDestroy(ge);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        sp_loop.stop();
+        cp.check();  // synchronises: the graph has run
+        uint32_t iters = 0;
+        read_small(&iters, offp + 1, 4, s);
+        CURC_CHECK(cudaGraphExecDestroy(ge));
+        CURC_CHECK(cudaGraphDestroy(g));
+        // the captured launches were counted once; the device replayed them
+        if (iters > 1) count_launches(body_launches * (iters - 1));
     }
-    cp.check();
     a.release(mk);
 }
 
@@ -448,7 +559,7 @@ __global__ void ends_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, 
 
 void full_match_packed(const BlockParams& p, const uint64_t* db, uint32_t* pre, uint32_t* suf, uint32_t cnt,
                        uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s) {
-    full_match_loop(PackedAcc{db, p.W, p.L}, pre, suf, cnt, next, prev, offset, a, s);
+    full_match_loop(PackedAcc{db, p.W, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, a, s);
 }
 
 void sort_ids_by_ascii(const uint8_t* reads, int L, uint32_t* ids, uint32_t m, Arena& a, cudaStream_t s) {
@@ -489,7 +600,7 @@ void full_match_ascii(const BlockParams& p, const uint8_t* reads, uint32_t* ids,
     select_flagged(ids, pf, pre, m, counts + 0, a, s);
     select_flagged(ids, sf, suf, m, counts + 1, a, s);
     const uint32_t cnt = read_scalar(counts + 0, s);
-    full_match_loop(AsciiAcc{reads, 0, p.L}, pre, suf, cnt, next, prev, offset, a, s);
+    full_match_loop(AsciiAcc{reads, 0, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, a, s);
     a.release(mk);
 }
 

@@ -14,6 +14,7 @@ namespace {
 std::atomic<uint64_t> g_launches{0};
 }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 uint64_t launches() { return g_launches.load(); }
 
 // ---------------------------------------------------------------- arena

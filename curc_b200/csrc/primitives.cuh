@@ -89,7 +89,8 @@ StageTimer*& active_timer();
 struct SubStage {
     StageTimer* t;
     size_t i = 0;
-    explicit SubStage(const char* name) : t(active_timer()) {
+    // on = false: no span (launches being captured into a graph)
+    explicit SubStage(const char* name, bool on = true) : t(on ? active_timer() : nullptr) {
         if (t) i = t->begin_span(name);
     }
     void stop() {

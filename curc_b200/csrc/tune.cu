@@ -3,8 +3,9 @@
 //
 // Knobs (struct Tuning): the overlap index's bucket table size as a multiple
 // of the prefix count, bits of the prefix presence bitmap per prefix, overlap
-// passes between host reads of the link count, and threads per block of the
-// mapping kernel.  None of them changes which prefixes a suffix meets, the
+// passes between host reads of the link count, threads per block of the
+// mapping kernel, and whether the full-match passes replay from a graph or
+// are queued launch by launch.  None of them changes which prefixes a suffix meets, the
 // order candidates are visited in, or any stream: the tests compare every
 // stage result and stream under each setting.  The k-mer length and the
 // other derived parameters (preprocess.cpp:295-313) are part of the format
@@ -14,7 +15,8 @@
 // the order above, each candidate timed by the device time of the stage it
 // affects (best of two runs).  Choices are cached per (read length, read
 // count rounded down to a power of two) in a small text file, one line per
-// bucket: "L log2n table_factor bitmap_bits check_every map_threads".
+// bucket: "L log2n table_factor bitmap_bits check_every map_threads
+// loop_graph" (lines without the last field take its default).
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -39,7 +41,10 @@ std::map<Key, Tuning> load_cache(const std::string& path) {
         std::istringstream ls(line);
         Key k;
         Tuning t;
-        if (ls >> k.L >> k.log2n >> t.table_factor >> t.bitmap_bits >> t.check_every >> t.map_threads) m[k] = t;
+        if (!(ls >> k.L >> k.log2n >> t.table_factor >> t.bitmap_bits >> t.check_every >> t.map_threads)) continue;
+        int g;
+        if (ls >> g) t.loop_graph = g;
+        m[k] = t;
     }
     return m;
 }
@@ -50,7 +55,8 @@ void save_cache(const std::string& path, const std::map<Key, Tuning>& m) {
         std::ofstream out(tmp, std::ios::trunc);
         for (const auto& kv : m)
             out << kv.first.L << ' ' << kv.first.log2n << ' ' << kv.second.table_factor << ' ' << kv.second.bitmap_bits
-                << ' ' << kv.second.check_every << ' ' << kv.second.map_threads << '\n';
+                << ' ' << kv.second.check_every << ' ' << kv.second.map_threads << ' ' << kv.second.loop_graph
+                << '\n';
         if (!out) throw std::runtime_error("autotune: cannot write " + tmp);
     }
     if (std::rename(tmp.c_str(), path.c_str()) != 0) throw std::runtime_error("autotune: cannot replace " + path);
@@ -63,7 +69,7 @@ bool valid(const Tuning& t) {
         return false;
     };
     return in(t.table_factor, {1, 2, 4, 8}) && in(t.bitmap_bits, {8, 16, 32}) && in(t.check_every, {2, 4, 8, 16}) &&
-           in(t.map_threads, {64, 128, 256});
+           in(t.map_threads, {64, 128, 256}) && in(t.loop_graph, {0, 1});
 }
 
 }  // namespace
@@ -75,7 +81,7 @@ extern "C" {
 
 int curc_ctx_set_tuning(curc_ctx* ctx, const int32_t* knobs) {
     if (!ctx || !knobs) return CURC_ERR_ARG;
-    Tuning t{knobs[0], knobs[1], knobs[2], knobs[3]};
+    Tuning t{knobs[0], knobs[1], knobs[2], knobs[3], knobs[4]};
     if (!curc::valid(t)) {
         ctx->err = "tuning: a knob outside its candidate values";
         return CURC_ERR_ARG;
@@ -91,6 +97,7 @@ int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs) {
     knobs[1] = t.bitmap_bits;
     knobs[2] = t.check_every;
     knobs[3] = t.map_threads;
+    knobs[4] = t.loop_graph;
     return CURC_OK;
 }
 
@@ -156,7 +163,8 @@ int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read
         const Knob knobs[] = {{&Tuning::table_factor, {1, 2, 4, 8}, "overlap"},
                               {&Tuning::bitmap_bits, {8, 16, 32}, "overlap"},
                               {&Tuning::check_every, {4, 8, 16}, "overlap"},
-                              {&Tuning::map_threads, {64, 128, 256}, "mapping"}};
+                              {&Tuning::map_threads, {64, 128, 256}, "mapping"},
+                              {&Tuning::loop_graph, {0, 1}, "full_match"}};
         for (const Knob& k : knobs) {
             float tbest = 1e30f;
             int vbest = best.*(k.field);

@@ -90,7 +90,9 @@ int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep);
  * overlap index's bucket table size as a multiple of the prefix count
  * {1, 2, 4, 8}, presence-bitmap bits per prefix {8, 16, 32}, overlap passes
  * between host reads of the link count {2, 4, 8, 16}, threads per block of
- * the mapping kernel {64, 128, 256}.  None changes any result: every stream
+ * the mapping kernel {64, 128, 256}, full-match passes replayed on the device
+ * from a CUDA graph with a conditional while node (1) or queued launch by
+ * launch from the host (0).  None changes any result: every stream
  * is the same under every setting; only the time does.  curc_autotune runs
  * the given block (device memory) under the candidates one knob at a time,
  * keeps the fastest, and sets it on the context; with cache_path, choices
@@ -98,8 +100,8 @@ int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep);
  * down to a power of two), and *from_cache tells whether the file had one.
  * The k-mer length and the other derived parameters are part of the format
  * and are not tuned. */
-int curc_ctx_set_tuning(curc_ctx* ctx, const int32_t* knobs);
-int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs);
+int curc_ctx_set_tuning(curc_ctx* ctx, const int32_t* knobs); /* knobs[5] */
+int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs);       /* knobs[5] */
 int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
                   int paired_end, const char* cache_path, int* from_cache);
 /* Loads a cache file written by curc_autotune: every later block run of the

@@ -1,7 +1,8 @@
 """The autotuner's knobs change no result, on a B200.
 
 Every knob value (overlap bucket table factor, presence-bitmap bits,
-passes between link-count reads, mapping threads per block) runs the same
+passes between link-count reads, mapping threads per block, full-match
+passes replayed from a graph or queued per launch) runs the same
 blocks; every stage result and stream must equal the default setting's, and
 the default setting's must equal the oracle's.  Then curc_autotune picks a
 setting on a block, caches it per (read length, read-count bucket), and a
@@ -14,7 +15,8 @@ from tests.oracle_lib import OracleBlock, STAGE_RESULTS, stream_dtype, stream_na
 
 pytestmark = pytest.mark.gpu
 
-KNOB_VALUES = {"table_factor": [1, 2, 8], "bitmap_bits": [8, 32], "check_every": [2, 16], "map_threads": [64, 256]}
+KNOB_VALUES = {"table_factor": [1, 2, 8], "bitmap_bits": [8, 32], "check_every": [2, 16], "map_threads": [64, 256],
+               "loop_graph": [0]}
 
 
 def _results(ctx, L):
