@@ -374,6 +374,12 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     // still link when they are different reads (the head and the tail of one
     // chain, which then closes into a cycle, as the reference's merge does)
     if (cnt == 0 || acc.L < 2) return;
+    if (cnt == 1) {  // one end of each kind: nothing links when both are the same read
+        uint32_t ends[2];
+        read_small(ends, pre, 4, s);
+        read_small(ends + 1, suf, 4, s);
+        if (ends[0] == ends[1]) return;
+    }
     auto mk = a.mark();
     uint32_t* suf2 = a.alloc<uint32_t>(cnt);
     uint32_t* tmp = a.alloc<uint32_t>(cnt);

@@ -34,7 +34,12 @@ void* Arena::alloc_bytes(size_t bytes) {
             high_water_ = std::max(high_water_, in_use());
             return p;
         }
-        if (cur_ + 1 < chunks_.size() && chunks_[cur_ + 1].size >= bytes) {
+        // chunks after the current one are free: take the first that is
+        // large enough, moved up to follow the current one
+        size_t fit = cur_ + 1;
+        while (fit < chunks_.size() && chunks_[fit].size < bytes) ++fit;
+        if (fit < chunks_.size()) {
+            std::rotate(chunks_.begin() + cur_ + 1, chunks_.begin() + fit, chunks_.begin() + fit + 1);
             ++cur_;
             chunks_[cur_].used = 0;
             continue;
@@ -43,7 +48,14 @@ void* Arena::alloc_bytes(size_t bytes) {
     }
     size_t sz = std::max(bytes, chunk_);
     char* p = nullptr;
-    CURC_CHECK(cudaMalloc(&p, sz));
+    if (cudaMalloc(&p, sz) != cudaSuccess) {
+        // out of memory: give back the free chunks (all too small) and retry
+        cudaGetLastError();
+        const size_t keep = chunks_.empty() ? 0 : cur_ + 1;
+        for (size_t i = keep; i < chunks_.size(); ++i) CURC_CHECK(cudaFree(chunks_[i].base));
+        chunks_.resize(keep);
+        CURC_CHECK(cudaMalloc(&p, sz));
+    }
     // keep chunks ordered as used: insert after the current one
     Chunk c{p, sz, bytes};
     if (chunks_.empty()) {
