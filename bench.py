@@ -191,6 +191,18 @@ def map_bytes(st, L, strand):
             + st[f"map_candidates_{strand}"] * (32 + win))
 
 
+# Algorithmic bytes of the full-match pass loop (stage a6), per list entry
+# per pass, from the loop's own counters: a suffix entry has its 32-base key
+# gathered (one 32-byte sector of its row), moves through two merge levels
+# (12 bytes read and 12 written each), is read once by the pairing (12) and
+# is compacted (4 read, its link word's sector 32, 4 written); a prefix
+# entry is compacted with its key (12 read, link sector 32, 12 written).
+# The pairing's binary searches over the prefix keys are not counted, so
+# this is a lower bound.
+def full_match_bytes(st):
+    return st.get("fm_suffix_entries", 0) * (32 + 2 * 24 + 12 + 40) + st.get("fm_prefix_entries", 0) * 56
+
+
 # DRAM bytes per listed suffix of the probe kernel, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum over its 96 launches) on the
 # 2M-pair case of the same generator: 5.662e9 bytes / 20.21e6 probes.  The
@@ -315,7 +327,8 @@ def run_ours(a, rank, world):
                       "unmapped_n", "overlap_passes", "contested", "records", "mismatches",
                       "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits",
                       "overlap_searched", "overlap_compares", "overlap_links", "map_reads_fwd", "map_probes_fwd",
-                      "map_candidates_fwd", "map_reads_rc", "map_probes_rc", "map_candidates_rc", "overlap_rows"],
+                      "map_candidates_fwd", "map_reads_rc", "map_probes_rc", "map_candidates_rc", "overlap_rows",
+                      "fm_passes", "fm_suffix_entries", "fm_prefix_entries"],
                      [int(x) for x in ctx.get("stats", np.uint64)]))
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     step_s = dev_ms / 1000.0 / a.steps
@@ -691,6 +704,7 @@ def run_batched(a):
         ctx.batch_drain(lambda tk: dig.__setitem__(tk, digest(ctx, blocks[tickets.index(tk)].shape[1])))
         out["batched"] = bases / (time.perf_counter() - t) / 1e6
         out["batched_streams_equal"] = all(dig[tk] == plain[i] for i, tk in enumerate(tickets))
+        ctx.trim()  # the drain's pipelines are made again by the next drain
         # autotune one block per (read length, read-count bucket), then drain with per-block choices
         import torch
         cache = os.path.join(td, "tune.txt")
@@ -704,6 +718,8 @@ def run_batched(a):
             seen[key] = ctx.autotune(d.data_ptr(), b.shape[0], b.shape[1], False, False, cache)[0]
             del d
         out["autotune_s"] = time.perf_counter() - t
+        ctx.trim()
+        torch.cuda.empty_cache()
         out["tuned_buckets"] = {f"L{k[0]}_2^{k[1]}": v for k, v in seen.items()}
         ctx.set_tuning(table_factor=4, bitmap_bits=16, check_every=8, map_threads=128)
         ctx.use_tuning_cache(cache)
@@ -843,6 +859,10 @@ def main():
                                "whole_sort_ms": sub.get("sort_dedupe.radix")}),
         "roofline_resolve": roof("resolve_kernel (overlap passes, stage a4)", resolve_bytes(st, r["L"]),
                                  sub.get("overlap.resolve", 0.0), passes),
+        "roofline_full_match": roof("full-match pass loop (stage a6: key gather, two merge levels, pairing, "
+                                    "two compactions per pass; one CUDA graph, or per-launch with --loop-graph 0)",
+                                    full_match_bytes(st), r["stage_ms"].get("full_match", 0.0),
+                                    max(1, st.get("fm_passes", 0)), {"passes": st.get("fm_passes", 0)}),
         "roofline_map": roof("map_kernel forward + reverse complement (stage a9)",
                              map_bytes(st, r["L"], "fwd") + map_bytes(st, r["L"], "rc"),
                              sub.get("mapping.map_fwd", 0.0) + sub.get("mapping.map_rc", 0.0), 2),

@@ -38,6 +38,7 @@ def lib() -> ctypes.CDLL:
         L.curc_block_get.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(c_p), ctypes.POINTER(c_u64)]
         L.curc_block_stage_ms.argtypes = [c_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
         L.curc_ctx_keep_intermediates.argtypes = [c_p, c_int]
+        L.curc_ctx_trim.argtypes = [c_p]
         L.curc_ctx_set_mismatch_model.argtypes = [c_p, c_p, c_u64]
         L.curc_ctx_set_tuning.argtypes = [c_p, c_p]
         L.curc_ctx_get_tuning.argtypes = [c_p, c_p]
@@ -196,6 +197,11 @@ class Context:
 
     def keep_intermediates(self, keep: bool):
         self._check(lib().curc_ctx_keep_intermediates(self._h, int(keep)), "curc_ctx_keep_intermediates")
+
+    def trim(self):
+        """Frees the device memory the context keeps between blocks (arena,
+        batch pipelines); the last run's results stay readable."""
+        self._check(lib().curc_ctx_trim(self._h), "curc_ctx_trim")
 
     def stage_ms(self, stage: str) -> float:
         v = ctypes.c_float()

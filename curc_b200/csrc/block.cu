@@ -44,6 +44,8 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
         if (it != tune_cache->end()) p.tune = it->second;
     }
     n = uint32_t(n_reads);
+    fm_tally = nullptr;
+    mo.tally = nullptr;
     host.clear();
     stage_ms.clear();
     pinned.reset();
@@ -128,6 +130,8 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
 
     // a6 (compress.cu:1576-1591)
     T.begin("full_match");
+    fm_tally = arena.alloc<unsigned long long>(3);
+    CURC_CHECK(cudaMemsetAsync(fm_tally, 0, 3 * sizeof(unsigned long long), s));
     {
         auto mk = arena.mark();
         uint8_t* pf = arena.alloc<uint8_t>(n_ref ? n_ref : 1);
@@ -141,7 +145,7 @@ void Block::run(const uint8_t* d_seq, uint64_t n_reads, int L, bool po, bool pe)
         select_flagged(ref_ids, pf, pre, n_ref, counts + 2, arena, s);
         select_flagged(ref_ids, sf, suf, n_ref, counts + 3, arena, s);
         const uint32_t cnt = read_scalar(counts + 3, s);
-        full_match_packed(p, db, pre, suf, cnt, next, prev, offset, arena, s);
+        full_match_packed(p, db, pre, suf, cnt, next, prev, offset, arena, s, fm_tally);
         arena.release(mk);
     }
     T.end();
@@ -320,6 +324,19 @@ int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* 
     *ptr = it->second.ptr;
     *bytes = it->second.size;
     return CURC_OK;
+}
+
+int curc_ctx_trim(curc_ctx* ctx) {
+    if (!ctx) return CURC_ERR_ARG;
+    if (ctx->batch && !ctx->batch->items.empty()) {
+        ctx->err = "trim: blocks are queued for a drain";
+        return CURC_ERR_STATE;
+    }
+    return guarded(ctx, [&] {
+        CURC_CHECK(cudaStreamSynchronize(ctx->block->stream));
+        if (ctx->batch) ctx->batch->pool.clear();  // the extra pipelines, input slots and staging
+        ctx->block->arena.trim();
+    });
 }
 
 int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep) {

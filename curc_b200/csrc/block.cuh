@@ -38,6 +38,7 @@ struct Block {
     Assembled hq;
     MapOut mo;
     OverlapStats ostats;
+    unsigned long long* fm_tally = nullptr;  // full-match counters (device, 3)
     // emission
     uint32_t n_map = 0, n_records = 0, n_ug = 0, n_un = 0, n_mis = 0;
     uint32_t *ug = nullptr, *un = nullptr, *pe_order = nullptr;

@@ -96,11 +96,23 @@ struct FmOff {
 // by read[off-1, L), so these counts give the base runs' bounds.  Each
 // thread counts in four 16-bit fields (a resident grid leaves it far fewer
 // than 65536 entries), then one atomic per block and base.
+// With tally: one thread adds the pass to the counters (passes with both
+// lists non-empty, their suffix and prefix entries; mp_dev is the prefix
+// list's length).
 template <class Acc>
 __global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, const uint32_t* __restrict__ m_dev,
-                                 FmOff fo, uint64_t* __restrict__ key, uint32_t* __restrict__ sym_count) {
+                                 FmOff fo, uint64_t* __restrict__ key, uint32_t* __restrict__ sym_count,
+                                 const uint32_t* __restrict__ mp_dev, unsigned long long* __restrict__ tally) {
     const uint32_t m = *m_dev;
     const int off = fo.get();
+    if (tally && blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t mp = *mp_dev;
+        if (m && mp) {
+            tally[0] += 1;
+            tally[1] += m;
+            tally[2] += mp;
+        }
+    }
     uint64_t c = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const uint32_t id = ids[i];
@@ -369,7 +381,7 @@ __global__ void fm_cond_kernel(cudaGraphConditionalHandle h, int* offp, const ui
 // one graph launch runs the whole loop.
 template <class Acc>
 void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt, uint32_t* next, uint32_t* prev,
-                     uint16_t* offset, bool use_graph, Arena& a, cudaStream_t s) {
+                     uint16_t* offset, bool use_graph, unsigned long long* tally, Arena& a, cudaStream_t s) {
     // nothing to link without ends; a single prefix and a single suffix can
     // still link when they are different reads (the head and the tail of one
     // chain, which then closes into a cycle, as the reference's merge does)
@@ -400,7 +412,7 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
     const int gk = resident_grid(list_keys_kernel<Acc>, 256, cnt);
     const int gm = resident_grid(merge_level_kernel<Acc>, 256, div_up(cnt, MP_ITEMS));
     const int gg = resident_grid(merge_groups_kernel<Acc>, 128, cnt);
-    list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, pre, len, FmOff{0, nullptr}, pk, nullptr);
+    list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, pre, len, FmOff{0, nullptr}, pk, nullptr, nullptr, nullptr);
     CURC_LAUNCH_CHECK();
     // 2-bit reads: the base runs' bounds come from counts taken with the keys
     constexpr bool by_count = Acc::ALPHA == 4;
@@ -423,7 +435,8 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
             run_bounds_kernel<Acc><<<1, 256, 0, s>>>(acc, suf, ms_in, fo, bounds);
             CURC_LAUNCH_CHECK();
         }
-        list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, suf, ms_in, fo, sk, by_count ? bounds : nullptr);
+        list_keys_kernel<Acc><<<gk, 256, 0, s>>>(acc, suf, ms_in, fo, sk, by_count ? bounds : nullptr, mp_in,
+                                                  tally);
         CURC_LAUNCH_CHECK();
         {
             // levels: runs merged in pairs, then pairs of pairs, ...; the last
@@ -564,8 +577,9 @@ __global__ void ends_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, 
 }  // namespace
 
 void full_match_packed(const BlockParams& p, const uint64_t* db, uint32_t* pre, uint32_t* suf, uint32_t cnt,
-                       uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s) {
-    full_match_loop(PackedAcc{db, p.W, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, a, s);
+                       uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s,
+                       unsigned long long* tally) {
+    full_match_loop(PackedAcc{db, p.W, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, tally, a, s);
 }
 
 void sort_ids_by_ascii(const uint8_t* reads, int L, uint32_t* ids, uint32_t m, Arena& a, cudaStream_t s) {
@@ -606,7 +620,7 @@ void full_match_ascii(const BlockParams& p, const uint8_t* reads, uint32_t* ids,
     select_flagged(ids, pf, pre, m, counts + 0, a, s);
     select_flagged(ids, sf, suf, m, counts + 1, a, s);
     const uint32_t cnt = read_scalar(counts + 0, s);
-    full_match_loop(AsciiAcc{reads, 0, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, a, s);
+    full_match_loop(AsciiAcc{reads, 0, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, nullptr, a, s);
     a.release(mk);
 }
 

@@ -95,8 +95,10 @@ __device__ __forceinline__ int ascii_mismatches(const uint64_t* __restrict__ ref
 // on the read's count so far).  The warp lists the candidates of 32 probes
 // at a time, evaluates them 32 at a time in that order, and stops after the
 // chunk in which a count <= target appears.  A candidate's count is exact
-// below the read's starting count (the bound of the early exit), which is
-// all the comparison needs.
+// below the smallest count met so far (the bound of the early exit, as in
+// the reference's loop; the same in every lane, and above target while the
+// loop runs), which is all the comparison needs: a candidate matters only
+// if it reaches target or strictly improves on that count.
 // One read per warp; returns (in every lane) the probes listed and the
 // candidates compared for the algorithmic-byte counters.
 template <bool RC>
@@ -163,7 +165,7 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
                 const uint64_t shift = RC ? uint64_t(L - k - oj) : uint64_t(oj);
                 if (refpos >= shift && refpos - shift + L <= ref_len) {
                     mp = refpos - shift;
-                    c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, init) : packed_mismatches<RC>(ref, mp, rd, L, init);
+                    c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best) : packed_mismatches<RC>(ref, mp, rd, L, best);
                 }
             }
             // the loop stops at the first count <= target

@@ -281,13 +281,16 @@ __global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t
     block_tally<unsigned long long>(rows, &tally[6]);
 }
 
+constexpr uint32_t RESOLVE_BATCH = 16;
+
 // A suffix alone on its run links directly.  A run claimed by several
 // suffixes is resolved by its lowest-index member, which visits the members
-// in list order (ascending index; runs are small, so repeated minimum
-// search) and gives each the first free non-self prefix, exactly the
-// sequential loop of compress.cu:1474.  The run's bookkeeping is reset for
-// the next pass by the thread that used it.  tally[2] counts links,
+// in list order (ascending index, in sorted batches from one walk of the
+// member list each) and gives each the first free non-self prefix, exactly
+// the sequential loop of compress.cu:1474.  The run's bookkeeping is reset
+// for the next pass by the thread that used it.  tally[2] counts links,
 // tally[3] the members of contested runs.
+
 __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32_t* __restrict__ suf,
                                                       const uint64_t* __restrict__ sufw,
                                                       const uint4* __restrict__ hlist,
@@ -310,20 +313,36 @@ __global__ void __launch_bounds__(512) resolve_kernel(OverlapCtx c, const uint32
                 take_from_bucket(c, h);
             }
         } else if (rs.lead == j) {
+            // members in ascending list index: each walk of the run's member
+            // list keeps the RESOLVE_BATCH smallest above the last one
+            // handled, in order, so a run of n members takes
+            // ceil(n / RESOLVE_BATCH) walks instead of n
             contested += n;
+            uint32_t buf[RESOLVE_BATCH];
             uint32_t last = 0;
             bool first = true;
-            for (uint32_t k = 0; k < n; ++k) {
-                uint32_t best = INVALID;
-                for (uint32_t m = rs.head; m != INVALID; m = gnext[m])
-                    if ((first || m > last) && m < best) best = m;
-                if (best == INVALID) break;
-                if (link_first_free(c, suf[best], sufw + uint64_t(best) * c.W, lo, e, off)) {
-                    linked[best] = 1;
-                    ++links;
-                    take_from_bucket(c, h);
+            for (;;) {
+                uint32_t cnt = 0;
+                for (uint32_t m = rs.head; m != INVALID; m = gnext[m]) {
+                    if (!first && m <= last) continue;
+                    if (cnt == RESOLVE_BATCH && m >= buf[RESOLVE_BATCH - 1]) continue;
+                    uint32_t t = cnt < RESOLVE_BATCH ? cnt++ : RESOLVE_BATCH - 1;
+                    while (t > 0 && buf[t - 1] > m) {
+                        buf[t] = buf[t - 1];
+                        --t;
+                    }
+                    buf[t] = m;
                 }
-                last = best;
+                for (uint32_t t = 0; t < cnt; ++t) {
+                    const uint32_t best = buf[t];
+                    if (link_first_free(c, suf[best], sufw + uint64_t(best) * c.W, lo, e, off)) {
+                        linked[best] = 1;
+                        ++links;
+                        take_from_bucket(c, h);
+                    }
+                }
+                if (cnt < RESOLVE_BATCH) break;
+                last = buf[RESOLVE_BATCH - 1];
                 first = false;
             }
         } else {

@@ -81,6 +81,13 @@ void Arena::reset() {
     cur_ = 0;
 }
 
+void Arena::trim() {
+    for (auto& c : chunks_) CURC_CHECK(cudaFree(c.base));
+    chunks_.clear();
+    cur_ = 0;
+    high_water_ = 0;
+}
+
 void Arena::release(const Mark& m) {
     if (chunks_.empty()) return;
     for (size_t i = m.chunk + 1; i < chunks_.size(); ++i) chunks_[i].used = 0;

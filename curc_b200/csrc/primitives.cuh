@@ -28,6 +28,9 @@ public:
     template <class T>
     T* alloc(size_t n) { return static_cast<T*>(alloc_bytes(n * sizeof(T))); }
     void reset();
+    // Frees every chunk (nothing may be in use: the stream work that used
+    // them must have completed; cudaFree waits for the device).
+    void trim();
     size_t high_water() const { return high_water_; }
     size_t in_use() const;
 

@@ -686,14 +686,17 @@ void Block::refmatch_all() {
     // passes: unlinked suffixes, suffixes probed, probes that met a prefix,
     // probes that searched a bucket, prefix comparisons; overlap links; for
     // the mapping, forward then reverse complement: reads searched, k-mer
-    // probes listed, candidate windows compared; prefix rows the probes read
-    unsigned long long mt[6] = {0, 0, 0, 0, 0, 0};
+    // probes listed, candidate windows compared; prefix rows the probes read;
+    // full-match passes with both lists non-empty, and over them the summed
+    // suffix and prefix list lengths
+    unsigned long long mt[6] = {0, 0, 0, 0, 0, 0}, ft[3] = {0, 0, 0};
     if (mo.tally) read_small(mt, mo.tally, sizeof(mt), s);
-    const uint64_t stats[26] = {n,          m,           NN,         n_ref,         U,           n_map,
+    if (fm_tally) read_small(ft, fm_tally, sizeof(ft), s);
+    const uint64_t stats[29] = {n,          m,           NN,         n_ref,         U,           n_map,
                                 n_ug,       n_un,        ostats.passes, ostats.contested, n_records, n_mis,
                                 ostats.suffixes, ostats.active_sum, ostats.probes, ostats.hits, ostats.searched,
                                 ostats.compares, ostats.links, mt[0], mt[1], mt[2], mt[3], mt[4], mt[5],
-                                ostats.rows};
+                                ostats.rows, ft[0], ft[1], ft[2]};
     put("stats", std::vector<uint8_t>(reinterpret_cast<const uint8_t*>(stats),
                                       reinterpret_cast<const uint8_t*>(stats) + sizeof(stats)));
 }

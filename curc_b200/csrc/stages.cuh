@@ -86,9 +86,12 @@ void chain_filter(uint32_t n, const uint32_t* sorted, uint32_t m, uint32_t* next
                   cudaStream_t s);
 
 // ---- a6/a7 (fullmatch.cu)
-// Packed reads: prefix/suffix lists are consumed (scratch).
+// Packed reads: prefix/suffix lists are consumed (scratch).  tally (device,
+// 3 counters, optional): passes with both lists non-empty, and their summed
+// suffix and prefix list lengths.
 void full_match_packed(const BlockParams& p, const uint64_t* db, uint32_t* pre, uint32_t* suf, uint32_t cnt,
-                       uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s);
+                       uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s,
+                       unsigned long long* tally = nullptr);
 // ASCII reads (N reads): sorts `ids` (count m) by content, links exact
 // duplicates, then runs the suffix-prefix merge.  next/prev/offset have
 // n_total entries and are initialised here.

@@ -86,6 +86,13 @@ int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint1
  * streams are always returned.  No reference counterpart. */
 int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep);
 
+/* Frees the device memory a context keeps between blocks: its pipeline's
+ * arena and the extra pipelines, input slots and pinned staging of the
+ * batched path (they are made again on the next run or drain).  Results of
+ * the last run stay readable.  CURC_ERR_STATE while blocks are queued.  No
+ * reference counterpart. */
+int curc_ctx_trim(curc_ctx* ctx);
+
 /* Autotuner (no counterpart in the reference).  Knobs, in this order: the
  * overlap index's bucket table size as a multiple of the prefix count
  * {1, 2, 4, 8}, presence-bitmap bits per prefix {8, 16, 32}, overlap passes
