@@ -210,6 +210,19 @@ def full_match_bytes(st):
 PROBE_DRAM_BYTES_PER_PROBE = 5.662e9 / 20.207e6
 
 
+STAT_NAMES = ["reads", "non_n", "n_reads", "pseudogenome_reads", "unmatched", "mapped", "unmapped",
+              "unmapped_n", "overlap_passes", "contested", "records", "mismatches",
+              "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits",
+              "overlap_searched", "overlap_compares", "overlap_links", "map_reads_fwd", "map_probes_fwd",
+              "map_candidates_fwd", "map_reads_rc", "map_probes_rc", "map_candidates_rc", "overlap_rows",
+              "fm_passes", "fm_suffix_entries", "fm_prefix_entries"]
+
+
+def block_stats(ctx):
+    """The last block run's counters (the library's "stats" result)."""
+    return dict(zip(STAT_NAMES, [int(x) for x in ctx.get("stats", np.uint64)]))
+
+
 def rank_seed(rank):
     """Seed of a rank's block: every rank compresses its own block of the same
     generator (independent blocks, weak scaling)."""
@@ -323,13 +336,7 @@ def run_ours(a, rank, world):
                                            "unmap_n_ref", "ref_off", "ref_len_map", "unmap_ref_off", "unmap_ref_len",
                                            "unmap_n_ref_off", "unmap_n_ref_len"])
     d2h += sum(ctx.get(f"mis_off_{m}").nbytes for m in range(1, L // 5 + 1))
-    stats = dict(zip(["reads", "non_n", "n_reads", "pseudogenome_reads", "unmatched", "mapped", "unmapped",
-                      "unmapped_n", "overlap_passes", "contested", "records", "mismatches",
-                      "overlap_suffixes", "overlap_active_sum", "overlap_probes", "overlap_hits",
-                      "overlap_searched", "overlap_compares", "overlap_links", "map_reads_fwd", "map_probes_fwd",
-                      "map_candidates_fwd", "map_reads_rc", "map_probes_rc", "map_candidates_rc", "overlap_rows",
-                      "fm_passes", "fm_suffix_entries", "fm_prefix_entries"],
-                     [int(x) for x in ctx.get("stats", np.uint64)]))
+    stats = block_stats(ctx)
     stats.update(dict(zip(["hq_len", "unmap_len", "unmap_n_len"], [int(x) for x in ctx.get("sizes", np.uint64)[:3]])))
     step_s = dev_ms / 1000.0 / a.steps
     step_s, e2e_s, e2e_plain_s = reduce_max([step_s, e2e_s, e2e_plain_s], world, f"cuda:{dev}")
@@ -601,6 +608,11 @@ def run_large(a):
                 ms.append(ctx.stage_ms("total"))
         stage = {k: ctx.stage_ms(k) for k in ["pack", "sort_dedupe", "overlap", "chain_filter", "full_match",
                                               "assembly", "mapping", "emit", "unmapped_refs", "refmatch"]}
+        out["block_stats"] = block_stats(ctx)
+        out["substage_ms"] = {k: round(ctx.stage_ms(k), 3) for k in
+                              ["mapping.index_fwd", "mapping.map_fwd", "mapping.index_rc", "mapping.map_rc",
+                               "overlap.probe", "overlap.resolve", "refmatch.probe_self", "full_match.graph"]
+                              if _has_stage(ctx, k)}
         pack_ms = stage["pack"]
         del d
         torch.cuda.empty_cache()
@@ -715,6 +727,7 @@ def run_batched(a):
             if key in seen:
                 continue
             d = torch.from_numpy(b.reshape(-1)).cuda()
+            print(f"autotune bucket L={key[0]} 2^{key[1]} on {b.shape[0]} reads", file=sys.stderr, flush=True)
             seen[key] = ctx.autotune(d.data_ptr(), b.shape[0], b.shape[1], False, False, cache)[0]
             del d
         out["autotune_s"] = time.perf_counter() - t

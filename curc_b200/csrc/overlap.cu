@@ -220,19 +220,22 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
     const uint32_t e = c.kr[h + 1];
     uint32_t count = e - lo;
     ++searched;
+    // lower bound; the entry it ends on (if below e) is the last one that
+    // compared >= 0, so its comparison decides equality without a re-read
+    int at_hi = 1;
     while (count > 0) {
         ++compares;
         const uint32_t step = count / 2, it = lo + step;
-        if (cmp_prefix(c, it, sr, off, cl, rows) < 0) {
+        const int r = cmp_prefix(c, it, sr, off, cl, rows);
+        if (r < 0) {
             lo = it + 1;
             count -= step + 1;
         } else {
             count = step;
+            at_hi = r;
         }
     }
-    if (lo >= e) return false;
-    ++compares;
-    if (cmp_prefix(c, lo, sr, off, cl, rows) != 0) return false;
+    if (lo >= e || at_hi != 0) return false;
     // run membership: count, lowest list index, and a list of members
     atomicAdd(&run[lo].claim, 1u);
     atomicMin(&run[lo].lead, j);

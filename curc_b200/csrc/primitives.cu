@@ -3,6 +3,7 @@
 #include <atomic>
 #include <cstring>
 #include <stdexcept>
+#include <string>
 
 #include <mutex>
 
@@ -54,7 +55,17 @@ void* Arena::alloc_bytes(size_t bytes) {
         const size_t keep = chunks_.empty() ? 0 : cur_ + 1;
         for (size_t i = keep; i < chunks_.size(); ++i) CURC_CHECK(cudaFree(chunks_[i].base));
         chunks_.resize(keep);
-        CURC_CHECK(cudaMalloc(&p, sz));
+        if (cudaMalloc(&p, sz) != cudaSuccess) {
+            cudaGetLastError();
+            size_t held = 0, fr = 0, tot = 0;
+            for (const auto& c : chunks_) held += c.size;
+            cudaMemGetInfo(&fr, &tot);
+            const std::string msg = "arena: out of device memory for " + std::to_string(sz >> 20) +
+                                    " MiB (the arena holds " + std::to_string(held >> 20) + " MiB in " +
+                                    std::to_string(chunks_.size()) + " chunks; " + std::to_string(fr >> 20) +
+                                    " MiB free on the device)";
+            throw CudaError(cudaErrorMemoryAllocation, msg.c_str());
+        }
     }
     // keep chunks ordered as used: insert after the current one
     Chunk c{p, sz, bytes};
@@ -77,6 +88,20 @@ size_t Arena::in_use() const {
 }
 
 void Arena::reset() {
+    // Several chunks (blocks of changing sizes grew the arena): give them
+    // back and keep one chunk that holds the largest run seen, so later runs
+    // allocate nothing and chunks do not pile up.  Nothing is in use here.
+    if (chunks_.size() > 1) {
+        const size_t mib = size_t(1) << 20;
+        const size_t need = std::max(chunk_, (high_water_ + mib - 1) / mib * mib);
+        for (auto& c : chunks_) CURC_CHECK(cudaFree(c.base));
+        chunks_.clear();
+        char* p = nullptr;
+        if (cudaMalloc(&p, need) == cudaSuccess)
+            chunks_.push_back(Chunk{p, need, 0});
+        else
+            cudaGetLastError();  // no room for one chunk: allocate on demand again
+    }
     for (auto& c : chunks_) c.used = 0;
     cur_ = 0;
 }

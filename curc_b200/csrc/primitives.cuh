@@ -14,9 +14,11 @@ namespace curc {
 
 uint64_t launches();
 
-// Bump allocator over large device chunks.  reset() keeps the chunks, so a
+// Bump allocator over large device chunks.  reset() keeps the memory, so a
 // pipeline that runs block after block allocates device memory only while
-// it grows.  Alignment 256 bytes (TMA and vector loads need 16).
+// it grows; when a run needed more than one chunk, reset() replaces them by
+// one chunk of the largest run's size.  Alignment 256 bytes (TMA and vector
+// loads need 16).
 class Arena {
 public:
     explicit Arena(size_t chunk = size_t(1) << 30) : chunk_(chunk) {}

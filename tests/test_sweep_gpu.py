@@ -15,7 +15,7 @@ from tests.oracle_lib import OracleBlock, STAGE_RESULTS, stream_dtype, stream_na
 
 pytestmark = pytest.mark.gpu
 
-SEEDS = [1, 2, 3]
+SEEDS = [1, 2, 3, 4, 5, 6]
 CASES_PER_SEED = 24
 MAX_READS = 1500
 
