@@ -83,9 +83,11 @@ struct OverlapControl {
 
 // a3+a4: k-mer index over prefix reads and the max_off-1 overlap passes.
 // `ctl` (test use only) replays another serialisation of the contested runs
-// and records every contested run.
+// and records every contested run.  `threads` run the per-pass searches in
+// parallel; the links are made in order, so results do not depend on it.
 void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_t>& sorted_ids,
-                  uint32_t* next, uint32_t* prev, uint16_t* offset, const OverlapControl* ctl = nullptr);
+                  uint32_t* next, uint32_t* prev, uint16_t* offset, const OverlapControl* ctl = nullptr,
+                  int threads = 1);
 
 // a5: chain filter; returns (ref ids, unmatched ids), both in sorted order.
 void chain_filter(size_t reads_count, const std::vector<uint32_t>& sorted_ids,
@@ -131,8 +133,10 @@ struct RefMatcherIndex {
     const uint64_t* ref = nullptr;
 };
 void refmatch_index(const uint64_t* ref, uint64_t ref_len, RefMatcherIndex& ix);
+// `threads` search the probe groups in parallel; the matches are taken in
+// group order, so results do not depend on it.
 void refmatch_apply(const RefMatcherIndex& ix, std::string& dest, bool dest_has_n, bool dest_is_ref,
-                    std::string& map_off, std::string& map_len);
+                    std::string& map_off, std::string& map_len, int threads = 1);
 
 // ---- whole block ----
 struct BlockInput {

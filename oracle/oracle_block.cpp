@@ -62,7 +62,7 @@ void compress_block(const Params& p, const BlockInput& in, BlockStreams& out, in
     OverlapControl ctl;
     ctl.picks = in.contest_picks;
     ctl.log = &out.contests;
-    overlap_link(p, in.db, out.sorted_ids, out.next.data(), out.prev.data(), out.offset.data(), &ctl);
+    overlap_link(p, in.db, out.sorted_ids, out.next.data(), out.prev.data(), out.offset.data(), &ctl, threads);
     // a5
     chain_filter(n, out.sorted_ids, out.next.data(), out.prev.data(), out.offset.data(), out.ref_ids,
                  out.unmatch_ids);
@@ -240,10 +240,11 @@ void compress_block(const Params& p, const BlockInput& in, BlockStreams& out, in
     if (hq.seq.size() >= 36) {
         RefMatcherIndex ix;
         refmatch_index(hq_bin.data(), hq.seq.size(), ix);
-        if (!out.unmap_ref.empty()) refmatch_apply(ix, out.unmap_ref, false, false, out.unmap_ref_off, out.unmap_ref_len);
+        if (!out.unmap_ref.empty())
+            refmatch_apply(ix, out.unmap_ref, false, false, out.unmap_ref_off, out.unmap_ref_len, threads);
         if (!out.unmap_n_ref.empty())
-            refmatch_apply(ix, out.unmap_n_ref, true, false, out.unmap_n_ref_off, out.unmap_n_ref_len);
-        refmatch_apply(ix, out.ref, false, true, out.ref_off, out.ref_len_map);
+            refmatch_apply(ix, out.unmap_n_ref, true, false, out.unmap_n_ref_off, out.unmap_n_ref_len, threads);
+        refmatch_apply(ix, out.ref, false, true, out.ref_off, out.ref_len_map, threads);
     }
 }
 

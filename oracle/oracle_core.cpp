@@ -160,7 +160,7 @@ static int cmp_shifted(const uint64_t* a, uint64_t aoff, const uint64_t* b, uint
 }
 
 void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_t>& sorted,
-                  uint32_t* next, uint32_t* prev, uint16_t* offset, const OverlapControl* ctl) {
+                  uint32_t* next, uint32_t* prev, uint16_t* offset, const OverlapControl* ctl, int threads) {
     const int W = p.unit, L = p.read_len, k = p.kmer_size, kip = p.kmer_index_pos;
     // compress.cu:1427-1438: prefix set (no duplicate predecessor) and suffix set
     std::vector<uint32_t> pre, suf;
@@ -195,8 +195,13 @@ void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_
         for (uint32_t s : suf)
             if (std::find(order.begin(), order.begin() + npick, s) == order.begin() + npick) order.push_back(s);
         std::vector<std::pair<uint32_t, uint32_t>> runs;  // (run, suffix) of suffixes with a matching prefix
-        for (uint32_t s : order) {
-            const uint64_t* sr = db + size_t(s) * W;
+        // the searches read only the prefix index and the reads, which no
+        // link changes, so they run in parallel; the links below are made
+        // one suffix at a time in the visiting order
+        std::vector<size_t> los(order.size()), his(order.size());
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads)
+        for (size_t i = 0; i < order.size(); ++i) {
+            const uint64_t* sr = db + size_t(order[i]) * W;
             uint32_t h = uint32_t(murmur64(word_at(sr, kip + off, k)) & mask);
             auto rng = std::equal_range(vk.begin(), vk.end(), h);
             size_t lo = rng.first - vk.begin(), hi = rng.second - vk.begin();
@@ -211,6 +216,13 @@ void overlap_link(const Params& p, const uint64_t* db, const std::vector<uint32_
                     cnt = step;
                 }
             }
+            los[i] = lo;
+            his[i] = hi;
+        }
+        for (size_t i = 0; i < order.size(); ++i) {
+            const uint32_t s = order[i];
+            const uint64_t* sr = db + size_t(s) * W;
+            const size_t lo = los[i], hi = his[i];
             if (ctl && ctl->log && lo < hi && cmp_shifted(db + size_t(va[lo]) * W, 0, sr, off, cl) == 0)
                 runs.push_back({uint32_t(lo), s});
             for (size_t q = lo; q < hi; ++q) {
@@ -653,7 +665,7 @@ static void write_frugal(std::string& s, uint64_t v) {  // PgSAHelpers::writeUIn
 }
 
 void refmatch_apply(const RefMatcherIndex& ix, std::string& dest, bool dest_has_n, bool dest_is_ref,
-                    std::string& map_off, std::string& map_len) {
+                    std::string& map_off, std::string& map_len, int threads) {
     // compress.cu:746-992
     map_off.clear();
     map_len.clear();
@@ -678,7 +690,7 @@ void refmatch_apply(const RefMatcherIndex& ix, std::string& dest, bool dest_has_
     };
     auto rsym = [&](uint64_t i) { return base_at(ix.ref, i); };
     std::vector<Match> m;
-    auto probe = [&](uint64_t dpos) -> bool {
+    auto probe = [&](uint64_t dpos, Match& found) -> bool {
         uint32_t h = marush36([&](int t) { return dsym(dpos + t); }) & ix.mask;
         uint64_t b = ix.key_ranges[h], e = ix.key_ranges[h + 1];
         for (uint64_t j = b; j < e; ++j) {
@@ -703,25 +715,33 @@ void refmatch_apply(const RefMatcherIndex& ix, std::string& dest, bool dest_has_
                 }
                 while (cl && dsym(dc++) == rsym(sc++)) --cl;
                 if (cl == 0) {
-                    m.push_back({p2 + 1, right - p1 - 1, p1 + 1});
+                    found = {p2 + 1, right - p1 - 1, p1 + 1};
                     return true;
                 }
             }
         }
         return false;
     };
-    if (!dest_has_n) {
-        // segments of 4 probes; the probes of the last segment at index dic
-        // or later take no hit (their 36-mer runs past the end, and a hit
-        // there would end past it, which the reference's compaction cannot
-        // handle: compress.cu:910-913, 960-963)
-        const uint64_t segs = (dic + 3) / 4;
-        for (uint64_t i = 0; i < segs; ++i)
-            for (uint64_t s = 0; s < 4 && i * 4 + s < dic; ++s)
-                if (probe((i * 4 + s) * RM_DEST_STEP)) break;
-    } else {
-        for (uint64_t i = 0; i < dic; ++i) probe(i * RM_DEST_STEP);
-    }
+    // Probe groups are independent (the first hit of a group wins) and read
+    // only the index and the strings, so they are searched in parallel and
+    // their matches taken in group order.
+    // Without N: groups of 4 probes; the probes of the last group at index
+    // dic or later take no hit (their 36-mer runs past the end, and a hit
+    // there would end past it, which the reference's compaction cannot
+    // handle: compress.cu:910-913, 960-963).  With N: one probe per group.
+    const uint64_t per = dest_has_n ? 1 : 4;
+    const uint64_t groups = (dic + per - 1) / per;
+    std::vector<Match> found(groups);
+    std::vector<uint8_t> hit(groups, 0);
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads)
+    for (uint64_t i = 0; i < groups; ++i)
+        for (uint64_t q = 0; q < per && i * per + q < dic; ++q)
+            if (probe((i * per + q) * RM_DEST_STEP, found[i])) {
+                hit[i] = 1;
+                break;
+            }
+    for (uint64_t i = 0; i < groups; ++i)
+        if (hit[i]) m.push_back(found[i]);
     if (m.size() > cap) m.resize(cap);  // capacity drop, first entries in index order kept
     if (m.empty()) return;
     for (auto& x : m) x.dst = dl - (x.dst + x.len);

@@ -29,3 +29,17 @@ def test_records_match_pseudogenome(case):
     # the read's bases at its position
     windows = hq[pos[:, None] + np.arange(L)[None, :]]
     assert np.array_equal(windows, seqs[ids])
+
+
+@pytest.mark.parametrize("case", ["se100_20k", "se250_8k", "pe150", "dups"])
+def test_oracle_results_do_not_depend_on_threads(case):
+    """The oracle searches overlap passes, RefMatcher probe groups and the
+    mapping in parallel but links and takes matches in order: one thread and
+    eight give the same stage results and streams."""
+    from tests.oracle_lib import STAGE_RESULTS, stream_dtype, stream_names
+    seqs, po, pe = CASES[case]()
+    one = OracleBlock(seqs, po, pe, threads=1)
+    many = OracleBlock(seqs, po, pe, threads=8)
+    names = list(STAGE_RESULTS.items()) + [(s, stream_dtype(s)) for s in stream_names(seqs.shape[1])]
+    bad = [nm for nm, dt in names if not np.array_equal(one.get(nm, dt), many.get(nm, dt))]
+    assert not bad, bad
