@@ -67,8 +67,9 @@ def parse():
                          "whole-file round trip and learned-coder bytes; batched: the 64 mixed blocks at full "
                          "scale, one block at a time against the batched drain, default against autotuned "
                          "launch choices, streams compared; each prints one JSON line")
-    ap.add_argument("--loop-graph", type=int, default=1, choices=[0, 1],
-                    help="full-match passes replayed from a CUDA graph (1) or queued launch by launch (0)")
+    ap.add_argument("--fm-loop", type=int, default=None, choices=[0, 1, 2],
+                    help="full-match pass loop: 0 a launch per kernel, 1 one CUDA graph, 2 one persistent "
+                         "cooperative kernel (default: the library's)")
     ap.add_argument("--large-reads", type=int, default=40_000_000)
     ap.add_argument("--batched-blocks", type=int, default=16)
     ap.add_argument("--batched-scale", type=float, default=0.1)
@@ -269,7 +270,8 @@ def run_ours(a, rank, world):
     dseq = host.to(f"cuda:{dev}")
     ctx = Context(dev)
     ctx.keep_intermediates(False)
-    ctx.set_tuning(loop_graph=a.loop_graph)
+    if a.fm_loop is not None:
+        ctx.set_tuning(fm_loop=a.fm_loop)
 
     def dev_step():
         ctx.block_run_device(dseq.data_ptr(), n, L, True, True)
@@ -881,7 +883,7 @@ def main():
         "roofline_resolve": roof("resolve_kernel (overlap passes, stage a4)", resolve_bytes(st, r["L"]),
                                  sub.get("overlap.resolve", 0.0), passes),
         "roofline_full_match": roof("full-match pass loop (stage a6: key gather, two merge levels, pairing, "
-                                    "two compactions per pass; one CUDA graph, or per-launch with --loop-graph 0)",
+                                    "two compactions per pass; one CUDA graph, or per-launch with --fm-loop 0)",
                                     full_match_bytes(st), r["stage_ms"].get("full_match", 0.0),
                                     max(1, st.get("fm_passes", 0)), {"passes": st.get("fm_passes", 0)}),
         "roofline_map": roof("map_kernel forward + reverse complement (stage a9)",

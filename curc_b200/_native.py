@@ -256,7 +256,7 @@ class Context:
                     "curc_compress_files")
         return reads.value, blocks.value
 
-    TUNING_KNOBS = ("table_factor", "bitmap_bits", "check_every", "map_threads", "loop_graph")
+    TUNING_KNOBS = ("table_factor", "bitmap_bits", "check_every", "map_threads", "fm_loop")
 
     def tuning(self) -> dict:
         k = (ctypes.c_int32 * len(self.TUNING_KNOBS))()

@@ -91,11 +91,28 @@ struct FmOff {
     __device__ __forceinline__ int get() const { return p ? *p : v; }
 };
 
-// Keys of the list entries at offset off.  With sym_count (2-bit reads
-// only), also how many entries have each base at off-1: the list is sorted
-// by read[off-1, L), so these counts give the base runs' bounds.  Each
-// thread counts in four 16-bit fields (a resident grid leaves it far fewer
-// than 65536 entries), then one atomic per block and base.
+// Keys of the list entries [t0, m) step ts at offset off.  With sym_count
+// (2-bit reads only), also how many entries have each base at off-1: the
+// list is sorted by read[off-1, L), so these counts give the base runs'
+// bounds.  Each thread counts in four 16-bit fields (a resident grid leaves
+// it far fewer than 65536 entries), then one atomic per block and base
+// (every thread of the block calls this).
+template <class Acc>
+__device__ __forceinline__ void list_keys_range(const Acc& acc, const uint32_t* __restrict__ ids, uint32_t m, int off,
+                                                uint64_t* __restrict__ key, uint32_t* __restrict__ sym_count,
+                                                uint32_t t0, uint32_t ts) {
+    uint64_t c = 0;
+    for (uint32_t i = t0; i < m; i += ts) {
+        const uint32_t id = ids[i];
+        key[i] = acc.key(id, off);
+        if constexpr (Acc::ALPHA == 4)
+            if (sym_count) c += 1ull << (16 * acc.sym(id, off - 1));
+    }
+    if constexpr (Acc::ALPHA == 4)
+        if (sym_count)
+            for (int b = 0; b < 4; ++b) block_tally<uint32_t>(uint32_t(c >> (16 * b)) & 0xFFFFu, sym_count + b);
+}
+
 // With tally: one thread adds the pass to the counters (passes with both
 // lists non-empty, their suffix and prefix entries; mp_dev is the prefix
 // list's length).
@@ -113,16 +130,7 @@ __global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, cons
             tally[2] += mp;
         }
     }
-    uint64_t c = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        const uint32_t id = ids[i];
-        key[i] = acc.key(id, off);
-        if constexpr (Acc::ALPHA == 4)
-            if (sym_count) c += 1ull << (16 * acc.sym(id, off - 1));
-    }
-    if constexpr (Acc::ALPHA == 4)
-        if (sym_count)
-            for (int b = 0; b < 4; ++b) block_tally<uint32_t>(uint32_t(c >> (16 * b)) & 0xFFFFu, sym_count + b);
+    list_keys_range(acc, ids, m, off, key, sym_count, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // bounds[c] = first index whose symbol at off-1 is >= c (the list is
@@ -130,16 +138,14 @@ __global__ void list_keys_kernel(Acc acc, const uint32_t* __restrict__ ids, cons
 // narrows all boundaries at once, 64 threads each: every round samples 64
 // evenly spaced positions of the boundary's interval, so a few rounds of
 // independent loads replace a chain of ~log2(m) dependent ones.
+// (One block of at least 256 threads; every thread calls it.)
 template <class Acc>
-__global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf,
-                                                         const uint32_t* __restrict__ m_dev, FmOff fo,
-                                                         uint32_t* __restrict__ bounds) {
-    const int off = fo.get();
+__device__ __forceinline__ void run_bounds_block(const Acc& acc, const uint32_t* __restrict__ suf, uint32_t m, int off,
+                                                 uint32_t* __restrict__ bounds) {
     constexpr int NB = Acc::ALPHA - 1;  // boundaries to find: symbols 1 .. ALPHA-1 (at most 4)
     constexpr uint32_t S = 64;          // samples per boundary and round
     __shared__ uint32_t lo_s[4], hi_s[4];
     __shared__ uint8_t sym_s[4][S];
-    const uint32_t m = *m_dev;
     const int b = int(threadIdx.x / S);
     const uint32_t t = threadIdx.x % S;
     // invariant for boundary b: indices < lo have symbol < b+1, indices >= hi
@@ -175,6 +181,13 @@ __global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t
     if (threadIdx.x < NB) bounds[threadIdx.x + 1] = lo_s[threadIdx.x];
 }
 
+template <class Acc>
+__global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t* __restrict__ suf,
+                                                         const uint32_t* __restrict__ m_dev, FmOff fo,
+                                                         uint32_t* __restrict__ bounds) {
+    run_bounds_block(acc, suf, *m_dev, fo.get(), bounds);
+}
+
 // Stable merge of the symbol runs by read[off, L), as a tree of pairwise
 // merges of adjacent runs (level l merges groups of 2^l runs; ties go to the
 // lower run, as in the reference's stable merges), each
@@ -186,15 +199,12 @@ __global__ void __launch_bounds__(256) run_bounds_kernel(Acc acc, const uint32_t
 // reads themselves only when the first key symbols are equal.
 constexpr int MP_ITEMS = 8;
 
-// bounds: the run bounds (ALPHA + 1 entries), or with `counts` the number of
-// entries per symbol, from which the bounds are summed.
+// Outputs [t0, m) step ts (in units of MP_ITEMS).
 template <class Acc>
-__global__ void merge_level_kernel(Acc acc, FmOff fo, const uint32_t* __restrict__ in, const uint64_t* __restrict__ ink,
-                                   uint32_t* __restrict__ out, uint64_t* __restrict__ outk,
-                                   const uint32_t* __restrict__ bounds, bool counts, const uint32_t* __restrict__ m_dev,
-                                   int width) {
-    const uint32_t m = *m_dev;
-    const int off = fo.get();
+__device__ __forceinline__ void merge_level_range(const Acc& acc, int off, const uint32_t* __restrict__ in,
+                                                  const uint64_t* __restrict__ ink, uint32_t* __restrict__ out,
+                                                  uint64_t* __restrict__ outk, const uint32_t* __restrict__ bounds,
+                                                  bool counts, uint32_t m, int width, uint64_t t0, uint64_t ts) {
     uint32_t bd[Acc::ALPHA + 1];
     if (counts) {
         bd[0] = 0;
@@ -211,8 +221,8 @@ __global__ void merge_level_kernel(Acc acc, FmOff fo, const uint32_t* __restrict
     auto cmp_at = [&](uint32_t x, uint32_t y) {
         return cmp_keyed(acc, ink[x], in[x], off, ink[y], in[y], off, len);
     };
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x * MP_ITEMS;
-    for (uint64_t d0 = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * MP_ITEMS; d0 < m; d0 += stride) {
+    const uint64_t stride = ts * MP_ITEMS;
+    for (uint64_t d0 = t0 * MP_ITEMS; d0 < m; d0 += stride) {
         const uint32_t dend = uint32_t(min(uint64_t(m), d0 + MP_ITEMS));
         uint32_t d = uint32_t(d0);
         int k = 0;
@@ -244,6 +254,17 @@ __global__ void merge_level_kernel(Acc acc, FmOff fo, const uint32_t* __restrict
             }
         }
     }
+}
+
+// bounds: the run bounds (ALPHA + 1 entries), or with `counts` the number of
+// entries per symbol, from which the bounds are summed.
+template <class Acc>
+__global__ void merge_level_kernel(Acc acc, FmOff fo, const uint32_t* __restrict__ in, const uint64_t* __restrict__ ink,
+                                   uint32_t* __restrict__ out, uint64_t* __restrict__ outk,
+                                   const uint32_t* __restrict__ bounds, bool counts, const uint32_t* __restrict__ m_dev,
+                                   int width) {
+    merge_level_range(acc, fo.get(), in, ink, out, outk, bounds, counts, *m_dev, width,
+                      uint64_t(blockIdx.x) * blockDim.x + threadIdx.x, uint64_t(gridDim.x) * blockDim.x);
 }
 
 // One thread per run of equal suffix strings: the reference's bucket merge
@@ -325,6 +346,223 @@ __global__ void merge_groups_kernel(Acc acc, uint32_t* pre, uint64_t* pk, const 
         group_one(acc, pre, pk, mp, suf, sk, ms, off, j, next, prev, offset);
 }
 
+// ---------------------------------------------------------------- persistent form
+//
+// One cooperative launch runs every pass: the phases of a pass (keys and
+// run bounds, the merge levels, the pairing, a two-phase compaction of both
+// lists) are separated by grid-wide barriers instead of kernel boundaries,
+// and the lists' lengths are read from device memory at the top of each
+// pass, so neither launches nor host reads separate the passes.  Every block
+// is resident (cooperative launch), which the barriers need.  The results
+// are those of the launch-per-kernel form: the same device functions do the
+// work, and the compaction keeps both lists in order (chunks in block order,
+// entries in index order inside a chunk).
+constexpr int FM_THREADS = 256;
+constexpr uint32_t FM_BARRIER_LIMIT = 1u << 22;  // ~0.3 s of 64 ns sleeps; a barrier takes microseconds
+
+// Grid-wide barrier with a bounded wait (cooperative launch: every block
+// resident).  word[0] counts arrivals, word[1] is the generation, word[2]
+// the error flag.  Block writes before the barrier are visible to every
+// block after it (block barrier, then a device-scope fence by the arriving
+// thread, and one after the wait).  Returns false once any block's wait
+// has run out: the caller leaves the loop, so no block waits for ever.
+__device__ __forceinline__ bool fm_grid_barrier(uint32_t* word, uint32_t nblocks) {
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile uint32_t* gen = word + 1;
+        volatile uint32_t* err = word + 2;
+        const uint32_t g = *gen;
+        __threadfence();
+        bool ok = *err == 0;
+        if (ok) {
+            if (atomicAdd(word, 1u) == nblocks - 1) {
+                word[0] = 0;
+                __threadfence();
+                atomicAdd(word + 1, 1u);
+            } else {
+                uint32_t spins = 0;
+                while (*gen == g) {
+                    if (*err != 0 || ++spins > FM_BARRIER_LIMIT) {
+                        atomicExch(word + 2, 1u);
+                        ok = false;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __threadfence();
+        s_ok = ok ? 1u : 0u;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+struct FmPersist {
+    uint32_t *pre, *tmp, *suf, *suf2, *mtmp;
+    uint64_t *pk, *tk, *sk, *sk2, *mk2;
+    uint32_t* bounds;             // run bounds, or base counts (2-bit reads; zero at launch)
+    uint32_t* len;                // [0] prefixes, [1] suffixes in the lists
+    uint32_t* bcnt;               // per block: kept prefixes, then kept suffixes (2 x gridDim)
+    uint32_t *next, *prev;
+    uint16_t* offset;
+    unsigned long long* tally;    // optional: passes, suffix and prefix entries
+    uint32_t* passes;             // passes run
+    uint32_t* barrier;            // fm_grid_barrier words (3; zero at launch)
+};
+
+// Block-wide exclusive scan of one value per thread (FM_THREADS threads);
+// returns the thread's exclusive prefix, *total the block's sum.
+__device__ __forceinline__ uint32_t fm_block_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= uint32_t(d)) incl += u;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < FM_THREADS / 32; ++w) {
+        const uint32_t c = s_warp[w];
+        before += w < int(warp) ? c : 0;
+        all += c;
+    }
+    __syncthreads();  // s_warp is reused by the next call
+    *total = all;
+    return before + incl - v;
+}
+
+// Block-wide sum (FM_THREADS threads).
+__device__ __forceinline__ uint32_t fm_block_sum(uint32_t v, uint32_t* s_warp) {
+    uint32_t t;
+    fm_block_scan(v, s_warp, &t);
+    return t;
+}
+
+template <class Acc>
+__global__ void __launch_bounds__(FM_THREADS) fm_persistent_kernel(Acc acc, FmPersist st) {
+    __shared__ uint32_t s_warp[FM_THREADS / 32];
+    auto sync = [&] { return fm_grid_barrier(st.barrier, gridDim.x); };
+    constexpr bool by_count = Acc::ALPHA == 4;
+    int levels = 0;
+    while ((1 << levels) < Acc::ALPHA) ++levels;
+    const uint32_t G = gridDim.x;
+    const uint64_t gt = uint64_t(blockIdx.x) * FM_THREADS + threadIdx.x, gs = uint64_t(G) * FM_THREADS;
+    uint32_t* pre = st.pre;
+    uint32_t* tmp = st.tmp;
+    uint64_t* pk = st.pk;
+    uint64_t* tk = st.tk;
+    uint32_t passes = 0;
+    for (int off = 1; off < acc.L; ++off) {
+        // the lengths were written before the last barrier; read past L1 so
+        // that every block sees the same values and takes the same barriers
+        const uint32_t mp = *reinterpret_cast<volatile const uint32_t*>(st.len);
+        const uint32_t ms = *reinterpret_cast<volatile const uint32_t*>(st.len + 1);
+        if (mp == 0 || ms == 0) break;
+        ++passes;
+        if (gt == 0 && st.tally) {
+            st.tally[0] += 1;
+            st.tally[1] += ms;
+            st.tally[2] += mp;
+        }
+        // keys of the suffixes at off (and, 2-bit reads, their base counts at off-1)
+        list_keys_range(acc, st.suf, ms, off, st.sk, by_count ? st.bounds : nullptr, uint32_t(gt), uint32_t(gs));
+        if (!by_count && blockIdx.x == 0) run_bounds_block(acc, st.suf, ms, off, st.bounds);
+        if (!sync()) break;
+        // merge levels: the last one writes suf2/sk2
+        bool alive = true;
+        {
+            const uint32_t* src = st.suf;
+            const uint64_t* srck = st.sk;
+            for (int l = 0; l < levels && alive; ++l) {
+                const bool last = l + 1 == levels;
+                uint32_t* dst = last ? st.suf2 : (l % 2 == 0 ? st.mtmp : st.suf);
+                uint64_t* dstk = last ? st.sk2 : (l % 2 == 0 ? st.mk2 : st.sk);
+                merge_level_range(acc, off, src, srck, dst, dstk, st.bounds, by_count, ms, 1 << l, gt, gs);
+                alive = sync();
+                src = dst;
+                srck = dstk;
+            }
+        }
+        if (!alive) break;
+        // pairing, one thread per run of equal suffix strings
+        for (uint64_t j = gt; j < ms; j += gs)
+            group_one(acc, pre, pk, mp, st.suf2, st.sk2, ms, off, uint32_t(j), st.next, st.prev, st.offset);
+        if (by_count && gt < 4) st.bounds[gt] = 0;  // counts of the next pass (the merges are done)
+        if (!sync()) break;
+        // compaction, phase 1: kept entries of this block's chunk of each list
+        const uint32_t cp = (mp + G - 1) / G, cs = (ms + G - 1) / G;
+        const uint32_t p0 = min(mp, blockIdx.x * cp), p1 = min(mp, p0 + cp);
+        const uint32_t s0 = min(ms, blockIdx.x * cs), s1 = min(ms, s0 + cs);
+        {
+            uint32_t kp = 0, ks = 0;
+            for (uint32_t i = p0 + threadIdx.x; i < p1; i += FM_THREADS) kp += st.prev[pre[i]] == INVALID;
+            for (uint32_t i = s0 + threadIdx.x; i < s1; i += FM_THREADS) ks += st.next[st.suf2[i]] == INVALID;
+            kp = fm_block_sum(kp, s_warp);
+            ks = fm_block_sum(ks, s_warp);
+            if (threadIdx.x == 0) {
+                st.bcnt[blockIdx.x] = kp;
+                st.bcnt[G + blockIdx.x] = ks;
+            }
+        }
+        if (!sync()) break;
+        // phase 2: this chunk's place from the chunks before it, then the
+        // kept entries in order
+        {
+            uint32_t bp = 0, bs = 0, tp = 0, ts = 0;
+            const volatile uint32_t* bc = st.bcnt;  // other blocks' counts, from L2
+            for (uint32_t b = threadIdx.x; b < G; b += FM_THREADS) {
+                const uint32_t a = bc[b], c = bc[G + b];
+                tp += a;
+                ts += c;
+                if (b < blockIdx.x) {
+                    bp += a;
+                    bs += c;
+                }
+            }
+            bp = fm_block_sum(bp, s_warp);
+            bs = fm_block_sum(bs, s_warp);
+            tp = fm_block_sum(tp, s_warp);
+            ts = fm_block_sum(ts, s_warp);
+            for (uint32_t i0 = p0; i0 < p1; i0 += FM_THREADS) {
+                const uint32_t i = i0 + threadIdx.x;
+                const bool keep = i < p1 && st.prev[pre[i]] == INVALID;
+                uint32_t tile;
+                const uint32_t r = fm_block_scan(keep ? 1u : 0u, s_warp, &tile);
+                if (keep) {
+                    tmp[bp + r] = pre[i];
+                    tk[bp + r] = pk[i];
+                }
+                bp += tile;
+            }
+            for (uint32_t i0 = s0; i0 < s1; i0 += FM_THREADS) {
+                const uint32_t i = i0 + threadIdx.x;
+                const bool keep = i < s1 && st.next[st.suf2[i]] == INVALID;
+                uint32_t tile;
+                const uint32_t r = fm_block_scan(keep ? 1u : 0u, s_warp, &tile);
+                if (keep) st.suf[bs + r] = st.suf2[i];
+                bs += tile;
+            }
+            if (gt == 0) {
+                st.len[0] = tp;
+                st.len[1] = ts;
+            }
+        }
+        uint32_t* t32 = pre;
+        pre = tmp;
+        tmp = t32;
+        uint64_t* t64 = pk;
+        pk = tk;
+        tk = t64;
+        if (!sync()) break;
+    }
+    if (gt == 0) *st.passes = passes;
+}
+
 // Compaction functors: keep the list entries whose link is still free.
 struct FreeLink {
     const uint32_t* ids;
@@ -373,15 +611,16 @@ __global__ void fm_cond_kernel(cudaGraphConditionalHandle h, int* offp, const ui
 
 // The passes run without a host round trip: list lengths stay on the
 // device (two slots per list, read by one pass and written by its
-// compaction) and kernels walk them with resident grids.  Two ways to queue
-// them, with the same results: one launch per kernel from the host, which
-// looks at the lengths every few passes to stop early (and times the
-// sub-stages); or (tune.loop_graph) a graph whose conditional `while` node
-// replays a pair of passes, the offset and the stop test on the device, so
-// one graph launch runs the whole loop.
+// compaction) and kernels walk them with resident grids.  Three forms, with
+// the same results (tune.fm_loop): 0, one launch per kernel from the host,
+// which looks at the lengths every few passes to stop early (and times the
+// sub-stages); 1, a graph whose conditional `while` node replays a pair of
+// passes, the offset and the stop test on the device, so one graph launch
+// runs the whole loop; 2, one persistent cooperative kernel whose phases
+// are separated by grid-wide barriers (fm_persistent_kernel).
 template <class Acc>
 void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt, uint32_t* next, uint32_t* prev,
-                     uint16_t* offset, bool use_graph, unsigned long long* tally, Arena& a, cudaStream_t s) {
+                     uint16_t* offset, int mode, unsigned long long* tally, Arena& a, cudaStream_t s) {
     // nothing to link without ends; a single prefix and a single suffix can
     // still link when they are different reads (the head and the tail of one
     // chain, which then closes into a cycle, as the reference's merge does)
@@ -474,7 +713,31 @@ void full_match_loop(const Acc& acc, uint32_t* pre, uint32_t* suf, uint32_t cnt,
         sp_comp.stop();
     };
 
-    if (!use_graph) {
+    if (mode == 2) {
+        SubStage sp_loop("full_match.persistent");
+        int dev = 0, sms = 0, per_sm = 0;
+        CURC_CHECK(cudaGetDevice(&dev));
+        CURC_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CURC_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fm_persistent_kernel<Acc>, FM_THREADS, 0));
+        if (per_sm < 1) throw std::runtime_error("full match: the persistent kernel does not fit on an SM");
+        const int grid = sms * per_sm;  // every block resident: the barriers need it
+        uint32_t* bcnt = a.alloc<uint32_t>(2 * size_t(grid));
+        uint32_t* barrier = a.alloc<uint32_t>(4);
+        CURC_CHECK(cudaMemsetAsync(bounds, 0, 8 * sizeof(uint32_t), s));
+        CURC_CHECK(cudaMemsetAsync(barrier, 0, 4 * sizeof(uint32_t), s));
+        FmPersist fp{pre,  tmp,  suf,  suf2,   mtmp,  pk,    tk,                                  sk,
+                     sk2,  mk2,  bounds, len,  bcnt,  next,  prev,                                offset,
+                     tally, reinterpret_cast<uint32_t*>(offp), barrier};
+        Acc acc_arg = acc;
+        void* args[] = {&acc_arg, &fp};
+        CURC_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(fm_persistent_kernel<Acc>), grid, FM_THREADS,
+                                               args, 0, s));
+        CURC_LAUNCH_CHECK();
+        sp_loop.stop();
+        uint32_t err = 0;
+        read_small(&err, barrier + 2, 4, s);
+        if (err) throw std::runtime_error("full match: a grid barrier wait of the persistent kernel ran out");
+    } else if (mode == 0) {
         constexpr int CHECK_EVERY = 8;
         int par = 0;
         for (int off = 1; off < acc.L; ++off, par ^= 1) {
@@ -579,7 +842,7 @@ __global__ void ends_flags_kernel(const uint32_t* __restrict__ ids, uint32_t m, 
 void full_match_packed(const BlockParams& p, const uint64_t* db, uint32_t* pre, uint32_t* suf, uint32_t cnt,
                        uint32_t* next, uint32_t* prev, uint16_t* offset, Arena& a, cudaStream_t s,
                        unsigned long long* tally) {
-    full_match_loop(PackedAcc{db, p.W, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, tally, a, s);
+    full_match_loop(PackedAcc{db, p.W, p.L}, pre, suf, cnt, next, prev, offset, p.tune.fm_loop, tally, a, s);
 }
 
 void sort_ids_by_ascii(const uint8_t* reads, int L, uint32_t* ids, uint32_t m, Arena& a, cudaStream_t s) {
@@ -620,7 +883,7 @@ void full_match_ascii(const BlockParams& p, const uint8_t* reads, uint32_t* ids,
     select_flagged(ids, pf, pre, m, counts + 0, a, s);
     select_flagged(ids, sf, suf, m, counts + 1, a, s);
     const uint32_t cnt = read_scalar(counts + 0, s);
-    full_match_loop(AsciiAcc{reads, 0, p.L}, pre, suf, cnt, next, prev, offset, p.tune.loop_graph, nullptr, a, s);
+    full_match_loop(AsciiAcc{reads, 0, p.L}, pre, suf, cnt, next, prev, offset, p.tune.fm_loop, nullptr, a, s);
     a.release(mk);
 }
 

@@ -20,7 +20,7 @@ std::string& ctxless_error();
 // threads per block of the mapping kernel (one warp per read).
 struct Tuning {
     int table_factor = 4, bitmap_bits = 16, check_every = 8, map_threads = 128;
-    int loop_graph = 1;  // full-match passes replayed from a graph (1) or queued per launch (0)
+    int fm_loop = 1;  // full-match pass loop: 0 a launch per kernel, 1 one graph, 2 one persistent kernel
 };
 
 // Autotuner cache key of a block: read length and read count rounded down

@@ -4,8 +4,8 @@
 // Knobs (struct Tuning): the overlap index's bucket table size as a multiple
 // of the prefix count, bits of the prefix presence bitmap per prefix, overlap
 // passes between host reads of the link count, threads per block of the
-// mapping kernel, and whether the full-match passes replay from a graph or
-// are queued launch by launch.  None of them changes which prefixes a suffix meets, the
+// mapping kernel, and the form of the full-match pass loop (a launch per
+// kernel, one graph, or one persistent kernel).  None of them changes which prefixes a suffix meets, the
 // order candidates are visited in, or any stream: the tests compare every
 // stage result and stream under each setting.  The k-mer length and the
 // other derived parameters (preprocess.cpp:295-313) are part of the format
@@ -16,7 +16,7 @@
 // affects (best of two runs).  Choices are cached per (read length, read
 // count rounded down to a power of two) in a small text file, one line per
 // bucket: "L log2n table_factor bitmap_bits check_every map_threads
-// loop_graph" (lines without the last field take its default).
+// fm_loop" (lines without the last field take its default).
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -43,7 +43,7 @@ std::map<Key, Tuning> load_cache(const std::string& path) {
         Tuning t;
         if (!(ls >> k.L >> k.log2n >> t.table_factor >> t.bitmap_bits >> t.check_every >> t.map_threads)) continue;
         int g;
-        if (ls >> g) t.loop_graph = g;
+        if (ls >> g) t.fm_loop = g;
         m[k] = t;
     }
     return m;
@@ -55,7 +55,7 @@ void save_cache(const std::string& path, const std::map<Key, Tuning>& m) {
         std::ofstream out(tmp, std::ios::trunc);
         for (const auto& kv : m)
             out << kv.first.L << ' ' << kv.first.log2n << ' ' << kv.second.table_factor << ' ' << kv.second.bitmap_bits
-                << ' ' << kv.second.check_every << ' ' << kv.second.map_threads << ' ' << kv.second.loop_graph
+                << ' ' << kv.second.check_every << ' ' << kv.second.map_threads << ' ' << kv.second.fm_loop
                 << '\n';
         if (!out) throw std::runtime_error("autotune: cannot write " + tmp);
     }
@@ -69,7 +69,7 @@ bool valid(const Tuning& t) {
         return false;
     };
     return in(t.table_factor, {1, 2, 4, 8}) && in(t.bitmap_bits, {8, 16, 32}) && in(t.check_every, {2, 4, 8, 16}) &&
-           in(t.map_threads, {64, 128, 256}) && in(t.loop_graph, {0, 1});
+           in(t.map_threads, {64, 128, 256}) && in(t.fm_loop, {0, 1, 2});
 }
 
 }  // namespace
@@ -97,7 +97,7 @@ int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs) {
     knobs[1] = t.bitmap_bits;
     knobs[2] = t.check_every;
     knobs[3] = t.map_threads;
-    knobs[4] = t.loop_graph;
+    knobs[4] = t.fm_loop;
     return CURC_OK;
 }
 
@@ -148,6 +148,7 @@ int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read
             blk.tune = t;
             float best = 1e30f;
             for (int r = 0; r < 2; ++r) {
+                blk.arena.reset();  // the input is the caller's memory, not the arena's
                 blk.run(reinterpret_cast<const uint8_t*>(seqs_dev), n, read_len, preserve_order != 0,
                         paired_end != 0);
                 best = std::min(best, blk.stage_ms.at(stage));
@@ -164,7 +165,7 @@ int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read
                               {&Tuning::bitmap_bits, {8, 16, 32}, "overlap"},
                               {&Tuning::check_every, {4, 8, 16}, "overlap"},
                               {&Tuning::map_threads, {64, 128, 256}, "mapping"},
-                              {&Tuning::loop_graph, {0, 1}, "full_match"}};
+                              {&Tuning::fm_loop, {0, 1, 2}, "full_match"}};
         for (const Knob& k : knobs) {
             float tbest = 1e30f;
             int vbest = best.*(k.field);

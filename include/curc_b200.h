@@ -97,9 +97,10 @@ int curc_ctx_trim(curc_ctx* ctx);
  * overlap index's bucket table size as a multiple of the prefix count
  * {1, 2, 4, 8}, presence-bitmap bits per prefix {8, 16, 32}, overlap passes
  * between host reads of the link count {2, 4, 8, 16}, threads per block of
- * the mapping kernel {64, 128, 256}, full-match passes replayed on the device
- * from a CUDA graph with a conditional while node (1) or queued launch by
- * launch from the host (0).  None changes any result: every stream
+ * the mapping kernel {64, 128, 256}, and the form of the full-match pass
+ * loop: a launch per kernel from the host (0), one CUDA graph whose
+ * conditional while node replays the passes (1), or one persistent
+ * cooperative kernel that runs every pass (2).  None changes any result: every stream
  * is the same under every setting; only the time does.  curc_autotune runs
  * the given block (device memory) under the candidates one knob at a time,
  * keeps the fastest, and sets it on the context; with cache_path, choices

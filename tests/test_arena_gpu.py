@@ -73,3 +73,21 @@ def test_trim_frees_device_memory_and_keeps_results():
         assert after > before
         ctx.block_run(b)
         assert _digest(ctx, 150) == d0
+
+
+def test_autotune_runs_do_not_accumulate_device_memory():
+    """curc_autotune runs the block about thirty times: each run starts from
+    an empty arena, so device memory after it is what one run needs."""
+    import torch
+    from curc_b200 import Context
+    b = _reads(300_000, 150, 9)
+    d = torch.from_numpy(b.reshape(-1).copy()).cuda()
+    with Context(0) as ctx:
+        ctx.keep_intermediates(False)
+        ctx.block_run_device(d.data_ptr(), b.shape[0], b.shape[1], False, False)
+        torch.cuda.synchronize()
+        before = torch.cuda.mem_get_info(0)[0]
+        ctx.autotune(d.data_ptr(), b.shape[0], b.shape[1], False, False)
+        torch.cuda.synchronize()
+        after = torch.cuda.mem_get_info(0)[0]
+    assert before - after < (1 << 30), (before, after)

@@ -2,8 +2,8 @@
 
 Every knob value (overlap bucket table factor, presence-bitmap bits,
 passes between link-count reads, mapping threads per block, full-match
-passes replayed from a graph or queued per launch) runs the same
-blocks; every stage result and stream must equal the default setting's, and
+pass loop as a launch per kernel, one graph or one persistent kernel) runs
+the same blocks; every stage result and stream must equal the default setting's, and
 the default setting's must equal the oracle's.  Then curc_autotune picks a
 setting on a block, caches it per (read length, read-count bucket), and a
 second call takes it from the cache."""
@@ -16,7 +16,7 @@ from tests.oracle_lib import OracleBlock, STAGE_RESULTS, stream_dtype, stream_na
 pytestmark = pytest.mark.gpu
 
 KNOB_VALUES = {"table_factor": [1, 2, 8], "bitmap_bits": [8, 32], "check_every": [2, 16], "map_threads": [64, 256],
-               "loop_graph": [0]}
+               "fm_loop": [0, 1, 2]}
 
 
 def _results(ctx, L):

@@ -46,6 +46,10 @@ def ctx():
 def test_random_configurations(ctx, seed):
     rnd = random.Random(seed)
     bad_cases = []
+    # seeds 4-6 run the full-match loop as one persistent kernel, the
+    # others in the library's default form
+    default = ctx.tuning()
+    ctx.set_tuning(**dict(default, fm_loop=2 if seed > 3 else default["fm_loop"]))
     for i in range(CASES_PER_SEED):
         w, params = draw(rnd, MAX_READS)
         seqs = w.sequences()
@@ -57,4 +61,5 @@ def test_random_configurations(ctx, seed):
                if not np.array_equal(ctx.get(nm, dt), ora.get(nm, dt))]
         if bad:
             bad_cases.append(f"case {i} {params}: {bad}")
+    ctx.set_tuning(**default)
     assert not bad_cases, "\n".join(bad_cases)
