@@ -165,7 +165,12 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
                 const uint64_t shift = RC ? uint64_t(L - k - oj) : uint64_t(oj);
                 if (refpos >= shift && refpos - shift + L <= ref_len) {
                     mp = refpos - shift;
-                    c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best) : packed_mismatches<RC>(ref, mp, rd, L, best);
+                    // the window of the best count so far (met again through
+                    // another probe) has that count, which neither reaches
+                    // target nor improves: not compared again
+                    if (!(best < init && mp == best_pos))
+                        c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best)
+                                : packed_mismatches<RC>(ref, mp, rd, L, best);
                 }
             }
             // the loop stops at the first count <= target
