@@ -56,21 +56,23 @@ struct MapIndex {
     uint64_t start;
 };
 
+// Chunk q (bases 32q .. 32q + nb - 1) of the read as compared with the
+// pseudogenome: the read's own word, or for the reverse-complement strand
+// the reverse complement of the matching bases from the read's end.
 template <bool RC>
+__device__ __forceinline__ uint64_t read_chunk(const uint64_t* __restrict__ rd, int L, int q) {
+    const int i = 32 * q, nb = L - i < 32 ? L - i : 32;
+    return RC ? revcomp_kmer(word_at(rd, L - i - nb, nb), nb) : word_at(rd, i, nb);
+}
+
+// util.cuh:233-270: 32-base chunks, early exit once the bound is reached.
+// rw: the read's chunks (read_chunk), computed once per read.
 __device__ __forceinline__ int packed_mismatches(const uint64_t* __restrict__ ref, uint64_t mp,
-                                                 const uint64_t* __restrict__ rd, int L, int bound) {
-    // util.cuh:233-270: 32-base chunks, early exit once the bound is reached
+                                                 const uint64_t* rw, int L, int bound) {
     int c = 0;
-    for (int i = 0; i < L && c < bound; i += 32) {
+    for (int i = 0, q = 0; i < L && c < bound; i += 32, ++q) {
         const int nb = L - i < 32 ? L - i : 32;
-        const uint64_t a = word_unaligned(ref, mp + i, nb);
-        uint64_t b;
-        if (!RC) {
-            b = word_at(rd, i, nb);
-        } else {
-            b = revcomp_kmer(word_at(rd, L - i - nb, nb), nb);
-        }
-        c += base_mismatches(a, b);
+        c += base_mismatches(word_unaligned(ref, mp + i, nb), rw[q]);
     }
     return c;
 }
@@ -107,12 +109,15 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
                                          const uint8_t* __restrict__ ndb, int L, int W, int k, int step,
                                          uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
                                          uint64_t* __restrict__ pos, uint32_t i, uint32_t lane, uint32_t& listed,
-                                         uint32_t& compared) {
+                                         uint32_t& compared, uint64_t* rw) {
     const int init = mm[i];
     if (init <= BlockParams::target_mm) return;
     const bool isn = i >= U;
     const uint64_t* rd = isn ? nullptr : udb + uint64_t(i) * W;
     const uint8_t* nd = isn ? ndb + uint64_t(i - U) * L : nullptr;
+    // the read's comparison words, once for all its candidates
+    if (!isn && int(lane) < W) rw[lane] = read_chunk<RC>(rd, L, int(lane));
+    __syncwarp();
     const int probes = (L - k) / BlockParams::read_step + 1;
     int best = init;  // smallest count met so far (the same in every lane)
     uint64_t best_pos = 0;
@@ -169,8 +174,7 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
                     // another probe) has that count, which neither reaches
                     // target nor improves: not compared again
                     if (!(best < init && mp == best_pos))
-                        c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best)
-                                : packed_mismatches<RC>(ref, mp, rd, L, best);
+                        c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best) : packed_mismatches(ref, mp, rw, L, best);
                 }
             }
             // the loop stops at the first count <= target
@@ -208,12 +212,14 @@ __global__ void __launch_bounds__(256) map_kernel(MapIndex ix, const uint64_t* _
                                                   const uint8_t* __restrict__ ndb, uint32_t NN, int L, int W, int k,
                                                   int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
                                                   uint64_t* __restrict__ pos, unsigned long long* __restrict__ tally) {
+    __shared__ uint64_t s_rw[256 / 32][16];  // per warp: the read's comparison words
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t listed = 0, compared = 0;
     const bool searched = i < U + NN && mm[i] > BlockParams::target_mm;
     if (i < U + NN)  // whole warp
-        map_read<RC>(ix, ref, ref_len, udb, U, ndb, L, W, k, step, mm, strand, pos, i, lane, listed, compared);
+        map_read<RC>(ix, ref, ref_len, udb, U, ndb, L, W, k, step, mm, strand, pos, i, lane, listed, compared,
+                     s_rw[threadIdx.x >> 5]);
     if (tally) {  // lane 0 carries its warp's counts
         block_tally<unsigned long long>(lane == 0 && searched ? 1u : 0u, &tally[0]);
         block_tally<unsigned long long>(lane == 0 ? listed : 0u, &tally[1]);
