@@ -11,12 +11,13 @@ streams returned to the host.  `value` is Mbases/s with the ASCII reads
 already in HBM (CUDA events).  `e2e` is the whole `curc -c` a user runs: the
 product binary, one process per step, from the FASTQ files to the closed
 archive (parse, copies to and from the device, device path, stream coders,
-archive write) -- the same work the reference arm times for the reference's
-own `curc -c`.  `e2e_same_sample` runs both binaries on identical files (the
-first pairs of the workload's own FASTQ files) for a like-for-like ratio.
+archive write) -- the same work, on the same files, that the reference arm
+times for the reference's own `curc -c`.  With --ref-sample-pairs both
+binaries are also timed on the first pairs of those files
+(`e2e_same_sample`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-    python bench.py --impl reference --ref-full   # the reference on the whole workload, once
+    python bench.py --impl reference --ref-sample-pairs 1000000   # the reference on a sample
 
 Under torchrun every rank compresses its own block (independent blocks, no
 collective: weak scaling); the time is the max over ranks.
@@ -52,10 +53,10 @@ def parse():
     ap.add_argument("--genome", type=int, default=50_000_000)
     ap.add_argument("--cpu-sample-pairs", type=int, default=300_000,
                     help="pairs of the CPU-baseline sample, drawn at the workload's coverage (genome scaled alike)")
-    ap.add_argument("--ref-sample-pairs", type=int, default=3_000_000,
-                    help="pairs per step of the reference arm (the first pairs of the workload's FASTQ files)")
-    ap.add_argument("--ref-full", action="store_true",
-                    help="reference arm: time one run on the whole workload instead of the sampled steps")
+    ap.add_argument("--ref-sample-pairs", type=int, default=0,
+                    help="reference arm: time the first pairs of the workload's FASTQ files instead of the whole "
+                         "workload (0: the whole workload, the files the headline e2e is timed on); the product's "
+                         "curc -c is then also timed on that sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cli", action="store_true", help="skip the whole-file `curc -c` measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain measurement")
@@ -476,16 +477,18 @@ def cli_measure(ctx, w, a, dev):
         full = curc_runs(files, td, a.steps, a.warmup, dev, "full")
         for f in files:
             os.remove(f)
-        ws = sample_of(w, a.ref_sample_pairs)
-        sfiles = ws.write(os.path.join(td, "sample"), name=FASTQ_NAME)
-        sample = curc_runs(sfiles, td, a.steps, a.warmup, dev, "sample")
+        sample = None
+        if a.ref_sample_pairs:
+            ws = sample_of(w, a.ref_sample_pairs)
+            sfiles = ws.write(os.path.join(td, "sample"), name=FASTQ_NAME)
+            runs = curc_runs(sfiles, td, a.steps, a.warmup, dev, "sample")
+            smean = sum(r["s"] for r in runs) / len(runs)
+            sample = {"value": ws.bases / smean / 1e6, "s": smean, "pairs": a.ref_sample_pairs,
+                      "archive_bytes": runs[0]["archive_bytes"], "line_stages": line_stages(runs)}
     mean = sum(r["s"] for r in full) / len(full)
-    smean = sum(r["s"] for r in sample) / len(sample)
     return {"s": mean, "value": w.bases / mean / 1e6, "archive_bytes": full[0]["archive_bytes"],
             "archive_bits_per_base": 8.0 * full[0]["archive_bytes"] / w.bases,
-            "line_stages": line_stages(full), "in_process_s": t_in, "host_stage_ms": host_ms,
-            "sample": {"value": ws.bases / smean / 1e6, "s": smean, "pairs": a.ref_sample_pairs,
-                       "archive_bytes": sample[0]["archive_bytes"], "line_stages": line_stages(sample)}}
+            "line_stages": line_stages(full), "in_process_s": t_in, "host_stage_ms": host_ms, "sample": sample}
 
 
 def batched_vs_plain(ctx, a):
@@ -548,15 +551,16 @@ def learned_eval(a):
 
 def run_reference(a):
     """The reference `curc -c` (built from its sources, oracle/_ref), one
-    process per step, on the first pairs of the workload's own FASTQ files
-    (or on the whole workload once with --ref-full), on this box."""
+    process per step, on the workload's own FASTQ files (the files the
+    product's headline e2e is timed on), or on their first pairs with
+    --ref-sample-pairs, on this box."""
     ref_dir = os.path.join(ROOT, "oracle", "_ref")
     exe = os.path.join(ref_dir, "curc_shared")
     if not os.path.exists(exe):
         return None, "reference build missing (oracle/_ref/curc_shared)"
     w = workload(a.pairs, a.genome, seed=1)
-    ws = w if a.ref_full else sample_of(w, a.ref_sample_pairs)
-    steps, warmup = (1, 0) if a.ref_full else (a.steps, a.warmup)
+    ws = sample_of(w, a.ref_sample_pairs) if a.ref_sample_pairs else w
+    steps, warmup = a.steps, a.warmup
     with tempfile.TemporaryDirectory() as td:
         files = ws.write(os.path.join(td, "in"), name=FASTQ_NAME)
         del w
@@ -794,11 +798,11 @@ def main():
             finish_dist(world)
             return
         v = ref["bases"] / ref["s"] / 1e6
-        what = ("the whole workload, once" if a.ref_full else
-                f"the first {ref['pairs']} pairs of the workload's FASTQ files ({ref['bases'] / 1e6:.0f} Mbases) "
-                "per step")
+        what = (f"the first {ref['pairs']} pairs of the workload's FASTQ files ({ref['bases'] / 1e6:.0f} Mbases) "
+                "per step" if a.ref_sample_pairs else
+                f"the workload's FASTQ files ({ref['bases'] / 1e6:.0f} Mbases) per step")
         out = {"metric": METRIC, "value": v, "unit": "Mbases/s", "n_gpus": 1, "steps": ref["steps"],
-               "warmup": 0 if a.ref_full else a.warmup, "ms_per_step": ref["s"] * 1000, "higher_is_better": True,
+               "warmup": a.warmup, "ms_per_step": ref["s"] * 1000, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
                "config": cfg,
                "cpu_baseline": {"value": v, "unit": "Mbases/s", "cores": os.cpu_count(), "kind": "reference",
@@ -898,8 +902,9 @@ def main():
     }
     if r["cli"]:
         out["cli"] = r["cli"]
-        out["e2e_same_sample"] = dict(r["cli"]["sample"], unit="Mbases/s",
-                                      note="the product's curc -c on the same files as the reference arm's steps")
+        if r["cli"]["sample"]:
+            out["e2e_same_sample"] = dict(r["cli"]["sample"], unit="Mbases/s",
+                                          note="the product's curc -c on the same files as the reference arm's steps")
     if r["batched"]:
         out["batched"] = r["batched"]
     if not a.no_learned and rank == 0:
