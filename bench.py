@@ -625,7 +625,10 @@ def run_large(a):
         out["block_stats"] = block_stats(ctx)
         out["substage_ms"] = {k: round(ctx.stage_ms(k), 3) for k in
                               ["mapping.index_fwd", "mapping.map_fwd", "mapping.index_rc", "mapping.map_rc",
-                               "overlap.probe", "overlap.resolve", "refmatch.probe_self", "full_match.graph"]
+                               "overlap.index", "overlap.index_mask", "overlap.filter", "overlap.probe",
+                               "overlap.resolve", "overlap.compact", "refmatch.index", "refmatch.probe_self",
+                               "refmatch.sort_unique", "refmatch.accept", "full_match.graph",
+                               "assembly.ranking", "assembly.order_place"]
                               if _has_stage(ctx, k)}
         pack_ms = stage["pack"]
         del d
