@@ -429,13 +429,15 @@ __global__ void __launch_bounds__(RS_THREADS) rs_hist_kernel(const K* __restrict
     hist[size_t(threadIdx.x) * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter: items are ranked in index order.  Within a round of 256
-// items, a warp ranks equal digits with match_any; warps are ordered by a
-// per-round prefix over per-warp counts; rounds accumulate per digit.  The
-// tile is first reordered by digit in shared memory (its digit counts come
-// from the scanned histogram: the difference of consecutive offsets), then
-// written out in that order, so that items of one digit leave as one
-// contiguous run and the stores coalesce.
+// Stable scatter: items are ranked in index order.  Warp w takes the
+// tile's items [512 w, 512 w + 512) in 16 rounds of 32 consecutive ones,
+// keeping them in registers, and ranks each among the warp's earlier items
+// of its digit with match_any and warp-private digit counters (no block
+// barrier inside); the warps' counts are then scanned per digit, and the
+// tile is reordered by digit in shared memory (its digit counts come from
+// the scanned histogram: the difference of consecutive offsets) and written
+// out in that order, so that items of one digit leave as one contiguous run
+// and the stores coalesce.
 template <class K, class V>
 __global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const K* __restrict__ kin, const V* __restrict__ vin,
                                                                 K* __restrict__ kout, V* __restrict__ vout, size_t n,
@@ -446,7 +448,6 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const K* __restr
     V* sv = reinterpret_cast<V*>(rs_smem + sizeof(K) * RS_TILE);
     __shared__ uint32_t gbase[256];
     __shared__ uint32_t tstart[256];
-    __shared__ uint32_t run[256];
     __shared__ uint32_t wcnt[RS_WARPS][256];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     {
@@ -458,69 +459,79 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter_kernel(const K* __restr
         gbase[tid] = g;
         tstart[tid] = nx - g;
     }
-    run[tid] = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) wcnt[w][tid] = 0;
     __syncthreads();
     // exclusive scan of the tile's digit counts (256 entries, one per thread)
     {
-        uint32_t v = tstart[tid];
+        __shared__ uint32_t wsum[RS_WARPS];
+        const uint32_t v = tstart[tid];
         uint32_t x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
             if (lane >= o) x += y;
         }
-        if (lane == 31) wcnt[0][warp] = x;
+        if (lane == 31) wsum[warp] = x;
         __syncthreads();
         uint32_t wbase = 0;
-        for (int w = 0; w < warp; ++w) wbase += wcnt[0][w];
-        __syncthreads();
+        for (int w = 0; w < warp; ++w) wbase += wsum[w];
         tstart[tid] = wbase + x - v;
     }
     const uint32_t lt_mask = (1u << lane) - 1u;
     const size_t base = size_t(blockIdx.x) * RS_TILE;
     const uint32_t items = uint32_t(min(size_t(RS_TILE), n - base));
-    for (int r = 0; r < RS_ROUNDS; ++r) {
-        const size_t idx = base + size_t(r) * RS_THREADS + tid;
-        if (base + size_t(r) * RS_THREADS >= n) break;  // uniform across the block
-        const bool valid = idx < n;
-        K k{};
-        V v{};
-        uint32_t d = 256;
-        if (valid) {
-            k = kin[idx];
-            if (vin) v = vin[idx];
-            d = digit_of(k, shift, mask);
-        }
+    // this warp's items, ranked within the warp
+    const size_t wb = base + size_t(warp) * (RS_TILE / RS_WARPS);
+    uint32_t* cnt = wcnt[warp];
+    K k[RS_ROUNDS];
+    V v[RS_ROUNDS];
+    uint32_t rk[RS_ROUNDS];
 #pragma unroll
-        for (int w = 0; w < RS_WARPS; ++w) wcnt[w][tid] = 0;
-        __syncthreads();
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+        const size_t idx = wb + size_t(r) * 32 + lane;
+        const bool valid = idx < n;
+        k[r] = valid ? kin[idx] : K{};
+        v[r] = (valid && vin) ? vin[idx] : V{};
+        const uint32_t d = valid ? digit_of(k[r], shift, mask) : 256u;
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        const uint32_t rank = __popc(peers & lt_mask);
-        if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
-        __syncthreads();
+        const uint32_t before = __popc(peers & lt_mask);
+        uint32_t c0 = 0;
+        if (valid) c0 = cnt[d];  // the warp's earlier items of digit d
+        __syncwarp();
+        if (valid && before == 0) cnt[d] = c0 + __popc(peers);
+        __syncwarp();
+        rk[r] = c0 + before;
+    }
+    __syncthreads();
+    // per digit: the items of earlier warps come first
+    {
         uint32_t acc = 0;
 #pragma unroll
         for (int w = 0; w < RS_WARPS; ++w) {
-            uint32_t c = wcnt[w][tid];
+            const uint32_t c = wcnt[w][tid];
             wcnt[w][tid] = acc;
             acc += c;
         }
-        __syncthreads();
-        if (valid) {
-            const uint32_t lp = tstart[d] + run[d] + wcnt[warp][d] + rank;
-            sk[lp] = k;
-            if (vin) sv[lp] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+        const size_t idx = wb + size_t(r) * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = digit_of(k[r], shift, mask);
+            const uint32_t lp = tstart[d] + cnt[d] + rk[r];
+            sk[lp] = k[r];
+            if (vin) sv[lp] = v[r];
         }
-        __syncthreads();
-        run[tid] += acc;
     }
     __syncthreads();
     // the tile in digit order: runs of one digit go to consecutive places
     for (uint32_t p = tid; p < items; p += RS_THREADS) {
-        const K k = sk[p];
-        const uint32_t d = digit_of(k, shift, mask);
+        const K kk = sk[p];
+        const uint32_t d = digit_of(kk, shift, mask);
         const uint32_t gpos = gbase[d] + (p - tstart[d]);
-        kout[gpos] = k;
+        kout[gpos] = kk;
         if (vout) vout[gpos] = sv[p];
     }
 }
