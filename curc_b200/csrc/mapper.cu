@@ -89,11 +89,6 @@ __device__ __forceinline__ int ascii_mismatches(const uint64_t* __restrict__ ref
     return c;
 }
 
-// Candidate buffer of a warp: fewer than 32 left over plus one probe chunk's
-// (32 probes, at most bucket_limit candidates each).
-constexpr uint32_t MAP_CBUF = 32 + 32 * BlockParams::bucket_limit;
-inline size_t map_smem_bytes(int threads) { return size_t(threads / 32) * (16 + MAP_CBUF) * sizeof(uint64_t); }
-
 // One warp per read.  The reference's loop visits the candidates of the
 // read's probes in order (probe offset, then bucket slot), takes each that
 // strictly improves the mismatch count, and stops at the first count
@@ -114,7 +109,7 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
                                          const uint8_t* __restrict__ ndb, int L, int W, int k, int step,
                                          uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
                                          uint64_t* __restrict__ pos, uint32_t i, uint32_t lane, uint32_t& listed,
-                                         uint32_t& compared, uint64_t* rw, uint64_t* cbuf) {
+                                         uint32_t& compared, uint64_t* rw) {
     const int init = mm[i];
     if (init <= BlockParams::target_mm) return;
     const bool isn = i >= U;
@@ -127,15 +122,6 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
     int best = init;  // smallest count met so far (the same in every lane)
     uint64_t best_pos = 0;
     bool done = false;
-    // candidate windows waiting to be compared, in the reference's order
-    // (probe, then bucket slot): a probe chunk's candidates are appended and
-    // compared 32 at a time, the fewer than 32 left over wait for the next
-    // probe chunk's, so lanes stay busy when a chunk lists few candidates.
-    // Windows that fall outside the pseudogenome are dropped here (they are
-    // never compared).  Chunk boundaries do not change the result: within a
-    // chunk the first count <= target wins, else the earliest smallest count
-    // if it improves, which is what the candidate-by-candidate loop gives.
-    uint32_t nbuf = 0;
     for (int p0 = 0; p0 < probes && !done; p0 += 32) {
         // this lane's probe: bucket range of its k-mer
         const int pj = p0 + int(lane);
@@ -164,7 +150,10 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
         listed += uint32_t(min(32, probes - p0));
         for (uint32_t cs = 0; cs < total; cs += 32) {
+            compared += min(32u, total - cs);
             const uint32_t ci = cs + lane;
+            int c = 0x7FFF;
+            uint64_t mp = 0;
             // owner lane: the first lane whose inclusive count exceeds ci
             uint32_t owner = 0;
 #pragma unroll
@@ -174,8 +163,6 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
             }
             const uint32_t ob = __shfl_sync(0xFFFFFFFFu, b, owner);
             const uint32_t oex = __shfl_sync(0xFFFFFFFFu, incl - cnt, owner);
-            bool valid = false;
-            uint64_t mp = 0;
             if (ci < total) {
                 const int oj = (p0 + int(owner)) * BlockParams::read_step;
                 const uint32_t q = ob + (ci - oex);
@@ -183,28 +170,13 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
                 const uint64_t shift = RC ? uint64_t(L - k - oj) : uint64_t(oj);
                 if (refpos >= shift && refpos - shift + L <= ref_len) {
                     mp = refpos - shift;
-                    valid = true;
+                    // the window of the best count so far (met again through
+                    // another probe) has that count, which neither reaches
+                    // target nor improves: not compared again
+                    if (!(best < init && mp == best_pos))
+                        c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best) : packed_mismatches(ref, mp, rw, L, best);
                 }
             }
-            const uint32_t vb = __ballot_sync(0xFFFFFFFFu, valid);
-            if (valid) cbuf[nbuf + __popc(vb & ((1u << lane) - 1u))] = mp;
-            nbuf += __popc(vb);
-        }
-        __syncwarp();
-        const bool last = p0 + 32 >= probes;
-        uint32_t head = 0;
-        while (nbuf - head >= 32 || (last && head < nbuf)) {
-            const uint32_t ci = head + lane;
-            const bool have = ci < nbuf;
-            const uint64_t mp = have ? cbuf[ci] : 0;
-            head += min(32u, nbuf - head);
-            // the window of the best count so far (met again through another
-            // probe) has that count, which neither reaches target nor
-            // improves: not compared again
-            const bool cmp = have && !(best < init && mp == best_pos);
-            int c = 0x7FFF;
-            if (cmp) c = isn ? ascii_mismatches<RC>(ref, mp, nd, L, best) : packed_mismatches(ref, mp, rw, L, best);
-            compared += __popc(__ballot_sync(0xFFFFFFFFu, cmp));
             // the loop stops at the first count <= target
             const uint32_t stop = __ballot_sync(0xFFFFFFFFu, c <= BlockParams::target_mm);
             if (stop) {
@@ -226,14 +198,6 @@ __device__ __forceinline__ void map_read(const MapIndex& ix, const uint64_t* __r
                 best_pos = fpos;
             }
         }
-        if (done || last) break;
-        // the fewer than 32 left over move to the front of the buffer
-        const uint32_t rest = nbuf - head;
-        const uint64_t v = lane < rest ? cbuf[head + lane] : 0;
-        __syncwarp();
-        if (lane < rest) cbuf[lane] = v;
-        __syncwarp();
-        nbuf = rest;
     }
     if (lane == 0 && best < init) {
         mm[i] = uint8_t(best);
@@ -248,17 +212,14 @@ __global__ void __launch_bounds__(256) map_kernel(MapIndex ix, const uint64_t* _
                                                   const uint8_t* __restrict__ ndb, uint32_t NN, int L, int W, int k,
                                                   int step, uint8_t* __restrict__ mm, uint8_t* __restrict__ strand,
                                                   uint64_t* __restrict__ pos, unsigned long long* __restrict__ tally) {
-    // per warp: the read's comparison words (16), then candidate windows
-    // waiting (MAP_CBUF); map_smem_bytes(blockDim.x) in all
-    extern __shared__ uint64_t s_map[];
-    uint64_t* s_warp = s_map + size_t(threadIdx.x >> 5) * (16 + MAP_CBUF);
+    __shared__ uint64_t s_rw[256 / 32][16];  // per warp: the read's comparison words
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t listed = 0, compared = 0;
     const bool searched = i < U + NN && mm[i] > BlockParams::target_mm;
     if (i < U + NN)  // whole warp
         map_read<RC>(ix, ref, ref_len, udb, U, ndb, L, W, k, step, mm, strand, pos, i, lane, listed, compared,
-                     s_warp, s_warp + 16);
+                     s_rw[threadIdx.x >> 5]);
     if (tally) {  // lane 0 carries its warp's counts
         block_tally<unsigned long long>(lane == 0 && searched ? 1u : 0u, &tally[0]);
         block_tally<unsigned long long>(lane == 0 ? listed : 0u, &tally[1]);
@@ -320,13 +281,12 @@ void map_reads(const BlockParams& p, const uint64_t* ref, uint64_t ref_len, cons
             const int mt = p.tune.map_threads;
             const int g = grid_for(uint64_t(total) * 32, mt);
             unsigned long long* t = out.tally ? out.tally + 3 * rc : nullptr;
-            const size_t sm = map_smem_bytes(mt);  // at most 28 KB: no attribute needed
             if (rc)
-                map_kernel<true><<<g, mt, sm, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
-                                                   out.strand, out.pos, t);
+                map_kernel<true><<<g, mt, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
+                                                  out.strand, out.pos, t);
             else
-                map_kernel<false><<<g, mt, sm, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
-                                                    out.strand, out.pos, t);
+                map_kernel<false><<<g, mt, 0, s>>>(ix, ref, ref_len, udb, U, ndb, NN, p.L, p.W, k, step, out.mm,
+                                                   out.strand, out.pos, t);
             CURC_LAUNCH_CHECK();
             a.release(mk);
         }
