@@ -28,6 +28,8 @@ def lib() -> ctypes.CDLL:
         L = ctypes.CDLL(LIB_PATH)
         c_p, c_u64, c_int = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
         L.curc_ctx_create.argtypes = [c_int, ctypes.POINTER(c_p)]
+        L.curc_ctx_create_deferred.argtypes = [c_int, ctypes.POINTER(c_p)]
+        L.curc_ctx_wait.argtypes = [c_p]
         L.curc_ctx_destroy.argtypes = [c_p]
         L.curc_ctx_destroy.restype = None
         L.curc_last_error.argtypes = [c_p]
@@ -144,11 +146,19 @@ def decompress_file(archive: str, out_prefix: str, bsc: str | None = None, tmpdi
 class Context:
     """One CUDA stream and device arena on one GPU (curc_ctx)."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, deferred: bool = False):
+        """deferred: the CUDA set-up runs on a thread of its own
+        (curc_ctx_create_deferred); compress_files parses its input
+        meanwhile, every other call waits for it."""
         self._h = ctypes.c_void_p()
-        rc = lib().curc_ctx_create(device, ctypes.byref(self._h))
+        create = lib().curc_ctx_create_deferred if deferred else lib().curc_ctx_create
+        rc = create(device, ctypes.byref(self._h))
         if rc != 0:
             raise CurcError(f"curc_ctx_create: {lib().curc_last_error(None).decode()}")
+
+    def wait(self):
+        """Waits for a deferred context's CUDA set-up (curc_ctx_wait)."""
+        self._check(lib().curc_ctx_wait(self._h), "curc_ctx_wait")
 
     def _check(self, rc: int, what: str):
         if rc != 0:

@@ -128,6 +128,7 @@ void run_staged(BatchWorker& w, const BatchItem& it, int wi, std::chrono::steady
 
 template <class F>
 int guarded_batch(curc_ctx* ctx, F&& f) {
+    if (const int rc = ctx_wait(ctx)) return rc;
     try {
         CURC_CHECK(cudaSetDevice(ctx->device));
         return f();

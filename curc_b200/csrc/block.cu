@@ -3,8 +3,11 @@
 // One block of reads stays resident in HBM from the H2D copy of its ASCII
 // sequences to the final streams; only the streams (and, on request, stage
 // intermediates for parity checks) come back to the host.
+#include <chrono>
+#include <future>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -206,11 +209,38 @@ std::string& ctxless_error() {
     thread_local std::string e;
     return e;
 }
+
+int ctx_wait(curc_ctx* ctx) noexcept {
+    if (!ctx->ready.valid()) return CURC_OK;
+    // several threads may wait at once (curc -c announces the set-up while
+    // it parses); the error text is written under a lock
+    static std::mutex err_mu;
+    try {
+        ctx->ready.get();
+    } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> g(err_mu);
+        ctx->err = e.what();
+        return CURC_ERR_CUDA;
+    }
+    const cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> g(err_mu);
+        ctx->err = cudaGetErrorString(e);
+        return CURC_ERR_CUDA;
+    }
+    return CURC_OK;
+}
+
+bool ctx_ready_now(const curc_ctx* ctx) {
+    return !ctx->ready.valid() || ctx->ready.wait_for(std::chrono::seconds(0)) == std::future_status::ready;
+}
 }  // namespace curc
 namespace {
 
 template <class F>
 int guarded(curc_ctx* ctx, F&& f) {
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     try {
         if (ctx) CURC_CHECK(cudaSetDevice(ctx->device));
         f();
@@ -262,8 +292,38 @@ int curc_device_count(int* count) {
     return CURC_OK;
 }
 
+int curc_ctx_create_deferred(int device, curc_ctx** out) {
+    if (!out) return CURC_ERR_ARG;
+    *out = nullptr;
+    try {
+        auto* c = new curc_ctx;
+        c->device = device;
+        // driver start, primary context and the pipeline's stream, on a
+        // thread of their own; the calls that need them wait (ctx_wait)
+        c->ready = std::async(std::launch::async, [c, device] {
+                       int count = 0;
+                       CURC_CHECK(cudaGetDeviceCount(&count));
+                       if (device < 0 || device >= count) throw std::invalid_argument("no such CUDA device");
+                       CURC_CHECK(cudaSetDevice(device));
+                       CURC_CHECK(cudaFree(nullptr));
+                       c->block = std::make_unique<curc::Block>();
+                   }).share();
+        *out = c;
+        return CURC_OK;
+    } catch (const std::exception& e) {
+        curc::ctxless_error() = e.what();
+        return CURC_ERR_STATE;
+    }
+}
+
+int curc_ctx_wait(curc_ctx* ctx) {
+    if (!ctx) return CURC_ERR_ARG;
+    return curc::ctx_wait(ctx);
+}
+
 void curc_ctx_destroy(curc_ctx* ctx) {
     if (!ctx) return;
+    if (ctx->ready.valid()) ctx->ready.wait();
     cudaSetDevice(ctx->device);
     delete ctx;
 }
@@ -273,6 +333,8 @@ const char* curc_last_error(const curc_ctx* ctx) { return ctx ? ctx->err.c_str()
 int curc_pack_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, uint64_t* packed_dev,
                      uint8_t* has_n_dev, void* stream) {
     if (!ctx || (!seqs_dev && n) || (!packed_dev && n) || (!has_n_dev && n)) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     if (read_len < 1 || read_len > 512) {
         ctx->err = "read length must be in [1, 512]";
         return CURC_ERR_ARG;
@@ -293,6 +355,8 @@ int curc_pack_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t r
 int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
                           int paired_end) {
     if (!ctx || (!seqs_dev && n)) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     return guarded(ctx, [&] {
         ctx->block->arena.reset();
         ctx->block->run(reinterpret_cast<const uint8_t*>(seqs_dev), n, read_len, preserve_order != 0,
@@ -303,6 +367,8 @@ int curc_block_run_device(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint1
 int curc_block_run(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read_len, int preserve_order,
                    int paired_end) {
     if (!ctx || (!seqs && n)) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     return guarded(ctx, [&] {
         curc::Block& b = *ctx->block;
         b.arena.reset();
@@ -315,6 +381,8 @@ int curc_block_run(curc_ctx* ctx, const char* seqs, uint64_t n, uint16_t read_le
 
 int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* bytes) {
     if (!ctx || !name || !ptr || !bytes) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     const curc::Block* blk = curc::batch_current() ? curc::batch_current() : ctx->block.get();
     auto it = blk->host.find(name);
     if (it == blk->host.end()) {
@@ -328,6 +396,8 @@ int curc_block_get(curc_ctx* ctx, const char* name, const void** ptr, uint64_t* 
 
 int curc_ctx_trim(curc_ctx* ctx) {
     if (!ctx) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     if (ctx->batch && !ctx->batch->items.empty()) {
         ctx->err = "trim: blocks are queued for a drain";
         return CURC_ERR_STATE;
@@ -341,6 +411,8 @@ int curc_ctx_trim(curc_ctx* ctx) {
 
 int curc_ctx_keep_intermediates(curc_ctx* ctx, int keep) {
     if (!ctx) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     ctx->block->keep_intermediates = keep != 0;
     return CURC_OK;
 }
@@ -349,6 +421,8 @@ uint64_t curc_kernel_launches(void) { return curc::launches(); }
 
 int curc_block_stage_ms(curc_ctx* ctx, const char* stage, float* ms) {
     if (!ctx || !stage || !ms) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     auto it = ctx->block->stage_ms.find(stage);
     if (it == ctx->block->stage_ms.end()) {
         ctx->err = std::string("unknown stage: ") + stage;

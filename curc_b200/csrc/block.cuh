@@ -1,5 +1,6 @@
 // Device-resident state of one block and the pipeline driver.
 #pragma once
+#include <future>
 #include <map>
 #include <memory>
 #include <string>
@@ -143,4 +144,22 @@ struct curc_ctx {
     // set: whole-file compression also tries the learned mismatch coder
     std::unique_ptr<curc::learned::Model> mismatch_model;
     std::string err;
+    // curc_ctx_create_deferred: the CUDA set-up running on its own thread
+    // (`block` exists once it is ready); invalid for curc_ctx_create
+    std::shared_future<void> ready;
+    curc_ctx() = default;
+    curc_ctx(const curc_ctx&) = delete;
+    curc_ctx& operator=(const curc_ctx&) = delete;
+    ~curc_ctx() {
+        if (ready.valid()) ready.wait();
+    }
 };
+
+namespace curc {
+// Waits for a deferred context's CUDA set-up (then makes its device current
+// on the calling thread): CURC_OK, or the set-up's error (in ctx->err).
+int ctx_wait(curc_ctx* ctx) noexcept;
+// Whether the set-up of a deferred context has finished (always true for
+// a context made by curc_ctx_create).
+bool ctx_ready_now(const curc_ctx* ctx);
+}  // namespace curc

@@ -24,23 +24,33 @@ namespace curc {
 
 namespace {
 
-// Owned copy of a block's streams for the coder threads.
+// A block's streams, owned for the coder threads: the block's pinned arena
+// (the streams copied back from the device) and its host-made streams are
+// handed over, not copied, and the block starts its next run with a fresh
+// arena.  The block keeps no views of them.
 struct Snapshot {
     host::BlockView view;
+    PinnedArena pinned;
     std::vector<std::vector<uint8_t>> store;
 };
 
-std::shared_ptr<Snapshot> snapshot(const Block& b) {
+std::shared_ptr<Snapshot> snapshot(Block& b) {
     auto s = std::make_shared<Snapshot>();
     s->view.reads_count = b.n;
     s->view.read_len = b.p.L;
     s->view.preserve_order = b.p.preserve_order;
     s->view.paired_end = b.p.paired_end;
+    s->pinned = std::move(b.pinned);
     s->store.reserve(b.host.size());
-    for (const auto& kv : b.host) {
-        s->store.emplace_back(kv.second.ptr, kv.second.ptr + kv.second.size);
-        s->view.streams[kv.first] = host::Buf{s->store.back().data(), s->store.back().size()};
+    for (auto& kv : b.host) {
+        if (!kv.second.own.empty()) {
+            s->store.push_back(std::move(kv.second.own));
+            s->view.streams[kv.first] = host::Buf{s->store.back().data(), s->store.back().size()};
+        } else {
+            s->view.streams[kv.first] = host::Buf{kv.second.ptr, kv.second.size};
+        }
     }
+    b.host.clear();
     return s;
 }
 
@@ -61,11 +71,16 @@ struct FileTimes {
     }
 };
 
+// With a deferred context (curc_ctx_create_deferred) the sink does not wait
+// for CUDA: until the context is ready, windows are parsed into host
+// buffers of their own, and once it is (looked at every window, waited for
+// at the block's end) they are copied to the device in order and the sink
+// continues as above.  The set-up thus runs while the FASTQ files are read.
 class DeviceSink : public host::IngestSink {
 public:
-    DeviceSink(Block& blk, bool po, bool pe, const host::CoderParams& cp, bool verbose, FileTimes& times,
+    DeviceSink(curc_ctx* ctx, bool po, bool pe, const host::CoderParams& cp, bool verbose, FileTimes& times,
                const learned::Model* model)
-        : blk_(blk), po_(po), pe_(pe), cp_(cp), verbose_(verbose), times_(times), model_(model) {
+        : ctx_(ctx), po_(po), pe_(pe), cp_(cp), verbose_(verbose), times_(times), model_(model) {
         cp_.on_time = [t = &times_](const char* what, double s) { t->add_coder(what, s); };
         cp_.on_learned = [t = &times_](uint64_t plain, uint64_t learned) {
             std::lock_guard<std::mutex> g(t->mu);
@@ -73,24 +88,43 @@ public:
             t->mis_learned += learned;
             t->learned_blocks += learned < plain;
         };
-        for (auto& e : ev_) CURC_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     ~DeviceSink() override {
+        if (!blk_) return;
         for (auto& e : ev_) cudaEventSynchronize(e);
         for (auto& e : ev_) cudaEventDestroy(e);
         for (auto& b : stage_)
             if (b.ptr) cudaFreeHost(b.ptr);
+        blk_->keep_intermediates = keep_inter_;
+    }
+    // The context's block, once CUDA is ready (wait: block until it is).
+    bool attach(bool wait) {
+        if (blk_) return true;
+        if (!wait && !ctx_ready_now(ctx_)) return false;
+        if (ctx_wait(ctx_) != CURC_OK) throw CudaError(cudaErrorInitializationError, ctx_->err.c_str());
+        Block* b = ctx_->block.get();
+        for (auto& e : ev_) CURC_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        keep_inter_ = b->keep_intermediates;
+        b->keep_intermediates = false;
+        blk_ = b;
+        return true;
     }
     void begin_block(size_t max_bytes, int L) override {
         t_begin_ = clk::now();
         L_ = L;
-        blk_.arena.reset();
-        dev_ = blk_.arena.alloc<uint8_t>(max_bytes + 16);
-        cap_ = max_bytes;
-        off_ = 0;
+        max_bytes_ = max_bytes;
         reads_ = 0;
+        dev_open_ = false;
+        if (attach(false)) open_device_block();
     }
     char* window_buffer(size_t bytes) override {
+        if (!attach(false)) {
+            host_win_ = true;
+            pend_.push_back(Pending{std::unique_ptr<char[]>(new char[bytes]), 0});
+            return pend_.back().data.get();
+        }
+        host_win_ = false;
+        flush_pending();
         cur_ ^= 1;
         Stage& st = stage_[cur_];
         CURC_CHECK(cudaEventSynchronize(ev_[cur_]));  // its last copy is done
@@ -104,24 +138,30 @@ public:
     }
     void window_done(uint64_t reads) override {
         const size_t bytes = size_t(reads) * size_t(L_);
+        reads_ += reads;
+        if (host_win_) {
+            pend_.back().bytes = bytes;
+            return;
+        }
         if (off_ + bytes > cap_) throw std::runtime_error("ingest: block larger than its bound");
         if (bytes)
-            CURC_CHECK(cudaMemcpyAsync(dev_ + off_, stage_[cur_].ptr, bytes, cudaMemcpyHostToDevice, blk_.stream));
-        CURC_CHECK(cudaEventRecord(ev_[cur_], blk_.stream));
+            CURC_CHECK(cudaMemcpyAsync(dev_ + off_, stage_[cur_].ptr, bytes, cudaMemcpyHostToDevice, blk_->stream));
+        CURC_CHECK(cudaEventRecord(ev_[cur_], blk_->stream));
         off_ += bytes;
-        reads_ += reads;
     }
     void end_block() override {
+        attach(true);
+        flush_pending();
         const auto ta = clk::now();
-        blk_.run(dev_, reads_, L_, po_, pe_);
+        blk_->run(dev_, reads_, L_, po_, pe_);
         const auto tb = clk::now();
-        auto snap = snapshot(blk_);
+        auto snap = snapshot(*blk_);
         if (model_) {
             // learned mode: the block's learned mismatch stream, from the
             // block's device state before the next block reuses it; the
             // writer keeps it when it is smaller than the plain coding
             const auto l0 = clk::now();
-            snap->view.learned_stream = learned::encode_stream(*model_, blk_);
+            snap->view.learned_stream = learned::encode_stream(*model_, *blk_);
             snap->view.learned_model.assign(reinterpret_cast<const char*>(model_), sizeof(learned::Model));
             times_.add_coder("learned", secs(l0, clk::now()));
         }
@@ -160,14 +200,45 @@ private:
         char* ptr = nullptr;
         size_t size = 0;
     };
-    Block& blk_;
+    // the device side of the current block: its input in the arena
+    void open_device_block() {
+        blk_->arena.reset();
+        dev_ = blk_->arena.alloc<uint8_t>(max_bytes_ + 16);
+        cap_ = max_bytes_;
+        off_ = 0;
+        dev_open_ = true;
+    }
+    // windows parsed before the context was ready, copied in order
+    void flush_pending() {
+        if (!dev_open_) open_device_block();
+        if (pend_.empty()) return;
+        for (auto& w : pend_) {
+            if (off_ + w.bytes > cap_) throw std::runtime_error("ingest: block larger than its bound");
+            // pageable source: the call returns once the bytes are staged
+            if (w.bytes) CURC_CHECK(cudaMemcpyAsync(dev_ + off_, w.data.get(), w.bytes, cudaMemcpyHostToDevice,
+                                                    blk_->stream));
+            off_ += w.bytes;
+        }
+        CURC_CHECK(cudaStreamSynchronize(blk_->stream));
+        pend_.clear();
+    }
+    struct Pending {
+        std::unique_ptr<char[]> data;
+        size_t bytes;
+    };
+    curc_ctx* ctx_;
+    Block* blk_ = nullptr;
+    bool keep_inter_ = false;
+    std::vector<Pending> pend_;
+    bool host_win_ = false, dev_open_ = false;
+    size_t max_bytes_ = 0;
     bool po_, pe_;
     host::CoderParams cp_;
     bool verbose_;
     FileTimes& times_;
     const learned::Model* model_;
     Stage stage_[2];
-    cudaEvent_t ev_[2];
+    cudaEvent_t ev_[2] = {nullptr, nullptr};
     int cur_ = 0, L_ = 0;
     uint8_t* dev_ = nullptr;
     size_t cap_ = 0, off_ = 0;
@@ -216,10 +287,9 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
         return CURC_ERR_ARG;
     }
     try {
-        CURC_CHECK(cudaSetDevice(ctx->device));
-        curc::Block& blk = *ctx->block;
-        const bool keep_inter = blk.keep_intermediates;
-        blk.keep_intermediates = false;
+        // a deferred context is not waited for here: the sink parses while
+        // its CUDA set-up runs (DeviceSink)
+        if (!ctx->ready.valid()) CURC_CHECK(cudaSetDevice(ctx->device));
         curc::host::CoderParams cp;
         cp.flzma2_level = flzma2_level;
         cp.flzma2_threads = flzma2_threads;
@@ -230,12 +300,14 @@ extern "C" int curc_compress_files(curc_ctx* ctx, const char* f1, const char* f2
         const bool verbose = std::getenv("CURC_VERBOSE") != nullptr;
         const auto t0 = std::chrono::steady_clock::now();
         curc::FileTimes times;
-        curc::DeviceSink sink(blk, preserve_order != 0, !s2.empty(), cp, verbose, times, ctx->mismatch_model.get());
+        curc::DeviceSink sink(ctx, preserve_order != 0, !s2.empty(), cp, verbose, times, ctx->mismatch_model.get());
         const auto res = curc::host::ingest_fastq(f1, s2, block_ratio, sink);
         const auto t1 = std::chrono::steady_clock::now();
         const int L = res.read_len;
         auto& bodies = sink.bodies;
-        blk.keep_intermediates = keep_inter;
+        // the block (an input without reads never attached the sink)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
+        curc::Block& blk = *ctx->block;
         FILE* out = std::fopen(archive_path, "wb");
         if (!out) throw std::runtime_error(std::string("cannot write ") + archive_path);
         const std::string hdr = curc::host::archive_header(preserve_order != 0, !s2.empty(), L, res.blocks);

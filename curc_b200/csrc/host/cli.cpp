@@ -4,6 +4,7 @@
 // [--preserve_order]` writes <working_dir>/<name>.curc.
 // Decompression: `curc -d -i in.curc -o name [--working_dir d]` writes
 // <working_dir>/<name>.seq (or <name>_1.seq and <name>_2.seq), host only.
+#include <thread>
 #include <dlfcn.h>
 #include <limits.h>
 #include <stdlib.h>
@@ -170,8 +171,9 @@ int main(int argc, char** argv) {
         std::puts("--coder is plain or learned");
         return 0;
     }
+    // the CUDA set-up runs on its own thread while the FASTQ input is read
     curc_ctx* ctx = nullptr;
-    if (curc_ctx_create(device, &ctx) != CURC_OK) {
+    if (curc_ctx_create_deferred(device, &ctx) != CURC_OK) {
         std::fprintf(stderr, "GPU assert: %s\n", curc_last_error(nullptr));
         return 1;
     }
@@ -180,14 +182,21 @@ int main(int argc, char** argv) {
         curc_ctx_destroy(ctx);
         return 0;
     }
-    int devices = 0;
-    curc_device_count(&devices);
-    // the reference's progress lines (compress.cu:2183-2190, preprocess.cpp)
-    std::printf("gpu context init finish\n");
-    std::printf("GPU device count : %d\n", devices);
-    std::fflush(stdout);
+    // the reference's progress lines (compress.cu:2183-2190, preprocess.cpp),
+    // printed when the set-up has finished
+    int init_rc = CURC_OK;
+    std::thread announce([&] {
+        init_rc = curc_ctx_wait(ctx);
+        if (init_rc != CURC_OK) return;
+        int devices = 0;
+        curc_device_count(&devices);
+        std::printf("gpu context init finish\n");
+        std::printf("GPU device count : %d\n", devices);
+        std::fflush(stdout);
+    });
     std::string tmp = wd + "/curc_tmp_XXXXXX";
     if (!mkdtemp(&tmp[0])) {
+        announce.join();
         std::puts("cannot create a working directory");
         return 1;
     }
@@ -198,7 +207,12 @@ int main(int argc, char** argv) {
     const int rc = curc_compress_files(ctx, files[0].c_str(), files.size() > 1 ? files[1].c_str() : nullptr,
                                        archive.c_str(), ratio, po, level, threads, bsc.c_str(), tmp.c_str(), &reads,
                                        &blocks);
+    announce.join();
     rmdir(tmp.c_str());
+    if (init_rc != CURC_OK) {
+        std::fprintf(stderr, "GPU assert: %s\n", curc_last_error(ctx));
+        return 1;
+    }
     if (rc != CURC_OK) {
         std::fprintf(stderr, "curc: %s\n", curc_last_error(ctx));
         curc_ctx_destroy(ctx);

@@ -854,6 +854,8 @@ const char* curc_learn_error(const curc_learn* L) { return L ? L->t.err.c_str() 
 
 int curc_learn_add_block(curc_learn* L, curc_ctx* ctx) {
     if (!L || !ctx) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     return guarded_learn(L, [&] {
         Block& b = *ctx->block;
         auto mk = b.arena.mark();
@@ -1010,6 +1012,8 @@ int curc_learn_set_model(curc_learn* L, const void* ptr, uint64_t bytes) {
 // over CHUNK_RECORDS records with mismatches).
 int curc_learn_encode(curc_learn* L, curc_ctx* ctx, const void** out, uint64_t* bytes) {
     if (!L || !ctx || !out || !bytes) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     return guarded_learn(L, [&] {
         Trainer& T = L->t;
         if (!T.quantised) throw std::runtime_error("learned: no quantised model");
@@ -1026,6 +1030,8 @@ int curc_learn_encode(curc_learn* L, curc_ctx* ctx, const void** out, uint64_t* 
 // number of anchors and *mismatched how many differ in any frequency.
 int curc_learn_infer_check(curc_learn* L, curc_ctx* ctx, uint64_t* anchors, uint64_t* mismatched) {
     if (!L || !ctx || !anchors || !mismatched) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     return guarded_learn(L, [&] {
         Trainer& T = L->t;
         if (!T.quantised) throw std::runtime_error("learned: no quantised model");
@@ -1066,6 +1072,8 @@ int curc_learn_infer_check(curc_learn* L, curc_ctx* ctx, uint64_t* anchors, uint
 // context's last block.  *ok = 1 when all match.
 int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint64_t bytes, int* ok) {
     if (!L || !ctx || !data || !ok) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     return guarded_learn(L, [&] {
         Trainer& T = L->t;
         Block& b = *ctx->block;
@@ -1116,6 +1124,8 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
 
 int curc_plain_mismatch_bytes(curc_ctx* ctx, uint64_t* out) {
     if (!ctx || !out) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     try {
         const Block& b = *ctx->block;
         host::BlockView v;
@@ -1134,6 +1144,8 @@ int curc_plain_mismatch_bytes(curc_ctx* ctx, uint64_t* out) {
 
 int curc_mismatch_general_bytes(curc_ctx* ctx, const char* bsc_path, const char* tmpdir, uint64_t* out) {
     if (!ctx || !bsc_path || !tmpdir || !out) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     try {
         const Block& b = *ctx->block;
         host::BlockView v;

@@ -161,6 +161,17 @@ PinnedArena::~PinnedArena() {
     for (auto& c : chunks_) cudaFreeHost(c.base);
 }
 
+PinnedArena& PinnedArena::operator=(PinnedArena&& o) noexcept {
+    if (this != &o) {
+        for (auto& c : chunks_) cudaFreeHost(c.base);
+        chunks_ = std::move(o.chunks_);
+        cur_ = o.cur_;
+        o.chunks_.clear();
+        o.cur_ = 0;
+    }
+    return *this;
+}
+
 uint8_t* PinnedArena::alloc(size_t bytes) {
     bytes = (bytes + 63) & ~size_t(63);
     while (cur_ < chunks_.size()) {

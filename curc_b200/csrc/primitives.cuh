@@ -53,7 +53,16 @@ private:
 // copied into it asynchronously and returned as views.
 class PinnedArena {
 public:
+    PinnedArena() = default;
     ~PinnedArena();
+    PinnedArena(const PinnedArena&) = delete;
+    PinnedArena& operator=(const PinnedArena&) = delete;
+    // moving hands the chunks over (views into them stay valid)
+    PinnedArena(PinnedArena&& o) noexcept : chunks_(std::move(o.chunks_)), cur_(o.cur_) {
+        o.chunks_.clear();
+        o.cur_ = 0;
+    }
+    PinnedArena& operator=(PinnedArena&& o) noexcept;
     uint8_t* alloc(size_t bytes);
     void reset();
 

@@ -81,6 +81,8 @@ extern "C" {
 
 int curc_ctx_set_tuning(curc_ctx* ctx, const int32_t* knobs) {
     if (!ctx || !knobs) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     Tuning t{knobs[0], knobs[1], knobs[2], knobs[3], knobs[4]};
     if (!curc::valid(t)) {
         ctx->err = "tuning: a knob outside its candidate values";
@@ -92,6 +94,8 @@ int curc_ctx_set_tuning(curc_ctx* ctx, const int32_t* knobs) {
 
 int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs) {
     if (!ctx || !knobs) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     const Tuning& t = ctx->block->tune;
     knobs[0] = t.table_factor;
     knobs[1] = t.bitmap_bits;
@@ -103,6 +107,8 @@ int curc_ctx_get_tuning(curc_ctx* ctx, int32_t* knobs) {
 
 int curc_ctx_use_tuning_cache(curc_ctx* ctx, const char* cache_path) {
     if (!ctx) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     try {
         if (!cache_path || !*cache_path) {
             ctx->block->tune_cache.reset();
@@ -122,6 +128,8 @@ int curc_ctx_use_tuning_cache(curc_ctx* ctx, const char* cache_path) {
 int curc_autotune(curc_ctx* ctx, const char* seqs_dev, uint64_t n, uint16_t read_len, int preserve_order,
                   int paired_end, const char* cache_path, int* from_cache) {
     if (!ctx || !seqs_dev || !n) return CURC_ERR_ARG;
+    if (ctx)
+        if (const int rc = curc::ctx_wait(ctx)) return rc;
     try {
         CURC_CHECK(cudaSetDevice(ctx->device));
         curc::Block& blk = *ctx->block;

@@ -37,6 +37,13 @@ typedef struct curc_ctx curc_ctx;
 /* Creates a context on `device` (get_device_count_and_init,
  * src/compress.cu:2183-2195, per device). */
 int curc_ctx_create(int device, curc_ctx** out);
+/* The same, returning at once: the CUDA set-up (driver start, context, the
+ * pipeline's stream; about a second on a fresh process) runs on a thread of
+ * its own.  curc_compress_files parses its FASTQ input meanwhile; every
+ * other call waits for the set-up and returns its error, if it failed.
+ * curc_ctx_wait waits for it explicitly.  No reference counterpart. */
+int curc_ctx_create_deferred(int device, curc_ctx** out);
+int curc_ctx_wait(curc_ctx* ctx);
 void curc_ctx_destroy(curc_ctx* ctx);
 /* Last error message of the context (or of creation when ctx is NULL). */
 const char* curc_last_error(const curc_ctx* ctx);

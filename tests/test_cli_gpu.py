@@ -70,6 +70,8 @@ def test_cli_archive(name, tmp_path):
     files = w.write(str(tmp_path / name))
     mine, out = run_cli(files, w.preserve_order, tmp_path, "prod")
     assert "archive size" in out
+    # the CUDA set-up runs while the input is parsed; its line still comes first
+    assert out.index("gpu context init finish") < out.index("reads count")
     assert mine == oracle(files, w.preserve_order, tmp_path)
     if META[name]["deterministic"] and name != "pe150_po_p8k":
         assert mine == open(os.path.join(GOLDEN, name + ".curc"), "rb").read()
@@ -84,3 +86,19 @@ def test_cli_multiblock(tmp_path):
     assert mine[4] >= 2  # blocks
     assert mine == oracle(files, False, tmp_path, ratio=0.3)
     assert decode_matches(os.path.join(tmp_path, "prod.curc"), w, tmp_path)
+
+
+def test_deferred_context_compresses_alike(tmp_path):
+    """curc_ctx_create_deferred: the FASTQ windows parsed before the CUDA
+    set-up has finished wait in host memory and reach the device in order;
+    the archive is the oracle's, over several windows and blocks."""
+    from curc_b200 import Context
+    w = synth.small_single(seed=32, n_reads=300_000, read_len=100, genome_len=800_000)
+    files = w.write(str(tmp_path / "df"), name=b"synthetic_read_")
+    bsc = os.path.join(ROOT, "curc_b200", "_build", "bsc")
+    arc = str(tmp_path / "deferred.curc")
+    with Context(0, deferred=True) as ctx:
+        ctx.compress_files(files, arc, 0.3, False, bsc, str(tmp_path))
+    mine = open(arc, "rb").read()
+    assert mine[4] >= 2  # blocks
+    assert mine == oracle(files, False, tmp_path, ratio=0.3)
