@@ -44,6 +44,7 @@
 
 #include "../../../include/curc_b200.h"
 #include "host.hpp"
+#include "stable_order.hpp"
 
 namespace curc {
 namespace host {
@@ -267,12 +268,11 @@ std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr
     std::vector<uint16_t> off_val;
     std::vector<int16_t> d_val;
     const uint32_t pairs = uint32_t(n / 2);
-    std::vector<uint32_t> rank;
-    for (uint32_t i = 0; i < n; i += 2) {
-        base.push_back(T(id_to_pos[i]));
-        rank.push_back(i >> 1);
-    }
-    std::stable_sort(rank.begin(), rank.end(), [&](uint32_t a, uint32_t b) { return base[a] < base[b]; });
+    base.reserve(pairs);
+    for (uint32_t i = 0; i < n; i += 2) base.push_back(T(id_to_pos[i]));
+    // pairs by their first mate's position, ties in pair order (the
+    // reference's stable sort, on host threads)
+    const std::vector<uint32_t> rank = stable_order(base.data(), base.size(), thr);
     int64_t ref_prev = 0, prev = 0;
     bool match = false;
     for (uint32_t q = 0; q < pairs; ++q) {

@@ -40,6 +40,7 @@
 
 #include "../../../include/curc_b200.h"
 #include "host.hpp"
+#include "stable_order.hpp"
 #include "../learned_model.hpp"
 
 namespace curc {
@@ -525,9 +526,8 @@ std::vector<uint64_t> pe_positions(const std::string& payload, uint32_t reads, i
     if (!r.done()) throw std::runtime_error("bytes after the pair position streams");
     const uint32_t pairs = reads / 2;
     if (first.size() != pairs || off_flag.size() != pairs) throw std::runtime_error("pair position streams disagree");
-    std::vector<uint32_t> order(pairs);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return first[a] < first[b]; });
+    // pairs by their first mate's position, ties in pair order
+    const std::vector<uint32_t> order = stable_order(first.data(), first.size(), threads);
     std::vector<uint64_t> second(pairs);
     size_t io = 0, idf = 0, idv = 0, iv = 0;
     int64_t ref_prev = 0, prev = 0;
