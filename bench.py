@@ -393,7 +393,8 @@ CURC_EXE = os.path.join(ROOT, "curc_b200", "_build", "curc")
 BSC_EXE = os.path.join(ROOT, "curc_b200", "_build", "bsc")
 HOST_STAGES = ["files.total", "files.ingest", "files.device", "files.snapshot", "files.until_last_block",
                "files.coder_tail", "files.coders", "coder.id_pos", "coder.strand", "coder.ref", "coder.maps",
-               "coder.mis_cnt", "coder.mis_base", "coder.mis_off", "coder.read_off", "coder.pe_order"]
+               "coder.mis_cnt", "coder.mis_base", "coder.mis_off", "coder.read_off", "coder.pe_order",
+               "coder.id_pos.fl2_base", "coder.id_pos.order", "coder.id_pos.split", "coder.id_pos.ppmd"]
 
 
 def sample_of(w, pairs):

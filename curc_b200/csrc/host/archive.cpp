@@ -261,8 +261,12 @@ std::string bsc_strand(const std::string& bsc, const std::string& dir, const voi
 }
 
 template <class T>
-std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr) {
+std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr, const CoderParams& cp) {
     // util.cuh:345-442
+    using clk = std::chrono::steady_clock;
+    auto mark = [&](const char* what, clk::time_point a) {
+        if (cp.on_time) cp.on_time(what, std::chrono::duration<double>(clk::now() - a).count());
+    };
     std::vector<T> base, notbase;
     std::vector<uint8_t> off_flag, off_first, d_flag, d_first;
     std::vector<uint16_t> off_val;
@@ -270,9 +274,23 @@ std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr
     const uint32_t pairs = uint32_t(n / 2);
     base.reserve(pairs);
     for (uint32_t i = 0; i < n; i += 2) base.push_back(T(id_to_pos[i]));
+    // the first mates' positions are coded as they are: their fast-lzma2
+    // stream runs while the pairs are ordered and split
+    auto fb = std::async(std::launch::async, [&] {
+        const auto a = clk::now();
+        std::string r = fl2(base.data(), base.size() * sizeof(T), level, thr);
+        mark("id_pos.fl2_base", a);
+        return r;
+    });
+    auto t = clk::now();
     // pairs by their first mate's position, ties in pair order (the
     // reference's stable sort, on host threads)
     const std::vector<uint32_t> rank = stable_order(base.data(), base.size(), thr);
+    mark("id_pos.order", t);
+    t = clk::now();
+    off_flag.reserve(pairs);
+    off_first.reserve(pairs);
+    off_val.reserve(pairs);
     int64_t ref_prev = 0, prev = 0;
     bool match = false;
     for (uint32_t q = 0; q < pairs; ++q) {
@@ -301,9 +319,10 @@ std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr
         }
         prev = int64_t(rel);
     }
-    auto fb = std::async(std::launch::async, [&] { return fl2(base.data(), base.size() * sizeof(T), level, thr); });
+    mark("id_pos.split", t);
     auto fn = std::async(std::launch::async, [&] { return fl2(notbase.data(), notbase.size() * sizeof(T), level, thr); });
     const double bm = COMPRESSION_ESTIMATION_UINT8_BITMAP;
+    t = clk::now();
     std::string mid = containers({
         [&] { return container(off_flag.data(), off_flag.size(), PPMD7_CODER, 3, bm); },
         [&] { return container(off_first.data(), off_first.size(), PPMD7_CODER, 3, bm); },
@@ -312,6 +331,7 @@ std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr
         [&] { return container(d_first.data(), d_first.size(), PPMD7_CODER, 3, bm); },
         [&] { return container(d_val.data(), d_val.size() * 2, PPMD7_CODER, 3, 1); },
     });
+    mark("id_pos.ppmd", t);
     std::string o = blob(fb.get());
     o += mid;
     o += blob(fn.get());
@@ -414,7 +434,7 @@ std::string encode_block(const BlockView& v, const CoderParams& cp) {
                 }
                 return fl2(p, n * 8, lvl, thr);
             }
-            return join_std ? pe_id_to_pos<uint32_t>(p, n, lvl, thr) : pe_id_to_pos<uint64_t>(p, n, lvl, thr);
+            return join_std ? pe_id_to_pos<uint32_t>(p, n, lvl, thr, cp) : pe_id_to_pos<uint64_t>(p, n, lvl, thr, cp);
         }); });
     }
     f_strand = std::async(std::launch::async, [&] { return timed(cp, "strand", [&] {
