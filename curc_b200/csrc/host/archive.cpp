@@ -264,8 +264,11 @@ template <class T>
 std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr, const CoderParams& cp) {
     // util.cuh:345-442
     using clk = std::chrono::steady_clock;
+    static const bool verbose = std::getenv("CURC_VERBOSE") != nullptr;
     auto mark = [&](const char* what, clk::time_point a) {
-        if (cp.on_time) cp.on_time(what, std::chrono::duration<double>(clk::now() - a).count());
+        const double sec = std::chrono::duration<double>(clk::now() - a).count();
+        if (verbose) std::fprintf(stderr, "curc:   coder %-16s %.3f s\n", what, sec);
+        if (cp.on_time) cp.on_time(what, sec);
     };
     std::vector<T> base, notbase;
     std::vector<uint8_t> off_flag, off_first, d_flag, d_first;
@@ -288,22 +291,47 @@ std::string pe_id_to_pos(const uint64_t* id_to_pos, size_t n, int level, int thr
     const std::vector<uint32_t> rank = stable_order(base.data(), base.size(), thr);
     mark("id_pos.order", t);
     t = clk::now();
-    off_flag.reserve(pairs);
-    off_first.reserve(pairs);
-    off_val.reserve(pairs);
+    // per pair, in that order: which mate comes first and their distance,
+    // read on host threads (the second mates' positions are read at random);
+    // the pairs within 16 bits go to their streams by a prefix count, the
+    // others, which carry the delta coder's state, in one pass
+    const size_t nt = chunk_count(pairs, thr);
+    std::vector<uint8_t> bef(pairs);
+    std::vector<T> relv(pairs);
+    off_flag.resize(pairs);
+    std::vector<size_t> n16(nt + 1, 0);
+    each_chunk(pairs, nt, [&](size_t lo, size_t hi, size_t c) {
+        size_t k = 0;
+        for (size_t q = lo; q < hi; ++q) {
+            const uint32_t i = rank[q] * 2;
+            const bool before = id_to_pos[i] < id_to_pos[i + 1];
+            const T rel = before ? T(id_to_pos[i + 1] - id_to_pos[i]) : T(id_to_pos[i] - id_to_pos[i + 1]);
+            bef[q] = before;
+            relv[q] = rel;
+            off_flag[q] = rel <= 0xFFFF;
+            k += off_flag[q];
+        }
+        n16[c + 1] = k;
+    });
+    for (size_t c = 0; c < nt; ++c) n16[c + 1] += n16[c];
+    off_first.resize(n16[nt]);
+    off_val.resize(n16[nt]);
+    each_chunk(pairs, nt, [&](size_t lo, size_t hi, size_t c) {
+        size_t p = n16[c];
+        for (size_t q = lo; q < hi; ++q)
+            if (off_flag[q]) {
+                off_first[p] = bef[q];
+                off_val[p] = uint16_t(relv[q]);
+                ++p;
+            }
+    });
     int64_t ref_prev = 0, prev = 0;
     bool match = false;
     for (uint32_t q = 0; q < pairs; ++q) {
+        if (off_flag[q]) continue;
         const uint32_t i = rank[q] * 2;
-        const bool before = id_to_pos[i] < id_to_pos[i + 1];
-        const T rel = before ? T(id_to_pos[i + 1] - id_to_pos[i]) : T(id_to_pos[i] - id_to_pos[i + 1]);
-        const bool in16 = rel <= 0xFFFF;
-        off_flag.push_back(in16);
-        if (in16) {
-            off_first.push_back(before);
-            off_val.push_back(uint16_t(rel));
-            continue;
-        }
+        const bool before = bef[q] != 0;
+        const T rel = relv[q];
         const int64_t delta = int64_t(rel) - ref_prev;
         const bool d16 = delta <= INT16_MAX && delta >= INT16_MIN;
         d_flag.push_back(d16);

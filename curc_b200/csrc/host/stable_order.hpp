@@ -18,21 +18,31 @@
 namespace curc {
 namespace host {
 
+// Chunks of [0, n) for up to `threads` threads (at least 65536 items each).
+inline size_t chunk_count(size_t n, int threads) {
+    return std::max<size_t>(1, std::min<size_t>(size_t(std::max(1, threads)), n / 65536 + 1));
+}
+
+// f(lo, hi, t) on each of the `nt` contiguous chunks of [0, n), one
+// std::thread per chunk (the calling thread takes chunk 0).
+template <class F>
+void each_chunk(size_t n, size_t nt, F&& f) {
+    const size_t chunk = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nt; ++t)
+        th.emplace_back([&, t] { f(std::min(n, t * chunk), std::min(n, (t + 1) * chunk), t); });
+    f(size_t(0), std::min(n, chunk), size_t(0));
+    for (auto& x : th) x.join();
+}
+
 template <class T>
 std::vector<uint32_t> stable_order(const T* key, size_t n, int threads = 16) {
     static_assert(sizeof(T) <= 8, "keys of at most 64 bits");
     std::vector<uint32_t> idx(n);
     for (size_t i = 0; i < n; ++i) idx[i] = uint32_t(i);
     if (n < 2) return idx;
-    const size_t nt = std::max<size_t>(1, std::min<size_t>(size_t(std::max(1, threads)), n / 65536 + 1));
-    const size_t chunk = (n + nt - 1) / nt;
-    auto each = [&](auto&& f) {  // f(lo, hi, t) on every chunk, one thread each
-        std::vector<std::thread> th;
-        for (size_t t = 1; t < nt; ++t)
-            th.emplace_back([&, t] { f(std::min(n, t * chunk), std::min(n, (t + 1) * chunk), t); });
-        f(size_t(0), std::min(n, chunk), size_t(0));
-        for (auto& x : th) x.join();
-    };
+    const size_t nt = chunk_count(n, threads);
+    auto each = [&](auto&& f) { each_chunk(n, nt, f); };
     std::vector<T> k(key, key + n), k2(n);
     std::vector<uint32_t> idx2(n);
     // bytes in which some keys differ

@@ -71,6 +71,10 @@ CASES = {
                                           preserve_order=False),
     "pe150_po": lambda: synth.paired_repeats(seed=66, pairs=8_000, read_len=150, genome_len=300_000,
                                              preserve_order=True),
+    # enough pairs for the position coder's threads to split the work, and
+    # mates far enough apart for its delta streams
+    "pe150_po_150k": lambda: synth.paired_repeats(seed=67, pairs=150_000, read_len=150, genome_len=2_000_000,
+                                                  preserve_order=True),
 }
 
 
