@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -194,6 +195,57 @@ LM_HD void model_freqs(const Model& M, const int* idx, int nidx, int gmax, uint3
     logits_to_freq(M, z + NB, gap_bin(gmax < 0 ? 0 : gmax) + 1, NG, fg);
 }
 
+// Host form of the network for the decoder, which evaluates it once per
+// anchor: the weights widened to int16 once (layer 1 transposed, so an
+// anchor's active inputs add whole rows) so that the products vectorise
+// (16-bit multiply-add).  The activations after requant lie in [0, 127], so
+// every product and sum is the int32 value model_freqs computes, and
+// integer sums are exact in any order: the frequencies are model_freqs's.
+struct HostModel {
+    const Model* M;
+    alignas(64) int16_t w1t[IN][HID];
+    alignas(64) int16_t w2[HID][HID];
+    alignas(64) int16_t w3[OUT][HID];
+    explicit HostModel(const Model& m) : M(&m) {
+        for (int h = 0; h < HID; ++h)
+            for (int i = 0; i < IN; ++i) w1t[i][h] = m.w1[h][i];
+        for (int h = 0; h < HID; ++h)
+            for (int t = 0; t < HID; ++t) w2[h][t] = m.w2[h][t];
+        for (int o = 0; o < OUT; ++o)
+            for (int t = 0; t < HID; ++t) w3[o][t] = m.w3[o][t];
+    }
+};
+
+inline void model_freqs_host(const HostModel& H, const int* idx, int nidx, int gmax, uint32_t* fb, uint32_t* fg) {
+    const Model& M = *H.M;
+    alignas(64) int32_t acc1[HID];
+    alignas(64) int16_t a1[HID], a2[HID];
+    for (int h = 0; h < HID; ++h) acc1[h] = M.b1[h];
+    for (int t = 0; t < nidx; ++t) {
+        const int16_t* row = H.w1t[idx[t]];
+#pragma omp simd
+        for (int h = 0; h < HID; ++h) acc1[h] += row[h];
+    }
+    for (int h = 0; h < HID; ++h) a1[h] = int16_t(requant(acc1[h], M.m1, M.sh1));
+    for (int h = 0; h < HID; ++h) {
+        int32_t acc = 0;
+        const int16_t* w = H.w2[h];
+#pragma omp simd reduction(+ : acc)
+        for (int t = 0; t < HID; ++t) acc += int32_t(w[t]) * int32_t(a1[t]);
+        a2[h] = int16_t(requant(acc + M.b2[h], M.m2, M.sh2));
+    }
+    int32_t z[OUT];
+    for (int o = 0; o < OUT; ++o) {
+        int32_t acc = 0;
+        const int16_t* w = H.w3[o];
+#pragma omp simd reduction(+ : acc)
+        for (int t = 0; t < HID; ++t) acc += int32_t(w[t]) * int32_t(a2[t]);
+        z[o] = acc + M.b3[o];
+    }
+    logits_to_freq(M, z, NB, NB, fb);
+    logits_to_freq(M, z + NB, gap_bin(gmax < 0 ? 0 : gmax) + 1, NG, fg);
+}
+
 // Context of the adaptive in-bin models.  One context: splitting them by
 // strand and read position (16 contexts) spread the 16384-record chunks too
 // thin and coded 1% larger on the ramped-error workload.
@@ -363,6 +415,7 @@ inline std::string decode_stream(const Model& M, const uint8_t* p, size_t bytes,
     }
     if (coff[nc] != bytes) return "learned stream: length disagrees with its chunks";
     int bad = 0;
+    const auto H = std::make_unique<HostModel>(M);
 #pragma omp parallel for schedule(dynamic) reduction(+ : bad)
     for (int c = 0; c < int(nc); ++c) {
         RangeDecoder dec(p + coff[c], size_t(coff[c + 1] - coff[c]));
@@ -382,7 +435,7 @@ inline std::string decode_stream(const Model& M, const uint8_t* p, size_t bytes,
                 }
                 const int n = anchor_features(ref, rl, pos[r], q, L, strand[r], prev, m - j, gmx, idx);
                 uint32_t fb[NB], fg[NG];
-                model_freqs(M, idx, n, gmx, fb, fg);
+                model_freqs_host(*H, idx, n, gmx, fb, fg);
                 if (j > 0) {
                     const uint32_t v = dec.peek(TOTAL);
                     uint32_t cum = 0;
