@@ -26,3 +26,14 @@ def test_learned_stream_round_trip(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "learned round trips ok" in r.stdout
+
+
+def test_host_network_form_gives_the_same_frequencies(tmp_path):
+    """The decoder's int16 form of the network (model_freqs_host) against the
+    integer model on full-range random weights (tests/helpers/host_model_check.cpp)."""
+    exe = str(tmp_path / "host_model_check")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-fopenmp", "-I", os.path.join(ROOT, "curc_b200", "csrc"), "-o", exe,
+                    os.path.join(ROOT, "tests", "helpers", "host_model_check.cpp")], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "host model ok" in r.stdout
