@@ -5,9 +5,11 @@
 //
 // B200 design: a persistent grid walks tiles of 64 reads.  Each tile is
 // 64*L contiguous bytes, moved into shared memory by a 1D TMA bulk copy
-// (cp.async.bulk + mbarrier) two tiles ahead of the compute (three stages),
-// so HBM reads are full-line, enough bytes are in flight per SM, and the
-// copies overlap the packing.  The block then works in two
+// (cp.async.bulk + mbarrier) one tile ahead of the compute (two stages),
+// so HBM reads are full-line and the copies overlap the packing; with two
+// stages a block's shared memory is small enough for 9 blocks per SM at
+// 150 bp, and the packing itself (a few instructions per byte) is what
+// more resident warps hide.  The block then works in two
 // conflict-free passes: every thread turns 16-byte groups of the tile into
 // 32 bits of codes (one 16-byte shared-memory load each), giving the tile's
 // bases as one contiguous 2-bit string, and then every thread cuts one
@@ -24,7 +26,7 @@ namespace curc {
 
 namespace {
 constexpr int PACK_READS = 64;
-constexpr int PACK_STAGES = 3;  // tiles in flight per block: PACK_STAGES - 1 copies ahead of the compute
+constexpr int PACK_STAGES = 2;  // tiles in flight per block: PACK_STAGES - 1 copies ahead of the compute
 constexpr uint32_t WAIT_LIMIT = 1u << 26;
 constexpr int MAX_DEVICES = 64;
 
@@ -62,21 +64,23 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 
 // Four ASCII bases (a little-endian word, first base in the low byte) to
-// eight bits, first base in the top two: bits 1-3 of the letters give
-// A/a 0, C/c 1, G/g 2, T/t 3 as ((c >> 1) ^ (c >> 2)) & 3, and one multiply
-// gathers the four 2-bit codes into the top byte.
-__device__ __forceinline__ uint32_t pack4(uint32_t x) {
-    const uint32_t t = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
-    return (t * 0x40100401u) >> 24;
-}
+// their 2-bit codes, one per byte: bits 1-3 of the letters give A/a 0,
+// C/c 1, G/g 2, T/t 3 as ((c >> 1) ^ (c >> 2)) & 3.
+__device__ __forceinline__ uint32_t codes4(uint32_t x) { return ((x >> 1) ^ (x >> 2)) & 0x03030303u; }
 
-// The four bytes are all A, C, G or T in either case (the common case,
-// where pack4 is exact and no N is present): rebuild them, in lower case,
-// from their codes.
-__device__ __forceinline__ bool acgt4(uint32_t x) {
-    const uint32_t t = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
-    const uint32_t sel = (t & 3u) | ((t >> 4) & 0x30u) | ((t >> 8) & 0x300u) | ((t >> 12) & 0x3000u);
-    return __byte_perm(0x74676361u, 0u, sel) == (x | 0x20202020u);
+// The codes as eight bits, first base in the top two, in the top byte of
+// the product (one multiply gathers them; no partial product carries into
+// that byte).
+__device__ __forceinline__ uint32_t gather4(uint32_t t) { return t * 0x40100401u; }
+
+// The letters that four codes stand for, in lower case ("acgt"[t_i] in
+// byte i).  u's byte 0 holds t0 | t1 << 4 and its byte 2 t2 | t3 << 4, so
+// one permute makes them the lookup's selector.  The four input bytes are
+// all A, C, G or T in either case exactly when this equals (x | 0x20202020):
+// setting bit 5 merges only a letter with its other case.
+__device__ __forceinline__ uint32_t letters4(uint32_t t) {
+    const uint32_t u = t | (t >> 4);
+    return __byte_perm(0x74676361u, 0u, __byte_perm(u, 0u, 0x4420u));
 }
 
 // Shared memory of one stage: the tile's bytes (a multiple of 128), then
@@ -181,8 +185,13 @@ __global__ void __launch_bounds__(512) pack_kernel(const uint8_t* __restrict__ s
         // pass 1: 16 bytes -> 32 bits of codes, first base in the top bits
         for (uint32_t g = threadIdx.x; g < groups; g += blockDim.x) {
             const uint4 x = reinterpret_cast<const uint4*>(buf)[g];
-            uint32_t c = (pack4(x.x) << 24) | (pack4(x.y) << 16) | (pack4(x.z) << 8) | pack4(x.w);
-            if (!(acgt4(x.x) & acgt4(x.y) & acgt4(x.z) & acgt4(x.w))) {
+            const uint32_t t0 = codes4(x.x), t1 = codes4(x.y), t2 = codes4(x.z), t3 = codes4(x.w);
+            // the top bytes of the four products: byte 3 from the first word
+            uint32_t c = __byte_perm(__byte_perm(gather4(t3), gather4(t2), 0x0073u),
+                                     __byte_perm(gather4(t1), gather4(t0), 0x0073u), 0x5410u);
+            const uint32_t d = (letters4(t0) ^ (x.x | 0x20202020u)) | (letters4(t1) ^ (x.y | 0x20202020u)) |
+                               (letters4(t2) ^ (x.z | 0x20202020u)) | (letters4(t3) ^ (x.w | 0x20202020u));
+            if (d != 0) {
                 // N, other letters: byte by byte
                 c = 0;
                 for (uint32_t j = 0; j < 16; ++j) {
