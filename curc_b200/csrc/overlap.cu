@@ -202,20 +202,17 @@ __device__ __forceinline__ int cmp_prefix(const OverlapCtx& c, uint32_t it, cons
     return cmp_span(c.db + uint64_t(c.va[it]) * c.W, 0, sr, off, cl);
 }
 
-// compress.cu:1476-1501: hash of the k-mer at kmer_index_pos+off, lower
-// bound of suffix[off, L) among the bucket's prefix[0, L-off).  Returns
-// whether an equal prefix exists; then the hit (list index, run start,
-// bucket end, bucket) is set and the suffix joins the run's claimers.
-__device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* __restrict__ sufw, uint32_t j, int off,
-                                          RunSlot* __restrict__ run, uint32_t* __restrict__ gnext, uint4& hitrec,
-                                          uint32_t& searched, uint32_t& compares, uint32_t& rows) {
+// compress.cu:1476-1501, the part after the hash: lower bound of
+// suffix[off, L) among the prefix[0, L-off) of bucket h (whose free bit was
+// set).  Returns whether an equal prefix exists; then the hit (list index,
+// run start, bucket end, bucket) is set and the suffix joins the run's
+// claimers.
+__device__ __forceinline__ bool search_bucket(const OverlapCtx& c, const uint64_t* __restrict__ sufw, uint32_t j,
+                                              uint32_t h, int off, RunSlot* __restrict__ run,
+                                              uint32_t* __restrict__ gnext, uint4& hitrec, uint32_t& searched,
+                                              uint32_t& compares, uint32_t& rows) {
     const int cl = c.L - off;
     const uint64_t* sr = sufw + uint64_t(j) * c.W;
-    const uint64_t hv = murmur64(word_at(sr, c.kip + off, c.k));
-    const uint32_t h = uint32_t(hv & c.mask);
-    // every prefix of the bucket has a predecessor already: no link is
-    // possible for any suffix that meets it, so none needs to claim it
-    if (!((c.bfree[h >> 5] >> (h & 31)) & 1u)) return false;
     uint32_t lo = c.kr[h];
     const uint32_t e = c.kr[h + 1];
     uint32_t count = e - lo;
@@ -244,38 +241,84 @@ __device__ __forceinline__ bool probe_one(const OverlapCtx& c, const uint64_t* _
     return true;
 }
 
+constexpr uint32_t PROBE_THREADS = 512;
+
 // Probes every listed suffix and lists the hits (hlist, *hcount; their
-// order is immaterial to the resolution).  tally[0] counts probes,
-// tally[1] hits, tally[4] probes that searched a bucket, tally[5] prefix
-// comparisons, tally[6] prefix rows read (for the algorithmic bytes of
-// the pass).
-__global__ void __launch_bounds__(512) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
-                                                    const uint32_t* __restrict__ plist,
-                                                    const uint32_t* __restrict__ pcount, int off,
-                                                    RunSlot* __restrict__ run, uint32_t* __restrict__ gnext,
-                                                    uint4* __restrict__ hlist, uint32_t* __restrict__ hcount,
-                                                    unsigned long long* __restrict__ tally) {
-    __shared__ uint4 s_hits[512];
-    __shared__ uint32_t s_n, s_base;
+// order is immaterial to the resolution).  Two phases per block, so that
+// the dependent loads of the bucket search run with full warps: every
+// thread hashes one listed suffix and tests its bucket's free bit (most
+// buckets have none left after the first passes), the suffixes that pass
+// are queued in shared memory (one slot range per warp, from a ballot),
+// and whenever a block's worth is queued, and at the end, each thread
+// searches the bucket of one queued suffix.  Which thread searches which
+// suffix does not change any result: a probe reads only the index and the
+// free bits, which no probe of the pass writes, and the run's claim count,
+// lowest member and member set do not depend on the order of the claims.
+// tally[0] counts probes, tally[1] hits, tally[4] probes that searched a
+// bucket, tally[5] prefix comparisons, tally[6] prefix rows read (for the
+// algorithmic bytes of the pass).
+__global__ void __launch_bounds__(PROBE_THREADS) probe_kernel(OverlapCtx c, const uint64_t* __restrict__ sufw,
+                                                              const uint32_t* __restrict__ plist,
+                                                              const uint32_t* __restrict__ pcount, int off,
+                                                              RunSlot* __restrict__ run, uint32_t* __restrict__ gnext,
+                                                              uint4* __restrict__ hlist, uint32_t* __restrict__ hcount,
+                                                              unsigned long long* __restrict__ tally) {
+    __shared__ uint4 s_hits[PROBE_THREADS];
+    // queued (suffix, bucket) pairs: fewer than PROBE_THREADS are left
+    // after a search round, and one round of hashing adds at most
+    // PROBE_THREADS
+    __shared__ uint2 s_q[2 * PROBE_THREADS];
+    __shared__ uint32_t s_n, s_base, s_qn;
     uint32_t probes = 0, hits = 0, searched = 0, compares = 0, rows = 0;
     const uint32_t np = *pcount;
-    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < np; b0 += gridDim.x * blockDim.x) {
-        const uint32_t q = b0 + threadIdx.x;
-        bool hit = false;
-        uint4 rec;
-        if (q < np) {
-            ++probes;
-            hit = probe_one(c, sufw, plist[q], off, run, gnext, rec, searched, compares, rows);
-            hits += hit;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (threadIdx.x == 0) s_qn = 0;
+    __syncthreads();
+    for (uint64_t b0 = uint64_t(blockIdx.x) * PROBE_THREADS;; b0 += uint64_t(gridDim.x) * PROBE_THREADS) {
+        const bool more = b0 < np;  // the same for the whole block
+        if (more) {
+            const uint64_t q = b0 + threadIdx.x;
+            bool keep = false;
+            uint32_t j = 0, h = 0;
+            if (q < np) {
+                ++probes;
+                j = plist[q];
+                const uint64_t* sr = sufw + uint64_t(j) * c.W;
+                h = uint32_t(murmur64(word_at(sr, c.kip + off, c.k)) & c.mask);
+                // every prefix of the bucket has a predecessor already: no
+                // link is possible for any suffix that meets it, so none
+                // needs to claim it
+                keep = (c.bfree[h >> 5] >> (h & 31)) & 1u;
+            }
+            const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+            uint32_t slot = 0;
+            if (lane == 0 && bal) slot = atomicAdd(&s_qn, uint32_t(__popc(bal)));
+            slot = __shfl_sync(0xffffffffu, slot, 0);
+            if (keep) s_q[slot + uint32_t(__popc(bal & ((1u << lane) - 1u)))] = make_uint2(j, h);
+            __syncthreads();
         }
-        if (threadIdx.x == 0) s_n = 0;
-        __syncthreads();
-        if (hit) s_hits[atomicAdd(&s_n, 1u)] = rec;
-        __syncthreads();
-        if (threadIdx.x == 0 && s_n) s_base = atomicAdd(hcount, s_n);
-        __syncthreads();
-        if (threadIdx.x < s_n) hlist[s_base + threadIdx.x] = s_hits[threadIdx.x];
-        __syncthreads();
+        const uint32_t qn = s_qn;  // the same for the whole block (read after a barrier)
+        if (qn >= PROBE_THREADS || (!more && qn > 0)) {
+            // search the last `take` queued suffixes; the rest stay in place
+            const uint32_t take = qn < PROBE_THREADS ? qn : PROBE_THREADS;
+            bool hit = false;
+            uint4 rec;
+            if (threadIdx.x < take) {
+                const uint2 e = s_q[qn - take + threadIdx.x];
+                hit = search_bucket(c, sufw, e.x, e.y, off, run, gnext, rec, searched, compares, rows);
+                hits += hit;
+            }
+            if (threadIdx.x == 0) s_n = 0;
+            __syncthreads();
+            if (threadIdx.x == 0) s_qn = qn - take;
+            if (hit) s_hits[atomicAdd(&s_n, 1u)] = rec;
+            __syncthreads();
+            if (threadIdx.x == 0 && s_n) s_base = atomicAdd(hcount, s_n);
+            __syncthreads();
+            if (threadIdx.x < s_n) hlist[s_base + threadIdx.x] = s_hits[threadIdx.x];
+            __syncthreads();
+        }
+        if (!more) break;
     }
     block_tally<unsigned long long>(probes, &tally[0]);
     block_tally<unsigned long long>(hits, &tally[1]);
@@ -519,7 +562,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
     set_u32_kernel<<<1, 1, 0, s>>>(dcount, ms);
     CURC_LAUNCH_CHECK();
     Compactor cp(ms, a, s);
-    const int gp = resident_grid(probe_kernel, 512, ms ? ms : 1);
+    const int gp = resident_grid(probe_kernel, PROBE_THREADS, ms ? ms : 1);
     const int gr = resident_grid(resolve_kernel, 512, ms ? ms : 1);
     const int CHECK_EVERY = p.tune.check_every;
     uint32_t passes = 0, active = ms;
@@ -564,7 +607,7 @@ void overlap_link(const BlockParams& p, const uint64_t* db, const uint32_t* sort
                ProbeFilter{linked, mask + uint64_t(off >> 5) * ms, uint32_t(off & 31)}, ProbeListMove{plist});
         sp_filter.stop();
         SubStage sp_pk("overlap.probe");
-        probe_kernel<<<gp, 512, 0, s>>>(c, sufw, plist, dcount + 1, off, run, gnext,
+        probe_kernel<<<gp, PROBE_THREADS, 0, s>>>(c, sufw, plist, dcount + 1, off, run, gnext,
                                         hlist, hcount + off, tally);
         CURC_LAUNCH_CHECK();
         sp_pk.stop();
