@@ -208,9 +208,9 @@ def full_match_bytes(st):
 
 # DRAM bytes per listed suffix of the probe kernel, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum over its 96 launches) on the
-# 2M-pair case of the same generator: 5.671e9 bytes / 20.21e6 probes.  The
+# 2M-pair case of the same generator: 5.767e9 bytes / 20.21e6 probes.  The
 # traffic of a launch at full size is this times its probes.
-PROBE_DRAM_BYTES_PER_PROBE = 5.671e9 / 20.207e6
+PROBE_DRAM_BYTES_PER_PROBE = 5.767e9 / 20.207e6
 
 
 STAT_NAMES = ["reads", "non_n", "n_reads", "pseudogenome_reads", "unmatched", "mapped", "unmapped",
