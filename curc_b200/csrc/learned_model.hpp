@@ -201,11 +201,37 @@ LM_HD void model_freqs(const Model& M, const int* idx, int nidx, int gmax, uint3
 // (16-bit multiply-add).  The activations after requant lie in [0, 127], so
 // every product and sum is the int32 value model_freqs computes, and
 // integer sums are exact in any order: the frequencies are model_freqs's.
+//
+// On x86-64 hosts with AVX2 or AVX-512 VNNI, layers 2 and 3 run on the
+// unsigned-by-signed byte dot-product instructions instead (chosen once, at
+// run time, from what the CPU reports): the activations, in [0, 127], are
+// the unsigned bytes and the int8 weights the signed ones, stored in groups
+// of four inputs per output.  VPDPBUSD sums four exact products into int32;
+// VPMADDUBSW sums two into int16, which cannot saturate here (|2 x 127 x
+// 128| < 2^15), before VPMADDWD widens them.  A model whose requantisation
+// multipliers are not positive (activations could then be negative) keeps
+// the int16 loops.
+#if !defined(__CUDACC__) && defined(__x86_64__) && defined(__GNUC__)
+#define LM_HOST_X86 1
+#include <immintrin.h>
+#endif
+
+constexpr int OUT_PAD = 32;  // layer-3 outputs padded to two 16-lane groups
+
+// The host form and the decoder that uses it have internal linkage: their
+// bodies depend on the compiler (the CUDA compiler's copy keeps the int16
+// loops), so no translation unit may share another's copy.
+namespace {
+
 struct HostModel {
+    enum Kind { INT16 = 0, AVX2 = 1, VNNI512 = 2 };
     const Model* M;
+    int kind = INT16;
     alignas(64) int16_t w1t[IN][HID];
     alignas(64) int16_t w2[HID][HID];
     alignas(64) int16_t w3[OUT][HID];
+    alignas(64) int8_t w2q[HID / 4][HID][4];      // [input group][output][input in group]
+    alignas(64) int8_t w3q[HID / 4][OUT_PAD][4];  // the same, outputs past OUT zero
     explicit HostModel(const Model& m) : M(&m) {
         for (int h = 0; h < HID; ++h)
             for (int i = 0; i < IN; ++i) w1t[i][h] = m.w1[h][i];
@@ -213,8 +239,67 @@ struct HostModel {
             for (int t = 0; t < HID; ++t) w2[h][t] = m.w2[h][t];
         for (int o = 0; o < OUT; ++o)
             for (int t = 0; t < HID; ++t) w3[o][t] = m.w3[o][t];
+        std::memset(w3q, 0, sizeof(w3q));
+        for (int t = 0; t < HID; ++t) {
+            for (int h = 0; h < HID; ++h) w2q[t / 4][h][t % 4] = m.w2[h][t];
+            for (int o = 0; o < OUT; ++o) w3q[t / 4][o][t % 4] = m.w3[o][t];
+        }
+        kind = best_kind();
+    }
+    // The fastest form this CPU runs for this model.
+    int best_kind() const {
+        if (M->m1 <= 0 || M->m2 <= 0) return INT16;
+#ifdef LM_HOST_X86
+        __builtin_cpu_init();
+        if (__builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw") &&
+            __builtin_cpu_supports("avx512vnni"))
+            return VNNI512;
+        if (__builtin_cpu_supports("avx2")) return AVX2;
+#endif
+        return INT16;
     }
 };
+
+#ifdef LM_HOST_X86
+// acc[o] = sum over t of a[t] * wq[t/4][o][t%4], for o < 16*groups16, t < HID
+// (a: HID unsigned bytes; acc: int32, overwritten).
+__attribute__((target("avx512f,avx512bw,avx512vnni"))) inline void dot_u8s8_vnni512(const int8_t* wq, int outs,
+                                                                                    const uint8_t* a, int32_t* acc) {
+    const int groups16 = outs / 16;
+    __m512i s[HID / 16];
+    for (int c = 0; c < groups16; ++c) s[c] = _mm512_setzero_si512();
+    for (int g = 0; g < HID / 4; ++g) {
+        int32_t four;
+        std::memcpy(&four, a + 4 * g, 4);
+        const __m512i x = _mm512_set1_epi32(four);
+        const int8_t* row = wq + size_t(g) * outs * 4;
+        for (int c = 0; c < groups16; ++c)
+            s[c] = _mm512_dpbusd_epi32(s[c], x, _mm512_load_si512(reinterpret_cast<const void*>(row + 64 * c)));
+    }
+    for (int c = 0; c < groups16; ++c) _mm512_storeu_si512(reinterpret_cast<void*>(acc + 16 * c), s[c]);
+}
+
+__attribute__((target("avx2"))) inline void dot_u8s8_avx2(const int8_t* wq, int outs, const uint8_t* a,
+                                                           int32_t* acc) {
+    const __m256i ones = _mm256_set1_epi16(1);
+    for (int c0 = 0; c0 < outs; c0 += 64) {  // 64 outputs (8 registers) at a time
+        __m256i s[8];
+        const int nc = std::min(8, (outs - c0) / 8);
+        for (int c = 0; c < nc; ++c) s[c] = _mm256_setzero_si256();
+        for (int g = 0; g < HID / 4; ++g) {
+            int32_t four;
+            std::memcpy(&four, a + 4 * g, 4);
+            const __m256i x = _mm256_set1_epi32(four);
+            const int8_t* row = wq + (size_t(g) * outs + c0) * 4;
+            for (int c = 0; c < nc; ++c) {
+                const __m256i w = _mm256_load_si256(reinterpret_cast<const __m256i*>(row + 32 * c));
+                s[c] = _mm256_add_epi32(s[c], _mm256_madd_epi16(_mm256_maddubs_epi16(x, w), ones));
+            }
+        }
+        for (int c = 0; c < nc; ++c) _mm256_storeu_si256(reinterpret_cast<__m256i*>(acc + c0 + 8 * c), s[c]);
+    }
+}
+#endif
 
 inline void model_freqs_host(const HostModel& H, const int* idx, int nidx, int gmax, uint32_t* fb, uint32_t* fg) {
     const Model& M = *H.M;
@@ -227,24 +312,40 @@ inline void model_freqs_host(const HostModel& H, const int* idx, int nidx, int g
         for (int h = 0; h < HID; ++h) acc1[h] += row[h];
     }
     for (int h = 0; h < HID; ++h) a1[h] = int16_t(requant(acc1[h], M.m1, M.sh1));
-    for (int h = 0; h < HID; ++h) {
-        int32_t acc = 0;
-        const int16_t* w = H.w2[h];
-#pragma omp simd reduction(+ : acc)
-        for (int t = 0; t < HID; ++t) acc += int32_t(w[t]) * int32_t(a1[t]);
-        a2[h] = int16_t(requant(acc + M.b2[h], M.m2, M.sh2));
-    }
     int32_t z[OUT];
-    for (int o = 0; o < OUT; ++o) {
-        int32_t acc = 0;
-        const int16_t* w = H.w3[o];
+#ifdef LM_HOST_X86
+    if (H.kind != HostModel::INT16) {
+        alignas(64) uint8_t u1[HID], u2[HID];
+        alignas(64) int32_t acc[HID > OUT_PAD ? HID : OUT_PAD];
+        for (int h = 0; h < HID; ++h) u1[h] = uint8_t(a1[h]);
+        const auto dot = H.kind == HostModel::VNNI512 ? dot_u8s8_vnni512 : dot_u8s8_avx2;
+        dot(&H.w2q[0][0][0], HID, u1, acc);
+        for (int h = 0; h < HID; ++h) u2[h] = uint8_t(requant(acc[h] + M.b2[h], M.m2, M.sh2));
+        dot(&H.w3q[0][0][0], OUT_PAD, u2, acc);
+        for (int o = 0; o < OUT; ++o) z[o] = acc[o] + M.b3[o];
+    } else
+#endif
+    {
+        for (int h = 0; h < HID; ++h) {
+            int32_t acc = 0;
+            const int16_t* w = H.w2[h];
 #pragma omp simd reduction(+ : acc)
-        for (int t = 0; t < HID; ++t) acc += int32_t(w[t]) * int32_t(a2[t]);
-        z[o] = acc + M.b3[o];
+            for (int t = 0; t < HID; ++t) acc += int32_t(w[t]) * int32_t(a1[t]);
+            a2[h] = int16_t(requant(acc + M.b2[h], M.m2, M.sh2));
+        }
+        for (int o = 0; o < OUT; ++o) {
+            int32_t acc = 0;
+            const int16_t* w = H.w3[o];
+#pragma omp simd reduction(+ : acc)
+            for (int t = 0; t < HID; ++t) acc += int32_t(w[t]) * int32_t(a2[t]);
+            z[o] = acc + M.b3[o];
+        }
     }
     logits_to_freq(M, z, NB, NB, fb);
     logits_to_freq(M, z + NB, gap_bin(gmax < 0 ? 0 : gmax) + 1, NG, fg);
 }
+
+}  // namespace
 
 // Context of the adaptive in-bin models.  One context: splitting them by
 // strand and read position (16 contexts) spread the 16384-record chunks too
@@ -380,6 +481,8 @@ private:
 // then the chunks.
 constexpr size_t CHUNK_RECORDS = 16384;
 
+namespace {
+
 // Decodes a learned stream.  Records come in emission order with their
 // position on the main pseudogenome `ref` (ASCII, length rl), strand and
 // mismatch count; the mismatches of record r are written from index first[r]
@@ -475,6 +578,8 @@ inline std::string decode_stream(const Model& M, const uint8_t* p, size_t bytes,
     }
     return bad ? "learned stream does not decode consistently" : "";
 }
+
+}  // namespace
 
 }  // namespace learned
 }  // namespace curc
