@@ -252,6 +252,7 @@ struct HostModel {
 #ifdef LM_HOST_X86
         __builtin_cpu_init();
         if (__builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw") &&
+            __builtin_cpu_supports("avx512dq") && __builtin_cpu_supports("avx512vl") &&
             __builtin_cpu_supports("avx512vnni"))
             return VNNI512;
         if (__builtin_cpu_supports("avx2")) return AVX2;
@@ -301,31 +302,24 @@ __attribute__((target("avx2"))) inline void dot_u8s8_avx2(const int8_t* wq, int 
 }
 #endif
 
-inline void model_freqs_host(const HostModel& H, const int* idx, int nidx, int gmax, uint32_t* fb, uint32_t* fg) {
+// The network at one anchor in form KIND.  Always inlined into the wrappers
+// below, so that its plain loops (layer 1, the requantisations) are
+// vectorised for the instruction set of the wrapper's form.
+template <int KIND>
+__attribute__((always_inline)) inline void host_freqs(const HostModel& H, const int* idx, int nidx, int gmax,
+                                                      uint32_t* fb, uint32_t* fg) {
     const Model& M = *H.M;
     alignas(64) int32_t acc1[HID];
-    alignas(64) int16_t a1[HID], a2[HID];
     for (int h = 0; h < HID; ++h) acc1[h] = M.b1[h];
     for (int t = 0; t < nidx; ++t) {
         const int16_t* row = H.w1t[idx[t]];
 #pragma omp simd
         for (int h = 0; h < HID; ++h) acc1[h] += row[h];
     }
-    for (int h = 0; h < HID; ++h) a1[h] = int16_t(requant(acc1[h], M.m1, M.sh1));
     int32_t z[OUT];
-#ifdef LM_HOST_X86
-    if (H.kind != HostModel::INT16) {
-        alignas(64) uint8_t u1[HID], u2[HID];
-        alignas(64) int32_t acc[HID > OUT_PAD ? HID : OUT_PAD];
-        for (int h = 0; h < HID; ++h) u1[h] = uint8_t(a1[h]);
-        const auto dot = H.kind == HostModel::VNNI512 ? dot_u8s8_vnni512 : dot_u8s8_avx2;
-        dot(&H.w2q[0][0][0], HID, u1, acc);
-        for (int h = 0; h < HID; ++h) u2[h] = uint8_t(requant(acc[h] + M.b2[h], M.m2, M.sh2));
-        dot(&H.w3q[0][0][0], OUT_PAD, u2, acc);
-        for (int o = 0; o < OUT; ++o) z[o] = acc[o] + M.b3[o];
-    } else
-#endif
-    {
+    if constexpr (KIND == HostModel::INT16) {
+        alignas(64) int16_t a1[HID], a2[HID];
+        for (int h = 0; h < HID; ++h) a1[h] = int16_t(requant(acc1[h], M.m1, M.sh1));
         for (int h = 0; h < HID; ++h) {
             int32_t acc = 0;
             const int16_t* w = H.w2[h];
@@ -341,8 +335,46 @@ inline void model_freqs_host(const HostModel& H, const int* idx, int nidx, int g
             z[o] = acc + M.b3[o];
         }
     }
+#ifdef LM_HOST_X86
+    else {
+        alignas(64) uint8_t u1[HID], u2[HID];
+        alignas(64) int32_t acc[HID > OUT_PAD ? HID : OUT_PAD];
+#pragma omp simd
+        for (int h = 0; h < HID; ++h) u1[h] = uint8_t(requant(acc1[h], M.m1, M.sh1));
+        if constexpr (KIND == HostModel::VNNI512)
+            dot_u8s8_vnni512(&H.w2q[0][0][0], HID, u1, acc);
+        else
+            dot_u8s8_avx2(&H.w2q[0][0][0], HID, u1, acc);
+#pragma omp simd
+        for (int h = 0; h < HID; ++h) u2[h] = uint8_t(requant(acc[h] + M.b2[h], M.m2, M.sh2));
+        if constexpr (KIND == HostModel::VNNI512)
+            dot_u8s8_vnni512(&H.w3q[0][0][0], OUT_PAD, u2, acc);
+        else
+            dot_u8s8_avx2(&H.w3q[0][0][0], OUT_PAD, u2, acc);
+        for (int o = 0; o < OUT; ++o) z[o] = acc[o] + M.b3[o];
+    }
+#endif
     logits_to_freq(M, z, NB, NB, fb);
     logits_to_freq(M, z + NB, gap_bin(gmax < 0 ? 0 : gmax) + 1, NG, fg);
+}
+
+#ifdef LM_HOST_X86
+__attribute__((target("avx512f,avx512bw,avx512dq,avx512vl,avx512vnni"))) inline void host_freqs_vnni512(
+    const HostModel& H, const int* idx, int nidx, int gmax, uint32_t* fb, uint32_t* fg) {
+    host_freqs<HostModel::VNNI512>(H, idx, nidx, gmax, fb, fg);
+}
+__attribute__((target("avx2"))) inline void host_freqs_avx2(const HostModel& H, const int* idx, int nidx, int gmax,
+                                                             uint32_t* fb, uint32_t* fg) {
+    host_freqs<HostModel::AVX2>(H, idx, nidx, gmax, fb, fg);
+}
+#endif
+
+inline void model_freqs_host(const HostModel& H, const int* idx, int nidx, int gmax, uint32_t* fb, uint32_t* fg) {
+#ifdef LM_HOST_X86
+    if (H.kind == HostModel::VNNI512) return host_freqs_vnni512(H, idx, nidx, gmax, fb, fg);
+    if (H.kind == HostModel::AVX2) return host_freqs_avx2(H, idx, nidx, gmax, fb, fg);
+#endif
+    host_freqs<HostModel::INT16>(H, idx, nidx, gmax, fb, fg);
 }
 
 }  // namespace
