@@ -985,6 +985,14 @@ void write_block(const Block& b, bool po, bool pe, int L, std::ofstream& o1, std
 
 }  // namespace
 
+std::string learned_decode(const void* model, const uint8_t* p, size_t bytes, const uint8_t* ref, uint64_t rl, int L,
+                           size_t records, const uint64_t* pos, const uint8_t* strand, const uint8_t* cnt,
+                           uint16_t* off, char* base) {
+    learned::Model M;
+    std::memcpy(&M, model, sizeof(M));
+    return learned::decode_stream(M, p, bytes, ref, rl, L, records, pos, strand, cnt, off, base);
+}
+
 ArchiveInfo archive_info(const std::string& archive) {
     const std::string data = read_whole(archive);
     Reader ar(data);

@@ -56,6 +56,14 @@ void general_mismatch_bytes(const BlockView& v, const CoderParams& cp, uint64_t 
 // Archive header (preprocess.cpp:261-266).
 std::string archive_header(bool po, bool pe, int read_len, int blocks);
 
+// The learned mismatch stream of a block decoded (learned::decode_stream)
+// by this host-compiled translation unit, whose copy of the host network
+// runs on the CPU's byte dot products where it has them; the arguments are
+// decode_stream's, with the model as its serialised bytes (sizeof(Model)).
+std::string learned_decode(const void* model, const uint8_t* p, size_t bytes, const uint8_t* ref, uint64_t rl, int L,
+                           size_t records, const uint64_t* pos, const uint8_t* strand, const uint8_t* cnt,
+                           uint16_t* off, char* base);
+
 // FASTQ ingest.  Reads single-end (f2 empty) or paired-end files in the
 // reference's 50 MB windows (25 MB per mate) cut at record boundaries by its
 // header heuristic, and closes a block once the bytes read since the last

@@ -1115,9 +1115,10 @@ int curc_learn_decode_check(curc_learn* L, curc_ctx* ctx, const void* data, uint
                 tbase[first[r] + j] = outcome_base(char(ref[pos[r] + uint64_t(q)]), ha[k + j + 1].tbase);
             }
         }
-        const std::string why = decode_stream(T.model, static_cast<const uint8_t*>(data), bytes, ref.data(),
-                                              ref.size(), Lr, Tn, pos.data(), strand.data(), mis.data(), off.data(),
-                                              base.data());
+        // decoded by the host-compiled copy of the decoder (the one `curc -d` runs)
+        const std::string why = host::learned_decode(&T.model, static_cast<const uint8_t*>(data), bytes,
+                                                     ref.data(), ref.size(), Lr, Tn,
+                                                     pos.data(), strand.data(), mis.data(), off.data(), base.data());
         *ok = why.empty() && off == toff && base == tbase ? 1 : 0;
     });
 }
