@@ -870,7 +870,7 @@ def main():
                                     "api": "curc_batch_submit/curc_batch_drain from pinned host memory, streams "
                                            "back to the host, no stream coders",
                                     "one_call_per_step": r["bases"] * world / r["e2e_plain_s"] / 1e6},
-        "roofline": {"kernel": "probe_kernel (overlap passes, stage a4; the largest share of the launch list)",
+        "roofline": {"kernel": "probe_kernel (overlap passes, stage a4; the memory-bound kernel with the largest share of the launch list: map_kernel<0> has a slightly larger share but is issue-bound, see roofline_map)",
                      "bound": "hbm", "achieved": probe_ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": probe_ach / peak if probe_ach else None,
                      "traffic": PROBE_DRAM_BYTES_PER_PROBE * st["overlap_probes"] / passes,
